@@ -1,0 +1,405 @@
+"""Benchmark: particle-potentials/s of NPME CalcV on one B200 (or N replicas).
+
+Workload: the 1/r derivative-match system of 1,000,000 points uniform in a
+100^3 box, charges uniform in [-1, 1] with zero net charge, B-spline order 6,
+FFT box 256^3, Rdir 8 (seeded synthetic data).  One step = one CalcV
+(direct sum + reciprocal sum, potential and gradient for every point) with
+the geometry set up once, as in the reference's compute-only timings.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+`value` is device-timed with inputs resident in HBM (CUDA events per step,
+L2 flushed between steps); `e2e` is the same metric through the C ABI with
+pinned host buffers, host<->device copies included.  With --gpus N under
+torchrun every rank runs an independent replica (a single solve does not
+shard); value = all ranks' points / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-potentials/s (CalcV, potential + gradient per point)"
+UNIT = "particle-potentials/s"
+
+# algorithmic work per launch ("Roofline accounting")
+DIRECT_FLOPS_PER_PAIR = {"laplace": lambda nd: 29 + 4 * nd,
+                         "ralpha": lambda nd: 32 + 4 * nd,
+                         "helmholtz": lambda nd: 91 + 8 * nd}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="npme_b200", choices=["npme_b200", "reference"])
+    ap.add_argument("--workload", default="laplace_dm_1m")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-port line")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return ap.parse_args()
+
+
+def workload(name):
+    from npme_b200 import workloads as wl
+    for w in wl.CONFIGS:
+        if w.name == name:
+            return w
+    raise SystemExit(f"unknown workload {name}")
+
+
+def config_of(w, precision, n_gpus):
+    return {"workload": w.name, "points": w.n, "box": list(w.box), "kernel": w.func,
+            "split": w.split, "alpha": w.alpha, "k0": [complex(w.k0).real, complex(w.k0).imag],
+            "BnOrder": w.order, "nDeriv": w.nDeriv, "grid": list(w.grid), "Rdir": w.Rdir,
+            "precision": ("fp32 bulk, fp64 per-target accumulation and output"
+                          if precision == "fp32" else "fp64 throughout"),
+            "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": f"{n_gpus} independent replicas" if n_gpus > 1 else "1 GPU"}
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(mx)) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def profile_traffic(kernel):
+    """dram bytes per launch for `kernel` from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_baseline(w, args):
+    """The reference's own CPU implementation (oracle/_ref, built from the
+    reference sources) timed on this host: setup once, then CalcV calls."""
+    from oracle import refbind as rb
+    c, q = w.generate()
+    cores = os.cpu_count() or 1
+    if rb.available(avx=True):
+        p = rb.make_params(w.func, w.split, w.Rdir, w.order, nDeriv=w.nDeriv, N=w.grid,
+                           alpha=w.alpha, k0=w.k0, nProc=cores, vecOption=1)
+        s = rb.RefSolver(p, c, avx=True)
+        kind = "reference"
+        calc = s.calcv
+        setup_s = s.setup_seconds
+    else:
+        from oracle import orcbind as ob
+        po = ob.params_from_workload(w)
+        kind = "port"
+        setup_s = None
+
+        def calc(qq):
+            return ob.calcv(po, c, qq, nthreads=cores)
+    return kind, cores, calc, q, setup_s
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = workload(args.workload)
+    kind, cores, calc, q, setup_s = cpu_baseline(w, args)
+    for _ in range(max(0, args.warmup)):
+        calc(q)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        calc(q)
+        ts.append(time.perf_counter() - t0)
+    total = sum(ts)
+    value = w.n * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(w, "fp64", 1),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"full workload ({w.n} points), {args.steps} CalcV "
+                                       f"calls after one SetUp ({setup_s and round(setup_s, 3)} s)"
+                                       + ("; AVX2 build, FFTs by the project FFT shim "
+                                          "(MKL absent)" if kind == "reference" else "")},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    import npme_b200
+    from npme_b200 import api
+
+    w = workload(args.workload)
+    c, q = w.generate()
+    s = npme_b200.Solver(api.params_from_workload(w, precision=args.precision, device=local))
+    t0 = time.perf_counter()
+    s.setup(c)
+    setup_seconds = time.perf_counter() - t0
+    info0 = s.info()
+    info0["pairs"] = s.count_pairs()
+
+    # resident inputs
+    dq = torch.from_numpy(q).to(dev)
+    dV = torch.empty((w.n, 4), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # a real stream: the legacy default stream's handle is 0, which the C ABI
+    # reads as "the handle's own stream"
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    sptr = stream.cuda_stream
+
+    def step():
+        s.calcv_device(dV.data_ptr(), dq.data_ptr(), sptr)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    s.set_timing(True)
+    stage_sum = {k: 0.0 for k in api.STAGES}
+    launches = 0
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        inf = s.info()
+        for k, v in inf["stage_ms"].items():
+            stage_sum[k] += v
+        launches += inf["launches"]
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    s.set_timing(False)
+
+    # end to end through the C ABI with pinned host buffers
+    qh = torch.from_numpy(q).pin_memory().numpy()
+    Vh = torch.empty((w.n, 4), dtype=torch.float64).pin_memory().numpy()
+    for _ in range(2):
+        s.calcv(qh, out=Vh)
+    e2e_ts = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s.calcv(qh, out=Vh)
+        e2e_ts.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    e2e_s = sum(e2e_ts)
+
+    if dist:
+        t = torch.tensor([ms / 1e3, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec, e2e_s = float(t[0]), float(t[1])
+    else:
+        sec = ms / 1e3
+    value = world * w.n * args.steps / sec
+    e2e_value = world * w.n * args.steps / e2e_s
+
+    extra = {}
+    if rank == 0:
+        # plain FP64 port of the same method on the same GPU (the 3x target's baseline)
+        if args.precision == "fp32" and not args.no_plain:
+            s64 = npme_b200.Solver(api.params_from_workload(w, precision="fp64", device=local))
+            s64.setup(c)
+            for _ in range(2):
+                s64.calcv_device(dV.data_ptr(), dq.data_ptr(), sptr)
+            torch.cuda.synchronize(dev)
+            k64 = max(3, args.steps // 4)
+            tt = 0.0
+            for _ in range(k64):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                s64.calcv_device(dV.data_ptr(), dq.data_ptr(), sptr)
+                b.record(stream)
+                torch.cuda.synchronize(dev)
+                tt += a.elapsed_time(b)
+            extra["plain_fp64"] = {"value": w.n * k64 / (tt / 1e3), "unit": UNIT,
+                                   "ms_per_step": tt / k64, "steps": k64}
+            # accuracy of both forms against the exact O(N^2) FP64 sum
+            Ve = s64.calcv_exact(q)
+            V64 = s64.calcv(q)
+            V32 = s.calcv(q)
+
+            def rr(a, b):
+                return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+            extra["accuracy_vs_exact_fp64"] = {
+                "fp32_bulk": {"rel_rms_V": rr(V32[:, 0], Ve[:, 0]),
+                              "rel_rms_gradV": rr(V32[:, 1:], Ve[:, 1:]),
+                              "max_abs_dV_over_max_V": float(np.abs(V32[:, 0] - Ve[:, 0]).max()
+                                                             / np.abs(Ve[:, 0]).max())},
+                "plain_fp64": {"rel_rms_V": rr(V64[:, 0], Ve[:, 0]),
+                               "rel_rms_gradV": rr(V64[:, 1:], Ve[:, 1:])}}
+            s64.close()
+
+    if rank == 0:
+        st = {k: v / args.steps for k, v in stage_sum.items()}
+        peaks = measured_peaks()
+        sm_mhz = clocks.get("sm_mhz") or peaks.get("clocks_under_load", {}).get("sm_mhz_median")
+        # dominant kernel: the direct sum (FP32 pipe); see DESIGN.md
+        nd = w.nDeriv
+        pairs = info0.get("pairs")
+        flops_pair = DIRECT_FLOPS_PER_PAIR[w.func](nd)
+        fp_peak = 148 * 128 * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
+        if args.precision == "fp64":
+            fp_peak /= 2
+        achieved = (pairs * flops_pair / (st["direct"] / 1e3) / 1e12
+                    if pairs and st["direct"] > 0 else None)
+        roofline = {"kernel": "direct_kernel", "bound": "fp32" if args.precision == "fp32" else "fp64",
+                    "achieved": achieved, "peak": fp_peak, "unit": "TFLOP/s",
+                    "frac": (achieved / fp_peak) if achieved else None,
+                    "traffic": profile_traffic("direct_kernel"),
+                    "peak_source": "nominal 148 SM x 128 lanes x 2 flop at the sampled median "
+                                   "SM clock (MEASURED_PEAKS.json has no FP32 figure)",
+                    "work": f"{pairs} unordered pairs within Rdir x {flops_pair} flop"}
+        hbm = peaks.get("hbm_gbs", 6535.7)
+        G = (w.grid[0] // 2) * (w.grid[1] // 2) * (w.grid[2] // 2)
+        sz = 4 if args.precision == "fp32" else 8
+        spread_bytes = w.n * (3 * sz + sz) + G * sz
+        interp_bytes = w.n * 3 * sz + G * sz + w.n * 4 * 8
+        stages = {k: {"ms": v} for k, v in st.items()}
+        for k, b in (("spread", spread_bytes), ("interp", interp_bytes)):
+            if st[k] > 0:
+                gbs = b / (st[k] / 1e3) / 1e9
+                stages[k].update({"algorithmic_bytes": b, "achieved_gbs": gbs,
+                                  "frac_of_measured_hbm": gbs / hbm})
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": max(3, args.warmup),
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+                "data": "synthetic (seeded Philox; points uniform in the box, charges "
+                        "uniform in [-1,1], net zero)",
+                "config": config_of(w, args.precision, world),
+                "e2e": {"value": e2e_value, "unit": UNIT,
+                        "h2d_bytes_per_step": int(q.nbytes),
+                        "d2h_bytes_per_step": int(w.n * 4 * 8),
+                        "api": "npme_gpu_calcv_real, pinned host buffers"},
+                "roofline": roofline, "stages": stages,
+                "gpu_launches": launches, "clocks": clocks,
+                "setup_seconds": setup_seconds}
+        line.update(extra)
+        if not args.no_cpu:
+            try:
+                kind, cores, calc, qq, setup_s = cpu_baseline(w, args)
+                calc(qq)
+                t0 = time.perf_counter()
+                reps = 2
+                for _ in range(reps):
+                    calc(qq)
+                cs = (time.perf_counter() - t0) / reps
+                line["cpu_baseline"] = {
+                    "value": w.n / cs, "unit": UNIT, "cores": cores, "kind": kind,
+                    "sample": f"full workload ({w.n} points): mean of {reps} CalcV calls after "
+                              f"one warm-up and one SetUp ({setup_s and round(setup_s, 2)} s)"
+                              + ("; reference AVX2 build, FFTs by the project FFT shim "
+                                 "(MKL absent)" if kind == "reference" else "")}
+            except Exception as e:  # the baseline must never break the GPU line
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
+                                        "kind": "unavailable", "sample": str(e)[:200]}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,156 @@
+/*
+ * npme_b200 — B200-native (sm_100a) potential evaluation for the
+ * non-periodic particle-mesh Ewald method (NPME).
+ *
+ * C ABI.  Plain pointers and sizes, no C++ or torch types.  Every entry point
+ * returns an npme_status and never exits the process; the message of the
+ * last failure is available from npme_gpu_last_error().
+ *
+ * The calls replace the reference's interface classes (ElkingD/npme,
+ * src/Interface.h) entry by entry:
+ *
+ *   reference                                          this ABI
+ *   -------------------------------------------------  ---------------------------
+ *   NPME_Interface_SetUpRealKernel / ComplexKernel     npme_gpu_create +
+ *     (src/Interface.cpp:884, 1066), SetUp                npme_gpu_setup
+ *     (src/Interface.h:393-395, 733-735)
+ *   NPME_InterfaceReal::ResetCoord (src/Interface.h:188)  npme_gpu_setup
+ *   NPME_InterfaceReal::CalcV      (src/Interface.h:192)  npme_gpu_calcv_real
+ *   NPME_InterfaceComplex::CalcV   (src/Interface.h:525)  npme_gpu_calcv_complex
+ *   NPME_InterfaceReal::CalcV_exact (src/Interface.h:200) npme_gpu_calcv_exact_real
+ *   NPME_InterfaceComplex::CalcV_exact (src/Interface.h:532)
+ *                                                      npme_gpu_calcv_exact_complex
+ *   NPME_InterfaceReal::Print      (src/Interface.h:209)  npme_gpu_get_info
+ *   NPME_KeywordInput defaults (src/Interface.cpp:53-517) npme_gpu_default_params
+ *   (destructor)                                       npme_gpu_destroy
+ *
+ * Data layout is the reference's: coord[3n] xyz interleaved (double);
+ * real charge[n] (double) or complex charge[2n] (re, im); output
+ * V[n][4] = (V, dV/dx, dV/dy, dV/dz) as double, or as complex
+ * (re, im) pairs, i.e. 8 doubles per point.  Outputs are in the caller's
+ * particle order.  Unlike the reference, inputs are never modified.
+ *
+ * Semantics kept from the reference: CalcV assumes the coordinates given to
+ * setup (geometry fixed, charges vary per call); setup again to change the
+ * geometry.  CalcV = direct sum - f_LR(0) q + reciprocal sum; CalcV_exact is
+ * the plain O(N^2) sum with no self term.
+ */
+#ifndef NPME_GPU_H
+#define NPME_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  NPME_OK = 0,
+  NPME_EINVAL = 1,   /* bad argument or parameter combination */
+  NPME_ENOMEM = 2,   /* device or host allocation failed */
+  NPME_ECUDA = 3,    /* CUDA / cuFFT error */
+  NPME_ETIMEOUT = 4, /* a bounded device wait ran out */
+  NPME_EBUSY = 5,    /* queue full */
+  NPME_ESTATE = 6    /* call out of order (e.g. calcv before setup) */
+} npme_status;
+
+/* funcType keyword: "Laplace", "Ralpha", "Helmholtz" */
+enum { NPME_FUNC_LAPLACE = 0, NPME_FUNC_RALPHA = 1, NPME_FUNC_HELMHOLTZ = 2 };
+/* EwaldSplit keyword: "DerivMatch", "LaplaceOrig" */
+enum { NPME_SPLIT_DERIVMATCH = 0, NPME_SPLIT_LAPLACE_ORIG = 1 };
+/* Arithmetic of the bulk work.  FP64: everything in double ("plain").
+ * FP32: spreading, FFT, interpolation and pair arithmetic in float with
+ * per-target accumulation and the output in double. */
+enum { NPME_PREC_FP64 = 0, NPME_PREC_FP32 = 1 };
+
+/* Keyword-compatible parameters (names of the reference's keywords). */
+typedef struct {
+  int funcType;     /* NPME_FUNC_* */
+  int EwaldSplit;   /* NPME_SPLIT_* */
+  double alpha;     /* r^alpha exponent (Ralpha) */
+  double k0_r;      /* Helmholtz wave number, real part */
+  double k0_i;      /* Helmholtz wave number, imaginary part */
+  double Rdir;      /* direct-space cutoff (required, > 0) */
+  double tol;       /* original-Ewald tolerance (default 1e-6) */
+  int nDeriv;       /* derivative-match order (default from BnOrder) */
+  int BnOrder;      /* B-spline order, even, 4..12 (default 8) */
+  long N1, N2, N3;  /* full FFT box, multiples of 4 (required) */
+  long n1, n2, n3;  /* reference block size keywords; accepted, not used */
+  double a1, a2, a3;       /* Fourier-extension window (default 4.0) */
+  double del1, del2, del3; /* Fourier-extension margin (default Rdir) */
+  int nNeigh;       /* direct-sum cells per Rdir (default 2) */
+  int nCellClust1D; /* accepted for keyword compatibility, not used */
+  int useCompactF;  /* accepted; both values give the same kernel */
+  int precision;    /* NPME_PREC_* (default FP32) */
+  int device;       /* CUDA device ordinal (default 0) */
+} npme_params;
+
+/* Read-back of the set-up state (the reference's Print). */
+typedef struct {
+  size_t nCharge;
+  double X, Y, Z;       /* PME-corrected extents */
+  double R[3];          /* translation used by the grid mapping */
+  double L[3];          /* periodic lengths 2 (X + del) */
+  double fself_r, fself_i; /* f_LR(0) */
+  double dm_a_r[32], dm_a_i[32]; /* derivative-match coefficients a[n] */
+  int nDeriv;
+  long nCells, nBricks, nNonEmptyBricks;
+  size_t deviceBytes;   /* device memory held by the handle */
+  float stage_ms[8];    /* last calcv with timing on: gather, spread, fft,
+                           multiply, ifft, direct, interp, total */
+  int launches;         /* kernels launched by the last calcv */
+} npme_info;
+
+typedef struct npme_handle npme_handle;
+
+/* Fills the reference's defaults (src/Interface.cpp:53-517; src/Constant.h). */
+void npme_gpu_default_params(npme_params *p);
+
+/* Validates p and creates a handle on p->device.  No geometry yet. */
+int npme_gpu_create(const npme_params *p, npme_handle **out);
+
+/* SetUp / ResetCoord: bins and sorts the points, builds the kernel transform,
+ * the FFT plans and all work buffers.  coord is a host pointer. */
+int npme_gpu_setup(npme_handle *h, size_t n, const double *coord);
+
+/* CalcV with host buffers (real kernels).  coord may be NULL; when given it
+ * must be the set-up geometry.  V: 4n doubles. */
+int npme_gpu_calcv_real(npme_handle *h, double *V, size_t n,
+                        const double *charge, const double *coord);
+
+/* CalcV with host buffers (complex kernels).  charge: 2n doubles,
+ * V: 8n doubles. */
+int npme_gpu_calcv_complex(npme_handle *h, double *V, size_t n,
+                           const double *charge, const double *coord);
+
+/* CalcV on device buffers already resident in HBM, enqueued on `stream`
+ * (a cudaStream_t, or NULL for the handle's own stream).  Charge and V
+ * layouts as above.  Returns after enqueueing; the caller synchronises. */
+int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge,
+                          void *stream);
+
+/* CalcV_exact: O(N^2) sum with the full kernel (FP64), host buffers. */
+int npme_gpu_calcv_exact_real(npme_handle *h, double *V, size_t n,
+                              const double *charge, const double *coord);
+int npme_gpu_calcv_exact_complex(npme_handle *h, double *V, size_t n,
+                                 const double *charge, const double *coord);
+
+/* Number of unordered point pairs with r <= Rdir in the set-up geometry
+ * (the work of the direct sum), counted on the device with the cell list. */
+int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs);
+
+/* Record per-stage CUDA-event timings for subsequent calcv calls. */
+int npme_gpu_set_timing(npme_handle *h, int enable);
+
+int npme_gpu_get_info(const npme_handle *h, npme_info *info);
+
+/* Copies the last error message of h (or of the library when h is NULL). */
+int npme_gpu_last_error(const npme_handle *h, char *buf, size_t len);
+
+int npme_gpu_destroy(npme_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NPME_GPU_H */

@@ -1,0 +1,242 @@
+"""ctypes binding of the npme_b200 C ABI (include/npme_gpu.h).
+
+Mirrors the reference's interface objects (ElkingD/npme src/Interface.h):
+``Solver(params)`` + ``setup(coord)`` is SetUp/ResetCoord, ``calcv(q)`` is
+CalcV, ``calcv_exact(q)`` is CalcV_exact and ``info()`` is Print.  Errors are
+raised as NPMEError carrying the library's status code and message, where the
+reference prints to std::cout and returns false.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EBUSY, ESTATE = range(7)
+FUNC = {"laplace": 0, "ralpha": 1, "helmholtz": 2}
+SPLIT = {"dm": 0, "derivmatch": 0, "orig": 1, "laplaceorig": 1}
+PREC_FP64, PREC_FP32 = 0, 1
+
+
+class NPMEError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"npme_gpu error {code}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    """npme_params (keyword names of the reference)."""
+    _fields_ = [
+        ("funcType", ctypes.c_int), ("EwaldSplit", ctypes.c_int),
+        ("alpha", ctypes.c_double), ("k0_r", ctypes.c_double),
+        ("k0_i", ctypes.c_double), ("Rdir", ctypes.c_double),
+        ("tol", ctypes.c_double), ("nDeriv", ctypes.c_int),
+        ("BnOrder", ctypes.c_int),
+        ("N1", ctypes.c_long), ("N2", ctypes.c_long), ("N3", ctypes.c_long),
+        ("n1", ctypes.c_long), ("n2", ctypes.c_long), ("n3", ctypes.c_long),
+        ("a1", ctypes.c_double), ("a2", ctypes.c_double), ("a3", ctypes.c_double),
+        ("del1", ctypes.c_double), ("del2", ctypes.c_double),
+        ("del3", ctypes.c_double),
+        ("nNeigh", ctypes.c_int), ("nCellClust1D", ctypes.c_int),
+        ("useCompactF", ctypes.c_int), ("precision", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("nCharge", ctypes.c_size_t),
+        ("X", ctypes.c_double), ("Y", ctypes.c_double), ("Z", ctypes.c_double),
+        ("R", ctypes.c_double * 3), ("L", ctypes.c_double * 3),
+        ("fself_r", ctypes.c_double), ("fself_i", ctypes.c_double),
+        ("dm_a_r", ctypes.c_double * 32), ("dm_a_i", ctypes.c_double * 32),
+        ("nDeriv", ctypes.c_int),
+        ("nCells", ctypes.c_long), ("nBricks", ctypes.c_long),
+        ("nNonEmptyBricks", ctypes.c_long), ("deviceBytes", ctypes.c_size_t),
+        ("stage_ms", ctypes.c_float * 8), ("launches", ctypes.c_int),
+    ]
+
+
+STAGES = ("gather", "spread", "fft", "multiply", "ifft", "direct", "interp", "total")
+
+# Every symbol include/npme_gpu.h declares.
+EXPORTS = (
+    "npme_gpu_default_params", "npme_gpu_create", "npme_gpu_setup",
+    "npme_gpu_calcv_real", "npme_gpu_calcv_complex", "npme_gpu_calcv_device",
+    "npme_gpu_calcv_exact_real", "npme_gpu_calcv_exact_complex",
+    "npme_gpu_count_pairs", "npme_gpu_set_timing", "npme_gpu_get_info",
+    "npme_gpu_last_error",
+    "npme_gpu_destroy",
+)
+
+_lib = None
+
+
+def lib_path():
+    return os.environ.get("NPME_GPU_LIB", os.path.join(HERE, "libnpme_gpu.so"))
+
+
+def load_library():
+    """Loads the CUDA library; raises if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not os.path.exists(path):
+        raise NPMEError(ECUDA, f"{path} is missing; build it with "
+                               "`python -m npme_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, sz, dp = ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)
+    L.npme_gpu_default_params.argtypes = [ctypes.POINTER(Params)]
+    L.npme_gpu_default_params.restype = None
+    L.npme_gpu_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(vp)]
+    L.npme_gpu_setup.argtypes = [vp, sz, dp]
+    for f in ("npme_gpu_calcv_real", "npme_gpu_calcv_complex",
+              "npme_gpu_calcv_exact_real", "npme_gpu_calcv_exact_complex"):
+        getattr(L, f).argtypes = [vp, dp, sz, dp, dp]
+    L.npme_gpu_calcv_device.argtypes = [vp, vp, vp, vp]
+    L.npme_gpu_set_timing.argtypes = [vp, ctypes.c_int]
+    L.npme_gpu_count_pairs.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.npme_gpu_get_info.argtypes = [vp, ctypes.POINTER(Info)]
+    L.npme_gpu_last_error.argtypes = [vp, ctypes.c_char_p, sz]
+    L.npme_gpu_destroy.argtypes = [vp]
+    for f in EXPORTS:
+        if f != "npme_gpu_default_params":
+            getattr(L, f).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _err(L, h, code):
+    buf = ctypes.create_string_buffer(1024)
+    L.npme_gpu_last_error(h, buf, 1024)
+    return NPMEError(code, buf.value.decode(errors="replace"))
+
+
+def make_params(func="laplace", split="dm", Rdir=8.0, order=8, nDeriv=None,
+                grid=(64, 64, 64), alpha=-1.0, k0=0.0, tol=1e-6, a=4.0,
+                dell=None, nNeigh=2, precision="fp32", device=0):
+    L = load_library()
+    p = Params()
+    L.npme_gpu_default_params(ctypes.byref(p))
+    p.funcType = FUNC[func.lower()]
+    p.EwaldSplit = SPLIT[split.lower()]
+    p.Rdir = Rdir
+    p.BnOrder = order
+    p.nDeriv = nDeriv if nDeriv is not None else (3 if order == 4 else (6 if order == 6 else 8))
+    p.N1, p.N2, p.N3 = grid
+    p.alpha = alpha
+    k0 = complex(k0)
+    p.k0_r, p.k0_i = k0.real, k0.imag
+    p.tol = tol
+    p.a1 = p.a2 = p.a3 = a
+    d = Rdir if dell is None else dell
+    p.del1 = p.del2 = p.del3 = d
+    p.nNeigh = nNeigh
+    p.precision = PREC_FP32 if precision == "fp32" else PREC_FP64
+    p.device = device
+    return p
+
+
+def params_from_workload(w, precision="fp32", device=0):
+    return make_params(w.func, w.split, w.Rdir, w.order, w.nDeriv, w.grid,
+                       w.alpha, w.k0, precision=precision, device=device)
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    """One NPME interface object on one GPU (SetUp once, CalcV many times)."""
+
+    def __init__(self, params):
+        self.L = load_library()
+        self.p = params
+        h = ctypes.c_void_p()
+        rc = self.L.npme_gpu_create(ctypes.byref(params), ctypes.byref(h))
+        if rc:
+            raise _err(self.L, None, rc)
+        self.h = h
+        self.complex = params.funcType == FUNC["helmholtz"]
+        self.n = 0
+
+    def _check(self, rc):
+        if rc:
+            raise _err(self.L, self.h, rc)
+
+    def setup(self, coord):
+        c = np.ascontiguousarray(coord, dtype=np.float64).reshape(-1, 3)
+        self._check(self.L.npme_gpu_setup(self.h, c.shape[0], _dp(c)))
+        self.n = c.shape[0]
+        return self
+
+    def _q(self, q):
+        q = np.asarray(q)
+        if self.complex:
+            return np.ascontiguousarray(q, dtype=np.complex128).view(np.float64)
+        if np.iscomplexobj(q):
+            raise NPMEError(EINVAL, "complex charges for a real kernel")
+        return np.ascontiguousarray(q, dtype=np.float64)
+
+    def calcv(self, q, out=None):
+        qb = self._q(q)
+        V = out if out is not None else np.empty(
+            (self.n, 4), np.complex128 if self.complex else np.float64)
+        f = self.L.npme_gpu_calcv_complex if self.complex else self.L.npme_gpu_calcv_real
+        self._check(f(self.h, _dp(V.view(np.float64)), self.n, _dp(qb), None))
+        return V
+
+    def calcv_exact(self, q):
+        qb = self._q(q)
+        V = np.empty((self.n, 4), np.complex128 if self.complex else np.float64)
+        f = (self.L.npme_gpu_calcv_exact_complex if self.complex
+             else self.L.npme_gpu_calcv_exact_real)
+        self._check(f(self.h, _dp(V.view(np.float64)), self.n, _dp(qb), None))
+        return V
+
+    def calcv_device(self, V_ptr, q_ptr, stream_ptr=None):
+        """CalcV on device pointers (ints), enqueued on stream_ptr."""
+        self._check(self.L.npme_gpu_calcv_device(
+            self.h, ctypes.c_void_p(V_ptr), ctypes.c_void_p(q_ptr),
+            ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def count_pairs(self):
+        """Unordered pairs with r <= Rdir (direct-sum work)."""
+        c = ctypes.c_ulonglong()
+        self._check(self.L.npme_gpu_count_pairs(self.h, ctypes.byref(c)))
+        return int(c.value)
+
+    def set_timing(self, on=True):
+        self._check(self.L.npme_gpu_set_timing(self.h, int(bool(on))))
+
+    def info(self):
+        i = Info()
+        self._check(self.L.npme_gpu_get_info(self.h, ctypes.byref(i)))
+        return {
+            "nCharge": i.nCharge, "X": i.X, "Y": i.Y, "Z": i.Z,
+            "R": list(i.R), "L": list(i.L),
+            "fself": complex(i.fself_r, i.fself_i),
+            "dm_a": [complex(i.dm_a_r[k], i.dm_a_i[k]) for k in range(i.nDeriv + 1)],
+            "nCells": i.nCells, "nBricks": i.nBricks,
+            "nNonEmptyBricks": i.nNonEmptyBricks, "deviceBytes": i.deviceBytes,
+            "stage_ms": dict(zip(STAGES, list(i.stage_ms))), "launches": i.launches,
+        }
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.npme_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,352 @@
+// Short-range direct sum over a cell list, and the exact O(N^2) sum.
+//
+// Direct sum (src/PotentialLaplace.cpp:201-264 and the pair kernels cited in
+// common.cuh): V_i = sum_{j != i, r_ij <= Rdir} q_j f_SR(r_ij),
+// dV_i/dx = sum q_j f1_SR(r_ij) (x_i - x_j).  Points are sorted by cell
+// (edge >= Rdir/nNeigh, row-major, z fastest), so the cells of one (x, y)
+// neighbour column with consecutive z are one contiguous range.  One CTA owns
+// one target cell; source ranges are staged through shared memory with their
+// cell offset applied (coordinates are kept relative to the point's own cell,
+// so float arithmetic keeps ~1e-7 relative resolution whatever the box size).
+// Each thread accumulates its target over a staged tile in the bulk
+// precision and adds the tile total to a double accumulator.  No atomics: the
+// result is deterministic and each output row is written once.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "internal.h"
+
+namespace npme {
+
+template <typename T>
+PairCoef<T> make_pair_coef(const npme_handle *h) {
+  PairCoef<T> k;
+  memset(&k, 0, sizeof(k));
+  const double R = h->p.Rdir, R2 = R * R;
+  k.func = h->p.funcType;
+  k.split = h->p.EwaldSplit;
+  k.nder = h->p.nDeriv;
+  k.R2 = (T)R2;
+  k.invR2 = (T)(1.0 / R2);
+  k.alpha = (T)h->p.alpha;
+  k.half_alpha = (T)(0.5 * h->p.alpha);
+  k.beta = (T)h->beta;
+  k.beta2 = (T)(h->beta * h->beta);
+  k.two_beta_rpi = (T)(2.0 * h->beta / std::sqrt(M_PI));
+  k.k0r = (T)h->p.k0_r;
+  k.k0i = (T)h->p.k0_i;
+  double s = 1.0;  // R^(2n)
+  for (int i = 0; i <= k.nder && i <= kMaxDeriv; i++) {
+    k.ar[i] = (T)(h->a_r[i] * s);
+    k.ai[i] = (T)(h->a_i[i] * s);
+    k.br[i] = (T)(h->b_r[i] * s);
+    k.bi[i] = (T)(h->b_i[i] * s);
+    s *= R2;
+  }
+  return k;
+}
+template PairCoef<float> make_pair_coef<float>(const npme_handle *);
+template PairCoef<double> make_pair_coef<double>(const npme_handle *);
+
+constexpr int kDirectBS = 64;
+
+template <typename T, bool CPLX, int FUNC, int SPLIT>
+__global__ void __launch_bounds__(kDirectBS) direct_kernel(
+    PairCoef<T> k, const typename Vec4<T>::type *__restrict__ cpos, const T *__restrict__ qc,
+    const int *__restrict__ cell_start, const uint32_t *__restrict__ cperm, int nc0, int nc1,
+    int nc2, T e0, T e1, T e2, int reach, double fself_r, double fself_i,
+    double *__restrict__ V) {
+  using V4 = typename Vec4<T>::type;
+  __shared__ V4 sp[kDirectBS];
+  __shared__ T sq[kDirectBS * (CPLX ? 2 : 1)];
+  const int cell = blockIdx.x;
+  const int cz = cell % nc2, cy = (cell / nc2) % nc1, cx = cell / (nc2 * nc1);
+  const int tbeg = cell_start[cell], tend = cell_start[cell + 1];
+  const T R2 = k.R2;
+  const double e0d = e0, e1d = e1, e2d = e2;
+  for (int t0 = tbeg; t0 < tend; t0 += kDirectBS) {
+    const int i = t0 + threadIdx.x;
+    const bool active = i < tend;
+    V4 ti = active ? cpos[i] : V4{0, 0, 0, 0};
+    double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
+    for (int dx = -reach; dx <= reach; dx++) {
+      const int sx = cx + dx;
+      if (sx < 0 || sx >= nc0) continue;
+      const double mx = (double)(abs(dx) > 0 ? abs(dx) - 1 : 0) * e0d;
+      for (int dy = -reach; dy <= reach; dy++) {
+        const int sy = cy + dy;
+        if (sy < 0 || sy >= nc1) continue;
+        const double my = (double)(abs(dy) > 0 ? abs(dy) - 1 : 0) * e1d;
+        const double rem = (double)R2 - mx * mx - my * my;
+        if (rem < 0) continue;
+        // cells with |dz| - 1 <= sqrt(rem) / e2 can hold a source within Rdir
+        const int zr = min(reach, 1 + (int)floor(sqrt(rem) / e2d));
+        const int z0 = max(cz - zr, 0), z1 = min(cz + zr, nc2 - 1);
+        const int colbase = (sx * nc1 + sy) * nc2;
+        const int jb = cell_start[colbase + z0], je = cell_start[colbase + z1 + 1];
+        const T ox = (T)dx * e0, oy = (T)dy * e1;
+        for (int j0 = jb; j0 < je; j0 += kDirectBS) {
+          __syncthreads();
+          const int j = j0 + threadIdx.x;
+          if (j < je) {
+            V4 s = cpos[j];
+            s.x += ox;
+            s.y += oy;
+            s.z += (s.w - (T)cz) * e2;
+            sp[threadIdx.x] = s;
+            if (CPLX) {
+              sq[2 * threadIdx.x] = qc[2 * (long)j];
+              sq[2 * threadIdx.x + 1] = qc[2 * (long)j + 1];
+            } else {
+              sq[threadIdx.x] = qc[j];
+            }
+          }
+          __syncthreads();
+          const int cnt = min(kDirectBS, je - j0);
+          T p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
+          const int self = i - j0;  // staged slot of the target itself, if present
+          for (int s = 0; s < cnt; s++) {
+            const V4 src = sp[s];
+            const T x = ti.x - src.x, y = ti.y - src.y, z = ti.z - src.z;
+            const T r2 = fma(x, x, fma(y, y, z * z));
+            if (r2 <= R2 && s != self) {
+              if (!CPLX) {
+                T f1;
+                const T f0 = pair_sr_real<T, FUNC, SPLIT>(k, r2, f1);
+                const T qj = sq[s];
+                const T g = f1 * qj;
+                p0 = fma(f0, qj, p0);
+                p1 = fma(g, x, p1);
+                p2 = fma(g, y, p2);
+                p3 = fma(g, z, p3);
+              } else {
+                T f0r, f0i, f1r, f1i;
+                pair_sr_helmholtz<T>(k, r2, f0r, f0i, f1r, f1i);
+                const T qr = sq[2 * s], qi = sq[2 * s + 1];
+                // f0 q and (f1 q) * (x, y, z), complex
+                p0 = fma(f0r, qr, fma(-f0i, qi, p0));
+                p0i = fma(f0r, qi, fma(f0i, qr, p0i));
+                const T gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
+                p1 = fma(gr, x, p1);
+                p2 = fma(gr, y, p2);
+                p3 = fma(gr, z, p3);
+                p1i = fma(gi, x, p1i);
+                p2i = fma(gi, y, p2i);
+                p3i = fma(gi, z, p3i);
+              }
+            }
+          }
+          acc[0] += (double)p0;
+          acc[1] += (double)p1;
+          acc[2] += (double)p2;
+          acc[3] += (double)p3;
+          if (CPLX) {
+            acci[0] += (double)p0i;
+            acci[1] += (double)p1i;
+            acci[2] += (double)p2i;
+            acci[3] += (double)p3i;
+          }
+        }
+      }
+    }
+    if (active) {
+      const long o = cperm[i];
+      if (CPLX) {
+        const double qr = qc[2 * (long)i], qi = qc[2 * (long)i + 1];
+        // V -= f_LR(0) q (src/Interface.cpp:2909-2910)
+        acc[0] -= fself_r * qr - fself_i * qi;
+        acci[0] -= fself_r * qi + fself_i * qr;
+        double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+#pragma unroll
+        for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
+      } else {
+        acc[0] -= fself_r * (double)qc[i];  // src/Interface.cpp:2061-2062
+        reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+      }
+    }
+  }
+}
+
+template <typename T, bool CPLX, int FUNC, int SPLIT>
+static void direct_launch(npme_handle *h, double *d_V, cudaStream_t s) {
+  const CellGeom &c = h->cells;
+  const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
+  direct_kernel<T, CPLX, FUNC, SPLIT><<<ncell, kDirectBS, 0, s>>>(
+      make_pair_coef<T>(h), (const typename Vec4<T>::type *)h->d_cpos, (const T *)h->d_qc,
+      h->d_cell_start, h->d_cperm, c.nc[0], c.nc[1], c.nc[2], (T)c.edge[0], (T)c.edge[1],
+      (T)c.edge[2], c.reach, h->fself_r, h->fself_i, d_V);
+}
+
+template <typename T>
+static void direct_prec(npme_handle *h, double *d_V, cudaStream_t s) {
+  const int f = h->p.funcType, sp = h->p.EwaldSplit;
+  if (f == NPME_FUNC_HELMHOLTZ) direct_launch<T, true, 2, 0>(h, d_V, s);
+  else if (sp == NPME_SPLIT_LAPLACE_ORIG) direct_launch<T, false, 0, 1>(h, d_V, s);
+  else if (f == NPME_FUNC_RALPHA) direct_launch<T, false, 1, 0>(h, d_V, s);
+  else direct_launch<T, false, 0, 0>(h, d_V, s);
+}
+
+void launch_direct(npme_handle *h, double *d_V, cudaStream_t s) {
+  if (h->fp32) direct_prec<float>(h, d_V, s);
+  else direct_prec<double>(h, d_V, s);
+  h->launches++;
+}
+
+// Ordered pairs with r <= Rdir, i != j, using the same cell walk as the
+// direct sum (work accounting for the roofline report).
+template <typename T>
+__global__ void __launch_bounds__(kDirectBS) count_pairs_kernel(
+    const typename Vec4<T>::type *__restrict__ cpos, const int *__restrict__ cell_start,
+    int nc0, int nc1, int nc2, T e0, T e1, T e2, int reach, T R2,
+    unsigned long long *__restrict__ count) {
+  using V4 = typename Vec4<T>::type;
+  __shared__ V4 sp[kDirectBS];
+  const int cell = blockIdx.x;
+  const int cz = cell % nc2, cy = (cell / nc2) % nc1, cx = cell / (nc2 * nc1);
+  const int tbeg = cell_start[cell], tend = cell_start[cell + 1];
+  unsigned long long mine = 0;
+  for (int t0 = tbeg; t0 < tend; t0 += kDirectBS) {
+    const int i = t0 + threadIdx.x;
+    const bool active = i < tend;
+    V4 ti = active ? cpos[i] : V4{0, 0, 0, 0};
+    for (int dx = -reach; dx <= reach; dx++) {
+      const int sx = cx + dx;
+      if (sx < 0 || sx >= nc0) continue;
+      for (int dy = -reach; dy <= reach; dy++) {
+        const int sy = cy + dy;
+        if (sy < 0 || sy >= nc1) continue;
+        const int z0 = max(cz - reach, 0), z1 = min(cz + reach, nc2 - 1);
+        const int colbase = (sx * nc1 + sy) * nc2;
+        const int jb = cell_start[colbase + z0], je = cell_start[colbase + z1 + 1];
+        for (int j0 = jb; j0 < je; j0 += kDirectBS) {
+          __syncthreads();
+          const int j = j0 + threadIdx.x;
+          if (j < je) {
+            V4 s = cpos[j];
+            s.x += (T)dx * e0;
+            s.y += (T)dy * e1;
+            s.z += (s.w - (T)cz) * e2;
+            sp[threadIdx.x] = s;
+          }
+          __syncthreads();
+          const int cnt = min(kDirectBS, je - j0);
+          if (active)
+            for (int s = 0; s < cnt; s++) {
+              const T x = ti.x - sp[s].x, y = ti.y - sp[s].y, z = ti.z - sp[s].z;
+              if (x * x + y * y + z * z <= R2 && j0 + s != i) mine++;
+            }
+        }
+      }
+    }
+  }
+  atomicAdd(count, mine);
+}
+
+void launch_count_pairs(npme_handle *h, unsigned long long *d_count, cudaStream_t s) {
+  const CellGeom &c = h->cells;
+  const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
+  const double R2 = h->p.Rdir * h->p.Rdir;
+  if (h->fp32)
+    count_pairs_kernel<float><<<ncell, kDirectBS, 0, s>>>(
+        (const float4 *)h->d_cpos, h->d_cell_start, c.nc[0], c.nc[1], c.nc[2],
+        (float)c.edge[0], (float)c.edge[1], (float)c.edge[2], c.reach, (float)R2, d_count);
+  else
+    count_pairs_kernel<double><<<ncell, kDirectBS, 0, s>>>(
+        (const double4 *)h->d_cpos, h->d_cell_start, c.nc[0], c.nc[1], c.nc[2], c.edge[0],
+        c.edge[1], c.edge[2], c.reach, R2, d_count);
+}
+
+// ---------------------------------------------------------------------------
+// Exact sum (src/PotentialLaplace.cpp:40-132, src/PotentialHelmholtz.cpp:41,
+// src/PotentialGenFunc.cpp:321): all pairs j != i with the full kernel, FP64,
+// no self term.  Sources are tiled through shared memory.
+
+constexpr int kExactBS = 128;
+
+template <int FUNC>
+__global__ void __launch_bounds__(kExactBS) exact_kernel(const double *__restrict__ coord,
+                                                          const double *__restrict__ q, long n,
+                                                          double alpha, double k0r, double k0i,
+                                                          double *__restrict__ V) {
+  constexpr bool CPLX = FUNC == 2;
+  __shared__ double4 sp[kExactBS];
+  __shared__ double2 sq[kExactBS];
+  const long i = blockIdx.x * (long)kExactBS + threadIdx.x;
+  const bool active = i < n;
+  double xi = 0, yi = 0, zi = 0;
+  if (active) xi = coord[3 * i], yi = coord[3 * i + 1], zi = coord[3 * i + 2];
+  double a[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+  for (long j0 = 0; j0 < n; j0 += kExactBS) {
+    __syncthreads();
+    const long j = j0 + threadIdx.x;
+    if (j < n) {
+      sp[threadIdx.x] = make_double4(coord[3 * j], coord[3 * j + 1], coord[3 * j + 2], 0.0);
+      sq[threadIdx.x] = CPLX ? make_double2(q[2 * j], q[2 * j + 1]) : make_double2(q[j], 0.0);
+    }
+    __syncthreads();
+    const int cnt = (int)min((long)kExactBS, n - j0);
+    for (int s = 0; s < cnt; s++) {
+      if (j0 + s == i) continue;
+      const double x = xi - sp[s].x, y = yi - sp[s].y, z = zi - sp[s].z;
+      const double r2 = x * x + y * y + z * z;
+      if (FUNC == 0) {
+        const double rinv = rsqrt(r2);
+        const double f0 = rinv, f1 = -rinv * rinv * rinv;
+        const double qj = sq[s].x;
+        a[0] += f0 * qj;
+        a[1] += f1 * qj * x;
+        a[2] += f1 * qj * y;
+        a[3] += f1 * qj * z;
+      } else if (FUNC == 1) {
+        const double f0 = pow(r2, 0.5 * alpha), f1 = alpha * f0 / r2;
+        const double qj = sq[s].x;
+        a[0] += f0 * qj;
+        a[1] += f1 * qj * x;
+        a[2] += f1 * qj * y;
+        a[3] += f1 * qj * z;
+      } else {
+        const double r = sqrt(r2);
+        double sn, cs;
+        sincos(k0r * r, &sn, &cs);
+        const double d = exp(-k0i * r) / r;
+        const double er = cs * d, ei = sn * d;
+        const double ikr = -k0i * er - k0r * ei, iki = k0r * er - k0i * ei;
+        const double f1r = (ikr - er / r) / r, f1i = (iki - ei / r) / r;
+        const double qr = sq[s].x, qi = sq[s].y;
+        a[0] += er * qr - ei * qi;
+        ai[0] += er * qi + ei * qr;
+        const double gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
+        a[1] += gr * x, a[2] += gr * y, a[3] += gr * z;
+        ai[1] += gi * x, ai[2] += gi * y, ai[3] += gi * z;
+      }
+    }
+  }
+  if (active) {
+    if (CPLX) {
+      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * i;
+      for (int m = 0; m < 4; m++) Vo[m] = make_double2(a[m], ai[m]);
+    } else {
+      reinterpret_cast<double4 *>(V)[i] = make_double4(a[0], a[1], a[2], a[3]);
+    }
+  }
+}
+
+void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s) {
+  const long n = (long)h->n;
+  const int blocks = (int)((n + kExactBS - 1) / kExactBS);
+  if (blocks == 0) return;
+  const int f = h->p.funcType;
+  if (f == 0)
+    exact_kernel<0><<<blocks, kExactBS, 0, s>>>(h->d_coord, d_q, n, h->p.alpha, h->p.k0_r,
+                                                 h->p.k0_i, d_V);
+  else if (f == 1)
+    exact_kernel<1><<<blocks, kExactBS, 0, s>>>(h->d_coord, d_q, n, h->p.alpha, h->p.k0_r,
+                                                 h->p.k0_i, d_V);
+  else
+    exact_kernel<2><<<blocks, kExactBS, 0, s>>>(h->d_coord, d_q, n, h->p.alpha, h->p.k0_r,
+                                                 h->p.k0_i, d_V);
+  h->launches++;
+}
+
+}  // namespace npme

@@ -1,0 +1,117 @@
+// Internal declarations of npme_b200: the handle and the kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/npme_gpu.h"
+#include "common.cuh"
+
+namespace npme {
+
+// Brick edge (grid points) of the spread tiles.
+constexpr int kBrick = 8;
+
+// Geometry of the reciprocal-space grid and of the brick decomposition.
+struct GridGeom {
+  long N[3];      // full FFT box
+  long H[3];      // charge octant N/2
+  long nb[3];     // bricks per axis over the octant
+  int order;
+};
+
+// Geometry of the direct-sum cell list.
+struct CellGeom {
+  int nc[3];       // cells per axis
+  double origin[3];
+  double edge[3];  // cell edge >= Rdir / nNeigh
+  int reach;       // neighbour cells per direction = nNeigh
+};
+
+// One spread/interp record per point in brick order.  g0 packs the three
+// stencil origins (10 bits each, grid index in the octant).
+template <typename T>
+struct BrickPoint {
+  T u[3];
+  uint32_t g0;
+  uint32_t orig;  // caller's index
+};
+
+struct Timing {
+  bool enabled = false;
+  cudaEvent_t ev[10] = {};
+};
+
+}  // namespace npme
+
+struct npme_handle {
+  npme_params p;
+  int device = 0;
+  bool complex_kernel = false;
+  bool fp32 = true;
+  bool ready = false;
+  std::string err;
+
+  // set-up state
+  size_t n = 0;
+  double box[9];  // X Y Z R[3] L[3]
+  double fself_r = 0, fself_i = 0;
+  double a_r[32], a_i[32], b_r[32], b_i[32];
+  double beta = 0;
+  npme::GridGeom grid;
+  npme::CellGeom cells;
+  long n_bricks = 0, n_nonempty = 0;
+
+  cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;  // direct sum runs here, overlapped with the FFTs
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cufftHandle plan_fwd = 0, plan_inv = 0;
+  bool plans = false;
+
+  // device buffers (all allocated in setup; calcv allocates nothing)
+  double *d_coord = nullptr;     // original order, FP64 (exact sum, FP64 direct)
+  void *d_bpts = nullptr;        // BrickPoint<T>[n]
+  int *d_brick_start = nullptr;  // [n_bricks + 1]
+  int *d_brick_list = nullptr;   // non-empty brick ids
+  void *d_cpos = nullptr;        // cell order positions: float4 (local xyz, cell z) or double4
+  uint32_t *d_cperm = nullptr;   // cell order -> caller index
+  int *d_cell_start = nullptr;   // [ncell + 1]
+  void *d_qb = nullptr;          // charges in brick order (T or T2)
+  void *d_qc = nullptr;          // charges in cell order (T or T2)
+  void *d_grid = nullptr;        // spread grid, real N1 N2 N3 (or complex)
+  void *d_kgrid = nullptr;       // transformed grid N1 N2 (N3/2+1) complex (real kernels)
+  void *d_theta = nullptr;       // theta, same layout as d_grid (real kernels)
+  void *d_G = nullptr;           // kernel transform on the octant (N/2+1)^3, T or T2
+  double *d_q_in = nullptr;      // staging for host charges (n or 2n doubles)
+  double *d_V = nullptr;         // staging for host output (4n or 8n doubles)
+  double *d_V_exact = nullptr;
+  int *d_err = nullptr;          // device error flag
+  size_t dev_bytes = 0;
+
+  npme::Timing timing;
+  bool timing_pending = false;
+  float stage_ms[8] = {0};
+  int launches = 0;
+};
+
+namespace npme {
+
+// recsum.cu
+int build_kernel_transform(npme_handle *h);  // F-hat, lambda^2 -> d_G
+void launch_gather_charges(npme_handle *h, const double *d_q, cudaStream_t s);
+void launch_spread(npme_handle *h, cudaStream_t s);
+void launch_multiply(npme_handle *h, cudaStream_t s);
+void launch_interp(npme_handle *h, double *d_V, cudaStream_t s);
+
+// direct.cu
+void launch_direct(npme_handle *h, double *d_V, cudaStream_t s);
+void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
+void launch_count_pairs(npme_handle *h, unsigned long long *d_count, cudaStream_t s);
+template <typename T>
+PairCoef<T> make_pair_coef(const npme_handle *h);
+
+}  // namespace npme

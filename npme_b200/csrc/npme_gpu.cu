@@ -1,0 +1,671 @@
+// C ABI of npme_b200 (include/npme_gpu.h): parameter handling, set-up
+// (derivative-match coefficients, box, point binning, buffers, FFT plans,
+// kernel transform) and the CalcV orchestration on CUDA streams.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using npme::BrickPoint;
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err;
+
+void set_global_err(const std::string &s) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_err = s;
+}
+
+int fail(npme_handle *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  else set_global_err(msg);
+  return code;
+}
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(h, NPME_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CKFFT(call)                                                              \
+  do {                                                                           \
+    cufftResult r_ = (call);                                                     \
+    if (r_ != CUFFT_SUCCESS)                                                     \
+      return fail(h, NPME_ECUDA, std::string(#call) + ": cufft error " + std::to_string((int)r_)); \
+  } while (0)
+
+// --- derivative-match coefficients (FP64, host) ---------------------------
+// (1/r d/dr)^n f at Rdir: r^alpha (src/FunctionDerivMatch.cpp:76-88) and
+// exp(i k0 r)/r (src/FunctionDerivMatch.cpp:42-55); a_n by back substitution
+// and b_n = 2 (n+1) a_{n+1} (src/FunctionDerivMatch.cpp:226-266).
+using cd = std::complex<double>;
+
+double calc_cnp(int n, int p, double R) {
+  if (n > p) return 0.0;
+  double c = 1.0;
+  for (int i = 0; i < p - n; i++) c *= R * R;
+  for (int i = 0; i < n; i++) c *= 2.0;
+  for (int i = p - n + 1; i <= p; i++) c *= (double)i;
+  return c;
+}
+
+void dm_coefficients(const npme_params &p, cd *a, cd *b) {
+  const int N = p.nDeriv;
+  const double R = p.Rdir, r2 = R * R;
+  cd f[32];
+  if (p.funcType == NPME_FUNC_HELMHOLTZ) {
+    const cd k0(p.k0_r, p.k0_i), I(0, 1);
+    const cd C = std::exp(I * k0 * R), A = k0 * k0 / r2;
+    f[0] = C / R;
+    if (N >= 1) f[1] = -C / R / r2 + I * k0 * C / r2;
+    for (int n = 2; n <= N; n++) f[n] = -(2.0 * n - 1.0) / r2 * f[n - 1] - A * f[n - 2];
+  } else {
+    const double alpha = p.funcType == NPME_FUNC_LAPLACE ? -1.0 : p.alpha;
+    f[0] = std::pow(R, alpha);
+    for (int n = 1; n <= N; n++) f[n] = f[n - 1] * (alpha - 2 * n + 2) / r2;
+  }
+  for (int q = 0; q <= N; q++) {
+    cd s = f[N - q];
+    for (int t = 0; t < q; t++) s -= calc_cnp(N - q, N - t, R) * a[N - t];
+    a[N - q] = s / calc_cnp(N - q, N - q, R);
+  }
+  for (int i = 0; i <= N - 1; i++) b[i] = a[i + 1] * 2.0 * (double)(i + 1);
+  b[N] = 0;
+}
+
+// beta with erfc(beta Rdir)/Rdir ~ tol (src/KernelFunctionLaplace.cpp:41-76)
+double orig_beta(double R, double tol) {
+  const double C = std::log(std::sqrt(M_PI) * tol * R);
+  double x = 0.1;
+  for (int n = 0; n < 1000; n++) {
+    const double F0 = x * x + std::log(x) + C, F1 = 2 * x + 1.0 / x;
+    if (std::fabs(F0) < 1e-12) return x / R;
+    x -= F0 / F1;
+  }
+  return -1.0;
+}
+
+// src/RecSumSupportFunctions.cpp:137-147
+double min_x_compact(double X0, double del, long order, long N) {
+  const double a1 = 1.0 - 2.0 * (order + 1) / N;
+  const double a2 = 1.0 - 4.0 * (order + 1) / N;
+  const double X = X0 / a1 - del / 2.0 * a2 / a1;
+  return X0 > X ? X0 : X;
+}
+
+// src/RecSumSupportFunctions.h:123-127
+long start_index(double w) { return w < 0 ? (long)(-w) + 1 : (long)(-w); }
+
+void release(npme_handle *h) {
+  if (h->plans) {
+    cufftDestroy(h->plan_fwd);
+    if (h->plan_inv != h->plan_fwd) cufftDestroy(h->plan_inv);
+    h->plans = false;
+  }
+  void *bufs[] = {h->d_coord, h->d_bpts, h->d_brick_start, h->d_brick_list, h->d_cpos,
+                  h->d_cperm, h->d_cell_start, h->d_qb, h->d_qc, h->d_grid, h->d_kgrid,
+                  h->d_theta, h->d_G, h->d_q_in, h->d_V, h->d_V_exact, h->d_err};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  h->d_coord = nullptr, h->d_bpts = nullptr, h->d_brick_start = nullptr;
+  h->d_brick_list = nullptr, h->d_cpos = nullptr, h->d_cperm = nullptr;
+  h->d_cell_start = nullptr, h->d_qb = nullptr, h->d_qc = nullptr, h->d_grid = nullptr;
+  h->d_kgrid = nullptr, h->d_theta = nullptr, h->d_G = nullptr, h->d_q_in = nullptr;
+  h->d_V = nullptr, h->d_V_exact = nullptr, h->d_err = nullptr;
+  h->dev_bytes = 0;
+  h->ready = false;
+}
+
+template <typename P>
+int dalloc(npme_handle *h, P **ptr, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc((void **)ptr, bytes);
+  if (e != cudaSuccess)
+    return fail(h, NPME_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+  h->dev_bytes += bytes;
+  return NPME_OK;
+}
+
+template <typename T>
+int upload_points(npme_handle *h, const double *coord) {
+  const size_t n = h->n;
+  const npme::GridGeom &g = h->grid;
+  const double *R = h->box + 3, *L = h->box + 6;
+  const int P = g.order;
+  // --- brick order for spread / interpolation ---
+  std::vector<BrickPoint<T>> pts(n);
+  std::vector<int> bid(n);
+  for (size_t i = 0; i < n; i++) {
+    uint32_t g0[3];
+    T u[3];
+    for (int d = 0; d < 3; d++) {
+      const double w = (double)g.N[d] / L[d] * (coord[3 * i + d] - R[d]);
+      const long ms = start_index(w);
+      const long o = ms + g.N[d] / 4;
+      if (o < 0 || o + P - 1 > g.H[d] - 1)
+        return fail(h, NPME_EINVAL,
+                    "point " + std::to_string(i) + " has a B-spline stencil outside the "
+                    "charge octant (axis " + std::to_string(d) + ")");
+      g0[d] = (uint32_t)o;
+      u[d] = (T)(w + (double)ms);
+    }
+    BrickPoint<T> &bp = pts[i];
+    bp.u[0] = u[0], bp.u[1] = u[1], bp.u[2] = u[2];
+    bp.g0 = (g0[0] << 20) | (g0[1] << 10) | g0[2];
+    bp.orig = (uint32_t)i;
+    bid[i] = (int)(((g0[0] / npme::kBrick) * g.nb[1] + g0[1] / npme::kBrick) * g.nb[2] +
+                   g0[2] / npme::kBrick);
+  }
+  const long nbt = g.nb[0] * g.nb[1] * g.nb[2];
+  std::vector<int> bstart(nbt + 1, 0);
+  for (size_t i = 0; i < n; i++) bstart[bid[i] + 1]++;
+  for (long b = 0; b < nbt; b++) bstart[b + 1] += bstart[b];
+  std::vector<int> fillp(bstart.begin(), bstart.end() - 1);
+  std::vector<BrickPoint<T>> sorted(n);
+  for (size_t i = 0; i < n; i++) sorted[fillp[bid[i]]++] = pts[i];
+  std::vector<int> blist;
+  for (long b = 0; b < nbt; b++)
+    if (bstart[b + 1] > bstart[b]) blist.push_back((int)b);
+  h->n_bricks = nbt;
+  h->n_nonempty = (long)blist.size();
+
+  // --- cell order for the direct sum ---
+  const npme::CellGeom &c = h->cells;
+  const long ncell = (long)c.nc[0] * c.nc[1] * c.nc[2];
+  std::vector<int> cid(n);
+  std::vector<double> loc(3 * n);
+  std::vector<int> cz(n);
+  for (size_t i = 0; i < n; i++) {
+    int ci[3];
+    for (int d = 0; d < 3; d++) {
+      long k = (long)std::floor((coord[3 * i + d] - c.origin[d]) / c.edge[d]);
+      k = std::max(0L, std::min(k, (long)c.nc[d] - 1));
+      ci[d] = (int)k;
+      loc[3 * i + d] = coord[3 * i + d] - (c.origin[d] + k * c.edge[d]);
+    }
+    cz[i] = ci[2];
+    cid[i] = (ci[0] * c.nc[1] + ci[1]) * c.nc[2] + ci[2];
+  }
+  std::vector<int> cstart(ncell + 1, 0);
+  for (size_t i = 0; i < n; i++) cstart[cid[i] + 1]++;
+  for (long b = 0; b < ncell; b++) cstart[b + 1] += cstart[b];
+  std::vector<int> cfill(cstart.begin(), cstart.end() - 1);
+  using V4 = typename npme::Vec4<T>::type;
+  std::vector<V4> cpos(n);
+  std::vector<uint32_t> cperm(n);
+  for (size_t i = 0; i < n; i++) {
+    const int s = cfill[cid[i]]++;
+    cpos[s] = V4{(T)loc[3 * i], (T)loc[3 * i + 1], (T)loc[3 * i + 2], (T)cz[i]};
+    cperm[s] = (uint32_t)i;
+  }
+
+  const int C = h->complex_kernel ? 2 : 1;
+  int rc;
+  if ((rc = dalloc(h, &h->d_coord, sizeof(double) * 3 * n))) return rc;
+  if ((rc = dalloc(h, (BrickPoint<T> **)&h->d_bpts, sizeof(BrickPoint<T>) * n))) return rc;
+  if ((rc = dalloc(h, &h->d_brick_start, sizeof(int) * (nbt + 1)))) return rc;
+  if ((rc = dalloc(h, &h->d_brick_list, sizeof(int) * std::max<size_t>(1, blist.size()))))
+    return rc;
+  if ((rc = dalloc(h, (V4 **)&h->d_cpos, sizeof(V4) * n))) return rc;
+  if ((rc = dalloc(h, &h->d_cperm, sizeof(uint32_t) * n))) return rc;
+  if ((rc = dalloc(h, &h->d_cell_start, sizeof(int) * (ncell + 1)))) return rc;
+  if ((rc = dalloc(h, (T **)&h->d_qb, sizeof(T) * C * n))) return rc;
+  if ((rc = dalloc(h, (T **)&h->d_qc, sizeof(T) * C * n))) return rc;
+  if ((rc = dalloc(h, &h->d_q_in, sizeof(double) * C * n))) return rc;
+  if ((rc = dalloc(h, &h->d_V, sizeof(double) * 4 * C * n))) return rc;
+  CK(cudaMemcpy(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_bpts, sorted.data(), sizeof(BrickPoint<T>) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_brick_start, bstart.data(), sizeof(int) * (nbt + 1),
+                cudaMemcpyHostToDevice));
+  if (!blist.empty())
+    CK(cudaMemcpy(h->d_brick_list, blist.data(), sizeof(int) * blist.size(),
+                  cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_cpos, cpos.data(), sizeof(V4) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_cperm, cperm.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_cell_start, cstart.data(), sizeof(int) * (ncell + 1),
+                cudaMemcpyHostToDevice));
+
+  // --- grids ---
+  const long *N = g.N;
+  const size_t Ntot = (size_t)N[0] * N[1] * N[2];
+  const size_t Mtot = (size_t)(N[0] / 2 + 1) * (N[1] / 2 + 1) * (N[2] / 2 + 1);
+  if (h->complex_kernel) {
+    if ((rc = dalloc(h, (T **)&h->d_grid, sizeof(T) * 2 * Ntot))) return rc;
+    if ((rc = dalloc(h, (T **)&h->d_G, sizeof(T) * 2 * Mtot))) return rc;
+  } else {
+    if ((rc = dalloc(h, (T **)&h->d_grid, sizeof(T) * Ntot))) return rc;
+    if ((rc = dalloc(h, (T **)&h->d_kgrid, sizeof(T) * 2 * (size_t)N[0] * N[1] * (N[2] / 2 + 1))))
+      return rc;
+    if ((rc = dalloc(h, (T **)&h->d_G, sizeof(T) * Mtot))) return rc;
+  }
+  return NPME_OK;
+}
+
+int make_plans(npme_handle *h) {
+  const long *N = h->grid.N;
+  const int n0 = (int)N[0], n1 = (int)N[1], n2 = (int)N[2];
+  if (h->complex_kernel) {
+    CKFFT(cufftPlan3d(&h->plan_fwd, n0, n1, n2, h->fp32 ? CUFFT_C2C : CUFFT_Z2Z));
+    h->plan_inv = h->plan_fwd;
+  } else {
+    CKFFT(cufftPlan3d(&h->plan_fwd, n0, n1, n2, h->fp32 ? CUFFT_R2C : CUFFT_D2Z));
+    cufftResult r = cufftPlan3d(&h->plan_inv, n0, n1, n2, h->fp32 ? CUFFT_C2R : CUFFT_Z2D);
+    if (r != CUFFT_SUCCESS) {
+      cufftDestroy(h->plan_fwd);
+      return fail(h, NPME_ECUDA, "cufftPlan3d (inverse) failed: " + std::to_string((int)r));
+    }
+  }
+  h->plans = true;
+  return NPME_OK;
+}
+
+int check_params(npme_handle *h, const npme_params &p) {
+  if (!(p.Rdir > 0)) return fail(h, NPME_EINVAL, "Rdir must be > 0");
+  if (p.funcType < 0 || p.funcType > 2) return fail(h, NPME_EINVAL, "unknown funcType");
+  if (p.EwaldSplit < 0 || p.EwaldSplit > 1) return fail(h, NPME_EINVAL, "unknown EwaldSplit");
+  if (p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG && p.funcType != NPME_FUNC_LAPLACE)
+    return fail(h, NPME_EINVAL, "EwaldSplit LaplaceOrig requires funcType Laplace");
+  if (p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG && !(p.tol > 0 && p.tol < 1))
+    return fail(h, NPME_EINVAL, "tol must be in (0, 1)");
+  if (p.EwaldSplit == NPME_SPLIT_DERIVMATCH && (p.nDeriv < 2 || p.nDeriv > npme::kMaxDeriv))
+    return fail(h, NPME_EINVAL, "nDeriv must be in [2, 15]");
+  if (p.BnOrder < 4 || p.BnOrder > 12 || (p.BnOrder & 1))
+    return fail(h, NPME_EINVAL, "BnOrder must be even and in [4, 12]");
+  const long Ns[3] = {p.N1, p.N2, p.N3};
+  for (int d = 0; d < 3; d++) {
+    if (Ns[d] % 4 != 0 || Ns[d] < 4)  // src/RecSumSupportFunctions.cpp:42-58
+      return fail(h, NPME_EINVAL, "N1, N2, N3 must be positive multiples of 4");
+    if (p.BnOrder >= Ns[d] / 4)  // src/RecSumSupportFunctions.cpp:61-79
+      return fail(h, NPME_EINVAL, "BnOrder must be < N/4 on every axis");
+    if (Ns[d] > 2048) return fail(h, NPME_EINVAL, "N1, N2, N3 must be <= 2048");
+  }
+  if (p.nNeigh < 1 || p.nNeigh > 4) return fail(h, NPME_EINVAL, "nNeigh must be in [1, 4]");
+  if (p.precision != NPME_PREC_FP32 && p.precision != NPME_PREC_FP64)
+    return fail(h, NPME_EINVAL, "unknown precision");
+  return NPME_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void npme_gpu_default_params(npme_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->funcType = NPME_FUNC_LAPLACE;
+  p->EwaldSplit = NPME_SPLIT_DERIVMATCH;
+  p->alpha = -1.0;
+  p->Rdir = 0.0;      // required
+  p->tol = 1.0e-6;    // src/Constant.h:50
+  p->BnOrder = 8;     // src/Constant.h:49
+  p->nDeriv = 8;      // src/Interface.cpp:452-455 for BnOrder 8
+  p->n1 = p->n2 = p->n3 = 16;
+  p->a1 = p->a2 = p->a3 = 4.0;    // src/Interface.cpp:97-99
+  p->del1 = p->del2 = p->del3 = -1.0;  // < 0 means Rdir (src/Interface.cpp:243-245)
+  p->nNeigh = 2;        // src/Constant.h:52
+  p->nCellClust1D = 3;  // src/Constant.h:53
+  p->useCompactF = 1;
+  p->precision = NPME_PREC_FP32;
+  p->device = 0;
+}
+
+int npme_gpu_create(const npme_params *p, npme_handle **out) {
+  if (!p || !out) return fail(nullptr, NPME_EINVAL, "null argument");
+  *out = nullptr;
+  npme_handle *h = new (std::nothrow) npme_handle;
+  if (!h) return fail(nullptr, NPME_ENOMEM, "host allocation failed");
+  h->p = *p;
+  if (h->p.del1 <= 0) h->p.del1 = h->p.Rdir;
+  if (h->p.del2 <= 0) h->p.del2 = h->p.Rdir;
+  if (h->p.del3 <= 0) h->p.del3 = h->p.Rdir;
+  int rc = check_params(h, h->p);
+  if (rc) {
+    set_global_err(h->err);
+    delete h;
+    return rc;
+  }
+  h->device = p->device;
+  h->complex_kernel = p->funcType == NPME_FUNC_HELMHOLTZ;
+  h->fp32 = p->precision == NPME_PREC_FP32;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+  for (int i = 0; i < 10 && e == cudaSuccess; i++) e = cudaEventCreate(&h->timing.ev[i]);
+  if (e != cudaSuccess) {
+    set_global_err(std::string("CUDA initialisation failed: ") + cudaGetErrorString(e));
+    delete h;
+    return NPME_ECUDA;
+  }
+  // coefficients of the splitting (host FP64)
+  memset(h->a_r, 0, sizeof(h->a_r));
+  memset(h->a_i, 0, sizeof(h->a_i));
+  memset(h->b_r, 0, sizeof(h->b_r));
+  memset(h->b_i, 0, sizeof(h->b_i));
+  if (h->p.EwaldSplit == NPME_SPLIT_DERIVMATCH) {
+    std::complex<double> a[32], b[32];
+    dm_coefficients(h->p, a, b);
+    for (int i = 0; i <= h->p.nDeriv; i++) {
+      h->a_r[i] = a[i].real(), h->a_i[i] = a[i].imag();
+      h->b_r[i] = b[i].real(), h->b_i[i] = b[i].imag();
+    }
+    // f_LR(0) = a[0] (src/Interface.cpp:1946-1952)
+    h->fself_r = h->a_r[0];
+    h->fself_i = h->a_i[0];
+  } else {
+    h->beta = orig_beta(h->p.Rdir, h->p.tol);
+    if (h->beta <= 0) {
+      set_global_err("original-Ewald beta did not converge");
+      npme_gpu_destroy(h);
+      return NPME_EINVAL;
+    }
+    h->fself_r = 2.0 * h->beta / std::sqrt(M_PI);  // beta erf(beta r)/(beta r) at r = 0
+    h->fself_i = 0;
+  }
+  *out = h;
+  return NPME_OK;
+}
+
+int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!coord && n) return fail(h, NPME_EINVAL, "null coord");
+  if (n == 0) return fail(h, NPME_EINVAL, "nCharge must be > 0");
+  if (n >= (size_t)1 << 31) return fail(h, NPME_EINVAL, "nCharge must be < 2^31");
+  CK(cudaSetDevice(h->device));
+  release(h);
+  h->n = n;
+  const npme_params &p = h->p;
+  // box (src/RecSumSupportFunctions.cpp:182-201, 276-296)
+  double mx[3] = {-1e300, -1e300, -1e300}, mn[3] = {1e300, 1e300, 1e300};
+  for (size_t i = 0; i < n; i++)
+    for (int d = 0; d < 3; d++) {
+      const double x = coord[3 * i + d];
+      if (!std::isfinite(x)) return fail(h, NPME_EINVAL, "non-finite coordinate");
+      mx[d] = std::max(mx[d], x);
+      mn[d] = std::min(mn[d], x);
+    }
+  const long Ns[3] = {p.N1, p.N2, p.N3};
+  const double dels[3] = {p.del1, p.del2, p.del3};
+  for (int d = 0; d < 3; d++) {
+    const double X0 = mx[d] - mn[d], R0 = 0.5 * (mx[d] + mn[d]);
+    const double X = min_x_compact(X0, dels[d], p.BnOrder, Ns[d]);
+    h->box[d] = X;
+    h->box[3 + d] = R0 + 0.5 * (X0 - X);
+    h->box[6 + d] = 2 * (X + dels[d]);
+    h->grid.N[d] = Ns[d];
+    h->grid.H[d] = Ns[d] / 2;
+    h->grid.nb[d] = (Ns[d] / 2 + npme::kBrick - 1) / npme::kBrick;
+  }
+  h->grid.order = p.BnOrder;
+  // cells of edge >= Rdir / nNeigh
+  const double target = p.Rdir / p.nNeigh;
+  long ncells = 1;
+  for (int d = 0; d < 3; d++) {
+    const double ext = mx[d] - mn[d];
+    int nc = (int)std::floor(ext / target);
+    nc = std::max(1, std::min(nc, 1 << 16));
+    h->cells.nc[d] = nc;
+    h->cells.edge[d] = (nc == 1) ? std::max(ext, target) : ext / nc;
+    h->cells.origin[d] = mn[d];
+    ncells *= nc;
+  }
+  if (ncells > (1L << 30)) return fail(h, NPME_EINVAL, "too many direct-sum cells");
+  h->cells.reach = p.nNeigh;
+  int rc = h->fp32 ? upload_points<float>(h, coord) : upload_points<double>(h, coord);
+  if (rc) {
+    release(h);
+    return rc;
+  }
+  if ((rc = make_plans(h))) {
+    release(h);
+    return rc;
+  }
+  if ((rc = npme::build_kernel_transform(h))) {
+    release(h);
+    return rc;
+  }
+  h->ready = true;
+  return NPME_OK;
+}
+
+static void tmark(npme_handle *h, int i, cudaStream_t s) {
+  if (h->timing.enabled) cudaEventRecord(h->timing.ev[i], s);
+}
+
+int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, void *stream) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!h->ready) return fail(h, NPME_ESTATE, "calcv before setup");
+  if (!d_V || !d_charge) return fail(h, NPME_EINVAL, "null buffer");
+  CK(cudaSetDevice(h->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  h->launches = 0;
+  const size_t gbytes = (h->fp32 ? 4 : 8) * (h->complex_kernel ? 2 : 1) *
+                        (size_t)h->grid.N[0] * h->grid.N[1] * h->grid.N[2];
+  tmark(h, 0, s);
+  npme::launch_gather_charges(h, d_charge, s);
+  tmark(h, 1, s);
+  // the direct sum runs on stream2, overlapped with the reciprocal sum
+  CK(cudaEventRecord(h->ev_fork, s));
+  CK(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
+  tmark(h, 8, h->stream2);
+  npme::launch_direct(h, d_V, h->stream2);
+  tmark(h, 9, h->stream2);
+  CK(cudaEventRecord(h->ev_join, h->stream2));
+  CK(cudaMemsetAsync(h->d_grid, 0, gbytes, s));
+  npme::launch_spread(h, s);
+  tmark(h, 2, s);
+  CKFFT(cufftSetStream(h->plan_fwd, s));
+  if (h->plan_inv != h->plan_fwd) CKFFT(cufftSetStream(h->plan_inv, s));
+  if (h->complex_kernel) {
+    if (h->fp32)
+      CKFFT(cufftExecC2C(h->plan_fwd, (cufftComplex *)h->d_grid, (cufftComplex *)h->d_grid,
+                         CUFFT_FORWARD));
+    else
+      CKFFT(cufftExecZ2Z(h->plan_fwd, (cufftDoubleComplex *)h->d_grid,
+                         (cufftDoubleComplex *)h->d_grid, CUFFT_FORWARD));
+  } else {
+    if (h->fp32)
+      CKFFT(cufftExecR2C(h->plan_fwd, (cufftReal *)h->d_grid, (cufftComplex *)h->d_kgrid));
+    else
+      CKFFT(cufftExecD2Z(h->plan_fwd, (cufftDoubleReal *)h->d_grid,
+                         (cufftDoubleComplex *)h->d_kgrid));
+  }
+  tmark(h, 3, s);
+  npme::launch_multiply(h, s);
+  tmark(h, 4, s);
+  if (h->complex_kernel) {
+    if (h->fp32)
+      CKFFT(cufftExecC2C(h->plan_inv, (cufftComplex *)h->d_grid, (cufftComplex *)h->d_grid,
+                         CUFFT_INVERSE));
+    else
+      CKFFT(cufftExecZ2Z(h->plan_inv, (cufftDoubleComplex *)h->d_grid,
+                         (cufftDoubleComplex *)h->d_grid, CUFFT_INVERSE));
+  } else {
+    if (h->fp32)
+      CKFFT(cufftExecC2R(h->plan_inv, (cufftComplex *)h->d_kgrid, (cufftReal *)h->d_grid));
+    else
+      CKFFT(cufftExecZ2D(h->plan_inv, (cufftDoubleComplex *)h->d_kgrid,
+                         (cufftDoubleReal *)h->d_grid));
+  }
+  tmark(h, 5, s);
+  CK(cudaStreamWaitEvent(s, h->ev_join, 0));
+  tmark(h, 6, s);
+  npme::launch_interp(h, d_V, s);
+  tmark(h, 7, s);
+  h->timing_pending = h->timing.enabled;
+  CK(cudaGetLastError());
+  return NPME_OK;
+}
+
+// Reads the stage events of the last timed calcv (waits for its last event).
+static void collect_timing(npme_handle *h) {
+  if (!h->timing.enabled || !h->timing_pending) return;
+  h->timing_pending = false;
+  cudaEvent_t *e = h->timing.ev;
+  if (cudaEventSynchronize(e[7]) != cudaSuccess || cudaEventSynchronize(e[9]) != cudaSuccess)
+    return;
+  float ms;
+  // gather, spread, fft, multiply, ifft, direct, interp, total
+  cudaEventElapsedTime(&ms, e[0], e[1]); h->stage_ms[0] = ms;
+  cudaEventElapsedTime(&ms, e[1], e[2]); h->stage_ms[1] = ms;
+  cudaEventElapsedTime(&ms, e[2], e[3]); h->stage_ms[2] = ms;
+  cudaEventElapsedTime(&ms, e[3], e[4]); h->stage_ms[3] = ms;
+  cudaEventElapsedTime(&ms, e[4], e[5]); h->stage_ms[4] = ms;
+  cudaEventElapsedTime(&ms, e[8], e[9]); h->stage_ms[5] = ms;
+  cudaEventElapsedTime(&ms, e[6], e[7]); h->stage_ms[6] = ms;
+  cudaEventElapsedTime(&ms, e[0], e[7]); h->stage_ms[7] = ms;
+}
+
+static int calcv_host(npme_handle *h, double *V, size_t n, const double *charge, bool cplx) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!h->ready) return fail(h, NPME_ESTATE, "calcv before setup");
+  if (cplx != h->complex_kernel)
+    return fail(h, NPME_EINVAL, cplx ? "complex call on a real kernel"
+                                     : "real call on a complex kernel");
+  if (n != h->n) return fail(h, NPME_EINVAL, "nCharge differs from setup");
+  if (!V || !charge) return fail(h, NPME_EINVAL, "null buffer");
+  CK(cudaSetDevice(h->device));
+  const int C = cplx ? 2 : 1;
+  CK(cudaMemcpyAsync(h->d_q_in, charge, sizeof(double) * C * n, cudaMemcpyHostToDevice,
+                     h->stream));
+  int rc = npme_gpu_calcv_device(h, h->d_V, h->d_q_in, h->stream);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(V, h->d_V, sizeof(double) * 4 * C * n, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  collect_timing(h);
+  return NPME_OK;
+}
+
+int npme_gpu_calcv_real(npme_handle *h, double *V, size_t n, const double *charge,
+                        const double *coord) {
+  (void)coord;
+  return calcv_host(h, V, n, charge, false);
+}
+
+int npme_gpu_calcv_complex(npme_handle *h, double *V, size_t n, const double *charge,
+                           const double *coord) {
+  (void)coord;
+  return calcv_host(h, V, n, charge, true);
+}
+
+static int exact_host(npme_handle *h, double *V, size_t n, const double *charge, bool cplx) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!h->ready) return fail(h, NPME_ESTATE, "calcv_exact before setup");
+  if (cplx != h->complex_kernel) return fail(h, NPME_EINVAL, "charge type mismatch");
+  if (n != h->n) return fail(h, NPME_EINVAL, "nCharge differs from setup");
+  if (!V || !charge) return fail(h, NPME_EINVAL, "null buffer");
+  CK(cudaSetDevice(h->device));
+  const int C = cplx ? 2 : 1;
+  CK(cudaMemcpyAsync(h->d_q_in, charge, sizeof(double) * C * n, cudaMemcpyHostToDevice,
+                     h->stream));
+  h->launches = 0;
+  npme::launch_exact(h, h->d_q_in, h->d_V, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(V, h->d_V, sizeof(double) * 4 * C * n, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return NPME_OK;
+}
+
+int npme_gpu_calcv_exact_real(npme_handle *h, double *V, size_t n, const double *charge,
+                              const double *coord) {
+  (void)coord;
+  return exact_host(h, V, n, charge, false);
+}
+
+int npme_gpu_calcv_exact_complex(npme_handle *h, double *V, size_t n, const double *charge,
+                                 const double *coord) {
+  (void)coord;
+  return exact_host(h, V, n, charge, true);
+}
+
+int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs) {
+  if (!h || !unordered_pairs) return fail(h, NPME_EINVAL, "null argument");
+  if (!h->ready) return fail(h, NPME_ESTATE, "count_pairs before setup");
+  CK(cudaSetDevice(h->device));
+  unsigned long long *d_count = nullptr;
+  CK(cudaMalloc(&d_count, sizeof(unsigned long long)));
+  cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), h->stream);
+  npme::launch_count_pairs(h, d_count, h->stream);
+  unsigned long long ordered = 0;
+  cudaError_t e = cudaMemcpyAsync(&ordered, d_count, sizeof(ordered), cudaMemcpyDeviceToHost,
+                                  h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_count);
+  if (e != cudaSuccess) return fail(h, NPME_ECUDA, cudaGetErrorString(e));
+  *unordered_pairs = ordered / 2;
+  return NPME_OK;
+}
+
+int npme_gpu_set_timing(npme_handle *h, int enable) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  h->timing.enabled = enable != 0;
+  return NPME_OK;
+}
+
+int npme_gpu_get_info(const npme_handle *hc, npme_info *info) {
+  if (!hc || !info) return fail(nullptr, NPME_EINVAL, "null argument");
+  // the stage-time cache is filled lazily: reading it is logically const
+  npme_handle *h = const_cast<npme_handle *>(hc);
+  collect_timing(h);
+  memset(info, 0, sizeof(*info));
+  info->nCharge = h->n;
+  info->X = h->box[0], info->Y = h->box[1], info->Z = h->box[2];
+  for (int d = 0; d < 3; d++) info->R[d] = h->box[3 + d], info->L[d] = h->box[6 + d];
+  info->fself_r = h->fself_r, info->fself_i = h->fself_i;
+  for (int i = 0; i < 32; i++) info->dm_a_r[i] = h->a_r[i], info->dm_a_i[i] = h->a_i[i];
+  info->nDeriv = h->p.nDeriv;
+  info->nCells = (long)h->cells.nc[0] * h->cells.nc[1] * h->cells.nc[2];
+  info->nBricks = h->n_bricks;
+  info->nNonEmptyBricks = h->n_nonempty;
+  info->deviceBytes = h->dev_bytes;
+  for (int i = 0; i < 8; i++) info->stage_ms[i] = h->stage_ms[i];
+  info->launches = h->launches;
+  return NPME_OK;
+}
+
+int npme_gpu_last_error(const npme_handle *h, char *buf, size_t len) {
+  if (!buf || len == 0) return NPME_EINVAL;
+  std::string s;
+  if (h) s = h->err;
+  else {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    s = g_err;
+  }
+  strncpy(buf, s.c_str(), len - 1);
+  buf[len - 1] = 0;
+  return NPME_OK;
+}
+
+int npme_gpu_destroy(npme_handle *h) {
+  if (!h) return NPME_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->stream2) cudaStreamSynchronize(h->stream2);
+  release(h);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->stream2) cudaStreamDestroy(h->stream2);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  for (int i = 0; i < 10; i++)
+    if (h->timing.ev[i]) cudaEventDestroy(h->timing.ev[i]);
+  delete h;
+  return NPME_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,629 @@
+// Reciprocal sum on the B200: kernel transform (set-up), charge spreading,
+// Fourier-space multiply and potential interpolation.  The FFTs themselves
+// are cuFFT calls issued from npme_gpu.cu.
+//
+// Grid convention: the charge octant of the reference's compact grid
+// (m in [-N/4, N/4), src/RecSumSupportFunctions.h:100-113) is stored at grid
+// index g = m + N/4 in [0, N/2) of a zero-padded N1 x N2 x N3 box.  The
+// convolution is cyclic on the full box and both input and output are
+// shifted by the same N/4, so theta on the octant equals the reference's
+// theta (src/RecSumV.cpp:766-840) without its 8 even/odd half transforms.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "internal.h"
+
+namespace npme {
+
+// ---------------------------------------------------------------------------
+// Kernel transform (FP64): sample the smooth kernel f_LR on the (N/2+1)^3
+// octant with the 8-image Fourier-extension window (src/RecSumGrid.cpp:45-162,
+// 388-424), transform each axis by the even-extension DFT (src/RecSumGrid.cpp:
+// 470-582, a DCT-I), then fold in lambda^2 and 1/(N1 N2 N3)
+// (src/RecSumV.cpp:639-707).
+
+struct LRKernel {
+  int func, split, nder;
+  double R2, alpha, beta, k0r, k0i;
+  double ar[32], ai[32];  // unscaled a_n (coefficients of r^(2n))
+};
+
+__device__ double2 lr_eval(const LRKernel &k, double r2) {
+  if (k.split == 1) {  // beta erf(beta r)/(beta r)
+    const double x = sqrt(r2) * k.beta;
+    double v;
+    if (x < 1e-3) {
+      const double x2 = x * x;
+      v = 1.1283791670955126 * (1.0 - x2 / 3.0 + x2 * x2 / 10.0);
+    } else {
+      v = erf(x) / x;
+    }
+    return make_double2(k.beta * v, 0.0);
+  }
+  if (r2 > k.R2) {
+    const double r = sqrt(r2);
+    if (k.func == 0) return make_double2(1.0 / r, 0.0);
+    if (k.func == 1) return make_double2(pow(r2, 0.5 * k.alpha), 0.0);
+    double s, c;
+    sincos(k.k0r * r, &s, &c);
+    const double d = exp(-k.k0i * r) / r;
+    return make_double2(c * d, s * d);
+  }
+  double pr = k.ar[k.nder], pi = k.ai[k.nder];
+  for (int n = k.nder - 1; n >= 0; n--) {
+    pr = fma(pr, r2, k.ar[n]);
+    pi = fma(pi, r2, k.ai[n]);
+  }
+  return make_double2(pr, pi);
+}
+
+__global__ void sample_fhat_kernel(LRKernel k, int M1, int M2, int M3,
+                                   const double *__restrict__ ax,  // 4*M per axis: x1,x2,T1,T2
+                                   const double *__restrict__ ay,
+                                   const double *__restrict__ az, double2 *out) {
+  const long total = (long)M1 * M2 * M3;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
+    double sr = 0, si = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int s1 = c >> 2, s2 = (c >> 1) & 1, s3 = c & 1;
+      const double x = ax[s1 * M1 + i1], y = ay[s2 * M2 + i2], z = az[s3 * M3 + i3];
+      const double t = ax[(2 + s1) * M1 + i1] * ay[(2 + s2) * M2 + i2] *
+                       az[(2 + s3) * M3 + i3];
+      if (t == 0.0) continue;
+      const double2 f = lr_eval(k, x * x + y * y + z * z);
+      sr += t * f.x;
+      si += t * f.y;
+    }
+    out[idx] = make_double2(sr, si);
+  }
+}
+
+// out[k] = f[0] + (-1)^k f[M-1] + 2 sum_{j=1}^{M-2} f[j] cos(2 pi j k / N)
+// along axis `ax` of an M1 x M2 x M3 array.
+__global__ void dct1_axis_kernel(const double2 *__restrict__ in, double2 *__restrict__ out,
+                                 int M1, int M2, int M3, int ax, int N,
+                                 const double *__restrict__ cosN) {
+  const long total = (long)M1 * M2 * M3;
+  const int M = ax == 0 ? M1 : (ax == 1 ? M2 : M3);
+  const long stride = ax == 0 ? (long)M2 * M3 : (ax == 1 ? M3 : 1);
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
+    const int k = ax == 0 ? i1 : (ax == 1 ? i2 : i3);
+    const long base = idx - (long)k * stride;
+    const double2 f0 = in[base], fl = in[base + (long)(M - 1) * stride];
+    const double sg = (k & 1) ? -1.0 : 1.0;
+    double sr = f0.x + sg * fl.x, si = f0.y + sg * fl.y;
+    int m = k;  // (j * k) mod N, advanced incrementally
+    for (int j = 1; j < M - 1; j++) {
+      const double c = 2.0 * cosN[m];
+      const double2 f = in[base + (long)j * stride];
+      sr = fma(c, f.x, sr);
+      si = fma(c, f.y, si);
+      m += k;
+      if (m >= N) m -= N;
+    }
+    out[idx] = make_double2(sr, si);
+  }
+}
+
+template <typename T, bool CPLX>
+__global__ void scale_fhat_kernel(const double2 *__restrict__ F, int M1, int M2, int M3,
+                                  const double *__restrict__ l1, const double *__restrict__ l2,
+                                  const double *__restrict__ l3, double inv_vol, T *G) {
+  const long total = (long)M1 * M2 * M3;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
+    const double s = l1[i1] * l2[i2] * l3[i3] * inv_vol;
+    if (CPLX) {
+      G[2 * idx] = (T)(F[idx].x * s);
+      G[2 * idx + 1] = (T)(F[idx].y * s);
+    } else {
+      G[idx] = (T)(F[idx].x * s);
+    }
+  }
+}
+
+// Host B-spline (same recurrence as the device one) for lambda^2.
+static double bspline_host(int n, double w) {
+  if (w < 0.0 || w >= (double)n) return 0.0;
+  const int i0 = (int)std::floor(w);
+  const double u = w - i0;
+  double c[64];
+  c[0] = 1.0;
+  for (int j = 1; j < n; j++)
+    for (int k = j; k >= 0; k--) {
+      const double x = u + k;
+      const double left = (k <= j - 1) ? c[k] : 0.0;
+      const double right = (k >= 1) ? c[k - 1] : 0.0;
+      c[k] = (x * left + ((double)(j + 1) - x) * right) / (double)j;
+    }
+  return c[i0];
+}
+
+// |1/sum_p B_n(p) exp(-2 pi i k p / N)|^2 for k = 0..N/2 (src/RecSumV.cpp:565-581)
+static void lambda2_host(long N, int order, std::vector<double> &out) {
+  out.resize(N / 2 + 1);
+  for (long k = 0; k <= N / 2; k++) {
+    const double z = (double)k / (double)N;
+    double dr = 0, di = 0;
+    for (int p = 0; p <= order; p++) {
+      const double b = bspline_host(order, p);
+      dr += b * std::cos(2.0 * M_PI * z * p);
+      di -= b * std::sin(2.0 * M_PI * z * p);
+    }
+    out[k] = 1.0 / (dr * dr + di * di);
+  }
+}
+
+static double hramp(double x, double a) {
+  const double erf_max = 6.0;
+  if (x < -1.0) return 0.0;
+  if (x > 1.0) return 1.0;
+  const double z = erf_max / a, xMax = z / std::sqrt(1.0 + z * z);
+  if (x >= xMax) return 1.0;
+  if (x <= -xMax) return 0.0;
+  return 0.5 * (1.0 + std::erf(a * x / std::sqrt(1.0 - x * x)));
+}
+
+// Top-hat window of half width X falling to 0 at Xmax (src/RecSumGrid.cpp:1124-1170)
+static double tsmooth(double x, double X, double Xmax, double a) {
+  const double del = (Xmax - X) * 0.5;
+  if (x < -X) return hramp((x + X + del) / del, a);
+  if (x <= X) return 1.0;
+  return hramp((-x + X + del) / del, a);
+}
+
+// x1, x2, T1, T2 for one axis (src/RecSumGrid.cpp:1181-1212)
+static void window_axis(long N, double X, double del, double a, std::vector<double> &v) {
+  const long M = N / 2 + 1;
+  const double Xmax = X + del, h = 2 * Xmax / N;
+  v.assign(4 * M, 0.0);
+  for (long i = 0; i < M; i++) {
+    const double x1 = i * h;
+    double x2, T1, T2;
+    if (x1 > X) {
+      T1 = tsmooth(x1, X, 2 * Xmax - X, a);
+      x2 = x1 - 2 * Xmax;
+      T2 = tsmooth(x2, X, 2 * Xmax - X, a);
+    } else if (x1 > -X) {
+      T1 = 1.0, x2 = 1.0, T2 = 0.0;
+    } else {
+      T1 = tsmooth(x1, X, 2 * Xmax - X, a);
+      x2 = x1 + 2 * Xmax;
+      T2 = tsmooth(x2, X, 2 * Xmax - X, a);
+    }
+    v[i] = x1, v[M + i] = x2, v[2 * M + i] = T1, v[3 * M + i] = T2;
+  }
+}
+
+#define NPME_CK(call)                                          \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) {                                   \
+      h->err = std::string(#call) + ": " + cudaGetErrorString(e_); \
+      return NPME_ECUDA;                                       \
+    }                                                          \
+  } while (0)
+
+int build_kernel_transform(npme_handle *h) {
+  const long *N = h->grid.N;
+  const int M1 = N[0] / 2 + 1, M2 = N[1] / 2 + 1, M3 = N[2] / 2 + 1;
+  const long MT = (long)M1 * M2 * M3;
+  const double dels[3] = {h->p.del1, h->p.del2, h->p.del3};
+  const double as[3] = {h->p.a1, h->p.a2, h->p.a3};
+  std::vector<double> ax[3], lam[3];
+  for (int d = 0; d < 3; d++) {
+    window_axis(N[d], h->box[d], dels[d], as[d], ax[d]);
+    lambda2_host(N[d], h->grid.order, lam[d]);
+  }
+  LRKernel k{};
+  k.func = h->p.funcType;
+  k.split = h->p.EwaldSplit;
+  k.nder = h->p.nDeriv;
+  k.R2 = h->p.Rdir * h->p.Rdir;
+  k.alpha = h->p.alpha;
+  k.beta = h->beta;
+  k.k0r = h->p.k0_r;
+  k.k0i = h->p.k0_i;
+  for (int i = 0; i <= k.nder && i < 32; i++) k.ar[i] = h->a_r[i], k.ai[i] = h->a_i[i];
+
+  const long maxN = std::max(N[0], std::max(N[1], N[2]));
+  double *d_ax[3] = {nullptr, nullptr, nullptr}, *d_l[3] = {nullptr, nullptr, nullptr};
+  double *d_cos = nullptr;
+  double2 *d_F = nullptr, *d_F2 = nullptr;
+  int rc = NPME_OK;
+  auto cleanup = [&]() {
+    for (int d = 0; d < 3; d++) cudaFree(d_ax[d]), cudaFree(d_l[d]);
+    cudaFree(d_cos);
+    cudaFree(d_F);
+    cudaFree(d_F2);
+  };
+  do {
+    bool fail = false;
+    for (int d = 0; d < 3 && !fail; d++) {
+      fail |= cudaMalloc(&d_ax[d], sizeof(double) * ax[d].size()) != cudaSuccess;
+      fail |= cudaMalloc(&d_l[d], sizeof(double) * lam[d].size()) != cudaSuccess;
+    }
+    fail |= cudaMalloc(&d_cos, sizeof(double) * maxN) != cudaSuccess;
+    fail |= cudaMalloc(&d_F, sizeof(double2) * MT) != cudaSuccess;
+    fail |= cudaMalloc(&d_F2, sizeof(double2) * MT) != cudaSuccess;
+    if (fail) {
+      h->err = "cudaMalloc failed while building the kernel transform";
+      rc = NPME_ENOMEM;
+      break;
+    }
+    for (int d = 0; d < 3; d++) {
+      cudaMemcpy(d_ax[d], ax[d].data(), sizeof(double) * ax[d].size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(d_l[d], lam[d].data(), sizeof(double) * lam[d].size(), cudaMemcpyHostToDevice);
+    }
+    const int threads = 256, blocks = 148 * 8;
+    sample_fhat_kernel<<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, d_ax[0], d_ax[1],
+                                                          d_ax[2], d_F);
+    double2 *src = d_F, *dst = d_F2;
+    for (int d = 0; d < 3; d++) {
+      std::vector<double> cs(N[d]);
+      for (long m = 0; m < N[d]; m++) cs[m] = std::cos(2.0 * M_PI * (double)m / (double)N[d]);
+      cudaMemcpyAsync(d_cos, cs.data(), sizeof(double) * N[d], cudaMemcpyHostToDevice, h->stream);
+      dct1_axis_kernel<<<blocks, threads, 0, h->stream>>>(src, dst, M1, M2, M3, d, (int)N[d], d_cos);
+      cudaStreamSynchronize(h->stream);  // cs is reused for the next axis
+      std::swap(src, dst);
+    }
+    const double inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);
+    if (h->fp32) {
+      if (h->complex_kernel)
+        scale_fhat_kernel<float, true><<<blocks, threads, 0, h->stream>>>(
+            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (float *)h->d_G);
+      else
+        scale_fhat_kernel<float, false><<<blocks, threads, 0, h->stream>>>(
+            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (float *)h->d_G);
+    } else {
+      if (h->complex_kernel)
+        scale_fhat_kernel<double, true><<<blocks, threads, 0, h->stream>>>(
+            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (double *)h->d_G);
+      else
+        scale_fhat_kernel<double, false><<<blocks, threads, 0, h->stream>>>(
+            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (double *)h->d_G);
+    }
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      h->err = std::string("kernel transform: ") + cudaGetErrorString(e);
+      rc = NPME_ECUDA;
+    }
+  } while (0);
+  cleanup();
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Per-call charge gather into brick order (spread/interp) and cell order
+// (direct sum), converted to the bulk precision.
+
+template <typename T, bool CPLX>
+__global__ void gather_kernel(const double *__restrict__ q, const BrickPoint<T> *__restrict__ bp,
+                              const uint32_t *__restrict__ cperm, T *__restrict__ qb,
+                              T *__restrict__ qc, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const uint32_t ob = bp[i].orig, oc = cperm[i];
+    if (CPLX) {
+      qb[2 * i] = (T)q[2 * (long)ob];
+      qb[2 * i + 1] = (T)q[2 * (long)ob + 1];
+      qc[2 * i] = (T)q[2 * (long)oc];
+      qc[2 * i + 1] = (T)q[2 * (long)oc + 1];
+    } else {
+      qb[i] = (T)q[ob];
+      qc[i] = (T)q[oc];
+    }
+  }
+}
+
+void launch_gather_charges(npme_handle *h, const double *d_q, cudaStream_t s) {
+  const int threads = 256;
+  const int blocks = (int)std::min<long>((h->n + threads - 1) / threads, 148 * 16);
+  if (h->fp32) {
+    if (h->complex_kernel)
+      gather_kernel<float, true><<<blocks, threads, 0, s>>>(
+          d_q, (const BrickPoint<float> *)h->d_bpts, h->d_cperm, (float *)h->d_qb,
+          (float *)h->d_qc, (long)h->n);
+    else
+      gather_kernel<float, false><<<blocks, threads, 0, s>>>(
+          d_q, (const BrickPoint<float> *)h->d_bpts, h->d_cperm, (float *)h->d_qb,
+          (float *)h->d_qc, (long)h->n);
+  } else {
+    if (h->complex_kernel)
+      gather_kernel<double, true><<<blocks, threads, 0, s>>>(
+          d_q, (const BrickPoint<double> *)h->d_bpts, h->d_cperm, (double *)h->d_qb,
+          (double *)h->d_qc, (long)h->n);
+    else
+      gather_kernel<double, false><<<blocks, threads, 0, s>>>(
+          d_q, (const BrickPoint<double> *)h->d_bpts, h->d_cperm, (double *)h->d_qb,
+          (double *)h->d_qc, (long)h->n);
+  }
+  h->launches++;
+}
+
+// ---------------------------------------------------------------------------
+// Spread (src/RecSumQ.cpp:184-314): Q[g] += q B1 B2 B3.  One CTA per
+// non-empty brick of kBrick^3 stencil origins.  The CTA accumulates its
+// points' stencils into a shared-memory tile of (kBrick + P - 1)^3 grid
+// points with shared atomics, then adds the tile to the global grid (global
+// atomics only where tiles of neighbouring bricks overlap: one add per tile
+// point instead of one per stencil point).  Complex charges are spread
+// without conjugation; with the cyclic convolution used here that gives the
+// reference's theta for conj(q) spreading (src/RecSumQ.cpp:337) because the
+// reference conjugates twice (src/RecSumV.cpp:672).
+
+template <typename T, int P, bool CPLX>
+__global__ void __launch_bounds__(256) spread_kernel(
+    const int *__restrict__ brick_list, const int *__restrict__ brick_start,
+    const BrickPoint<T> *__restrict__ bp, const T *__restrict__ q, T *__restrict__ grid,
+    int nb2, int nb3, long N1, long N2, long N3) {
+  constexpr int TL = kBrick + P - 1;
+  constexpr int TV = TL * TL * TL;
+  constexpr int C = CPLX ? 2 : 1;
+  extern __shared__ unsigned char smem_raw[];
+  T *tile = reinterpret_cast<T *>(smem_raw);
+  const int brick = brick_list[blockIdx.x];
+  const int b3 = brick % nb3, b2 = (brick / nb3) % nb2, b1 = brick / (nb3 * nb2);
+  for (int t = threadIdx.x; t < TV * C; t += blockDim.x) tile[t] = T(0);
+  __syncthreads();
+  const int beg = brick_start[brick], end = brick_start[brick + 1];
+  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const BrickPoint<T> pt = bp[i];
+    T w1[P], w2[P], w3[P], dummy[P];
+    bspline_weights<T, P, false>(pt.u[0], w1, dummy);
+    bspline_weights<T, P, false>(pt.u[1], w2, dummy);
+    bspline_weights<T, P, false>(pt.u[2], w3, dummy);
+    const int l1 = (int)(pt.g0 >> 20) - b1 * kBrick;
+    const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
+    const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
+    T qr = q[C * (long)i], qi = CPLX ? q[2 * (long)i + 1] : T(0);
+#pragma unroll
+    for (int t1 = 0; t1 < P; t1++) {
+#pragma unroll
+      for (int t2 = 0; t2 < P; t2++) {
+        const T c12 = w1[t1] * w2[t2];
+        T *row = tile + C * (((l1 + t1) * TL + (l2 + t2)) * TL + l3);
+#pragma unroll
+        for (int t3 = 0; t3 < P; t3++) {
+          const T c = c12 * w3[t3];
+          atomicAdd(row + C * t3, c * qr);
+          if (CPLX) atomicAdd(row + C * t3 + 1, c * qi);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const long g1 = (long)b1 * kBrick, g2 = (long)b2 * kBrick, g3 = (long)b3 * kBrick;
+  for (int t = threadIdx.x; t < TV; t += blockDim.x) {
+    const int i3 = t % TL, i2 = (t / TL) % TL, i1 = t / (TL * TL);
+    if (g1 + i1 >= N1) continue;
+    if (g2 + i2 >= N2 || g3 + i3 >= N3) continue;  // beyond the box: always zero
+    const long gi = ((g1 + i1) * N2 + (g2 + i2)) * N3 + (g3 + i3);
+    if (CPLX) {
+      const T vr = tile[2 * t], vi = tile[2 * t + 1];
+      if (vr != T(0)) atomicAdd(grid + 2 * gi, vr);
+      if (vi != T(0)) atomicAdd(grid + 2 * gi + 1, vi);
+    } else {
+      const T v = tile[t];
+      if (v != T(0)) atomicAdd(grid + gi, v);
+    }
+  }
+}
+
+template <typename T, bool CPLX, int P>
+static void spread_dispatch(npme_handle *h, cudaStream_t s) {
+  constexpr int TL = kBrick + P - 1;
+  const size_t smem = sizeof(T) * TL * TL * TL * (CPLX ? 2 : 1);
+  auto kern = spread_kernel<T, P, CPLX>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<(unsigned)h->n_nonempty, 256, smem, s>>>(
+      h->d_brick_list, h->d_brick_start, (const BrickPoint<T> *)h->d_bpts,
+      (const T *)h->d_qb, (T *)h->d_grid, (int)h->grid.nb[1], (int)h->grid.nb[2],
+      h->grid.N[0], h->grid.N[1], h->grid.N[2]);
+}
+
+template <typename T, bool CPLX>
+static void spread_order(npme_handle *h, cudaStream_t s) {
+  switch (h->grid.order) {
+    case 4: spread_dispatch<T, CPLX, 4>(h, s); break;
+    case 6: spread_dispatch<T, CPLX, 6>(h, s); break;
+    case 8: spread_dispatch<T, CPLX, 8>(h, s); break;
+    case 10: spread_dispatch<T, CPLX, 10>(h, s); break;
+    case 12: spread_dispatch<T, CPLX, 12>(h, s); break;
+  }
+}
+
+void launch_spread(npme_handle *h, cudaStream_t s) {
+  if (h->n_nonempty == 0) return;
+  if (h->fp32) {
+    if (h->complex_kernel) spread_order<float, true>(h, s);
+    else spread_order<float, false>(h, s);
+  } else {
+    if (h->complex_kernel) spread_order<double, true>(h, s);
+    else spread_order<double, false>(h, s);
+  }
+  h->launches++;
+}
+
+// ---------------------------------------------------------------------------
+// Fourier-space multiply by the kernel transform G (compact octant storage,
+// |k| folding as in src/RecSumV.cpp:639-707).  Real kernels: R2C half
+// spectrum N1 x N2 x (N3/2+1), G real.  Complex kernels: full N^3 spectrum,
+// G complex.
+
+template <typename T>
+__global__ void multiply_real_kernel(typename Vec2<T>::type *__restrict__ X,
+                                     const T *__restrict__ G, long N1, long N2, long N3h,
+                                     int M2, int M3) {
+  const long total = N1 * N2 * N3h;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const long k3 = idx % N3h, k2 = (idx / N3h) % N2, k1 = idx / (N3h * N2);
+    const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
+    const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
+    const T g = __ldg(G + (f1 * M2 + f2) * M3 + k3);
+    typename Vec2<T>::type v = X[idx];
+    v.x *= g;
+    v.y *= g;
+    X[idx] = v;
+  }
+}
+
+template <typename T>
+__global__ void multiply_cplx_kernel(typename Vec2<T>::type *__restrict__ X,
+                                     const typename Vec2<T>::type *__restrict__ G, long N1,
+                                     long N2, long N3, int M2, int M3) {
+  const long total = N1 * N2 * N3;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const long k3 = idx % N3, k2 = (idx / N3) % N2, k1 = idx / (N3 * N2);
+    const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
+    const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
+    const long f3 = k3 <= N3 / 2 ? k3 : N3 - k3;
+    const typename Vec2<T>::type g = G[(f1 * M2 + f2) * M3 + f3];
+    typename Vec2<T>::type v = X[idx], o;
+    o.x = v.x * g.x - v.y * g.y;
+    o.y = v.x * g.y + v.y * g.x;
+    X[idx] = o;
+  }
+}
+
+void launch_multiply(npme_handle *h, cudaStream_t s) {
+  const long *N = h->grid.N;
+  const int M2 = N[1] / 2 + 1, M3 = N[2] / 2 + 1;
+  const int threads = 256, blocks = 148 * 16;
+  if (h->complex_kernel) {
+    if (h->fp32)
+      multiply_cplx_kernel<float><<<blocks, threads, 0, s>>>(
+          (float2 *)h->d_grid, (const float2 *)h->d_G, N[0], N[1], N[2], M2, M3);
+    else
+      multiply_cplx_kernel<double><<<blocks, threads, 0, s>>>(
+          (double2 *)h->d_grid, (const double2 *)h->d_G, N[0], N[1], N[2], M2, M3);
+  } else {
+    if (h->fp32)
+      multiply_real_kernel<float><<<blocks, threads, 0, s>>>(
+          (float2 *)h->d_kgrid, (const float *)h->d_G, N[0], N[1], N[2] / 2 + 1, M2, M3);
+    else
+      multiply_real_kernel<double><<<blocks, threads, 0, s>>>(
+          (double2 *)h->d_kgrid, (const double *)h->d_G, N[0], N[1], N[2] / 2 + 1, M2, M3);
+  }
+  h->launches++;
+}
+
+// ---------------------------------------------------------------------------
+// Interpolation (src/RecSumV.cpp:201-306, 308-434): V += sum theta B1 B2 B3,
+// dV/dx_d += (N_d / L_d) sum theta dB_d ..., real kernels keep the real part
+// (src/RecSumV.cpp:395-398).  One thread per point in brick order; V is
+// accumulated into the caller-order output, which already holds the direct
+// sum.
+
+template <typename T, int P, bool CPLX>
+__global__ void __launch_bounds__(256) interp_kernel(
+    const BrickPoint<T> *__restrict__ bp, const T *__restrict__ theta, double *__restrict__ V,
+    long n, long N2, long N3, T c1, T c2, T c3) {
+  constexpr int C = CPLX ? 2 : 1;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const BrickPoint<T> pt = bp[i];
+    T w1[P], w2[P], w3[P], d1[P], d2[P], d3[P];
+    bspline_weights<T, P, true>(pt.u[0], w1, d1);
+    bspline_weights<T, P, true>(pt.u[1], w2, d2);
+    bspline_weights<T, P, true>(pt.u[2], w3, d3);
+    const long g1 = pt.g0 >> 20, g2 = (pt.g0 >> 10) & 1023u, g3 = pt.g0 & 1023u;
+    T v[4] = {0, 0, 0, 0}, vi[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int t1 = 0; t1 < P; t1++) {
+#pragma unroll
+      for (int t2 = 0; t2 < P; t2++) {
+        const T *row = theta + C * (((g1 + t1) * N2 + (g2 + t2)) * N3 + g3);
+        T tb = 0, td = 0, tbi = 0, tdi = 0;
+#pragma unroll
+        for (int t3 = 0; t3 < P; t3++) {
+          const T th = __ldg(row + C * t3);
+          tb = fma(th, w3[t3], tb);
+          td = fma(th, d3[t3], td);
+          if (CPLX) {
+            const T thi = __ldg(row + C * t3 + 1);
+            tbi = fma(thi, w3[t3], tbi);
+            tdi = fma(thi, d3[t3], tdi);
+          }
+        }
+        const T A1 = w1[t1] * w2[t2], A2 = d1[t1] * w2[t2], A3 = w1[t1] * d2[t2];
+        v[0] = fma(A1, tb, v[0]);
+        v[1] = fma(A2, tb, v[1]);
+        v[2] = fma(A3, tb, v[2]);
+        v[3] = fma(A1, td, v[3]);
+        if (CPLX) {
+          vi[0] = fma(A1, tbi, vi[0]);
+          vi[1] = fma(A2, tbi, vi[1]);
+          vi[2] = fma(A3, tbi, vi[2]);
+          vi[3] = fma(A1, tdi, vi[3]);
+        }
+      }
+    }
+    const T sc[4] = {T(1), c1, c2, c3};
+    const long o = pt.orig;
+    if (CPLX) {
+      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        double2 a = Vo[m];
+        a.x += (double)(v[m] * sc[m]);
+        a.y += (double)(vi[m] * sc[m]);
+        Vo[m] = a;
+      }
+    } else {
+      double4 *Vo = reinterpret_cast<double4 *>(V) + o;
+      double4 a = *Vo;
+      a.x += (double)v[0];
+      a.y += (double)(v[1] * c1);
+      a.z += (double)(v[2] * c2);
+      a.w += (double)(v[3] * c3);
+      *Vo = a;
+    }
+  }
+}
+
+template <typename T, bool CPLX, int P>
+static void interp_dispatch(npme_handle *h, double *d_V, cudaStream_t s) {
+  const int threads = 256;
+  const int blocks = (int)std::min<long>((h->n + threads - 1) / threads, 148 * 32);
+  const double *L = h->box + 6;
+  interp_kernel<T, P, CPLX><<<blocks, threads, 0, s>>>(
+      (const BrickPoint<T> *)h->d_bpts, (const T *)h->d_grid, d_V, (long)h->n, h->grid.N[1],
+      h->grid.N[2], (T)(h->grid.N[0] / L[0]), (T)(h->grid.N[1] / L[1]),
+      (T)(h->grid.N[2] / L[2]));
+}
+
+template <typename T, bool CPLX>
+static void interp_order(npme_handle *h, double *d_V, cudaStream_t s) {
+  switch (h->grid.order) {
+    case 4: interp_dispatch<T, CPLX, 4>(h, d_V, s); break;
+    case 6: interp_dispatch<T, CPLX, 6>(h, d_V, s); break;
+    case 8: interp_dispatch<T, CPLX, 8>(h, d_V, s); break;
+    case 10: interp_dispatch<T, CPLX, 10>(h, d_V, s); break;
+    case 12: interp_dispatch<T, CPLX, 12>(h, d_V, s); break;
+  }
+}
+
+void launch_interp(npme_handle *h, double *d_V, cudaStream_t s) {
+  if (h->fp32) {
+    if (h->complex_kernel) interp_order<float, true>(h, d_V, s);
+    else interp_order<float, false>(h, d_V, s);
+  } else {
+    if (h->complex_kernel) interp_order<double, true>(h, d_V, s);
+    else interp_order<double, false>(h, d_V, s);
+  }
+  h->launches++;
+}
+
+}  // namespace npme

