@@ -99,6 +99,8 @@ typedef struct {
   float stage_ms[8];    /* last calcv with timing on: gather, spread, fft,
                            multiply, ifft, direct, interp, total */
   int launches;         /* kernels launched by the last calcv */
+  long nGroups;         /* FP32 direct sum: warp groups of <= 32 points */
+  double candidatesPerPoint; /* FP32 direct sum: staged sources per target */
 } npme_info;
 
 typedef struct npme_handle npme_handle;

@@ -55,6 +55,7 @@ class Info(ctypes.Structure):
         ("nCells", ctypes.c_long), ("nBricks", ctypes.c_long),
         ("nNonEmptyBricks", ctypes.c_long), ("deviceBytes", ctypes.c_size_t),
         ("stage_ms", ctypes.c_float * 8), ("launches", ctypes.c_int),
+        ("nGroups", ctypes.c_long), ("candidatesPerPoint", ctypes.c_double),
     ]
 
 
@@ -222,6 +223,7 @@ class Solver:
             "nCells": i.nCells, "nBricks": i.nBricks,
             "nNonEmptyBricks": i.nNonEmptyBricks, "deviceBytes": i.deviceBytes,
             "stage_ms": dict(zip(STAGES, list(i.stage_ms))), "launches": i.launches,
+            "nGroups": i.nGroups, "candidatesPerPoint": i.candidatesPerPoint,
         }
 
     def close(self):

@@ -82,30 +82,36 @@ __device__ __forceinline__ void bspline_weights(T u, T (&w)[P], T (&dw)[P]) {
 }
 
 // Horner in s for the scaled derivative-match polynomial and its radial
-// derivative.  Returns f_LR, writes (1/r) d f_LR/dr.
-template <typename T>
+// derivative.  Returns f_LR, writes (1/r) d f_LR/dr.  ND > 0 is the degree
+// known at compile time (fully unrolled, coefficients read at fixed offsets
+// of the parameter bank); ND == 0 reads the degree from k.nder.
+template <typename T, int ND>
 __device__ __forceinline__ T dm_poly_real(const PairCoef<T> &k, T s, T &f1) {
-  const int N = k.nder;
+  const int N = ND > 0 ? ND : k.nder;
   T p = k.ar[N];
+#pragma unroll
   for (int n = N - 1; n >= 0; n--) p = fma(p, s, k.ar[n]);
   T d = k.br[N - 1];
+#pragma unroll
   for (int n = N - 2; n >= 0; n--) d = fma(d, s, k.br[n]);
   f1 = d;
   return p;
 }
 
-template <typename T>
+template <typename T, int ND>
 __device__ __forceinline__ void dm_poly_cplx(const PairCoef<T> &k, T s, T &pr, T &pi,
                                              T &dr, T &di) {
-  const int N = k.nder;
+  const int N = ND > 0 ? ND : k.nder;
   pr = k.ar[N];
   pi = k.ai[N];
+#pragma unroll
   for (int n = N - 1; n >= 0; n--) {
     pr = fma(pr, s, k.ar[n]);
     pi = fma(pi, s, k.ai[n]);
   }
   dr = k.br[N - 1];
   di = k.bi[N - 1];
+#pragma unroll
   for (int n = N - 2; n >= 0; n--) {
     dr = fma(dr, s, k.br[n]);
     di = fma(di, s, k.bi[n]);
@@ -117,7 +123,7 @@ __device__ __forceinline__ void dm_poly_cplx(const PairCoef<T> &k, T s, T &pr, T
 // (src/PotentialLaplace.cpp:488-612, src/KernelFunctionRalpha.cpp:723-757);
 // erfc(beta r)/r for the original split (src/PotentialLaplace.cpp:614-719).
 // The caller has already checked r2 <= R2 and r2 > 0.
-template <typename T, int FUNC, int SPLIT>
+template <typename T, int FUNC, int SPLIT, int ND = 0>
 __device__ __forceinline__ T pair_sr_real(const PairCoef<T> &k, T r2, T &f1) {
   if (SPLIT == 1) {
     const T rinv = rsqrt_t(r2);
@@ -128,7 +134,7 @@ __device__ __forceinline__ T pair_sr_real(const PairCoef<T> &k, T r2, T &f1) {
     return f0;
   }
   T g1;
-  const T g0 = dm_poly_real(k, r2 * k.invR2, g1);
+  const T g0 = dm_poly_real<T, ND>(k, r2 * k.invR2, g1);
   if (FUNC == 0) {
     const T rinv = rsqrt_t(r2);
     f1 = -rinv * rinv * rinv - g1;
@@ -142,7 +148,7 @@ __device__ __forceinline__ T pair_sr_real(const PairCoef<T> &k, T r2, T &f1) {
 
 // Helmholtz short-range kernel exp(i k0 r)/r minus the DM polynomial
 // (src/PotentialHelmholtz.cpp:353-418).
-template <typename T>
+template <typename T, int ND = 0>
 __device__ __forceinline__ void pair_sr_helmholtz(const PairCoef<T> &k, T r2, T &f0r,
                                                   T &f0i, T &f1r, T &f1i) {
   const T rinv = rsqrt_t(r2);
@@ -156,7 +162,7 @@ __device__ __forceinline__ void pair_sr_helmholtz(const PairCoef<T> &k, T r2, T 
   const T iki = k.k0r * er - k.k0i * ei;
   const T e1r = (ikr - er * rinv) * rinv, e1i = (iki - ei * rinv) * rinv;
   T pr, pi, dr, di;
-  dm_poly_cplx(k, r2 * k.invR2, pr, pi, dr, di);
+  dm_poly_cplx<T, ND>(k, r2 * k.invR2, pr, pi, dr, di);
   f0r = er - pr;
   f0i = ei - pi;
   f1r = e1r - dr;

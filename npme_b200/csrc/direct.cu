@@ -51,7 +51,7 @@ template PairCoef<double> make_pair_coef<double>(const npme_handle *);
 
 constexpr int kDirectBS = 64;
 
-template <typename T, bool CPLX, int FUNC, int SPLIT>
+template <typename T, bool CPLX, int FUNC, int SPLIT, int ND>
 __global__ void __launch_bounds__(kDirectBS) direct_kernel(
     PairCoef<T> k, const typename Vec4<T>::type *__restrict__ cpos, const T *__restrict__ qc,
     const int *__restrict__ cell_start, const uint32_t *__restrict__ cperm, int nc0, int nc1,
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
             if (r2 <= R2 && s != self) {
               if (!CPLX) {
                 T f1;
-                const T f0 = pair_sr_real<T, FUNC, SPLIT>(k, r2, f1);
+                const T f0 = pair_sr_real<T, FUNC, SPLIT, ND>(k, r2, f1);
                 const T qj = sq[s];
                 const T g = f1 * qj;
                 p0 = fma(f0, qj, p0);
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
                 p3 = fma(g, z, p3);
               } else {
                 T f0r, f0i, f1r, f1i;
-                pair_sr_helmholtz<T>(k, r2, f0r, f0i, f1r, f1i);
+                pair_sr_helmholtz<T, ND>(k, r2, f0r, f0i, f1r, f1i);
                 const T qr = sq[2 * s], qi = sq[2 * s + 1];
                 // f0 q and (f1 q) * (x, y, z), complex
                 p0 = fma(f0r, qr, fma(-f0i, qi, p0));
@@ -168,14 +168,167 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
   }
 }
 
-template <typename T, bool CPLX, int FUNC, int SPLIT>
-static void direct_launch(npme_handle *h, double *d_V, cudaStream_t s) {
+// ---------------------------------------------------------------------------
+// FP32 bulk direct sum over warp groups (see build_groups in npme_gpu.cu).
+// One warp owns one group of <= 32 targets (one per lane) and walks the
+// group's source segments in chunks of 32: every lane loads one source
+// (FP64 position), the warp stages the chunk in shared memory as float
+// coordinates relative to the group centre (the FP64 difference is rounded
+// once, so close pairs keep ~1e-7 absolute resolution) and every lane then
+// sweeps the staged chunk for its target.  The next chunk's loads are issued
+// before the sweep, so global latency hides behind the arithmetic.  Warps
+// are independent: only __syncwarp, no block barrier.
+
+constexpr int kGroupWarps = 4;
+
+template <bool CPLX, int FUNC, int SPLIT, int ND>
+__global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
+    PairCoef<float> k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    double fself_r, double fself_i, double *__restrict__ V) {
+  __shared__ float4 sp[kGroupWarps][32];
+  __shared__ float sqi[kGroupWarps][CPLX ? 32 : 1];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform; nothing below synchronises the block
+  const int4 G = groups[g];
+  const double4 c = gcen[g];
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  // idle lanes sit far outside the cutoff
+  float tx = 1e18f, ty = 1e18f, tz = 1e18f;
+  if (active) {
+    const double4 p = gpos[ti];
+    tx = (float)(p.x - c.x), ty = (float)(p.y - c.y), tz = (float)(p.z - c.z);
+  }
+  const float R2 = k.R2;
+  double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
+
+  int seg = G.z, off = 0;
+  double4 pf = make_double4(0, 0, 0, 0);
+  float pq = 0.f, pqi = 0.f;
+  int pcnt = 0;
+  auto load = [&](int sg, int of) {
+    const int2 S = segs[sg];
+    const int cnt = min(32, S.y - of);
+    if (lane < cnt) {
+      const long j = (long)S.x + of + lane;
+      pf = gpos[j];
+      if (CPLX) {
+        pq = qg[2 * j];
+        pqi = qg[2 * j + 1];
+      } else {
+        pq = qg[j];
+      }
+    }
+    return cnt;
+  };
+  if (seg < G.w) pcnt = load(seg, 0);
+  while (seg < G.w) {
+    __syncwarp();
+    if (lane < pcnt) {
+      sp[wid][lane] = make_float4((float)(pf.x - c.x), (float)(pf.y - c.y),
+                                  (float)(pf.z - c.z), pq);
+      if (CPLX) sqi[wid][lane] = pqi;
+    }
+    __syncwarp();
+    const int cnt = pcnt;
+    off += 32;
+    if (off >= segs[seg].y) {
+      seg++;
+      off = 0;
+    }
+    if (seg < G.w) pcnt = load(seg, off);
+    float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
+#pragma unroll 4
+    for (int s = 0; s < cnt; s++) {
+      const float4 src = sp[wid][s];
+      const float x = tx - src.x, y = ty - src.y, z = tz - src.z;
+      const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+      if (r2 <= R2 && r2 > 0.f) {
+        if (!CPLX) {
+          float f1;
+          const float f0 = pair_sr_real<float, FUNC, SPLIT, ND>(k, r2, f1);
+          const float gq = f1 * src.w;
+          p0 = fmaf(f0, src.w, p0);
+          p1 = fmaf(gq, x, p1);
+          p2 = fmaf(gq, y, p2);
+          p3 = fmaf(gq, z, p3);
+        } else {
+          float f0r, f0i, f1r, f1i;
+          pair_sr_helmholtz<float, ND>(k, r2, f0r, f0i, f1r, f1i);
+          const float qr = src.w, qi = sqi[wid][s];
+          p0 = fmaf(f0r, qr, fmaf(-f0i, qi, p0));
+          p0i = fmaf(f0r, qi, fmaf(f0i, qr, p0i));
+          const float gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
+          p1 = fmaf(gr, x, p1);
+          p2 = fmaf(gr, y, p2);
+          p3 = fmaf(gr, z, p3);
+          p1i = fmaf(gi, x, p1i);
+          p2i = fmaf(gi, y, p2i);
+          p3i = fmaf(gi, z, p3i);
+        }
+      }
+    }
+    acc[0] += p0, acc[1] += p1, acc[2] += p2, acc[3] += p3;
+    if (CPLX) acci[0] += p0i, acci[1] += p1i, acci[2] += p2i, acci[3] += p3i;
+  }
+  if (active) {
+    const long o = perm[ti];
+    if (CPLX) {
+      const double qr = qg[2 * (long)ti], qi = qg[2 * (long)ti + 1];
+      acc[0] -= fself_r * qr - fself_i * qi;  // src/Interface.cpp:2909-2910
+      acci[0] -= fself_r * qi + fself_i * qr;
+      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+#pragma unroll
+      for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
+    } else {
+      acc[0] -= fself_r * (double)qg[ti];  // src/Interface.cpp:2061-2062
+      reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+    }
+  }
+}
+
+template <bool CPLX, int FUNC, int SPLIT, int ND>
+static void groups_launch_nd(npme_handle *h, double *d_V, cudaStream_t s) {
+  const long blocks = (h->n_groups + kGroupWarps - 1) / kGroupWarps;
+  if (blocks == 0) return;
+  direct_groups_kernel<CPLX, FUNC, SPLIT, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
+      make_pair_coef<float>(h), h->d_gpos, (const float *)h->d_qc, h->d_groups, h->d_gcen,
+      h->d_segs, h->d_cperm, h->n_groups, h->fself_r, h->fself_i, d_V);
+}
+
+template <bool CPLX, int FUNC, int SPLIT>
+static void groups_launch(npme_handle *h, double *d_V, cudaStream_t s) {
+  switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
+    case 3: groups_launch_nd<CPLX, FUNC, SPLIT, 3>(h, d_V, s); break;
+    case 6: groups_launch_nd<CPLX, FUNC, SPLIT, 6>(h, d_V, s); break;
+    case 8: groups_launch_nd<CPLX, FUNC, SPLIT, 8>(h, d_V, s); break;
+    default: groups_launch_nd<CPLX, FUNC, SPLIT, 0>(h, d_V, s); break;
+  }
+}
+
+template <typename T, bool CPLX, int FUNC, int SPLIT, int ND>
+static void direct_launch_nd(npme_handle *h, double *d_V, cudaStream_t s) {
   const CellGeom &c = h->cells;
   const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
-  direct_kernel<T, CPLX, FUNC, SPLIT><<<ncell, kDirectBS, 0, s>>>(
+  direct_kernel<T, CPLX, FUNC, SPLIT, ND><<<ncell, kDirectBS, 0, s>>>(
       make_pair_coef<T>(h), (const typename Vec4<T>::type *)h->d_cpos, (const T *)h->d_qc,
       h->d_cell_start, h->d_cperm, c.nc[0], c.nc[1], c.nc[2], (T)c.edge[0], (T)c.edge[1],
       (T)c.edge[2], c.reach, h->fself_r, h->fself_i, d_V);
+}
+
+// Dispatch on the derivative-match degree: the reference's defaults (3, 6, 8
+// for B-spline orders 4, 6, 8) get fully unrolled polynomials.
+template <typename T, bool CPLX, int FUNC, int SPLIT>
+static void direct_launch(npme_handle *h, double *d_V, cudaStream_t s) {
+  switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
+    case 3: direct_launch_nd<T, CPLX, FUNC, SPLIT, 3>(h, d_V, s); break;
+    case 6: direct_launch_nd<T, CPLX, FUNC, SPLIT, 6>(h, d_V, s); break;
+    case 8: direct_launch_nd<T, CPLX, FUNC, SPLIT, 8>(h, d_V, s); break;
+    default: direct_launch_nd<T, CPLX, FUNC, SPLIT, 0>(h, d_V, s); break;
+  }
 }
 
 template <typename T>
@@ -188,8 +341,17 @@ static void direct_prec(npme_handle *h, double *d_V, cudaStream_t s) {
 }
 
 void launch_direct(npme_handle *h, double *d_V, cudaStream_t s) {
-  if (h->fp32) direct_prec<float>(h, d_V, s);
-  else direct_prec<double>(h, d_V, s);
+  if (h->use_groups) {
+    const int f = h->p.funcType, sp = h->p.EwaldSplit;
+    if (f == NPME_FUNC_HELMHOLTZ) groups_launch<true, 2, 0>(h, d_V, s);
+    else if (sp == NPME_SPLIT_LAPLACE_ORIG) groups_launch<false, 0, 1>(h, d_V, s);
+    else if (f == NPME_FUNC_RALPHA) groups_launch<false, 1, 0>(h, d_V, s);
+    else groups_launch<false, 0, 0>(h, d_V, s);
+  } else if (h->fp32) {
+    direct_prec<float>(h, d_V, s);
+  } else {
+    direct_prec<double>(h, d_V, s);
+  }
   h->launches++;
 }
 

@@ -92,6 +92,17 @@ struct npme_handle {
   int *d_err = nullptr;          // device error flag
   size_t dev_bytes = 0;
 
+  // FP32 direct sum: warp groups of <= 32 z-sorted points of one xy column
+  // and, per group, the source segments (neighbour-column z ranges) that can
+  // hold a point within Rdir of the group.  Built once per geometry.
+  bool use_groups = false;
+  long n_groups = 0, n_segs = 0;
+  double cand_per_point = 0;     // staged source candidates per target point
+  double4 *d_gpos = nullptr;     // group order, FP64 positions
+  int4 *d_groups = nullptr;      // (first point, count, first segment, end segment)
+  double4 *d_gcen = nullptr;     // group frame origin (bbox centre)
+  int2 *d_segs = nullptr;        // (first point, count)
+
   npme::Timing timing;
   bool timing_pending = false;
   float stage_ms[8] = {0};

@@ -124,6 +124,11 @@ void release(npme_handle *h) {
   h->d_cell_start = nullptr, h->d_qb = nullptr, h->d_qc = nullptr, h->d_grid = nullptr;
   h->d_kgrid = nullptr, h->d_theta = nullptr, h->d_G = nullptr, h->d_q_in = nullptr;
   h->d_V = nullptr, h->d_V_exact = nullptr, h->d_err = nullptr;
+  void *gbufs[] = {h->d_gpos, h->d_groups, h->d_gcen, h->d_segs};
+  for (void *b : gbufs)
+    if (b) cudaFree(b);
+  h->d_gpos = nullptr, h->d_groups = nullptr, h->d_gcen = nullptr, h->d_segs = nullptr;
+  h->n_groups = h->n_segs = 0;
   h->dev_bytes = 0;
   h->ready = false;
 }
@@ -136,6 +141,120 @@ int dalloc(npme_handle *h, P **ptr, size_t bytes) {
     return fail(h, NPME_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
                                     " bytes failed: " + cudaGetErrorString(e));
   h->dev_bytes += bytes;
+  return NPME_OK;
+}
+
+// Warp groups for the FP32 direct sum.  Points are binned into xy columns of
+// edge ~(32 / density)^(1/3) and sorted by z inside each column; each run of
+// 32 consecutive points of a column is one group (a compact, roughly cubic
+// cluster).  For every group the source segments are the z ranges of the
+// neighbour columns that can hold a point within Rdir of the group's
+// bounding box: |dz| <= sqrt(Rdir^2 - d_xy^2) with d_xy the distance from
+// the bounding box to the column in the xy plane.  Geometry is fixed between
+// CalcV calls (the reference's contract), so this is set-up work.  Returns
+// the group-order permutation in `order`.
+int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &order) {
+  const size_t n = h->n;
+  const double R = h->p.Rdir, R2 = R * R;
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (size_t i = 0; i < n; i++)
+    for (int d = 0; d < 3; d++) {
+      mn[d] = std::min(mn[d], coord[3 * i + d]);
+      mx[d] = std::max(mx[d], coord[3 * i + d]);
+    }
+  // column edge from the mean density of the bounding box (degenerate axes
+  // are given a nominal thickness of Rdir / 4)
+  double vol = 1.0;
+  for (int d = 0; d < 3; d++) vol *= std::max(mx[d] - mn[d], 0.25 * R);
+  double e = std::cbrt(32.0 * vol / (double)n);
+  e = std::max(e, 1e-3 * R);
+  int nc[2];
+  double edge[2];
+  for (int d = 0; d < 2; d++) {
+    const double ext = mx[d] - mn[d];
+    nc[d] = std::max(1, std::min((int)std::ceil(ext / e), 1 << 14));
+    edge[d] = std::max(ext / nc[d], 1e-12);
+  }
+  const long ncol = (long)nc[0] * nc[1];
+  std::vector<int> col(n);
+  for (size_t i = 0; i < n; i++) {
+    int c0 = std::min(nc[0] - 1, std::max(0, (int)((coord[3 * i] - mn[0]) / edge[0])));
+    int c1 = std::min(nc[1] - 1, std::max(0, (int)((coord[3 * i + 1] - mn[1]) / edge[1])));
+    col[i] = c0 * nc[1] + c1;
+  }
+  order.resize(n);
+  for (size_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    if (col[a] != col[b]) return col[a] < col[b];
+    if (coord[3 * a + 2] != coord[3 * b + 2]) return coord[3 * a + 2] < coord[3 * b + 2];
+    return a < b;
+  });
+  std::vector<long> cstart(ncol + 1, 0);
+  for (size_t i = 0; i < n; i++) cstart[col[i] + 1]++;
+  for (long c = 0; c < ncol; c++) cstart[c + 1] += cstart[c];
+  std::vector<double> zs(n);
+  for (size_t k = 0; k < n; k++) zs[k] = coord[3 * (size_t)order[k] + 2];
+
+  std::vector<int4> groups;
+  std::vector<double4> cen;
+  std::vector<int2> segs;
+  double cand = 0;
+  for (long c = 0; c < ncol; c++) {
+    const int c0 = (int)(c / nc[1]), c1 = (int)(c % nc[1]);
+    for (long p0 = cstart[c]; p0 < cstart[c + 1]; p0 += 32) {
+      const long p1 = std::min(p0 + 32, cstart[c + 1]);
+      double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
+      for (long k = p0; k < p1; k++)
+        for (int d = 0; d < 3; d++) {
+          const double x = coord[3 * (size_t)order[k] + d];
+          bl[d] = std::min(bl[d], x);
+          bh[d] = std::max(bh[d], x);
+        }
+      const int seg0 = (int)segs.size();
+      const int r0 = (int)std::min<double>(nc[0], std::ceil(R / edge[0]) + 1);
+      const int r1 = (int)std::min<double>(nc[1], std::ceil(R / edge[1]) + 1);
+      for (int s0 = std::max(0, c0 - r0); s0 <= std::min(nc[0] - 1, c0 + r0); s0++) {
+        const double lo0 = mn[0] + s0 * edge[0], hi0 = lo0 + edge[0];
+        const double dx = std::max(0.0, std::max(lo0 - bh[0], bl[0] - hi0));
+        for (int s1 = std::max(0, c1 - r1); s1 <= std::min(nc[1] - 1, c1 + r1); s1++) {
+          const double lo1 = mn[1] + s1 * edge[1], hi1 = lo1 + edge[1];
+          const double dy = std::max(0.0, std::max(lo1 - bh[1], bl[1] - hi1));
+          const double d2 = dx * dx + dy * dy;
+          if (d2 > R2) continue;
+          const double hz = std::sqrt(R2 - d2);
+          const long sc = (long)s0 * nc[1] + s1;
+          const double *zb = zs.data() + cstart[sc], *ze = zs.data() + cstart[sc + 1];
+          const long a = std::lower_bound(zb, ze, bl[2] - hz) - zs.data();
+          const long b = std::upper_bound(zb, ze, bh[2] + hz) - zs.data();
+          if (b > a) {
+            segs.push_back(make_int2((int)a, (int)(b - a)));
+            cand += (double)(b - a) * (double)(p1 - p0);
+          }
+        }
+      }
+      groups.push_back(make_int4((int)p0, (int)(p1 - p0), seg0, (int)segs.size()));
+      cen.push_back(make_double4(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]),
+                                 0.5 * (bl[2] + bh[2]), 0.0));
+    }
+  }
+  std::vector<double4> gpos(n);
+  for (size_t k = 0; k < n; k++) {
+    const double *x = coord + 3 * (size_t)order[k];
+    gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
+  }
+  h->n_groups = (long)groups.size();
+  h->n_segs = (long)segs.size();
+  h->cand_per_point = cand / (double)n;
+  int rc;
+  if ((rc = dalloc(h, &h->d_gpos, sizeof(double4) * n))) return rc;
+  if ((rc = dalloc(h, &h->d_groups, sizeof(int4) * groups.size()))) return rc;
+  if ((rc = dalloc(h, &h->d_gcen, sizeof(double4) * cen.size()))) return rc;
+  if ((rc = dalloc(h, &h->d_segs, sizeof(int2) * std::max<size_t>(1, segs.size())))) return rc;
+  CK(cudaMemcpy(h->d_gpos, gpos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_groups, groups.data(), sizeof(int4) * groups.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_gcen, cen.data(), sizeof(double4) * cen.size(), cudaMemcpyHostToDevice));
+  if (!segs.empty())
+    CK(cudaMemcpy(h->d_segs, segs.data(), sizeof(int2) * segs.size(), cudaMemcpyHostToDevice));
   return NPME_OK;
 }
 
@@ -214,6 +333,8 @@ int upload_points(npme_handle *h, const double *coord) {
 
   const int C = h->complex_kernel ? 2 : 1;
   int rc;
+  // the FP32 direct sum walks warp groups: charges are gathered in group order
+  if (h->use_groups && (rc = build_groups(h, coord, cperm))) return rc;
   if ((rc = dalloc(h, &h->d_coord, sizeof(double) * 3 * n))) return rc;
   if ((rc = dalloc(h, (BrickPoint<T> **)&h->d_bpts, sizeof(BrickPoint<T>) * n))) return rc;
   if ((rc = dalloc(h, &h->d_brick_start, sizeof(int) * (nbt + 1)))) return rc;
@@ -425,6 +546,9 @@ int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
   }
   if (ncells > (1L << 30)) return fail(h, NPME_EINVAL, "too many direct-sum cells");
   h->cells.reach = p.nNeigh;
+  // FP32 bulk mode uses the warp-group direct sum; FP64 keeps the plain
+  // cell-list port
+  h->use_groups = h->fp32;
   int rc = h->fp32 ? upload_points<float>(h, coord) : upload_points<double>(h, coord);
   if (rc) {
     release(h);
@@ -636,6 +760,8 @@ int npme_gpu_get_info(const npme_handle *hc, npme_info *info) {
   info->deviceBytes = h->dev_bytes;
   for (int i = 0; i < 8; i++) info->stage_ms[i] = h->stage_ms[i];
   info->launches = h->launches;
+  info->nGroups = h->n_groups;
+  info->candidatesPerPoint = h->cand_per_point;
   return NPME_OK;
 }
 

@@ -4,8 +4,9 @@ the full benchmark sizes.
 
 Tolerances (relative RMS over all points):
   FP64 mode vs reference / oracle:        1e-12 (same algorithm, FP64 throughout)
-  FP32 bulk mode vs FP64 oracle:          V 2e-6, gradient 3e-5
-  either mode vs the exact O(N^2) sum:    1e-5 (the method's own error at these grids)
+  FP32 bulk mode vs FP64:                 V 1e-5 (the stated FP32-mode bound),
+                                          gradient 3e-5
+  either mode vs the exact O(N^2) sum:    1e-4 at the full sizes (method error)
 """
 import dataclasses
 import os
@@ -23,7 +24,7 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 FP64_TOL = 1e-12
-FP32_V_TOL = 2e-6
+FP32_V_TOL = 1e-5
 FP32_G_TOL = 3e-5
 
 
@@ -129,7 +130,11 @@ def test_ragged_and_tiny_systems(n):
     q = q + 0.25  # re-centring leaves a single charge at 0; use a non-neutral system
     Vo = ob.calcv(ob.params_from_workload(w), c, q)
     with solver(w, "fp64") as s:
-        assert rel(s.calcv(q), Vo) < 1e-11
+        V = s.calcv(q)
+    # a lone point's potential is a cancellation to ~1e-16: compare absolutely
+    # against the scale |q| / Rdir of its terms
+    scale = np.abs(q).max() / w.Rdir
+    assert np.abs(V - Vo).max() <= 1e-11 * scale + 1e-12 * np.abs(Vo).max()
 
 
 def test_degenerate_planar_and_linear_geometry():
