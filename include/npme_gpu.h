@@ -126,10 +126,20 @@ int npme_gpu_calcv_complex(npme_handle *h, double *V, size_t n,
                            const double *charge, const double *coord);
 
 /* CalcV on device buffers already resident in HBM, enqueued on `stream`
- * (a cudaStream_t, or NULL for the handle's own stream).  Charge and V
+ * (a cudaStream_t; NULL is the default stream, as in CUDA).  Charge and V
  * layouts as above.  Returns after enqueueing; the caller synchronises. */
 int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge,
                           void *stream);
+
+/* Short-range direct sum alone on device buffers: V = sum_{j != i,
+ * r_ij <= Rdir} q_j f_SR(r_ij) and its gradient, no self term, V overwritten.
+ * Replaces NPME_PotLaplace_SR_DM_DirectSum_V1 / _SR_Original_DirectSum_V1
+ * (src/PotentialLaplace.h:33-44), NPME_PotHelmholtz_SR_DM_DirectSum_V1
+ * (src/PotentialHelmholtz.cpp:194) and NPME_PotGenFunc_DirectSum_V1
+ * (src/PotentialGenFunc.cpp:140) for the set-up geometry.  Layouts and
+ * stream semantics as npme_gpu_calcv_device. */
+int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_charge,
+                               void *stream);
 
 /* CalcV_exact: O(N^2) sum with the full kernel (FP64), host buffers. */
 int npme_gpu_calcv_exact_real(npme_handle *h, double *V, size_t n,

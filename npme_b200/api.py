@@ -65,6 +65,7 @@ STAGES = ("gather", "spread", "fft", "multiply", "ifft", "direct", "interp", "to
 EXPORTS = (
     "npme_gpu_default_params", "npme_gpu_create", "npme_gpu_setup",
     "npme_gpu_calcv_real", "npme_gpu_calcv_complex", "npme_gpu_calcv_device",
+    "npme_gpu_direct_sum_device",
     "npme_gpu_calcv_exact_real", "npme_gpu_calcv_exact_complex",
     "npme_gpu_count_pairs", "npme_gpu_set_timing", "npme_gpu_get_info",
     "npme_gpu_last_error",
@@ -97,6 +98,7 @@ def load_library():
               "npme_gpu_calcv_exact_real", "npme_gpu_calcv_exact_complex"):
         getattr(L, f).argtypes = [vp, dp, sz, dp, dp]
     L.npme_gpu_calcv_device.argtypes = [vp, vp, vp, vp]
+    L.npme_gpu_direct_sum_device.argtypes = [vp, vp, vp, vp]
     L.npme_gpu_set_timing.argtypes = [vp, ctypes.c_int]
     L.npme_gpu_count_pairs.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.npme_gpu_get_info.argtypes = [vp, ctypes.POINTER(Info)]
@@ -200,6 +202,12 @@ class Solver:
     def calcv_device(self, V_ptr, q_ptr, stream_ptr=None):
         """CalcV on device pointers (ints), enqueued on stream_ptr."""
         self._check(self.L.npme_gpu_calcv_device(
+            self.h, ctypes.c_void_p(V_ptr), ctypes.c_void_p(q_ptr),
+            ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def direct_sum_device(self, V_ptr, q_ptr, stream_ptr=None):
+        """Short-range direct sum alone (no self term) on device pointers."""
+        self._check(self.L.npme_gpu_direct_sum_device(
             self.h, ctypes.c_void_p(V_ptr), ctypes.c_void_p(q_ptr),
             ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 

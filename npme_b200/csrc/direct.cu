@@ -173,22 +173,33 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
 // One warp owns one group of <= 32 targets (one per lane) and walks the
 // group's source segments in chunks of 32: every lane loads one source
 // (FP64 position), the warp stages the chunk in shared memory as float
-// coordinates relative to the group centre (the FP64 difference is rounded
-// once, so close pairs keep ~1e-7 absolute resolution) and every lane then
-// sweeps the staged chunk for its target.  The next chunk's loads are issued
-// before the sweep, so global latency hides behind the arithmetic.  Warps
-// are independent: only __syncwarp, no block barrier.
+// coordinates relative to the group centre and every lane then sweeps the
+// staged chunk for its target.  The next chunk's loads are issued before the
+// sweep, so global latency hides behind the arithmetic.  Warps are
+// independent: only __syncwarp, no block barrier.
+//
+// Coordinates: each FP64 offset from the group centre is split into a float
+// head and the float residual (hi + lo).  The distance test and the pair
+// arithmetic use the heads; for the rare close pairs (r^2 < refine2) the
+// difference is recomputed as (t_hi - s_hi) + (t_lo - s_lo), which is exact
+// to ~1e-15 because the heads of two close points subtract exactly.  Without
+// this, a pair at r ~ 0.01 in a group of radius ~2 carries a ~1e-5 relative
+// error that dominates the gradient.
 
 constexpr int kGroupWarps = 4;
+#ifndef NPME_DIRECT_UNROLL
+#define NPME_DIRECT_UNROLL 8
+#endif
+constexpr int kDirectUnroll = NPME_DIRECT_UNROLL;  // pair-loop unroll factor
 
 template <bool CPLX, int FUNC, int SPLIT, int ND>
 __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
     PairCoef<float> k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
     const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
     const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
-    double fself_r, double fself_i, double *__restrict__ V) {
-  __shared__ float4 sp[kGroupWarps][32];
-  __shared__ float sqi[kGroupWarps][CPLX ? 32 : 1];
+    float refine2, double fself_r, double fself_i, double *__restrict__ V) {
+  __shared__ float4 sp[kGroupWarps][32];   // (x_hi, y_hi, z_hi, q) / q.re
+  __shared__ float4 slo[kGroupWarps][32];  // (x_lo, y_lo, z_lo, q.im)
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long g = (long)blockIdx.x * kGroupWarps + wid;
   if (g >= ngroups) return;  // warp-uniform; nothing below synchronises the block
@@ -197,40 +208,45 @@ __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
   const int ti = G.x + lane;
   const bool active = lane < G.y;
   // idle lanes sit far outside the cutoff
-  float tx = 1e18f, ty = 1e18f, tz = 1e18f;
+  float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f;
   if (active) {
     const double4 p = gpos[ti];
-    tx = (float)(p.x - c.x), ty = (float)(p.y - c.y), tz = (float)(p.z - c.z);
+    const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+    tx = (float)dx, ty = (float)dy, tz = (float)dz;
+    tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
   }
   const float R2 = k.R2;
   double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
 
-  int seg = G.z, off = 0;
-  double4 pf = make_double4(0, 0, 0, 0);
+  // register prefetch of the next chunk: lane l holds source l of the chunk
+  int seg = G.z, off = 0, pcnt = 0;
+  double px = 0, py = 0, pz = 0;
   float pq = 0.f, pqi = 0.f;
-  int pcnt = 0;
-  auto load = [&](int sg, int of) {
-    const int2 S = segs[sg];
-    const int cnt = min(32, S.y - of);
-    if (lane < cnt) {
-      const long j = (long)S.x + of + lane;
-      pf = gpos[j];
-      if (CPLX) {
-        pq = qg[2 * j];
-        pqi = qg[2 * j + 1];
-      } else {
-        pq = qg[j];
-      }
-    }
-    return cnt;
-  };
-  if (seg < G.w) pcnt = load(seg, 0);
+#define NPME_PREFETCH(SG, OF)                                  \
+  {                                                            \
+    const int2 S_ = segs[SG];                                  \
+    pcnt = min(32, S_.y - (OF));                               \
+    if (lane < pcnt) {                                         \
+      const long j_ = (long)S_.x + (OF) + lane;                \
+      const double4 p_ = gpos[j_];                             \
+      px = p_.x, py = p_.y, pz = p_.z;                         \
+      if (CPLX) {                                              \
+        pq = qg[2 * j_];                                       \
+        pqi = qg[2 * j_ + 1];                                  \
+      } else {                                                 \
+        pq = qg[j_];                                           \
+      }                                                        \
+    }                                                          \
+  }
+  if (seg < G.w) NPME_PREFETCH(seg, 0);
   while (seg < G.w) {
     __syncwarp();
     if (lane < pcnt) {
-      sp[wid][lane] = make_float4((float)(pf.x - c.x), (float)(pf.y - c.y),
-                                  (float)(pf.z - c.z), pq);
-      if (CPLX) sqi[wid][lane] = pqi;
+      const double dx = px - c.x, dy = py - c.y, dz = pz - c.z;
+      const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+      sp[wid][lane] = make_float4(hx, hy, hz, pq);
+      slo[wid][lane] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy),
+                                   (float)(dz - (double)hz), pqi);
     }
     __syncwarp();
     const int cnt = pcnt;
@@ -239,14 +255,21 @@ __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
       seg++;
       off = 0;
     }
-    if (seg < G.w) pcnt = load(seg, off);
+    if (seg < G.w) NPME_PREFETCH(seg, off);
     float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
-#pragma unroll 4
+#pragma unroll kDirectUnroll
     for (int s = 0; s < cnt; s++) {
       const float4 src = sp[wid][s];
-      const float x = tx - src.x, y = ty - src.y, z = tz - src.z;
-      const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+      float x = tx - src.x, y = ty - src.y, z = tz - src.z;
+      float r2 = fmaf(x, x, fmaf(y, y, z * z));
       if (r2 <= R2 && r2 > 0.f) {
+        if (r2 < refine2) {  // close pair: exact difference from head + residual
+          const float4 lo = slo[wid][s];
+          x += tlx - lo.x;
+          y += tly - lo.y;
+          z += tlz - lo.z;
+          r2 = fmaf(x, x, fmaf(y, y, z * z));
+        }
         if (!CPLX) {
           float f1;
           const float f0 = pair_sr_real<float, FUNC, SPLIT, ND>(k, r2, f1);
@@ -258,7 +281,7 @@ __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
         } else {
           float f0r, f0i, f1r, f1i;
           pair_sr_helmholtz<float, ND>(k, r2, f0r, f0i, f1r, f1i);
-          const float qr = src.w, qi = sqi[wid][s];
+          const float qr = src.w, qi = slo[wid][s].w;
           p0 = fmaf(f0r, qr, fmaf(-f0i, qi, p0));
           p0i = fmaf(f0r, qi, fmaf(f0i, qr, p0i));
           const float gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
@@ -290,69 +313,76 @@ __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
   }
 }
 
+#undef NPME_PREFETCH
+
 template <bool CPLX, int FUNC, int SPLIT, int ND>
-static void groups_launch_nd(npme_handle *h, double *d_V, cudaStream_t s) {
+static void groups_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   const long blocks = (h->n_groups + kGroupWarps - 1) / kGroupWarps;
   if (blocks == 0) return;
   direct_groups_kernel<CPLX, FUNC, SPLIT, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
-      make_pair_coef<float>(h), h->d_gpos, (const float *)h->d_qc, h->d_groups, h->d_gcen,
-      h->d_segs, h->d_cperm, h->n_groups, h->fself_r, h->fself_i, d_V);
+      make_pair_coef<float>(h), h->d_gpos, (const float *)a.q, h->d_groups, h->d_gcen,
+      h->d_segs, h->d_cperm, h->n_groups, (float)h->refine2, a.fself_r, a.fself_i, a.V);
 }
 
 template <bool CPLX, int FUNC, int SPLIT>
-static void groups_launch(npme_handle *h, double *d_V, cudaStream_t s) {
+static void groups_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
-    case 3: groups_launch_nd<CPLX, FUNC, SPLIT, 3>(h, d_V, s); break;
-    case 6: groups_launch_nd<CPLX, FUNC, SPLIT, 6>(h, d_V, s); break;
-    case 8: groups_launch_nd<CPLX, FUNC, SPLIT, 8>(h, d_V, s); break;
-    default: groups_launch_nd<CPLX, FUNC, SPLIT, 0>(h, d_V, s); break;
+    case 3: groups_launch_nd<CPLX, FUNC, SPLIT, 3>(h, a, s); break;
+    case 6: groups_launch_nd<CPLX, FUNC, SPLIT, 6>(h, a, s); break;
+    case 8: groups_launch_nd<CPLX, FUNC, SPLIT, 8>(h, a, s); break;
+    default: groups_launch_nd<CPLX, FUNC, SPLIT, 0>(h, a, s); break;
   }
 }
 
 template <typename T, bool CPLX, int FUNC, int SPLIT, int ND>
-static void direct_launch_nd(npme_handle *h, double *d_V, cudaStream_t s) {
+static void direct_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   const CellGeom &c = h->cells;
   const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
   direct_kernel<T, CPLX, FUNC, SPLIT, ND><<<ncell, kDirectBS, 0, s>>>(
-      make_pair_coef<T>(h), (const typename Vec4<T>::type *)h->d_cpos, (const T *)h->d_qc,
+      make_pair_coef<T>(h), (const typename Vec4<T>::type *)h->d_cpos, (const T *)a.q,
       h->d_cell_start, h->d_cperm, c.nc[0], c.nc[1], c.nc[2], (T)c.edge[0], (T)c.edge[1],
-      (T)c.edge[2], c.reach, h->fself_r, h->fself_i, d_V);
+      (T)c.edge[2], c.reach, a.fself_r, a.fself_i, a.V);
 }
 
 // Dispatch on the derivative-match degree: the reference's defaults (3, 6, 8
 // for B-spline orders 4, 6, 8) get fully unrolled polynomials.
 template <typename T, bool CPLX, int FUNC, int SPLIT>
-static void direct_launch(npme_handle *h, double *d_V, cudaStream_t s) {
+static void direct_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
-    case 3: direct_launch_nd<T, CPLX, FUNC, SPLIT, 3>(h, d_V, s); break;
-    case 6: direct_launch_nd<T, CPLX, FUNC, SPLIT, 6>(h, d_V, s); break;
-    case 8: direct_launch_nd<T, CPLX, FUNC, SPLIT, 8>(h, d_V, s); break;
-    default: direct_launch_nd<T, CPLX, FUNC, SPLIT, 0>(h, d_V, s); break;
+    case 3: direct_launch_nd<T, CPLX, FUNC, SPLIT, 3>(h, a, s); break;
+    case 6: direct_launch_nd<T, CPLX, FUNC, SPLIT, 6>(h, a, s); break;
+    case 8: direct_launch_nd<T, CPLX, FUNC, SPLIT, 8>(h, a, s); break;
+    default: direct_launch_nd<T, CPLX, FUNC, SPLIT, 0>(h, a, s); break;
   }
 }
 
 template <typename T>
-static void direct_prec(npme_handle *h, double *d_V, cudaStream_t s) {
+static void direct_prec(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   const int f = h->p.funcType, sp = h->p.EwaldSplit;
-  if (f == NPME_FUNC_HELMHOLTZ) direct_launch<T, true, 2, 0>(h, d_V, s);
-  else if (sp == NPME_SPLIT_LAPLACE_ORIG) direct_launch<T, false, 0, 1>(h, d_V, s);
-  else if (f == NPME_FUNC_RALPHA) direct_launch<T, false, 1, 0>(h, d_V, s);
-  else direct_launch<T, false, 0, 0>(h, d_V, s);
+  if (f == NPME_FUNC_HELMHOLTZ) direct_launch<T, true, 2, 0>(h, a, s);
+  else if (sp == NPME_SPLIT_LAPLACE_ORIG) direct_launch<T, false, 0, 1>(h, a, s);
+  else if (f == NPME_FUNC_RALPHA) direct_launch<T, false, 1, 0>(h, a, s);
+  else direct_launch<T, false, 0, 0>(h, a, s);
+}
+
+void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  if (h->use_groups) {
+    const int f = h->p.funcType, sp = h->p.EwaldSplit;
+    if (f == NPME_FUNC_HELMHOLTZ) groups_launch<true, 2, 0>(h, a, s);
+    else if (sp == NPME_SPLIT_LAPLACE_ORIG) groups_launch<false, 0, 1>(h, a, s);
+    else if (f == NPME_FUNC_RALPHA) groups_launch<false, 1, 0>(h, a, s);
+    else groups_launch<false, 0, 0>(h, a, s);
+  } else if (h->fp32) {
+    direct_prec<float>(h, a, s);
+  } else {
+    direct_prec<double>(h, a, s);
+  }
+  h->launches++;
 }
 
 void launch_direct(npme_handle *h, double *d_V, cudaStream_t s) {
-  if (h->use_groups) {
-    const int f = h->p.funcType, sp = h->p.EwaldSplit;
-    if (f == NPME_FUNC_HELMHOLTZ) groups_launch<true, 2, 0>(h, d_V, s);
-    else if (sp == NPME_SPLIT_LAPLACE_ORIG) groups_launch<false, 0, 1>(h, d_V, s);
-    else if (f == NPME_FUNC_RALPHA) groups_launch<false, 1, 0>(h, d_V, s);
-    else groups_launch<false, 0, 0>(h, d_V, s);
-  } else if (h->fp32) {
-    direct_prec<float>(h, d_V, s);
-  } else {
-    direct_prec<double>(h, d_V, s);
-  }
-  h->launches++;
+  DirectArgs a{h->d_qc, h->fself_r, h->fself_i, d_V};
+  launch_direct_args(h, a, s);
 }
 
 // Ordered pairs with r <= Rdir, i != j, using the same cell walk as the

@@ -98,6 +98,7 @@ struct npme_handle {
   bool use_groups = false;
   long n_groups = 0, n_segs = 0;
   double cand_per_point = 0;     // staged source candidates per target point
+  double refine2 = 0;            // r^2 below which pair differences are refined
   double4 *d_gpos = nullptr;     // group order, FP64 positions
   int4 *d_groups = nullptr;      // (first point, count, first segment, end segment)
   double4 *d_gcen = nullptr;     // group frame origin (bbox centre)
@@ -119,7 +120,18 @@ void launch_multiply(npme_handle *h, cudaStream_t s);
 void launch_interp(npme_handle *h, double *d_V, cudaStream_t s);
 
 // direct.cu
+// One direct-sum launch: charges already in the direct-sum order (group
+// order for FP32 bulk, cell order for FP64), the self term f_LR(0) q to
+// subtract from V (zero for the bare short-range sum), and the output.
+struct DirectArgs {
+  const void *q;
+  double fself_r, fself_i;
+  double *V;
+};
 void launch_direct(npme_handle *h, double *d_V, cudaStream_t s);
+void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s);
+// caller-order charges (double) -> direct-sum order in the bulk precision
+void launch_gather_direct(npme_handle *h, const double *d_q, void *d_qdst, cudaStream_t s);
 void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
 void launch_count_pairs(npme_handle *h, unsigned long long *d_count, cudaStream_t s);
 template <typename T>

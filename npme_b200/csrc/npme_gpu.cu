@@ -245,6 +245,9 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   h->n_groups = (long)groups.size();
   h->n_segs = (long)segs.size();
   h->cand_per_point = cand / (double)n;
+  // heads of offsets up to ~the group half-diagonal carry ~6e-8 e absolute
+  // error; below r = e/4 the relative error would exceed ~1e-6, so refine
+  h->refine2 = (0.25 * e) * (0.25 * e);
   int rc;
   if ((rc = dalloc(h, &h->d_gpos, sizeof(double4) * n))) return rc;
   if ((rc = dalloc(h, &h->d_groups, sizeof(int4) * groups.size()))) return rc;
@@ -575,7 +578,7 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   if (!h->ready) return fail(h, NPME_ESTATE, "calcv before setup");
   if (!d_V || !d_charge) return fail(h, NPME_EINVAL, "null buffer");
   CK(cudaSetDevice(h->device));
-  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
   h->launches = 0;
   const size_t gbytes = (h->fp32 ? 4 : 8) * (h->complex_kernel ? 2 : 1) *
                         (size_t)h->grid.N[0] * h->grid.N[1] * h->grid.N[2];
@@ -716,6 +719,21 @@ int npme_gpu_calcv_exact_complex(npme_handle *h, double *V, size_t n, const doub
                                  const double *coord) {
   (void)coord;
   return exact_host(h, V, n, charge, true);
+}
+
+int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_charge,
+                               void *stream) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!h->ready) return fail(h, NPME_ESTATE, "direct_sum before setup");
+  if (!d_V || !d_charge) return fail(h, NPME_EINVAL, "null buffer");
+  CK(cudaSetDevice(h->device));
+  cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
+  h->launches = 0;
+  npme::launch_gather_direct(h, d_charge, h->d_qc, s);
+  npme::DirectArgs a{h->d_qc, 0.0, 0.0, d_V};
+  npme::launch_direct_args(h, a, s);
+  CK(cudaGetLastError());
+  return NPME_OK;
 }
 
 int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs) {

@@ -350,6 +350,41 @@ void launch_gather_charges(npme_handle *h, const double *d_q, cudaStream_t s) {
   h->launches++;
 }
 
+// Charges into the direct-sum order only (the bare short-range sum).
+template <typename T, bool CPLX>
+__global__ void gather_one_kernel(const double *__restrict__ q,
+                                  const uint32_t *__restrict__ perm, T *__restrict__ dst,
+                                  long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const long o = perm[i];
+    if (CPLX) {
+      dst[2 * i] = (T)q[2 * o];
+      dst[2 * i + 1] = (T)q[2 * o + 1];
+    } else {
+      dst[i] = (T)q[o];
+    }
+  }
+}
+
+void launch_gather_direct(npme_handle *h, const double *d_q, void *d_qdst, cudaStream_t s) {
+  const int threads = 256;
+  const int blocks = (int)std::min<long>((h->n + threads - 1) / threads, 148 * 16);
+  const long n = (long)h->n;
+  if (h->fp32) {
+    if (h->complex_kernel)
+      gather_one_kernel<float, true><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (float *)d_qdst, n);
+    else
+      gather_one_kernel<float, false><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (float *)d_qdst, n);
+  } else {
+    if (h->complex_kernel)
+      gather_one_kernel<double, true><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (double *)d_qdst, n);
+    else
+      gather_one_kernel<double, false><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (double *)d_qdst, n);
+  }
+  h->launches++;
+}
+
 // ---------------------------------------------------------------------------
 // Spread (src/RecSumQ.cpp:184-314): Q[g] += q B1 B2 B3.  One CTA per
 // non-empty brick of kBrick^3 stencil origins.  The CTA accumulates its
