@@ -141,6 +141,20 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge,
 int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_charge,
                                void *stream);
 
+/* The same short-range direct sum for callers that cannot call cudaMalloc
+ * when they need it (for example code inside another framework's pre-reserved
+ * memory pool, or a latency-critical loop that must not let an allocation
+ * synchronise the device).  No counterpart in the reference.  Allocates
+ * nothing: its scratch (the charges gathered into the direct-sum order) is a
+ * static 8 MiB device array that every GPU loading the library holds until
+ * exit, so at most 2,097,152 points (FP32 real), 1,048,576 (FP32 complex,
+ * FP64 real) or 524,288 (FP64 complex); larger handles get NPME_EINVAL.  The
+ * first call on a device looks the array up (and loads the module): make it
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race.  Output and arguments as npme_gpu_direct_sum_device. */
+int npme_gpu_direct_sum_device_noalloc(npme_handle *h, double *d_V,
+                                       const double *d_charge, void *stream);
+
 /* CalcV_exact: O(N^2) sum with the full kernel (FP64), host buffers. */
 int npme_gpu_calcv_exact_real(npme_handle *h, double *V, size_t n,
                               const double *charge, const double *coord);

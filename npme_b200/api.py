@@ -65,7 +65,7 @@ STAGES = ("gather", "spread", "fft", "multiply", "ifft", "direct", "interp", "to
 EXPORTS = (
     "npme_gpu_default_params", "npme_gpu_create", "npme_gpu_setup",
     "npme_gpu_calcv_real", "npme_gpu_calcv_complex", "npme_gpu_calcv_device",
-    "npme_gpu_direct_sum_device",
+    "npme_gpu_direct_sum_device", "npme_gpu_direct_sum_device_noalloc",
     "npme_gpu_calcv_exact_real", "npme_gpu_calcv_exact_complex",
     "npme_gpu_count_pairs", "npme_gpu_set_timing", "npme_gpu_get_info",
     "npme_gpu_last_error",
@@ -99,6 +99,7 @@ def load_library():
         getattr(L, f).argtypes = [vp, dp, sz, dp, dp]
     L.npme_gpu_calcv_device.argtypes = [vp, vp, vp, vp]
     L.npme_gpu_direct_sum_device.argtypes = [vp, vp, vp, vp]
+    L.npme_gpu_direct_sum_device_noalloc.argtypes = [vp, vp, vp, vp]
     L.npme_gpu_set_timing.argtypes = [vp, ctypes.c_int]
     L.npme_gpu_count_pairs.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.npme_gpu_get_info.argtypes = [vp, ctypes.POINTER(Info)]
@@ -208,6 +209,13 @@ class Solver:
     def direct_sum_device(self, V_ptr, q_ptr, stream_ptr=None):
         """Short-range direct sum alone (no self term) on device pointers."""
         self._check(self.L.npme_gpu_direct_sum_device(
+            self.h, ctypes.c_void_p(V_ptr), ctypes.c_void_p(q_ptr),
+            ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def direct_sum_device_noalloc(self, V_ptr, q_ptr, stream_ptr=None):
+        """The direct sum through the entry point that allocates nothing (its
+        scratch is a static device array; see include/npme_gpu.h)."""
+        self._check(self.L.npme_gpu_direct_sum_device_noalloc(
             self.h, ctypes.c_void_p(V_ptr), ctypes.c_void_p(q_ptr),
             ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 
