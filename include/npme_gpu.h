@@ -111,6 +111,15 @@ void npme_gpu_default_params(npme_params *p);
 /* Validates p and creates a handle on p->device.  No geometry yet. */
 int npme_gpu_create(const npme_params *p, npme_handle **out);
 
+/* Replaces the parameters of a handle (kernel, splitting, Rdir, B-spline
+ * order, FFT box, precision ...; not the device).  Waits for the handle's
+ * enqueued work, keeps its device buffers and takes its FFT plans from the
+ * process-wide plan cache at the next setup, which must follow before CalcV.
+ * No counterpart in the reference, whose interface objects are set up once;
+ * it lets a server reuse one handle for requests with different
+ * parameters.  On error the old parameters stay in force. */
+int npme_gpu_set_params(npme_handle *h, const npme_params *p);
+
 /* SetUp / ResetCoord: bins and sorts the points, builds the kernel transform,
  * the FFT plans and all work buffers.  coord is a host pointer. */
 int npme_gpu_setup(npme_handle *h, size_t n, const double *coord);
@@ -154,6 +163,24 @@ int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_char
  * the GPU race.  Output and arguments as npme_gpu_direct_sum_device. */
 int npme_gpu_direct_sum_device_noalloc(npme_handle *h, double *d_V,
                                        const double *d_charge, void *stream);
+
+/* Batched CalcV (no counterpart in the reference, which evaluates one system
+ * per call): runs CalcV for `count` set-up handles of the same device in one
+ * pass, one kernel launch per stage and launch class (same B-spline order,
+ * same pair-kernel coefficients), FFTs per system.  Sizes, kernels, orders and
+ * FFT boxes may differ between members.  d_V[i] / d_charge[i] are device
+ * buffers laid out as for npme_gpu_calcv_device.  Enqueued on `stream`
+ * (NULL: the default stream); the direct sums run on the batch's second
+ * stream, joined before the interpolation.  A member handle must not be set
+ * up again, nor used in another batch, before npme_gpu_batch_sync returns. */
+typedef struct npme_batch npme_batch;
+int npme_gpu_batch_create(int device, npme_batch **out);
+int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *handles, int count,
+                         double *const *d_V, const double *const *d_charge,
+                         void *stream);
+int npme_gpu_batch_sync(npme_batch *b);
+int npme_gpu_batch_last_error(const npme_batch *b, char *buf, size_t len);
+int npme_gpu_batch_destroy(npme_batch *b);
 
 /* CalcV_exact: O(N^2) sum with the full kernel (FP64), host buffers. */
 int npme_gpu_calcv_exact_real(npme_handle *h, double *V, size_t n,

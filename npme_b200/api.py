@@ -63,10 +63,12 @@ STAGES = ("gather", "spread", "fft", "multiply", "ifft", "direct", "interp", "to
 
 # Every symbol include/npme_gpu.h declares.
 EXPORTS = (
-    "npme_gpu_default_params", "npme_gpu_create", "npme_gpu_setup",
+    "npme_gpu_default_params", "npme_gpu_create", "npme_gpu_set_params", "npme_gpu_setup",
     "npme_gpu_calcv_real", "npme_gpu_calcv_complex", "npme_gpu_calcv_device",
     "npme_gpu_direct_sum_device", "npme_gpu_direct_sum_device_noalloc",
     "npme_gpu_calcv_exact_real", "npme_gpu_calcv_exact_complex",
+    "npme_gpu_batch_create", "npme_gpu_calcv_batch", "npme_gpu_batch_sync",
+    "npme_gpu_batch_last_error", "npme_gpu_batch_destroy",
     "npme_gpu_count_pairs", "npme_gpu_set_timing", "npme_gpu_get_info",
     "npme_gpu_last_error",
     "npme_gpu_destroy",
@@ -100,6 +102,12 @@ def load_library():
     L.npme_gpu_calcv_device.argtypes = [vp, vp, vp, vp]
     L.npme_gpu_direct_sum_device.argtypes = [vp, vp, vp, vp]
     L.npme_gpu_direct_sum_device_noalloc.argtypes = [vp, vp, vp, vp]
+    L.npme_gpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    L.npme_gpu_calcv_batch.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int,
+                                       ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
+    L.npme_gpu_batch_sync.argtypes = [vp]
+    L.npme_gpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, sz]
+    L.npme_gpu_batch_destroy.argtypes = [vp]
     L.npme_gpu_set_timing.argtypes = [vp, ctypes.c_int]
     L.npme_gpu_count_pairs.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.npme_gpu_get_info.argtypes = [vp, ctypes.POINTER(Info)]
@@ -169,6 +177,14 @@ class Solver:
     def _check(self, rc):
         if rc:
             raise _err(self.L, self.h, rc)
+
+    def set_params(self, params):
+        """New parameters for this handle (same device); setup must follow."""
+        self._check(self.L.npme_gpu_set_params(self.h, ctypes.byref(params)))
+        self.p = params
+        self.complex = params.funcType == FUNC["helmholtz"]
+        self.n = 0
+        return self
 
     def setup(self, coord):
         c = np.ascontiguousarray(coord, dtype=np.float64).reshape(-1, 3)
@@ -258,3 +274,47 @@ class Solver:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Batch:
+    """Batched CalcV over many set-up Solvers (npme_gpu_calcv_batch)."""
+
+    def __init__(self, device=0):
+        self.L = load_library()
+        b = ctypes.c_void_p()
+        rc = self.L.npme_gpu_batch_create(device, ctypes.byref(b))
+        if rc:
+            raise NPMEError(rc, "batch create failed")
+        self.b = b
+
+    def _err(self, rc):
+        buf = ctypes.create_string_buffer(1024)
+        self.L.npme_gpu_batch_last_error(self.b, buf, 1024)
+        return NPMEError(rc, buf.value.decode(errors="replace"))
+
+    def calcv(self, solvers, V_ptrs, q_ptrs, stream_ptr=None):
+        """Enqueues CalcV for every solver; pointers are device addresses."""
+        n = len(solvers)
+        H = (ctypes.c_void_p * n)(*[s.h.value for s in solvers])
+        Vp = (ctypes.c_void_p * n)(*V_ptrs)
+        Qp = (ctypes.c_void_p * n)(*q_ptrs)
+        rc = self.L.npme_gpu_calcv_batch(self.b, H, n, Vp, Qp,
+                                         ctypes.c_void_p(stream_ptr) if stream_ptr else None)
+        if rc:
+            raise self._err(rc)
+
+    def sync(self):
+        rc = self.L.npme_gpu_batch_sync(self.b)
+        if rc:
+            raise self._err(rc)
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.npme_gpu_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,309 @@
+// Device bodies of the per-call kernels, shared by the single-system kernels
+// (recsum.cu, direct.cu) and the multi-system batch kernels (batch.cu).  Each
+// body processes one unit of work (one point, one brick, one spectrum
+// element, one warp group) of one system; the kernels only map threads to
+// (system, unit).
+#pragma once
+
+#include "internal.h"
+
+namespace npme {
+
+constexpr int kGroupWarps = 4;  // warps per CTA of the FP32 direct sum
+#ifndef NPME_DIRECT_UNROLL
+#define NPME_DIRECT_UNROLL 8
+#endif
+constexpr int kDirectUnroll = NPME_DIRECT_UNROLL;  // pair-loop unroll factor
+
+// Charges into brick order (spread/interp) and direct-sum order.
+template <typename T, bool CPLX>
+__device__ __forceinline__ void gather_body(const double *__restrict__ q,
+                                            const BrickPoint<T> *__restrict__ bp,
+                                            const uint32_t *__restrict__ cperm,
+                                            T *__restrict__ qb, T *__restrict__ qc, long i) {
+  const uint32_t ob = bp[i].orig, oc = cperm[i];
+  if (CPLX) {
+    qb[2 * i] = (T)q[2 * (long)ob];
+    qb[2 * i + 1] = (T)q[2 * (long)ob + 1];
+    qc[2 * i] = (T)q[2 * (long)oc];
+    qc[2 * i + 1] = (T)q[2 * (long)oc + 1];
+  } else {
+    qb[i] = (T)q[ob];
+    qc[i] = (T)q[oc];
+  }
+}
+
+// Spread of one brick by the whole CTA (src/RecSumQ.cpp:184-314): the
+// brick's points accumulate their p^3 stencils into the shared tile of
+// (kBrick + P - 1)^3 grid points, which is then added to the global grid.
+template <typename T, int P, bool CPLX>
+__device__ __forceinline__ void spread_brick_body(int brick, const int *__restrict__ brick_start,
+                                                  const BrickPoint<T> *__restrict__ bp,
+                                                  const T *__restrict__ q, T *__restrict__ grid,
+                                                  int nb2, int nb3, long N1, long N2, long N3,
+                                                  T *tile) {
+  constexpr int TL = kBrick + P - 1;
+  constexpr int TV = TL * TL * TL;
+  constexpr int C = CPLX ? 2 : 1;
+  const int b3 = brick % nb3, b2 = (brick / nb3) % nb2, b1 = brick / (nb3 * nb2);
+  for (int t = threadIdx.x; t < TV * C; t += blockDim.x) tile[t] = T(0);
+  __syncthreads();
+  const int beg = brick_start[brick], end = brick_start[brick + 1];
+  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const BrickPoint<T> pt = bp[i];
+    T w1[P], w2[P], w3[P], dummy[P];
+    bspline_weights<T, P, false>(pt.u[0], w1, dummy);
+    bspline_weights<T, P, false>(pt.u[1], w2, dummy);
+    bspline_weights<T, P, false>(pt.u[2], w3, dummy);
+    const int l1 = (int)(pt.g0 >> 20) - b1 * kBrick;
+    const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
+    const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
+    T qr = q[C * (long)i], qi = CPLX ? q[2 * (long)i + 1] : T(0);
+#pragma unroll
+    for (int t1 = 0; t1 < P; t1++) {
+#pragma unroll
+      for (int t2 = 0; t2 < P; t2++) {
+        const T c12 = w1[t1] * w2[t2];
+        T *row = tile + C * (((l1 + t1) * TL + (l2 + t2)) * TL + l3);
+#pragma unroll
+        for (int t3 = 0; t3 < P; t3++) {
+          const T c = c12 * w3[t3];
+          atomicAdd(row + C * t3, c * qr);
+          if (CPLX) atomicAdd(row + C * t3 + 1, c * qi);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const long g1 = (long)b1 * kBrick, g2 = (long)b2 * kBrick, g3 = (long)b3 * kBrick;
+  for (int t = threadIdx.x; t < TV; t += blockDim.x) {
+    const int i3 = t % TL, i2 = (t / TL) % TL, i1 = t / (TL * TL);
+    if (g1 + i1 >= N1) continue;
+    if (g2 + i2 >= N2 || g3 + i3 >= N3) continue;  // beyond the box: always zero
+    const long gi = ((g1 + i1) * N2 + (g2 + i2)) * N3 + (g3 + i3);
+    if (CPLX) {
+      const T vr = tile[2 * t], vi = tile[2 * t + 1];
+      if (vr != T(0)) atomicAdd(grid + 2 * gi, vr);
+      if (vi != T(0)) atomicAdd(grid + 2 * gi + 1, vi);
+    } else {
+      const T v = tile[t];
+      if (v != T(0)) atomicAdd(grid + gi, v);
+    }
+  }
+}
+
+// X(k) *= G(|k1|, |k2|, k3) on the R2C half spectrum (src/RecSumV.cpp:639-707).
+template <typename T>
+__device__ __forceinline__ void multiply_real_body(typename Vec2<T>::type *__restrict__ X,
+                                                   const T *__restrict__ G, long idx, long N1,
+                                                   long N2, long N3h, int M2, int M3) {
+  const long k3 = idx % N3h, k2 = (idx / N3h) % N2, k1 = idx / (N3h * N2);
+  const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
+  const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
+  const T g = __ldg(G + (f1 * M2 + f2) * M3 + k3);
+  typename Vec2<T>::type v = X[idx];
+  v.x *= g;
+  v.y *= g;
+  X[idx] = v;
+}
+
+// X(k) *= G(|k1|, |k2|, |k3|) on the full complex spectrum.
+template <typename T>
+__device__ __forceinline__ void multiply_cplx_body(typename Vec2<T>::type *__restrict__ X,
+                                                   const typename Vec2<T>::type *__restrict__ G,
+                                                   long idx, long N1, long N2, long N3, int M2,
+                                                   int M3) {
+  const long k3 = idx % N3, k2 = (idx / N3) % N2, k1 = idx / (N3 * N2);
+  const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
+  const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
+  const long f3 = k3 <= N3 / 2 ? k3 : N3 - k3;
+  const typename Vec2<T>::type g = G[(f1 * M2 + f2) * M3 + f3];
+  typename Vec2<T>::type v = X[idx], o;
+  o.x = v.x * g.x - v.y * g.y;
+  o.y = v.x * g.y + v.y * g.x;
+  X[idx] = o;
+}
+
+// Interpolation of one point (src/RecSumV.cpp:201-306): V += sum theta B B B,
+// grad += (N/L) sum theta dB ..., added into the caller-order output.
+template <typename T, int P, bool CPLX>
+__device__ __forceinline__ void interp_body(const BrickPoint<T> &pt, const T *__restrict__ theta,
+                                            double *__restrict__ V, long N2, long N3, T c1, T c2,
+                                            T c3) {
+  constexpr int C = CPLX ? 2 : 1;
+  T w1[P], w2[P], w3[P], d1[P], d2[P], d3[P];
+  bspline_weights<T, P, true>(pt.u[0], w1, d1);
+  bspline_weights<T, P, true>(pt.u[1], w2, d2);
+  bspline_weights<T, P, true>(pt.u[2], w3, d3);
+  const long g1 = pt.g0 >> 20, g2 = (pt.g0 >> 10) & 1023u, g3 = pt.g0 & 1023u;
+  T v[4] = {0, 0, 0, 0}, vi[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int t1 = 0; t1 < P; t1++) {
+#pragma unroll
+    for (int t2 = 0; t2 < P; t2++) {
+      const T *row = theta + C * (((g1 + t1) * N2 + (g2 + t2)) * N3 + g3);
+      T tb = 0, td = 0, tbi = 0, tdi = 0;
+#pragma unroll
+      for (int t3 = 0; t3 < P; t3++) {
+        const T th = __ldg(row + C * t3);
+        tb = fma(th, w3[t3], tb);
+        td = fma(th, d3[t3], td);
+        if (CPLX) {
+          const T thi = __ldg(row + C * t3 + 1);
+          tbi = fma(thi, w3[t3], tbi);
+          tdi = fma(thi, d3[t3], tdi);
+        }
+      }
+      const T A1 = w1[t1] * w2[t2], A2 = d1[t1] * w2[t2], A3 = w1[t1] * d2[t2];
+      v[0] = fma(A1, tb, v[0]);
+      v[1] = fma(A2, tb, v[1]);
+      v[2] = fma(A3, tb, v[2]);
+      v[3] = fma(A1, td, v[3]);
+      if (CPLX) {
+        vi[0] = fma(A1, tbi, vi[0]);
+        vi[1] = fma(A2, tbi, vi[1]);
+        vi[2] = fma(A3, tbi, vi[2]);
+        vi[3] = fma(A1, tdi, vi[3]);
+      }
+    }
+  }
+  const T sc[4] = {T(1), c1, c2, c3};
+  const long o = pt.orig;
+  if (CPLX) {
+    double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      double2 a = Vo[m];
+      a.x += (double)(v[m] * sc[m]);
+      a.y += (double)(vi[m] * sc[m]);
+      Vo[m] = a;
+    }
+  } else {
+    double4 *Vo = reinterpret_cast<double4 *>(V) + o;
+    double4 a = *Vo;
+    a.x += (double)v[0];
+    a.y += (double)(v[1] * c1);
+    a.z += (double)(v[2] * c2);
+    a.w += (double)(v[3] * c3);
+    *Vo = a;
+  }
+}
+
+// FP32 direct sum of one warp group (see direct.cu for the scheme).  sp and
+// slo are this warp's 32-entry shared staging arrays.
+template <bool CPLX, int FUNC, int SPLIT, int ND>
+__device__ __forceinline__ void direct_group_body(
+    const PairCoef<float> &k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
+    const int4 G, const double4 c, const int2 *__restrict__ segs,
+    const uint32_t *__restrict__ perm, float refine2, double fself_r, double fself_i,
+    double *__restrict__ V, float4 *sp, float4 *slo, int lane) {
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  // idle lanes sit far outside the cutoff
+  float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f;
+  if (active) {
+    const double4 p = gpos[ti];
+    const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+    tx = (float)dx, ty = (float)dy, tz = (float)dz;
+    tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
+  }
+  const float R2 = k.R2;
+  double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
+
+  // register prefetch of the next chunk: lane l holds source l of the chunk
+  int seg = G.z, off = 0, pcnt = 0;
+  double px = 0, py = 0, pz = 0;
+  float pq = 0.f, pqi = 0.f;
+#define NPME_PREFETCH(SG, OF)                                  \
+  {                                                            \
+    const int2 S_ = segs[SG];                                  \
+    pcnt = min(32, S_.y - (OF));                               \
+    if (lane < pcnt) {                                         \
+      const long j_ = (long)S_.x + (OF) + lane;                \
+      const double4 p_ = gpos[j_];                             \
+      px = p_.x, py = p_.y, pz = p_.z;                         \
+      if (CPLX) {                                              \
+        pq = qg[2 * j_];                                       \
+        pqi = qg[2 * j_ + 1];                                  \
+      } else {                                                 \
+        pq = qg[j_];                                           \
+      }                                                        \
+    }                                                          \
+  }
+  if (seg < G.w) NPME_PREFETCH(seg, 0);
+  while (seg < G.w) {
+    __syncwarp();
+    if (lane < pcnt) {
+      const double dx = px - c.x, dy = py - c.y, dz = pz - c.z;
+      const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+      sp[lane] = make_float4(hx, hy, hz, pq);
+      slo[lane] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy),
+                              (float)(dz - (double)hz), pqi);
+    }
+    __syncwarp();
+    const int cnt = pcnt;
+    off += 32;
+    if (off >= segs[seg].y) {
+      seg++;
+      off = 0;
+    }
+    if (seg < G.w) NPME_PREFETCH(seg, off);
+    float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
+#pragma unroll kDirectUnroll
+    for (int s = 0; s < cnt; s++) {
+      const float4 src = sp[s];
+      float x = tx - src.x, y = ty - src.y, z = tz - src.z;
+      float r2 = fmaf(x, x, fmaf(y, y, z * z));
+      if (r2 <= R2 && r2 > 0.f) {
+        if (r2 < refine2) {  // close pair: exact difference from head + residual
+          const float4 lo = slo[s];
+          x += tlx - lo.x;
+          y += tly - lo.y;
+          z += tlz - lo.z;
+          r2 = fmaf(x, x, fmaf(y, y, z * z));
+        }
+        if (!CPLX) {
+          float f1;
+          const float f0 = pair_sr_real<float, FUNC, SPLIT, ND>(k, r2, f1);
+          const float gq = f1 * src.w;
+          p0 = fmaf(f0, src.w, p0);
+          p1 = fmaf(gq, x, p1);
+          p2 = fmaf(gq, y, p2);
+          p3 = fmaf(gq, z, p3);
+        } else {
+          float f0r, f0i, f1r, f1i;
+          pair_sr_helmholtz<float, ND>(k, r2, f0r, f0i, f1r, f1i);
+          const float qr = src.w, qi = slo[s].w;
+          p0 = fmaf(f0r, qr, fmaf(-f0i, qi, p0));
+          p0i = fmaf(f0r, qi, fmaf(f0i, qr, p0i));
+          const float gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
+          p1 = fmaf(gr, x, p1);
+          p2 = fmaf(gr, y, p2);
+          p3 = fmaf(gr, z, p3);
+          p1i = fmaf(gi, x, p1i);
+          p2i = fmaf(gi, y, p2i);
+          p3i = fmaf(gi, z, p3i);
+        }
+      }
+    }
+    acc[0] += p0, acc[1] += p1, acc[2] += p2, acc[3] += p3;
+    if (CPLX) acci[0] += p0i, acci[1] += p1i, acci[2] += p2i, acci[3] += p3i;
+  }
+#undef NPME_PREFETCH
+  if (active) {
+    const long o = perm[ti];
+    if (CPLX) {
+      const double qr = qg[2 * (long)ti], qi = qg[2 * (long)ti + 1];
+      acc[0] -= fself_r * qr - fself_i * qi;  // src/Interface.cpp:2909-2910
+      acci[0] -= fself_r * qi + fself_i * qr;
+      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+#pragma unroll
+      for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
+    } else {
+      acc[0] -= fself_r * (double)qg[ti];  // src/Interface.cpp:2061-2062
+      reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+    }
+  }
+}
+
+}  // namespace npme

@@ -15,6 +15,7 @@
 
 #include <cmath>
 
+#include "bodies.cuh"
 #include "internal.h"
 
 namespace npme {
@@ -186,12 +187,6 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
 // this, a pair at r ~ 0.01 in a group of radius ~2 carries a ~1e-5 relative
 // error that dominates the gradient.
 
-constexpr int kGroupWarps = 4;
-#ifndef NPME_DIRECT_UNROLL
-#define NPME_DIRECT_UNROLL 8
-#endif
-constexpr int kDirectUnroll = NPME_DIRECT_UNROLL;  // pair-loop unroll factor
-
 template <bool CPLX, int FUNC, int SPLIT, int ND>
 __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
     PairCoef<float> k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
@@ -203,117 +198,10 @@ __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long g = (long)blockIdx.x * kGroupWarps + wid;
   if (g >= ngroups) return;  // warp-uniform; nothing below synchronises the block
-  const int4 G = groups[g];
-  const double4 c = gcen[g];
-  const int ti = G.x + lane;
-  const bool active = lane < G.y;
-  // idle lanes sit far outside the cutoff
-  float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f;
-  if (active) {
-    const double4 p = gpos[ti];
-    const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
-    tx = (float)dx, ty = (float)dy, tz = (float)dz;
-    tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
-  }
-  const float R2 = k.R2;
-  double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
-
-  // register prefetch of the next chunk: lane l holds source l of the chunk
-  int seg = G.z, off = 0, pcnt = 0;
-  double px = 0, py = 0, pz = 0;
-  float pq = 0.f, pqi = 0.f;
-#define NPME_PREFETCH(SG, OF)                                  \
-  {                                                            \
-    const int2 S_ = segs[SG];                                  \
-    pcnt = min(32, S_.y - (OF));                               \
-    if (lane < pcnt) {                                         \
-      const long j_ = (long)S_.x + (OF) + lane;                \
-      const double4 p_ = gpos[j_];                             \
-      px = p_.x, py = p_.y, pz = p_.z;                         \
-      if (CPLX) {                                              \
-        pq = qg[2 * j_];                                       \
-        pqi = qg[2 * j_ + 1];                                  \
-      } else {                                                 \
-        pq = qg[j_];                                           \
-      }                                                        \
-    }                                                          \
-  }
-  if (seg < G.w) NPME_PREFETCH(seg, 0);
-  while (seg < G.w) {
-    __syncwarp();
-    if (lane < pcnt) {
-      const double dx = px - c.x, dy = py - c.y, dz = pz - c.z;
-      const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
-      sp[wid][lane] = make_float4(hx, hy, hz, pq);
-      slo[wid][lane] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy),
-                                   (float)(dz - (double)hz), pqi);
-    }
-    __syncwarp();
-    const int cnt = pcnt;
-    off += 32;
-    if (off >= segs[seg].y) {
-      seg++;
-      off = 0;
-    }
-    if (seg < G.w) NPME_PREFETCH(seg, off);
-    float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
-#pragma unroll kDirectUnroll
-    for (int s = 0; s < cnt; s++) {
-      const float4 src = sp[wid][s];
-      float x = tx - src.x, y = ty - src.y, z = tz - src.z;
-      float r2 = fmaf(x, x, fmaf(y, y, z * z));
-      if (r2 <= R2 && r2 > 0.f) {
-        if (r2 < refine2) {  // close pair: exact difference from head + residual
-          const float4 lo = slo[wid][s];
-          x += tlx - lo.x;
-          y += tly - lo.y;
-          z += tlz - lo.z;
-          r2 = fmaf(x, x, fmaf(y, y, z * z));
-        }
-        if (!CPLX) {
-          float f1;
-          const float f0 = pair_sr_real<float, FUNC, SPLIT, ND>(k, r2, f1);
-          const float gq = f1 * src.w;
-          p0 = fmaf(f0, src.w, p0);
-          p1 = fmaf(gq, x, p1);
-          p2 = fmaf(gq, y, p2);
-          p3 = fmaf(gq, z, p3);
-        } else {
-          float f0r, f0i, f1r, f1i;
-          pair_sr_helmholtz<float, ND>(k, r2, f0r, f0i, f1r, f1i);
-          const float qr = src.w, qi = slo[wid][s].w;
-          p0 = fmaf(f0r, qr, fmaf(-f0i, qi, p0));
-          p0i = fmaf(f0r, qi, fmaf(f0i, qr, p0i));
-          const float gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
-          p1 = fmaf(gr, x, p1);
-          p2 = fmaf(gr, y, p2);
-          p3 = fmaf(gr, z, p3);
-          p1i = fmaf(gi, x, p1i);
-          p2i = fmaf(gi, y, p2i);
-          p3i = fmaf(gi, z, p3i);
-        }
-      }
-    }
-    acc[0] += p0, acc[1] += p1, acc[2] += p2, acc[3] += p3;
-    if (CPLX) acci[0] += p0i, acci[1] += p1i, acci[2] += p2i, acci[3] += p3i;
-  }
-  if (active) {
-    const long o = perm[ti];
-    if (CPLX) {
-      const double qr = qg[2 * (long)ti], qi = qg[2 * (long)ti + 1];
-      acc[0] -= fself_r * qr - fself_i * qi;  // src/Interface.cpp:2909-2910
-      acci[0] -= fself_r * qi + fself_i * qr;
-      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
-#pragma unroll
-      for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
-    } else {
-      acc[0] -= fself_r * (double)qg[ti];  // src/Interface.cpp:2061-2062
-      reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
-    }
-  }
+  direct_group_body<CPLX, FUNC, SPLIT, ND>(k, gpos, qg, groups[g], gcen[g], segs, perm, refine2,
+                                           fself_r, fself_i, V, sp[wid], slo[wid], lane);
 }
 
-#undef NPME_PREFETCH
 
 template <bool CPLX, int FUNC, int SPLIT, int ND>
 static void groups_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {

@@ -5,6 +5,8 @@
 #include <cufft.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -46,6 +48,14 @@ struct Timing {
   cudaEvent_t ev[10] = {};
 };
 
+// A cuFFT plan shared by every handle with the same FFT box and type (fft.cu).
+struct FFTPlan {
+  cufftHandle plan = 0;
+  int type = 0;
+  size_t work = 0;  // work-area bytes the caller provides
+  std::mutex mu;    // guards stream / work-area binding + enqueue
+};
+
 }  // namespace npme
 
 struct npme_handle {
@@ -69,8 +79,8 @@ struct npme_handle {
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;  // direct sum runs here, overlapped with the FFTs
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cufftHandle plan_fwd = 0, plan_inv = 0;
-  bool plans = false;
+  npme::FFTPlan *pf = nullptr, *pi = nullptr;  // shared plans (not owned)
+  void *d_work = nullptr;                        // this handle's cuFFT work area
 
   // device buffers (all allocated in setup; calcv allocates nothing)
   double *d_coord = nullptr;     // original order, FP64 (exact sum, FP64 direct)
@@ -91,6 +101,12 @@ struct npme_handle {
   double *d_V_exact = nullptr;
   int *d_err = nullptr;          // device error flag
   size_t dev_bytes = 0;
+  std::map<void *, size_t> caps;  // pointer field -> capacity of its buffer
+  // kernel-transform construction scratch (kept to reuse across set-ups)
+  double2 *d_ft0 = nullptr, *d_ft1 = nullptr;
+  double *d_fax[3] = {nullptr, nullptr, nullptr};
+  double *d_flam[3] = {nullptr, nullptr, nullptr};
+  double *d_fcos[3] = {nullptr, nullptr, nullptr};
 
   // FP32 direct sum: warp groups of <= 32 z-sorted points of one xy column
   // and, per group, the source segments (neighbour-column z ranges) that can
@@ -111,6 +127,14 @@ struct npme_handle {
 };
 
 namespace npme {
+
+// npme_gpu.cu: capacity-tracked device buffer owned by the handle
+int handle_buffer(npme_handle *h, void **field, size_t bytes);
+
+// fft.cu
+int prepare_plans(npme_handle *h);
+int fft_forward(npme_handle *h, cudaStream_t s);
+int fft_inverse(npme_handle *h, cudaStream_t s);
 
 // recsum.cu
 int build_kernel_transform(npme_handle *h);  // F-hat, lambda^2 -> d_G

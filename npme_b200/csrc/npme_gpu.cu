@@ -109,40 +109,52 @@ double min_x_compact(double X0, double del, long order, long N) {
 long start_index(double w) { return w < 0 ? (long)(-w) + 1 : (long)(-w); }
 
 void release(npme_handle *h) {
-  if (h->plans) {
-    cufftDestroy(h->plan_fwd);
-    if (h->plan_inv != h->plan_fwd) cufftDestroy(h->plan_inv);
-    h->plans = false;
+  h->pf = h->pi = nullptr;  // shared plans stay in the process-wide cache
+  // every device buffer was obtained through dalloc, which records the
+  // address of the pointer field it fills
+  for (auto &kv : h->caps) {
+    void **field = (void **)kv.first;
+    if (*field) cudaFree(*field);
+    *field = nullptr;
   }
-  void *bufs[] = {h->d_coord, h->d_bpts, h->d_brick_start, h->d_brick_list, h->d_cpos,
-                  h->d_cperm, h->d_cell_start, h->d_qb, h->d_qc, h->d_grid, h->d_kgrid,
-                  h->d_theta, h->d_G, h->d_q_in, h->d_V, h->d_V_exact, h->d_err};
-  for (void *b : bufs)
-    if (b) cudaFree(b);
-  h->d_coord = nullptr, h->d_bpts = nullptr, h->d_brick_start = nullptr;
-  h->d_brick_list = nullptr, h->d_cpos = nullptr, h->d_cperm = nullptr;
-  h->d_cell_start = nullptr, h->d_qb = nullptr, h->d_qc = nullptr, h->d_grid = nullptr;
-  h->d_kgrid = nullptr, h->d_theta = nullptr, h->d_G = nullptr, h->d_q_in = nullptr;
-  h->d_V = nullptr, h->d_V_exact = nullptr, h->d_err = nullptr;
-  void *gbufs[] = {h->d_gpos, h->d_groups, h->d_gcen, h->d_segs};
-  for (void *b : gbufs)
-    if (b) cudaFree(b);
-  h->d_gpos = nullptr, h->d_groups = nullptr, h->d_gcen = nullptr, h->d_segs = nullptr;
+  h->caps.clear();
   h->n_groups = h->n_segs = 0;
   h->dev_bytes = 0;
   h->ready = false;
 }
 
+// Device buffer of at least `bytes`: reused when the handle already holds a
+// large enough one (set-up of a new geometry on the same handle allocates
+// only what grew), otherwise freed and allocated again.
 template <typename P>
 int dalloc(npme_handle *h, P **ptr, size_t bytes) {
   if (bytes == 0) bytes = 16;
+  size_t &cap = h->caps[(void *)ptr];
+  if (*ptr && cap >= bytes) return NPME_OK;
+  if (*ptr) {
+    cudaFree(*ptr);
+    h->dev_bytes -= cap;
+    *ptr = nullptr;
+    cap = 0;
+  }
   cudaError_t e = cudaMalloc((void **)ptr, bytes);
-  if (e != cudaSuccess)
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
     return fail(h, NPME_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
                                     " bytes failed: " + cudaGetErrorString(e));
+  }
+  cap = bytes;
   h->dev_bytes += bytes;
   return NPME_OK;
 }
+
+}  // namespace
+
+int npme::handle_buffer(npme_handle *h, void **field, size_t bytes) {
+  return dalloc(h, field, bytes);
+}
+
+namespace {
 
 // Warp groups for the FP32 direct sum.  Points are binned into xy columns of
 // edge ~(32 / density)^(1/3) and sorted by z inside each column; each run of
@@ -182,18 +194,26 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
     int c1 = std::min(nc[1] - 1, std::max(0, (int)((coord[3 * i + 1] - mn[1]) / edge[1])));
     col[i] = c0 * nc[1] + c1;
   }
-  order.resize(n);
-  for (size_t i = 0; i < n; i++) order[i] = (uint32_t)i;
-  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-    if (col[a] != col[b]) return col[a] < col[b];
-    if (coord[3 * a + 2] != coord[3 * b + 2]) return coord[3 * a + 2] < coord[3 * b + 2];
-    return a < b;
-  });
+  // counting sort by column (stable), then each column by (z, index)
   std::vector<long> cstart(ncol + 1, 0);
   for (size_t i = 0; i < n; i++) cstart[col[i] + 1]++;
   for (long c = 0; c < ncol; c++) cstart[c + 1] += cstart[c];
+  order.resize(n);
+  {
+    std::vector<long> fill(cstart.begin(), cstart.end() - 1);
+    for (size_t i = 0; i < n; i++) order[fill[col[i]]++] = (uint32_t)i;
+  }
   std::vector<double> zs(n);
-  for (size_t k = 0; k < n; k++) zs[k] = coord[3 * (size_t)order[k] + 2];
+  {
+    std::vector<std::pair<double, uint32_t>> zc;
+    for (long c = 0; c < ncol; c++) {
+      const long b = cstart[c], e1 = cstart[c + 1];
+      zc.resize(e1 - b);
+      for (long k = b; k < e1; k++) zc[k - b] = {coord[3 * (size_t)order[k] + 2], order[k]};
+      std::sort(zc.begin(), zc.end());
+      for (long k = b; k < e1; k++) zs[k] = zc[k - b].first, order[k] = zc[k - b].second;
+    }
+  }
 
   std::vector<int4> groups;
   std::vector<double4> cen;
@@ -378,24 +398,6 @@ int upload_points(npme_handle *h, const double *coord) {
   return NPME_OK;
 }
 
-int make_plans(npme_handle *h) {
-  const long *N = h->grid.N;
-  const int n0 = (int)N[0], n1 = (int)N[1], n2 = (int)N[2];
-  if (h->complex_kernel) {
-    CKFFT(cufftPlan3d(&h->plan_fwd, n0, n1, n2, h->fp32 ? CUFFT_C2C : CUFFT_Z2Z));
-    h->plan_inv = h->plan_fwd;
-  } else {
-    CKFFT(cufftPlan3d(&h->plan_fwd, n0, n1, n2, h->fp32 ? CUFFT_R2C : CUFFT_D2Z));
-    cufftResult r = cufftPlan3d(&h->plan_inv, n0, n1, n2, h->fp32 ? CUFFT_C2R : CUFFT_Z2D);
-    if (r != CUFFT_SUCCESS) {
-      cufftDestroy(h->plan_fwd);
-      return fail(h, NPME_ECUDA, "cufftPlan3d (inverse) failed: " + std::to_string((int)r));
-    }
-  }
-  h->plans = true;
-  return NPME_OK;
-}
-
 int check_params(npme_handle *h, const npme_params &p) {
   if (!(p.Rdir > 0)) return fail(h, NPME_EINVAL, "Rdir must be > 0");
   if (p.funcType < 0 || p.funcType > 2) return fail(h, NPME_EINVAL, "unknown funcType");
@@ -420,6 +422,41 @@ int check_params(npme_handle *h, const npme_params &p) {
   if (p.precision != NPME_PREC_FP32 && p.precision != NPME_PREC_FP64)
     return fail(h, NPME_EINVAL, "unknown precision");
   return NPME_OK;
+}
+
+// Derived state of the parameters: kernel kind, precision and the splitting
+// coefficients (host FP64).
+int apply_params(npme_handle *h) {
+  h->complex_kernel = h->p.funcType == NPME_FUNC_HELMHOLTZ;
+  h->fp32 = h->p.precision == NPME_PREC_FP32;
+  memset(h->a_r, 0, sizeof(h->a_r));
+  memset(h->a_i, 0, sizeof(h->a_i));
+  memset(h->b_r, 0, sizeof(h->b_r));
+  memset(h->b_i, 0, sizeof(h->b_i));
+  h->beta = 0;
+  if (h->p.EwaldSplit == NPME_SPLIT_DERIVMATCH) {
+    std::complex<double> a[32], b[32];
+    dm_coefficients(h->p, a, b);
+    for (int i = 0; i <= h->p.nDeriv; i++) {
+      h->a_r[i] = a[i].real(), h->a_i[i] = a[i].imag();
+      h->b_r[i] = b[i].real(), h->b_i[i] = b[i].imag();
+    }
+    // f_LR(0) = a[0] (src/Interface.cpp:1946-1952)
+    h->fself_r = h->a_r[0];
+    h->fself_i = h->a_i[0];
+  } else {
+    h->beta = orig_beta(h->p.Rdir, h->p.tol);
+    if (h->beta <= 0) return fail(h, NPME_EINVAL, "original-Ewald beta did not converge");
+    h->fself_r = 2.0 * h->beta / std::sqrt(M_PI);  // beta erf(beta r)/(beta r) at r = 0
+    h->fself_i = 0;
+  }
+  return NPME_OK;
+}
+
+void fill_default_del(npme_params &p) {
+  if (p.del1 <= 0) p.del1 = p.Rdir;
+  if (p.del2 <= 0) p.del2 = p.Rdir;
+  if (p.del3 <= 0) p.del3 = p.Rdir;
 }
 
 }  // namespace
@@ -452,9 +489,7 @@ int npme_gpu_create(const npme_params *p, npme_handle **out) {
   npme_handle *h = new (std::nothrow) npme_handle;
   if (!h) return fail(nullptr, NPME_ENOMEM, "host allocation failed");
   h->p = *p;
-  if (h->p.del1 <= 0) h->p.del1 = h->p.Rdir;
-  if (h->p.del2 <= 0) h->p.del2 = h->p.Rdir;
-  if (h->p.del3 <= 0) h->p.del3 = h->p.Rdir;
+  fill_default_del(h->p);
   int rc = check_params(h, h->p);
   if (rc) {
     set_global_err(h->err);
@@ -462,8 +497,6 @@ int npme_gpu_create(const npme_params *p, npme_handle **out) {
     return rc;
   }
   h->device = p->device;
-  h->complex_kernel = p->funcType == NPME_FUNC_HELMHOLTZ;
-  h->fp32 = p->precision == NPME_PREC_FP32;
   cudaError_t e = cudaSetDevice(h->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
@@ -475,32 +508,35 @@ int npme_gpu_create(const npme_params *p, npme_handle **out) {
     delete h;
     return NPME_ECUDA;
   }
-  // coefficients of the splitting (host FP64)
-  memset(h->a_r, 0, sizeof(h->a_r));
-  memset(h->a_i, 0, sizeof(h->a_i));
-  memset(h->b_r, 0, sizeof(h->b_r));
-  memset(h->b_i, 0, sizeof(h->b_i));
-  if (h->p.EwaldSplit == NPME_SPLIT_DERIVMATCH) {
-    std::complex<double> a[32], b[32];
-    dm_coefficients(h->p, a, b);
-    for (int i = 0; i <= h->p.nDeriv; i++) {
-      h->a_r[i] = a[i].real(), h->a_i[i] = a[i].imag();
-      h->b_r[i] = b[i].real(), h->b_i[i] = b[i].imag();
-    }
-    // f_LR(0) = a[0] (src/Interface.cpp:1946-1952)
-    h->fself_r = h->a_r[0];
-    h->fself_i = h->a_i[0];
-  } else {
-    h->beta = orig_beta(h->p.Rdir, h->p.tol);
-    if (h->beta <= 0) {
-      set_global_err("original-Ewald beta did not converge");
-      npme_gpu_destroy(h);
-      return NPME_EINVAL;
-    }
-    h->fself_r = 2.0 * h->beta / std::sqrt(M_PI);  // beta erf(beta r)/(beta r) at r = 0
-    h->fself_i = 0;
+  if ((rc = apply_params(h))) {
+    set_global_err(h->err);
+    npme_gpu_destroy(h);
+    return rc;
   }
   *out = h;
+  return NPME_OK;
+}
+
+int npme_gpu_set_params(npme_handle *h, const npme_params *p) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!p) return fail(h, NPME_EINVAL, "null params");
+  if (p->device != h->device) return fail(h, NPME_EINVAL, "set_params cannot change the device");
+  npme_params q = *p;
+  fill_default_del(q);
+  int rc = check_params(h, q);
+  if (rc) return rc;
+  CK(cudaSetDevice(h->device));
+  // work already enqueued may still read the handle's buffers and plans
+  if (h->stream) CK(cudaStreamSynchronize(h->stream));
+  if (h->stream2) CK(cudaStreamSynchronize(h->stream2));
+  const npme_params old = h->p;
+  h->p = q;
+  if ((rc = apply_params(h))) {
+    h->p = old;
+    apply_params(h);
+    return rc;
+  }
+  h->ready = false;  // buffers and plans are kept; setup rebuilds the rest
   return NPME_OK;
 }
 
@@ -510,7 +546,13 @@ int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
   if (n == 0) return fail(h, NPME_EINVAL, "nCharge must be > 0");
   if (n >= (size_t)1 << 31) return fail(h, NPME_EINVAL, "nCharge must be < 2^31");
   CK(cudaSetDevice(h->device));
-  release(h);
+  // A handle that was set up before keeps its buffers (grown when needed),
+  // its FFT plans (the FFT box is a handle parameter) and its kernel-transform
+  // scratch: only the geometry-dependent state is rebuilt (ResetCoord,
+  // src/Interface.cpp:1958-1987).
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->stream2) cudaStreamSynchronize(h->stream2);
+  h->ready = false;
   h->n = n;
   const npme_params &p = h->p;
   // box (src/RecSumSupportFunctions.cpp:182-201, 276-296)
@@ -557,7 +599,7 @@ int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
     release(h);
     return rc;
   }
-  if ((rc = make_plans(h))) {
+  if ((rc = npme::prepare_plans(h))) {
     release(h);
     return rc;
   }
@@ -595,39 +637,12 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   CK(cudaMemsetAsync(h->d_grid, 0, gbytes, s));
   npme::launch_spread(h, s);
   tmark(h, 2, s);
-  CKFFT(cufftSetStream(h->plan_fwd, s));
-  if (h->plan_inv != h->plan_fwd) CKFFT(cufftSetStream(h->plan_inv, s));
-  if (h->complex_kernel) {
-    if (h->fp32)
-      CKFFT(cufftExecC2C(h->plan_fwd, (cufftComplex *)h->d_grid, (cufftComplex *)h->d_grid,
-                         CUFFT_FORWARD));
-    else
-      CKFFT(cufftExecZ2Z(h->plan_fwd, (cufftDoubleComplex *)h->d_grid,
-                         (cufftDoubleComplex *)h->d_grid, CUFFT_FORWARD));
-  } else {
-    if (h->fp32)
-      CKFFT(cufftExecR2C(h->plan_fwd, (cufftReal *)h->d_grid, (cufftComplex *)h->d_kgrid));
-    else
-      CKFFT(cufftExecD2Z(h->plan_fwd, (cufftDoubleReal *)h->d_grid,
-                         (cufftDoubleComplex *)h->d_kgrid));
-  }
+  int frc = npme::fft_forward(h, s);
+  if (frc) return frc;
   tmark(h, 3, s);
   npme::launch_multiply(h, s);
   tmark(h, 4, s);
-  if (h->complex_kernel) {
-    if (h->fp32)
-      CKFFT(cufftExecC2C(h->plan_inv, (cufftComplex *)h->d_grid, (cufftComplex *)h->d_grid,
-                         CUFFT_INVERSE));
-    else
-      CKFFT(cufftExecZ2Z(h->plan_inv, (cufftDoubleComplex *)h->d_grid,
-                         (cufftDoubleComplex *)h->d_grid, CUFFT_INVERSE));
-  } else {
-    if (h->fp32)
-      CKFFT(cufftExecC2R(h->plan_inv, (cufftComplex *)h->d_kgrid, (cufftReal *)h->d_grid));
-    else
-      CKFFT(cufftExecZ2D(h->plan_inv, (cufftDoubleComplex *)h->d_kgrid,
-                         (cufftDoubleReal *)h->d_grid));
-  }
+  if ((frc = npme::fft_inverse(h, s))) return frc;
   tmark(h, 5, s);
   CK(cudaStreamWaitEvent(s, h->ev_join, 0));
   tmark(h, 6, s);

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <vector>
 
+#include "bodies.cuh"
 #include "internal.h"
 
 namespace npme {
@@ -234,71 +235,61 @@ int build_kernel_transform(npme_handle *h) {
   k.k0i = h->p.k0_i;
   for (int i = 0; i <= k.nder && i < 32; i++) k.ar[i] = h->a_r[i], k.ai[i] = h->a_i[i];
 
-  const long maxN = std::max(N[0], std::max(N[1], N[2]));
-  double *d_ax[3] = {nullptr, nullptr, nullptr}, *d_l[3] = {nullptr, nullptr, nullptr};
-  double *d_cos = nullptr;
-  double2 *d_F = nullptr, *d_F2 = nullptr;
+  // scratch kept by the handle, so a new geometry on the same handle reuses it
   int rc = NPME_OK;
-  auto cleanup = [&]() {
-    for (int d = 0; d < 3; d++) cudaFree(d_ax[d]), cudaFree(d_l[d]);
-    cudaFree(d_cos);
-    cudaFree(d_F);
-    cudaFree(d_F2);
-  };
-  do {
-    bool fail = false;
-    for (int d = 0; d < 3 && !fail; d++) {
-      fail |= cudaMalloc(&d_ax[d], sizeof(double) * ax[d].size()) != cudaSuccess;
-      fail |= cudaMalloc(&d_l[d], sizeof(double) * lam[d].size()) != cudaSuccess;
-    }
-    fail |= cudaMalloc(&d_cos, sizeof(double) * maxN) != cudaSuccess;
-    fail |= cudaMalloc(&d_F, sizeof(double2) * MT) != cudaSuccess;
-    fail |= cudaMalloc(&d_F2, sizeof(double2) * MT) != cudaSuccess;
-    if (fail) {
-      h->err = "cudaMalloc failed while building the kernel transform";
-      rc = NPME_ENOMEM;
-      break;
-    }
-    for (int d = 0; d < 3; d++) {
-      cudaMemcpy(d_ax[d], ax[d].data(), sizeof(double) * ax[d].size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(d_l[d], lam[d].data(), sizeof(double) * lam[d].size(), cudaMemcpyHostToDevice);
-    }
-    const int threads = 256, blocks = 148 * 8;
-    sample_fhat_kernel<<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, d_ax[0], d_ax[1],
-                                                          d_ax[2], d_F);
-    double2 *src = d_F, *dst = d_F2;
-    for (int d = 0; d < 3; d++) {
-      std::vector<double> cs(N[d]);
-      for (long m = 0; m < N[d]; m++) cs[m] = std::cos(2.0 * M_PI * (double)m / (double)N[d]);
-      cudaMemcpyAsync(d_cos, cs.data(), sizeof(double) * N[d], cudaMemcpyHostToDevice, h->stream);
-      dct1_axis_kernel<<<blocks, threads, 0, h->stream>>>(src, dst, M1, M2, M3, d, (int)N[d], d_cos);
-      cudaStreamSynchronize(h->stream);  // cs is reused for the next axis
-      std::swap(src, dst);
-    }
-    const double inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);
-    if (h->fp32) {
-      if (h->complex_kernel)
-        scale_fhat_kernel<float, true><<<blocks, threads, 0, h->stream>>>(
-            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (float *)h->d_G);
-      else
-        scale_fhat_kernel<float, false><<<blocks, threads, 0, h->stream>>>(
-            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (float *)h->d_G);
-    } else {
-      if (h->complex_kernel)
-        scale_fhat_kernel<double, true><<<blocks, threads, 0, h->stream>>>(
-            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (double *)h->d_G);
-      else
-        scale_fhat_kernel<double, false><<<blocks, threads, 0, h->stream>>>(
-            src, M1, M2, M3, d_l[0], d_l[1], d_l[2], inv_vol, (double *)h->d_G);
-    }
-    cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) {
-      h->err = std::string("kernel transform: ") + cudaGetErrorString(e);
-      rc = NPME_ECUDA;
-    }
-  } while (0);
-  cleanup();
+  if ((rc = handle_buffer(h, (void **)&h->d_ft0, sizeof(double2) * MT)) ||
+      (rc = handle_buffer(h, (void **)&h->d_ft1, sizeof(double2) * MT)))
+    return rc;
+  for (int d = 0; d < 3; d++) {
+    if ((rc = handle_buffer(h, (void **)&h->d_fax[d], sizeof(double) * ax[d].size())) ||
+        (rc = handle_buffer(h, (void **)&h->d_flam[d], sizeof(double) * lam[d].size())) ||
+        (rc = handle_buffer(h, (void **)&h->d_fcos[d], sizeof(double) * N[d])))
+      return rc;
+  }
+  std::vector<double> cs[3];
+  for (int d = 0; d < 3; d++) {
+    cs[d].resize(N[d]);
+    for (long m = 0; m < N[d]; m++) cs[d][m] = std::cos(2.0 * M_PI * (double)m / (double)N[d]);
+    cudaMemcpyAsync(h->d_fax[d], ax[d].data(), sizeof(double) * ax[d].size(),
+                    cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_flam[d], lam[d].data(), sizeof(double) * lam[d].size(),
+                    cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_fcos[d], cs[d].data(), sizeof(double) * N[d], cudaMemcpyHostToDevice,
+                    h->stream);
+  }
+  const int threads = 256, blocks = 148 * 8;
+  sample_fhat_kernel<<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, h->d_fax[0], h->d_fax[1],
+                                                        h->d_fax[2], h->d_ft0);
+  double2 *src = h->d_ft0, *dst = h->d_ft1;
+  for (int d = 0; d < 3; d++) {
+    dct1_axis_kernel<<<blocks, threads, 0, h->stream>>>(src, dst, M1, M2, M3, d, (int)N[d],
+                                                        h->d_fcos[d]);
+    std::swap(src, dst);
+  }
+  const double inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);
+  double *const *l = h->d_flam;
+  if (h->fp32) {
+    if (h->complex_kernel)
+      scale_fhat_kernel<float, true><<<blocks, threads, 0, h->stream>>>(
+          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (float *)h->d_G);
+    else
+      scale_fhat_kernel<float, false><<<blocks, threads, 0, h->stream>>>(
+          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (float *)h->d_G);
+  } else {
+    if (h->complex_kernel)
+      scale_fhat_kernel<double, true><<<blocks, threads, 0, h->stream>>>(
+          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (double *)h->d_G);
+    else
+      scale_fhat_kernel<double, false><<<blocks, threads, 0, h->stream>>>(
+          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (double *)h->d_G);
+  }
+  // the host vectors above are read by the asynchronous copies: wait here
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    h->err = std::string("kernel transform: ") + cudaGetErrorString(e);
+    rc = NPME_ECUDA;
+  }
   return rc;
 }
 
@@ -311,18 +302,8 @@ __global__ void gather_kernel(const double *__restrict__ q, const BrickPoint<T> 
                               const uint32_t *__restrict__ cperm, T *__restrict__ qb,
                               T *__restrict__ qc, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x) {
-    const uint32_t ob = bp[i].orig, oc = cperm[i];
-    if (CPLX) {
-      qb[2 * i] = (T)q[2 * (long)ob];
-      qb[2 * i + 1] = (T)q[2 * (long)ob + 1];
-      qc[2 * i] = (T)q[2 * (long)oc];
-      qc[2 * i + 1] = (T)q[2 * (long)oc + 1];
-    } else {
-      qb[i] = (T)q[ob];
-      qc[i] = (T)q[oc];
-    }
-  }
+       i += (long)gridDim.x * blockDim.x)
+    gather_body<T, CPLX>(q, bp, cperm, qb, qc, i);
 }
 
 void launch_gather_charges(npme_handle *h, const double *d_q, cudaStream_t s) {
@@ -401,57 +382,9 @@ __global__ void __launch_bounds__(256) spread_kernel(
     const int *__restrict__ brick_list, const int *__restrict__ brick_start,
     const BrickPoint<T> *__restrict__ bp, const T *__restrict__ q, T *__restrict__ grid,
     int nb2, int nb3, long N1, long N2, long N3) {
-  constexpr int TL = kBrick + P - 1;
-  constexpr int TV = TL * TL * TL;
-  constexpr int C = CPLX ? 2 : 1;
   extern __shared__ unsigned char smem_raw[];
-  T *tile = reinterpret_cast<T *>(smem_raw);
-  const int brick = brick_list[blockIdx.x];
-  const int b3 = brick % nb3, b2 = (brick / nb3) % nb2, b1 = brick / (nb3 * nb2);
-  for (int t = threadIdx.x; t < TV * C; t += blockDim.x) tile[t] = T(0);
-  __syncthreads();
-  const int beg = brick_start[brick], end = brick_start[brick + 1];
-  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
-    const BrickPoint<T> pt = bp[i];
-    T w1[P], w2[P], w3[P], dummy[P];
-    bspline_weights<T, P, false>(pt.u[0], w1, dummy);
-    bspline_weights<T, P, false>(pt.u[1], w2, dummy);
-    bspline_weights<T, P, false>(pt.u[2], w3, dummy);
-    const int l1 = (int)(pt.g0 >> 20) - b1 * kBrick;
-    const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
-    const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
-    T qr = q[C * (long)i], qi = CPLX ? q[2 * (long)i + 1] : T(0);
-#pragma unroll
-    for (int t1 = 0; t1 < P; t1++) {
-#pragma unroll
-      for (int t2 = 0; t2 < P; t2++) {
-        const T c12 = w1[t1] * w2[t2];
-        T *row = tile + C * (((l1 + t1) * TL + (l2 + t2)) * TL + l3);
-#pragma unroll
-        for (int t3 = 0; t3 < P; t3++) {
-          const T c = c12 * w3[t3];
-          atomicAdd(row + C * t3, c * qr);
-          if (CPLX) atomicAdd(row + C * t3 + 1, c * qi);
-        }
-      }
-    }
-  }
-  __syncthreads();
-  const long g1 = (long)b1 * kBrick, g2 = (long)b2 * kBrick, g3 = (long)b3 * kBrick;
-  for (int t = threadIdx.x; t < TV; t += blockDim.x) {
-    const int i3 = t % TL, i2 = (t / TL) % TL, i1 = t / (TL * TL);
-    if (g1 + i1 >= N1) continue;
-    if (g2 + i2 >= N2 || g3 + i3 >= N3) continue;  // beyond the box: always zero
-    const long gi = ((g1 + i1) * N2 + (g2 + i2)) * N3 + (g3 + i3);
-    if (CPLX) {
-      const T vr = tile[2 * t], vi = tile[2 * t + 1];
-      if (vr != T(0)) atomicAdd(grid + 2 * gi, vr);
-      if (vi != T(0)) atomicAdd(grid + 2 * gi + 1, vi);
-    } else {
-      const T v = tile[t];
-      if (v != T(0)) atomicAdd(grid + gi, v);
-    }
-  }
+  spread_brick_body<T, P, CPLX>(brick_list[blockIdx.x], brick_start, bp, q, grid, nb2, nb3, N1,
+                                N2, N3, reinterpret_cast<T *>(smem_raw));
 }
 
 template <typename T, bool CPLX, int P>
@@ -501,16 +434,8 @@ __global__ void multiply_real_kernel(typename Vec2<T>::type *__restrict__ X,
                                      int M2, int M3) {
   const long total = N1 * N2 * N3h;
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x) {
-    const long k3 = idx % N3h, k2 = (idx / N3h) % N2, k1 = idx / (N3h * N2);
-    const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
-    const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
-    const T g = __ldg(G + (f1 * M2 + f2) * M3 + k3);
-    typename Vec2<T>::type v = X[idx];
-    v.x *= g;
-    v.y *= g;
-    X[idx] = v;
-  }
+       idx += (long)gridDim.x * blockDim.x)
+    multiply_real_body<T>(X, G, idx, N1, N2, N3h, M2, M3);
 }
 
 template <typename T>
@@ -519,17 +444,8 @@ __global__ void multiply_cplx_kernel(typename Vec2<T>::type *__restrict__ X,
                                      long N2, long N3, int M2, int M3) {
   const long total = N1 * N2 * N3;
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x) {
-    const long k3 = idx % N3, k2 = (idx / N3) % N2, k1 = idx / (N3 * N2);
-    const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
-    const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
-    const long f3 = k3 <= N3 / 2 ? k3 : N3 - k3;
-    const typename Vec2<T>::type g = G[(f1 * M2 + f2) * M3 + f3];
-    typename Vec2<T>::type v = X[idx], o;
-    o.x = v.x * g.x - v.y * g.y;
-    o.y = v.x * g.y + v.y * g.x;
-    X[idx] = o;
-  }
+       idx += (long)gridDim.x * blockDim.x)
+    multiply_cplx_body<T>(X, G, idx, N1, N2, N3, M2, M3);
 }
 
 void launch_multiply(npme_handle *h, cudaStream_t s) {
@@ -565,67 +481,9 @@ template <typename T, int P, bool CPLX>
 __global__ void __launch_bounds__(256) interp_kernel(
     const BrickPoint<T> *__restrict__ bp, const T *__restrict__ theta, double *__restrict__ V,
     long n, long N2, long N3, T c1, T c2, T c3) {
-  constexpr int C = CPLX ? 2 : 1;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x) {
-    const BrickPoint<T> pt = bp[i];
-    T w1[P], w2[P], w3[P], d1[P], d2[P], d3[P];
-    bspline_weights<T, P, true>(pt.u[0], w1, d1);
-    bspline_weights<T, P, true>(pt.u[1], w2, d2);
-    bspline_weights<T, P, true>(pt.u[2], w3, d3);
-    const long g1 = pt.g0 >> 20, g2 = (pt.g0 >> 10) & 1023u, g3 = pt.g0 & 1023u;
-    T v[4] = {0, 0, 0, 0}, vi[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int t1 = 0; t1 < P; t1++) {
-#pragma unroll
-      for (int t2 = 0; t2 < P; t2++) {
-        const T *row = theta + C * (((g1 + t1) * N2 + (g2 + t2)) * N3 + g3);
-        T tb = 0, td = 0, tbi = 0, tdi = 0;
-#pragma unroll
-        for (int t3 = 0; t3 < P; t3++) {
-          const T th = __ldg(row + C * t3);
-          tb = fma(th, w3[t3], tb);
-          td = fma(th, d3[t3], td);
-          if (CPLX) {
-            const T thi = __ldg(row + C * t3 + 1);
-            tbi = fma(thi, w3[t3], tbi);
-            tdi = fma(thi, d3[t3], tdi);
-          }
-        }
-        const T A1 = w1[t1] * w2[t2], A2 = d1[t1] * w2[t2], A3 = w1[t1] * d2[t2];
-        v[0] = fma(A1, tb, v[0]);
-        v[1] = fma(A2, tb, v[1]);
-        v[2] = fma(A3, tb, v[2]);
-        v[3] = fma(A1, td, v[3]);
-        if (CPLX) {
-          vi[0] = fma(A1, tbi, vi[0]);
-          vi[1] = fma(A2, tbi, vi[1]);
-          vi[2] = fma(A3, tbi, vi[2]);
-          vi[3] = fma(A1, tdi, vi[3]);
-        }
-      }
-    }
-    const T sc[4] = {T(1), c1, c2, c3};
-    const long o = pt.orig;
-    if (CPLX) {
-      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
-#pragma unroll
-      for (int m = 0; m < 4; m++) {
-        double2 a = Vo[m];
-        a.x += (double)(v[m] * sc[m]);
-        a.y += (double)(vi[m] * sc[m]);
-        Vo[m] = a;
-      }
-    } else {
-      double4 *Vo = reinterpret_cast<double4 *>(V) + o;
-      double4 a = *Vo;
-      a.x += (double)v[0];
-      a.y += (double)(v[1] * c1);
-      a.z += (double)(v[2] * c2);
-      a.w += (double)(v[3] * c3);
-      *Vo = a;
-    }
-  }
+       i += (long)gridDim.x * blockDim.x)
+    interp_body<T, P, CPLX>(bp[i], theta, V, N2, N3, c1, c2, c3);
 }
 
 template <typename T, bool CPLX, int P>

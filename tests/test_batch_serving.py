@@ -1,0 +1,168 @@
+"""Batched CalcV, the continuous-batching server and the autotuner."""
+import numpy as np
+import pytest
+
+from conftest import rel
+import npme_b200
+from npme_b200 import api, autotune, serving
+
+
+def test_autotune_choices_are_valid():
+    for kern in ("laplace", "ralpha", "helmholtz"):
+        for n in (1000, 10_000, 200_000):
+            side = n ** (1 / 3)
+            ch = autotune.choose(kern, n, (side, side, side))
+            assert ch["table_errV"] * 5 <= 1e-5
+            assert ch["order"] in (6, 8, 10) and ch["Rdir"] > 0
+            for N in ch["grid"]:
+                assert N % 4 == 0 and ch["order"] < N // 4
+    # larger systems get larger grids, same spacing regime
+    a = autotune.choose("laplace", 2000, (12.6,) * 3)["grid"][0]
+    b = autotune.choose("laplace", 150_000, (53.1,) * 3)["grid"][0]
+    assert b > a
+
+
+def test_serving_stream_shape():
+    reqs = serving.serving_stream(count=64, seed=7)
+    assert len(reqs) == 64
+    assert all(1000 <= r.n <= 200_000 for r in reqs)
+    assert all(b.arrival >= a.arrival for a, b in zip(reqs, reqs[1:]))
+    kinds = {r.kernel for r in reqs}
+    assert kinds <= {"laplace", "ralpha", "helmholtz"}
+    for r in reqs:
+        if r.kernel != "helmholtz":
+            assert abs(r.q.sum()) < 1e-9 * r.n
+
+
+def _mixed_systems():
+    reqs = serving.serving_stream(count=12, n_min=1000, n_max=30_000, seed=11)
+    # force every kernel in the mix
+    for r, k in zip(reqs[:3], ("laplace", "ralpha", "helmholtz")):
+        if r.kernel != k:
+            g = np.random.Generator(np.random.Philox(r.rid))
+            r.kernel = k
+            r.q = (g.uniform(-1, 1, r.n) + 1j * g.uniform(-1, 1, r.n)) if k == "helmholtz" \
+                else g.uniform(-1, 1, r.n) - 0.0
+            if k != "helmholtz":
+                r.q -= r.q.mean()
+    return reqs
+
+
+@pytest.mark.gpu
+def test_batch_equals_single_system_path():
+    torch = pytest.importorskip("torch")
+    reqs = _mixed_systems()
+    solvers, dq, dV, alone = [], [], [], []
+    for r in reqs:
+        s = npme_b200.Solver(serving.params_for(r)).setup(r.coord)
+        solvers.append(s)
+        alone.append(s.calcv(r.q))
+        qv = np.ascontiguousarray(r.q)
+        dq.append(torch.from_numpy(qv.view(np.float64) if np.iscomplexobj(qv) else qv).cuda())
+        dV.append(torch.zeros((r.n, 8 if np.iscomplexobj(qv) else 4), dtype=torch.float64,
+                              device="cuda"))
+    b = api.Batch(0)
+    st = torch.cuda.Stream()
+    for _ in range(2):  # twice: the batch object reuses its buffers
+        b.calcv(solvers, [x.data_ptr() for x in dV], [x.data_ptr() for x in dq], st.cuda_stream)
+        b.sync()
+        st.synchronize()
+        for r, V, ref in zip(reqs, dV, alone):
+            got = V.cpu().numpy()
+            got = got.view(np.complex128) if np.iscomplexobj(r.q) else got
+            # spreading adds with float atomics, so the order of additions (and
+            # the last bits) may differ between runs
+            assert rel(got, ref) < 1e-6, r.rid
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_served_results_equal_alone_results():
+    pytest.importorskip("torch")
+    reqs = serving.serving_stream(count=40, n_min=1000, n_max=40_000, seed=13, rate=2000.0)
+    srv = serving.Server(max_batch=16, setup_workers=4)
+    stats = srv.run(reqs, realtime=True)
+    srv.close()
+    assert stats["requests"] == 40 and stats["batches"] >= 3
+    assert stats["p99_latency_s"] >= stats["p50_latency_s"] > 0
+    for r in reqs:
+        with npme_b200.Solver(serving.params_for(r)) as s:
+            alone = s.setup(r.coord).calcv(r.q)
+        assert rel(r.V, alone) < 1e-6, r.rid
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kern", ["laplace", "ralpha", "helmholtz"])
+def test_autotuned_solves_meet_the_accuracy_target(kern):
+    n = 6000
+    g = np.random.Generator(np.random.Philox(31))
+    c = g.random((n, 3)) * n ** (1 / 3)
+    if kern == "helmholtz":
+        q = g.uniform(-1, 1, n) + 1j * g.uniform(-1, 1, n)
+    else:
+        q = g.uniform(-1, 1, n)
+        q -= q.mean()
+    r = serving.Request(0, kern, c, q)
+    with npme_b200.Solver(serving.params_for(r)) as s:
+        V = s.setup(c).calcv(q)
+        Ve = s.calcv_exact(q)
+    assert rel(V[:, 0], Ve[:, 0]) < 1e-5
+
+
+@pytest.mark.gpu
+def test_set_params_retunes_a_handle():
+    """One handle taken through three parameter sets (kernel, order, FFT box
+    and precision change) gives the results of fresh handles."""
+    reqs = _mixed_systems()[:3]
+    precisions = ("fp32", "fp32", "fp64")
+    s = None
+    for r, prec in zip(reqs, precisions):
+        p = serving.params_for(r, precision=prec)
+        s = npme_b200.Solver(p) if s is None else s.set_params(p)
+        got = s.setup(r.coord).calcv(r.q)
+        with npme_b200.Solver(serving.params_for(r, precision=prec)) as fresh:
+            ref = fresh.setup(r.coord).calcv(r.q)
+        assert rel(got, ref) < (1e-6 if prec == "fp32" else 1e-12), (r.rid, prec)
+    # calcv before the setup that must follow set_params is refused
+    s.set_params(serving.params_for(reqs[0]))
+    with pytest.raises(api.NPMEError):
+        s.calcv(reqs[0].q)
+    s.close()
+
+
+def test_handle_pool_reuses_and_retunes(monkeypatch):
+    """Pool logic on the host: exact match first, then any free handle of the
+    same device and precision (given the new parameters), then a new one."""
+    made = []
+
+    class FakeSolver:
+        def __init__(self, p):
+            self.p, self.closed = p, False
+            made.append(self)
+
+        def set_params(self, p):
+            self.p = p
+            return self
+
+        def close(self):
+            self.closed = True
+
+    monkeypatch.setattr(api, "Solver", FakeSolver)
+    pool = serving.HandlePool(capacity=2)
+    pa = api.make_params("laplace", grid=(32, 32, 32), order=6)
+    pb = api.make_params("helmholtz", grid=(48, 48, 48), order=8, k0=0.5)
+    pc = api.make_params("laplace", grid=(32, 32, 32), order=6, precision="fp64")
+    a = pool.get(pa)
+    pool.put(a)
+    assert pool.get(pa) is a and pool.created == 1 and pool.retuned == 0
+    pool.put(a)
+    b = pool.get(pb)  # retuned from a
+    assert b is a and b.p is pb and pool.retuned == 1
+    c = pool.get(pc)  # nothing free of that precision
+    assert c is not a and pool.created == 2
+    pool.put(b), pool.put(c), pool.put(FakeSolver(pa))  # capacity 2: the third is closed
+    assert made[-1].closed and pool.count == 2
+    pool.close()
+    assert b.closed and c.closed and pool.count == 0

@@ -106,6 +106,21 @@ def test_permutation_invariance():
     assert rel(Vp, V[perm]) < 1e-12
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_reset_coord_reuses_the_handle(prec):
+    # ResetCoord semantics: one handle, several geometries of different size
+    base = SMALL["laplace_dm_4k"]
+    sizes = [4000, 1500, 6000, 2500]
+    with npme_b200.Solver(api.params_from_workload(base, precision=prec)) as s:
+        for k, n in enumerate(sizes):
+            w = dataclasses.replace(base, n=n, seed=900 + k)
+            c, q = w.generate()
+            V = s.setup(c).calcv(q)
+            with npme_b200.Solver(api.params_from_workload(w, precision=prec)) as fresh:
+                Vf = fresh.setup(c).calcv(q)
+            assert rel(V, Vf) < (1e-12 if prec == "fp64" else 1e-6)
+
+
 def test_inputs_not_modified():
     w = SMALL["laplace_dm_4k"]
     c, q = w.generate()
