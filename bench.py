@@ -217,7 +217,6 @@ def run_serving(args):
     warm = serving.serving_stream(count=24, n_max=20_000, seed=99, rate=1e4)
     srv = serving.Server(device=local)
     srv.run(warm, realtime=False)
-    srv.batches.clear()
     sampler = ClockSampler(local)
     sampler.start()
     stats = srv.run(mine, realtime=True)

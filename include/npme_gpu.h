@@ -182,6 +182,69 @@ int npme_gpu_batch_sync(npme_batch *b);
 int npme_gpu_batch_last_error(const npme_batch *b, char *buf, size_t len);
 int npme_gpu_batch_destroy(npme_batch *b);
 
+/* Serving queue (the submit/poll surface of a serving deployment; no
+ * counterpart in the reference, which evaluates one system per call).  A
+ * server owns one device; requests are independent systems, each with its
+ * own parameters, geometry and charges.  Requests are admitted in arrival
+ * order while the estimated device bytes of the requests in flight stay
+ * under hbm_budget; set-up threads prepare them on pooled handles (exact
+ * parameter match, else an idle handle given the new parameters, else a new
+ * one); a dispatch thread runs all prepared requests as one batched CalcV
+ * (npme_gpu_calcv_batch), writes each result into the caller's V and
+ * completes its ticket.  Thread-safe: any thread may submit, poll or wait.
+ * coord, charge and V are host buffers laid out as for npme_gpu_calcv_real /
+ * _complex; the caller keeps them alive and unchanged until the ticket is
+ * done or failed. */
+typedef struct npme_server npme_server;
+typedef struct {
+  int device;
+  int setup_threads;   /* host threads running set-up (default 8) */
+  int max_batch;       /* systems per batched CalcV (default 64) */
+  size_t hbm_budget;   /* device bytes in flight; 0: half the free memory */
+  int pool_capacity;   /* idle handles kept for reuse (default 64) */
+} npme_server_config;
+enum {
+  NPME_TICKET_QUEUED = 0,  /* waiting for admission */
+  NPME_TICKET_SETUP = 1,   /* being set up */
+  NPME_TICKET_READY = 2,   /* set up, waiting for the GPU */
+  NPME_TICKET_RUNNING = 3, /* in a batch on the GPU */
+  NPME_TICKET_DONE = 4,    /* V written */
+  NPME_TICKET_FAILED = 5   /* see npme_ticket_info.error */
+};
+typedef struct {
+  int state;            /* NPME_TICKET_* */
+  int status;           /* npme_status of a finished request */
+  double t_submit, t_admit, t_ready, t_done; /* seconds since server creation */
+  int batch_size;       /* requests in the batch that ran it */
+  size_t footprint;     /* estimated device bytes while in flight */
+  char error[256];
+} npme_ticket_info;
+typedef struct {
+  unsigned long long submitted, completed, failed;
+  unsigned long long batches, batched_requests;
+  unsigned long long handles_created, handles_retuned;
+  int idle_handles;
+  size_t in_flight_bytes, hbm_budget;
+  double clock_s;       /* seconds since server creation */
+} npme_server_stats;
+void npme_gpu_server_default_config(npme_server_config *c);
+int npme_gpu_server_create(const npme_server_config *c, npme_server **out);
+int npme_gpu_submit(npme_server *s, const npme_params *p, size_t n,
+                    const double *coord, const double *charge, double *V,
+                    unsigned long long *ticket);
+/* state <- NPME_TICKET_* of the ticket */
+int npme_gpu_poll(npme_server *s, unsigned long long ticket, int *state);
+/* Blocks until the ticket is done or failed (timeout_s < 0: no limit);
+ * returns the request's status, or NPME_ETIMEOUT. */
+int npme_gpu_wait(npme_server *s, unsigned long long ticket, double timeout_s);
+int npme_gpu_ticket_info(npme_server *s, unsigned long long ticket,
+                         npme_ticket_info *info);
+/* Forgets a finished ticket (NPME_ESTATE while it is in flight). */
+int npme_gpu_release_ticket(npme_server *s, unsigned long long ticket);
+int npme_gpu_server_stats(npme_server *s, npme_server_stats *st);
+/* Completes every submitted request, then frees the server and its handles. */
+int npme_gpu_server_destroy(npme_server *s);
+
 /* CalcV_exact: O(N^2) sum with the full kernel (FP64), host buffers. */
 int npme_gpu_calcv_exact_real(npme_handle *h, double *V, size_t n,
                               const double *charge, const double *coord);

@@ -59,6 +59,32 @@ class Info(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("setup_threads", ctypes.c_int),
+                ("max_batch", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
+                ("pool_capacity", ctypes.c_int)]
+
+
+class TicketInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_ready", ctypes.c_double), ("t_done", ctypes.c_double),
+                ("batch_size", ctypes.c_int), ("footprint", ctypes.c_size_t),
+                ("error", ctypes.c_char * 256)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_ulonglong), ("completed", ctypes.c_ulonglong),
+                ("failed", ctypes.c_ulonglong), ("batches", ctypes.c_ulonglong),
+                ("batched_requests", ctypes.c_ulonglong),
+                ("handles_created", ctypes.c_ulonglong),
+                ("handles_retuned", ctypes.c_ulonglong), ("idle_handles", ctypes.c_int),
+                ("in_flight_bytes", ctypes.c_size_t), ("hbm_budget", ctypes.c_size_t),
+                ("clock_s", ctypes.c_double)]
+
+
+TICKET_QUEUED, TICKET_SETUP, TICKET_READY, TICKET_RUNNING, TICKET_DONE, TICKET_FAILED = range(6)
+
 STAGES = ("gather", "spread", "fft", "multiply", "ifft", "direct", "interp", "total")
 
 # Every symbol include/npme_gpu.h declares.
@@ -72,7 +98,11 @@ EXPORTS = (
     "npme_gpu_count_pairs", "npme_gpu_set_timing", "npme_gpu_get_info",
     "npme_gpu_last_error",
     "npme_gpu_destroy",
+    "npme_gpu_server_default_config", "npme_gpu_server_create", "npme_gpu_submit",
+    "npme_gpu_poll", "npme_gpu_wait", "npme_gpu_ticket_info", "npme_gpu_release_ticket",
+    "npme_gpu_server_stats", "npme_gpu_server_destroy",
 )
+VOID_EXPORTS = ("npme_gpu_default_params", "npme_gpu_server_default_config")
 
 _lib = None
 
@@ -114,7 +144,7 @@ def load_library():
     L.npme_gpu_last_error.argtypes = [vp, ctypes.c_char_p, sz]
     L.npme_gpu_destroy.argtypes = [vp]
     for f in EXPORTS:
-        if f != "npme_gpu_default_params":
+        if f not in VOID_EXPORTS:
             getattr(L, f).restype = ctypes.c_int
     _lib = L
     return L
@@ -312,6 +342,93 @@ class Batch:
         if getattr(self, "b", None):
             self.L.npme_gpu_batch_destroy(self.b)
             self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NativeServer:
+    """The library's serving queue (npme_gpu_submit / poll / wait).
+
+    ``submit`` keeps references to the request's arrays until ``result``
+    releases the ticket, so the buffers outlive the work."""
+
+    def __init__(self, device=0, setup_threads=8, max_batch=64, hbm_budget=0,
+                 pool_capacity=64):
+        self.L = load_library()
+        c = ServerConfig()
+        self.L.npme_gpu_server_default_config(ctypes.byref(c))
+        c.device, c.setup_threads, c.max_batch = device, setup_threads, max_batch
+        c.hbm_budget, c.pool_capacity = int(hbm_budget), pool_capacity
+        s = ctypes.c_void_p()
+        rc = self.L.npme_gpu_server_create(ctypes.byref(c), ctypes.byref(s))
+        if rc:
+            raise NPMEError(rc, "server create failed")
+        self.s = s
+        self.keep = {}
+
+    def submit(self, params, coord, q):
+        c = np.ascontiguousarray(coord, dtype=np.float64).reshape(-1, 3)
+        cplx = params.funcType == FUNC["helmholtz"]
+        if cplx:
+            qb = np.ascontiguousarray(q, dtype=np.complex128).view(np.float64)
+        else:
+            qb = np.ascontiguousarray(q, dtype=np.float64)
+        V = np.empty((c.shape[0], 8 if cplx else 4), dtype=np.float64)
+        t = ctypes.c_ulonglong()
+        rc = self.L.npme_gpu_submit(self.s, ctypes.byref(params), c.shape[0], _dp(c), _dp(qb),
+                                    _dp(V), ctypes.byref(t))
+        if rc:
+            raise NPMEError(rc, "submit refused")
+        self.keep[t.value] = (params, c, qb, V, cplx)
+        return t.value
+
+    def poll(self, ticket):
+        st = ctypes.c_int()
+        rc = self.L.npme_gpu_poll(self.s, ctypes.c_ulonglong(ticket), ctypes.byref(st))
+        if rc:
+            raise NPMEError(rc, "unknown ticket")
+        return st.value
+
+    def info(self, ticket):
+        i = TicketInfo()
+        rc = self.L.npme_gpu_ticket_info(self.s, ctypes.c_ulonglong(ticket), ctypes.byref(i))
+        if rc:
+            raise NPMEError(rc, "unknown ticket")
+        return {"state": i.state, "status": i.status, "t_submit": i.t_submit,
+                "t_admit": i.t_admit, "t_ready": i.t_ready, "t_done": i.t_done,
+                "batch_size": i.batch_size, "footprint": i.footprint,
+                "error": i.error.decode(errors="replace")}
+
+    def wait(self, ticket, timeout=-1.0):
+        """Blocks until the ticket finishes; returns its status (or ETIMEOUT)."""
+        return self.L.npme_gpu_wait(self.s, ctypes.c_ulonglong(ticket), ctypes.c_double(timeout))
+
+    def result(self, ticket, timeout=-1.0):
+        """Waits, releases the ticket and returns (V, ticket info)."""
+        rc = self.wait(ticket, timeout)
+        if rc == ETIMEOUT:
+            raise NPMEError(rc, "timed out")
+        info = self.info(ticket)
+        self.L.npme_gpu_release_ticket(self.s, ctypes.c_ulonglong(ticket))
+        _, _, _, V, cplx = self.keep.pop(ticket)
+        if rc:
+            raise NPMEError(rc, info["error"])
+        return (V.view(np.complex128) if cplx else V), info
+
+    def stats(self):
+        st = ServerStats()
+        self.L.npme_gpu_server_stats(self.s, ctypes.byref(st))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "s", None):
+            self.L.npme_gpu_server_destroy(self.s)
+            self.s = None
+            self.keep.clear()
 
     def __del__(self):
         try:

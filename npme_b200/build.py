@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libnpme_gpu.so")
-SOURCES = ["npme_gpu.cu", "recsum.cu", "direct.cu", "noalloc.cu", "batch.cu", "fft.cu"]
+SOURCES = ["npme_gpu.cu", "recsum.cu", "direct.cu", "noalloc.cu", "batch.cu", "fft.cu",
+           "server.cu"]
 HEADERS = ["common.cuh", "bodies.cuh", "internal.h",
            os.path.join("..", "..", "include", "npme_gpu.h")]
 

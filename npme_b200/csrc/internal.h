@@ -81,6 +81,7 @@ struct npme_handle {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   npme::FFTPlan *pf = nullptr, *pi = nullptr;  // shared plans (not owned)
   void *d_work = nullptr;                        // this handle's cuFFT work area
+  cudaMemPool_t pool = nullptr;                  // device memory pool (shared, not owned)
 
   // device buffers (all allocated in setup; calcv allocates nothing)
   double *d_coord = nullptr;     // original order, FP64 (exact sum, FP64 direct)

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -108,15 +109,58 @@ double min_x_compact(double X0, double del, long order, long N) {
 // src/RecSumSupportFunctions.h:123-127
 long start_index(double w) { return w < 0 ? (long)(-w) + 1 : (long)(-w); }
 
+// Device memory of all handles comes from one stream-ordered pool per device
+// (cudaMallocFromPoolAsync / cudaFreeAsync on the handle's stream).  Unlike
+// cudaMalloc / cudaFree, neither synchronises the device, so a handle that
+// grows its buffers during set-up does not stall the CalcV of other handles
+// running meanwhile; freed blocks stay in the pool for the next handle.  The
+// pool returns its memory to the device when the last handle of the device
+// is destroyed.
+std::mutex g_pool_mu;
+std::map<int, std::pair<cudaMemPool_t, int>> g_pools;  // device -> (pool, live handles)
+
+int pool_acquire(npme_handle *h) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(h->device);
+  if (it == g_pools.end()) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = h->device;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess)
+      return fail(h, NPME_ECUDA, std::string("cudaMemPoolCreate: ") + cudaGetErrorString(e));
+    unsigned long long keep = ~0ull;  // keep freed blocks for reuse
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    it = g_pools.emplace(h->device, std::make_pair(pool, 0)).first;
+  }
+  it->second.second++;
+  h->pool = it->second.first;
+  return NPME_OK;
+}
+
+void pool_release(npme_handle *h) {
+  if (!h->pool) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(h->device);
+  if (it != g_pools.end() && --it->second.second == 0) cudaMemPoolTrimTo(it->second.first, 0);
+  h->pool = nullptr;
+}
+
+// Frees every device buffer of the handle (stream-ordered; the caller has
+// synchronised the handle's streams).
 void release(npme_handle *h) {
   h->pf = h->pi = nullptr;  // shared plans stay in the process-wide cache
   // every device buffer was obtained through dalloc, which records the
   // address of the pointer field it fills
   for (auto &kv : h->caps) {
     void **field = (void **)kv.first;
-    if (*field) cudaFree(*field);
+    if (*field) cudaFreeAsync(*field, h->stream);
     *field = nullptr;
   }
+  if (!h->caps.empty()) cudaStreamSynchronize(h->stream);
   h->caps.clear();
   h->n_groups = h->n_segs = 0;
   h->dev_bytes = 0;
@@ -125,22 +169,24 @@ void release(npme_handle *h) {
 
 // Device buffer of at least `bytes`: reused when the handle already holds a
 // large enough one (set-up of a new geometry on the same handle allocates
-// only what grew), otherwise freed and allocated again.
+// only what grew), otherwise freed and allocated again from the pool, in
+// the order of the handle's stream.
 template <typename P>
 int dalloc(npme_handle *h, P **ptr, size_t bytes) {
   if (bytes == 0) bytes = 16;
   size_t &cap = h->caps[(void *)ptr];
   if (*ptr && cap >= bytes) return NPME_OK;
   if (*ptr) {
-    cudaFree(*ptr);
+    cudaFreeAsync(*ptr, h->stream);
     h->dev_bytes -= cap;
     *ptr = nullptr;
     cap = 0;
   }
-  cudaError_t e = cudaMalloc((void **)ptr, bytes);
+  cudaError_t e = cudaMallocFromPoolAsync((void **)ptr, bytes, h->pool, h->stream);
   if (e != cudaSuccess) {
     *ptr = nullptr;
-    return fail(h, NPME_ENOMEM, "cudaMalloc of " + std::to_string(bytes) +
+    cudaGetLastError();
+    return fail(h, NPME_ENOMEM, "device allocation of " + std::to_string(bytes) +
                                     " bytes failed: " + cudaGetErrorString(e));
   }
   cap = bytes;
@@ -273,11 +319,14 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   if ((rc = dalloc(h, &h->d_groups, sizeof(int4) * groups.size()))) return rc;
   if ((rc = dalloc(h, &h->d_gcen, sizeof(double4) * cen.size()))) return rc;
   if ((rc = dalloc(h, &h->d_segs, sizeof(int2) * std::max<size_t>(1, segs.size())))) return rc;
-  CK(cudaMemcpy(h->d_gpos, gpos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_groups, groups.data(), sizeof(int4) * groups.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_gcen, cen.data(), sizeof(double4) * cen.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(h->d_gpos, gpos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_groups, groups.data(), sizeof(int4) * groups.size(),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_gcen, cen.data(), sizeof(double4) * cen.size(), cudaMemcpyHostToDevice,
+                     h->stream));
   if (!segs.empty())
-    CK(cudaMemcpy(h->d_segs, segs.data(), sizeof(int2) * segs.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->d_segs, segs.data(), sizeof(int2) * segs.size(), cudaMemcpyHostToDevice,
+                       h->stream));
   return NPME_OK;
 }
 
@@ -370,17 +419,19 @@ int upload_points(npme_handle *h, const double *coord) {
   if ((rc = dalloc(h, (T **)&h->d_qc, sizeof(T) * C * n))) return rc;
   if ((rc = dalloc(h, &h->d_q_in, sizeof(double) * C * n))) return rc;
   if ((rc = dalloc(h, &h->d_V, sizeof(double) * 4 * C * n))) return rc;
-  CK(cudaMemcpy(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_bpts, sorted.data(), sizeof(BrickPoint<T>) * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_brick_start, bstart.data(), sizeof(int) * (nbt + 1),
-                cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_bpts, sorted.data(), sizeof(BrickPoint<T>) * n, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->d_brick_start, bstart.data(), sizeof(int) * (nbt + 1),
+                     cudaMemcpyHostToDevice, h->stream));
   if (!blist.empty())
-    CK(cudaMemcpy(h->d_brick_list, blist.data(), sizeof(int) * blist.size(),
-                  cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_cpos, cpos.data(), sizeof(V4) * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_cperm, cperm.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_cell_start, cstart.data(), sizeof(int) * (ncell + 1),
-                cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->d_brick_list, blist.data(), sizeof(int) * blist.size(),
+                       cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_cpos, cpos.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_cperm, cperm.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->d_cell_start, cstart.data(), sizeof(int) * (ncell + 1),
+                     cudaMemcpyHostToDevice, h->stream));
 
   // --- grids ---
   const long *N = g.N;
@@ -505,8 +556,13 @@ int npme_gpu_create(const npme_params *p, npme_handle **out) {
   for (int i = 0; i < 10 && e == cudaSuccess; i++) e = cudaEventCreate(&h->timing.ev[i]);
   if (e != cudaSuccess) {
     set_global_err(std::string("CUDA initialisation failed: ") + cudaGetErrorString(e));
-    delete h;
+    npme_gpu_destroy(h);
     return NPME_ECUDA;
+  }
+  if ((rc = pool_acquire(h))) {
+    set_global_err(h->err);
+    npme_gpu_destroy(h);
+    return rc;
   }
   if ((rc = apply_params(h))) {
     set_global_err(h->err);
@@ -817,6 +873,7 @@ int npme_gpu_destroy(npme_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->stream2) cudaStreamSynchronize(h->stream2);
   release(h);
+  pool_release(h);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);

@@ -1,0 +1,457 @@
+// Native serving queue: npme_gpu_submit / npme_gpu_poll / npme_gpu_wait.
+//
+// A server owns one device.  Requests (parameters, geometry, charges and the
+// caller's output buffer) are admitted in arrival order while the estimated
+// device bytes of the requests in flight stay under the budget; set-up
+// threads bin and upload each admitted request on a pooled handle (exact
+// parameter match first, else an idle handle given the new parameters with
+// npme_gpu_set_params, else a new one) and upload its charges; one dispatch
+// thread runs every set-up request it finds as one batched CalcV
+// (npme_gpu_calcv_batch), copies each result into the caller's buffer and
+// completes the tickets.  Set-up of the next requests overlaps the batch on
+// the GPU.  All state is guarded by one mutex; the GPU work itself runs
+// outside it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  unsigned long long id = 0;
+  npme_params p;
+  size_t n = 0;
+  const double *coord = nullptr;
+  const double *charge = nullptr;
+  double *V = nullptr;
+  size_t footprint = 0;
+  int state = NPME_TICKET_QUEUED;
+  int status = NPME_OK;
+  std::string err;
+  npme_handle *h = nullptr;
+  double t_submit = 0, t_admit = 0, t_ready = 0, t_done = 0;
+  int batch_size = 0;
+};
+
+using Key = std::tuple<int, int, int, int, double, double, double, double, long, long, long, int>;
+
+Key key_of(const npme_params &p) {
+  return Key(p.funcType, p.EwaldSplit, p.BnOrder, p.nDeriv, p.Rdir, p.alpha, p.k0_r, p.k0_i,
+             p.N1, p.N2, p.N3, p.precision);
+}
+
+bool complex_kernel(const npme_params &p) { return p.funcType == NPME_FUNC_HELMHOLTZ; }
+
+// Device bytes a request holds while it is in flight: the spread grid and
+// spectrum, the kernel transform and its construction scratch, the per-point
+// records of the spreading and of the direct sum, charges and results.
+size_t footprint(const npme_params &p, size_t n) {
+  const size_t s = p.precision == NPME_PREC_FP32 ? 4 : 8;
+  const size_t cx = complex_kernel(p) ? 2 : 1;
+  const size_t N = (size_t)p.N1 * p.N2 * p.N3;
+  const size_t M = (size_t)(p.N1 / 2 + 1) * (p.N2 / 2 + 1) * (p.N3 / 2 + 1);
+  size_t grid = N * s * cx;
+  if (cx == 1) grid += (size_t)p.N1 * p.N2 * (p.N3 / 2 + 1) * 2 * s;
+  return grid + M * (s * cx + 32) + n * (260 + 40 * cx);
+}
+
+}  // namespace
+
+struct npme_server {
+  npme_server_config cfg;
+  Clock::time_point t0;
+  npme_batch *batch = nullptr;
+  cudaStream_t stream = nullptr;
+
+  std::mutex mu;
+  std::condition_variable cv_setup, cv_ready, cv_done;
+  bool stopping = false;
+  unsigned long long next_id = 1;
+  std::unordered_map<unsigned long long, Request *> tickets;
+  std::deque<Request *> waiting, admitted, ready;
+  size_t in_flight = 0;
+  std::map<Key, std::vector<npme_handle *>> idle;
+  int idle_count = 0;
+  npme_server_stats stats;
+  std::vector<std::thread> workers;
+  std::thread dispatcher;
+
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+  // Moves waiting requests to the set-up queue while the budget allows (a
+  // request larger than the budget runs alone).  Caller holds mu.
+  void admit() {
+    bool any = false;
+    while (!waiting.empty()) {
+      Request *r = waiting.front();
+      if (in_flight != 0 && in_flight + r->footprint > cfg.hbm_budget) break;
+      waiting.pop_front();
+      in_flight += r->footprint;
+      r->t_admit = now();
+      admitted.push_back(r);
+      any = true;
+    }
+    if (any) cv_setup.notify_all();
+  }
+
+  // An idle handle for parameters p: one with the same parameters if there
+  // is one (*exact), else any of the same precision.  Caller holds mu.
+  npme_handle *take_idle(const npme_params &p, bool *exact) {
+    auto it = idle.find(key_of(p));
+    if (it != idle.end() && !it->second.empty()) {
+      npme_handle *h = it->second.back();
+      it->second.pop_back();
+      idle_count--;
+      *exact = true;
+      return h;
+    }
+    for (auto &kv : idle) {
+      if (!kv.second.empty() && std::get<11>(kv.first) == p.precision) {
+        npme_handle *h = kv.second.back();
+        kv.second.pop_back();
+        idle_count--;
+        *exact = false;
+        return h;
+      }
+    }
+    return nullptr;
+  }
+
+  // Caller holds mu; returns the handle to destroy outside the lock, if any.
+  npme_handle *give_back(npme_handle *h) {
+    if (!h) return nullptr;
+    if (idle_count < cfg.pool_capacity) {
+      idle[key_of(h->p)].push_back(h);
+      idle_count++;
+      return nullptr;
+    }
+    return h;
+  }
+
+  // Completes a request.  Caller holds mu.
+  void finish(Request *r, int status, const std::string &msg) {
+    r->status = status;
+    r->err = msg;
+    r->state = status == NPME_OK ? NPME_TICKET_DONE : NPME_TICKET_FAILED;
+    r->t_done = now();
+    in_flight -= r->footprint;
+    if (status == NPME_OK) stats.completed++;
+    else stats.failed++;
+    admit();
+    cv_done.notify_all();
+  }
+
+  void setup_loop();
+  void dispatch_loop();
+};
+
+void npme_server::setup_loop() {
+  cudaSetDevice(cfg.device);
+  for (;;) {
+    Request *r;
+    npme_handle *h = nullptr;
+    bool exact = false;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      // on shutdown, stay until every request has been admitted and set up
+      cv_setup.wait(lk, [&] { return !admitted.empty() || (stopping && waiting.empty()); });
+      if (admitted.empty()) return;
+      r = admitted.front();
+      admitted.pop_front();
+      r->state = NPME_TICKET_SETUP;
+      h = take_idle(r->p, &exact);
+      if (!h) stats.handles_created++;
+      else if (!exact) stats.handles_retuned++;
+    }
+    int rc = NPME_OK;
+    std::string msg;
+    if (!h) {
+      rc = npme_gpu_create(&r->p, &h);
+      if (rc) {
+        char buf[512];
+        npme_gpu_last_error(nullptr, buf, sizeof buf);
+        msg = buf;
+        h = nullptr;
+      }
+    } else if (!exact) {
+      rc = npme_gpu_set_params(h, &r->p);
+      if (rc) msg = h->err;
+    }
+    if (!rc) {
+      rc = npme_gpu_setup(h, r->n, r->coord);
+      if (rc) msg = h->err;
+    }
+    if (!rc) {
+      const size_t words = (complex_kernel(r->p) ? 2 : 1) * r->n;
+      cudaError_t e = cudaMemcpyAsync(h->d_q_in, r->charge, sizeof(double) * words,
+                                      cudaMemcpyHostToDevice, h->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+      if (e != cudaSuccess) {
+        rc = NPME_ECUDA;
+        msg = std::string("charge upload: ") + cudaGetErrorString(e);
+      }
+    }
+    npme_handle *drop = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (rc) {
+        drop = give_back(h);
+        finish(r, rc, msg);
+      } else {
+        r->h = h;
+        r->t_ready = now();
+        r->state = NPME_TICKET_READY;
+        ready.push_back(r);
+        cv_ready.notify_one();
+      }
+    }
+    if (drop) npme_gpu_destroy(drop);
+  }
+}
+
+void npme_server::dispatch_loop() {
+  cudaSetDevice(cfg.device);
+  std::vector<Request *> rs;
+  std::vector<npme_handle *> hs;
+  std::vector<double *> dV;
+  std::vector<const double *> dq;
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv_ready.wait(lk, [&] {
+        return !ready.empty() ||
+               (stopping && waiting.empty() && admitted.empty() && in_flight == 0);
+      });
+      if (ready.empty()) return;
+      rs.clear();
+      while (!ready.empty() && (int)rs.size() < cfg.max_batch) {
+        rs.push_back(ready.front());
+        ready.pop_front();
+      }
+      for (Request *r : rs) r->state = NPME_TICKET_RUNNING;
+    }
+    hs.clear(), dV.clear(), dq.clear();
+    for (Request *r : rs) {
+      hs.push_back(r->h);
+      dV.push_back(r->h->d_V);
+      dq.push_back(r->h->d_q_in);
+    }
+    int rc = npme_gpu_calcv_batch(batch, hs.data(), (int)hs.size(), dV.data(), dq.data(), stream);
+    if (!rc) rc = npme_gpu_batch_sync(batch);
+    std::string msg;
+    if (rc) {
+      char buf[512];
+      npme_gpu_batch_last_error(batch, buf, sizeof buf);
+      msg = buf;
+    }
+    std::vector<int> rcs(rs.size(), rc);
+    if (!rc) {
+      for (size_t i = 0; i < rs.size(); i++) {
+        Request *r = rs[i];
+        const size_t words = (complex_kernel(r->p) ? 8 : 4) * r->n;
+        cudaError_t e = cudaMemcpyAsync(r->V, r->h->d_V, sizeof(double) * words,
+                                        cudaMemcpyDeviceToHost, stream);
+        if (e != cudaSuccess) rcs[i] = NPME_ECUDA;
+      }
+      cudaError_t e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) {
+        std::fill(rcs.begin(), rcs.end(), (int)NPME_ECUDA);
+        msg = std::string("result copy: ") + cudaGetErrorString(e);
+      }
+    }
+    std::vector<npme_handle *> drop;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stats.batches++;
+      stats.batched_requests += rs.size();
+      for (size_t i = 0; i < rs.size(); i++) {
+        Request *r = rs[i];
+        r->batch_size = (int)rs.size();
+        if (npme_handle *d = give_back(r->h)) drop.push_back(d);
+        r->h = nullptr;
+        finish(r, rcs[i], rcs[i] ? (msg.empty() ? std::string("result copy failed") : msg) : "");
+      }
+    }
+    for (npme_handle *d : drop) npme_gpu_destroy(d);
+  }
+}
+
+extern "C" {
+
+void npme_gpu_server_default_config(npme_server_config *c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+  c->device = 0;
+  c->setup_threads = 8;
+  c->max_batch = 64;
+  c->hbm_budget = 0;
+  c->pool_capacity = 64;
+}
+
+int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
+  if (!cfg || !out) return NPME_EINVAL;
+  *out = nullptr;
+  if (cfg->setup_threads < 1 || cfg->setup_threads > 256 || cfg->max_batch < 1 ||
+      cfg->pool_capacity < 0)
+    return NPME_EINVAL;
+  npme_server *s = new (std::nothrow) npme_server;
+  if (!s) return NPME_ENOMEM;
+  s->cfg = *cfg;
+  s->t0 = Clock::now();
+  memset(&s->stats, 0, sizeof(s->stats));
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e == cudaSuccess && s->cfg.hbm_budget == 0) {
+    size_t fr = 0, tot = 0;
+    e = cudaMemGetInfo(&fr, &tot);
+    s->cfg.hbm_budget = fr / 2;
+  }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete s;
+    return NPME_ECUDA;
+  }
+  int rc = npme_gpu_batch_create(cfg->device, &s->batch);
+  if (rc) {
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return rc;
+  }
+  for (int i = 0; i < cfg->setup_threads; i++) s->workers.emplace_back([s] { s->setup_loop(); });
+  s->dispatcher = std::thread([s] { s->dispatch_loop(); });
+  *out = s;
+  return NPME_OK;
+}
+
+int npme_gpu_submit(npme_server *s, const npme_params *p, size_t n, const double *coord,
+                    const double *charge, double *V, unsigned long long *ticket) {
+  if (!s || !p || !coord || !charge || !V || !ticket || n == 0) return NPME_EINVAL;
+  if (p->device != s->cfg.device) return NPME_EINVAL;
+  Request *r = new (std::nothrow) Request;
+  if (!r) return NPME_ENOMEM;
+  r->p = *p;
+  r->n = n;
+  r->coord = coord, r->charge = charge, r->V = V;
+  r->footprint = footprint(*p, n);
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stopping) {
+    delete r;
+    return NPME_ESTATE;
+  }
+  r->id = s->next_id++;
+  r->t_submit = s->now();
+  s->tickets[r->id] = r;
+  s->waiting.push_back(r);
+  s->stats.submitted++;
+  s->admit();
+  *ticket = r->id;
+  return NPME_OK;
+}
+
+int npme_gpu_poll(npme_server *s, unsigned long long ticket, int *state) {
+  if (!s || !state) return NPME_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return NPME_EINVAL;
+  *state = it->second->state;
+  return NPME_OK;
+}
+
+int npme_gpu_wait(npme_server *s, unsigned long long ticket, double timeout_s) {
+  if (!s) return NPME_EINVAL;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return NPME_EINVAL;
+  Request *r = it->second;
+  auto done = [&] { return r->state == NPME_TICKET_DONE || r->state == NPME_TICKET_FAILED; };
+  if (timeout_s < 0) s->cv_done.wait(lk, done);
+  else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done))
+    return NPME_ETIMEOUT;
+  return r->status;
+}
+
+int npme_gpu_ticket_info(npme_server *s, unsigned long long ticket, npme_ticket_info *info) {
+  if (!s || !info) return NPME_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return NPME_EINVAL;
+  const Request *r = it->second;
+  info->state = r->state;
+  info->status = r->status;
+  info->t_submit = r->t_submit;
+  info->t_admit = r->t_admit;
+  info->t_ready = r->t_ready;
+  info->t_done = r->t_done;
+  info->batch_size = r->batch_size;
+  info->footprint = r->footprint;
+  strncpy(info->error, r->err.c_str(), sizeof(info->error) - 1);
+  info->error[sizeof(info->error) - 1] = 0;
+  return NPME_OK;
+}
+
+int npme_gpu_release_ticket(npme_server *s, unsigned long long ticket) {
+  if (!s) return NPME_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return NPME_EINVAL;
+  Request *r = it->second;
+  if (r->state != NPME_TICKET_DONE && r->state != NPME_TICKET_FAILED) return NPME_ESTATE;
+  s->tickets.erase(it);
+  delete r;
+  return NPME_OK;
+}
+
+int npme_gpu_server_stats(npme_server *s, npme_server_stats *st) {
+  if (!s || !st) return NPME_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *st = s->stats;
+  st->idle_handles = s->idle_count;
+  st->in_flight_bytes = s->in_flight;
+  st->hbm_budget = s->cfg.hbm_budget;
+  st->clock_s = s->now();
+  return NPME_OK;
+}
+
+int npme_gpu_server_destroy(npme_server *s) {
+  if (!s) return NPME_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+  }
+  s->cv_setup.notify_all();
+  s->cv_ready.notify_all();
+  // requests still waiting for admission are admitted as the ones in flight
+  // complete; every submitted request completes before the threads end
+  for (;;) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->waiting.empty() && s->admitted.empty() && s->ready.empty() && s->in_flight == 0) break;
+    s->cv_done.wait_for(lk, std::chrono::milliseconds(10));
+  }
+  s->cv_setup.notify_all();
+  s->cv_ready.notify_all();
+  for (auto &t : s->workers) t.join();
+  s->dispatcher.join();
+  for (auto &kv : s->idle)
+    for (npme_handle *h : kv.second) npme_gpu_destroy(h);
+  for (auto &kv : s->tickets) delete kv.second;
+  npme_gpu_batch_destroy(s->batch);
+  cudaStreamDestroy(s->stream);
+  delete s;
+  return NPME_OK;
+}
+
+}  // extern "C"

@@ -132,37 +132,30 @@ def test_set_params_retunes_a_handle():
     s.close()
 
 
-def test_handle_pool_reuses_and_retunes(monkeypatch):
-    """Pool logic on the host: exact match first, then any free handle of the
-    same device and precision (given the new parameters), then a new one."""
-    made = []
-
-    class FakeSolver:
-        def __init__(self, p):
-            self.p, self.closed = p, False
-            made.append(self)
-
-        def set_params(self, p):
-            self.p = p
-            return self
-
-        def close(self):
-            self.closed = True
-
-    monkeypatch.setattr(api, "Solver", FakeSolver)
-    pool = serving.HandlePool(capacity=2)
-    pa = api.make_params("laplace", grid=(32, 32, 32), order=6)
-    pb = api.make_params("helmholtz", grid=(48, 48, 48), order=8, k0=0.5)
-    pc = api.make_params("laplace", grid=(32, 32, 32), order=6, precision="fp64")
-    a = pool.get(pa)
-    pool.put(a)
-    assert pool.get(pa) is a and pool.created == 1 and pool.retuned == 0
-    pool.put(a)
-    b = pool.get(pb)  # retuned from a
-    assert b is a and b.p is pb and pool.retuned == 1
-    c = pool.get(pc)  # nothing free of that precision
-    assert c is not a and pool.created == 2
-    pool.put(b), pool.put(c), pool.put(FakeSolver(pa))  # capacity 2: the third is closed
-    assert made[-1].closed and pool.count == 2
-    pool.close()
-    assert b.closed and c.closed and pool.count == 0
+@pytest.mark.gpu
+def test_native_queue_errors_budget_and_tickets():
+    """A request with invalid parameters fails alone; with a 1-byte budget
+    every request runs alone (admission); tickets report their life cycle."""
+    reqs = serving.serving_stream(count=6, n_min=1000, n_max=8000, seed=17, rate=1e4)
+    srv = api.NativeServer(0, setup_threads=2, max_batch=8, hbm_budget=1, pool_capacity=2)
+    bad = serving.params_for(reqs[0])
+    bad.BnOrder = 7  # odd order: refused at set-up
+    tb = srv.submit(bad, reqs[0].coord, reqs[0].q)
+    ts = [srv.submit(serving.params_for(r), r.coord, r.q) for r in reqs]
+    with pytest.raises(api.NPMEError) as e:
+        srv.result(tb)
+    assert e.value.code == api.EINVAL and "BnOrder" in str(e.value)
+    for r, t in zip(reqs, ts):
+        assert srv.wait(t, 60.0) == api.OK
+        assert srv.poll(t) == api.TICKET_DONE
+        V, info = srv.result(t)
+        assert info["batch_size"] == 1  # the budget admits one request at a time
+        assert info["t_submit"] <= info["t_admit"] <= info["t_ready"] <= info["t_done"]
+        with npme_b200.Solver(serving.params_for(r)) as s:
+            alone = s.setup(r.coord).calcv(r.q)
+        assert rel(V, alone) < 1e-6
+    with pytest.raises(api.NPMEError):
+        srv.poll(ts[0])  # released
+    st = srv.stats()
+    assert st["completed"] == 6 and st["failed"] == 1 and st["idle_handles"] <= 2
+    srv.close()
