@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256) batch_interp_kernel(const BatchSys *__res
 }
 
 template <bool CPLX, int FUNC, int SPLIT, int ND>
-__global__ void __launch_bounds__(32 * kGroupWarps) batch_direct_kernel(
+__global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) batch_direct_kernel(
     PairCoef<float> k, const BatchSys *__restrict__ sys, const long long *__restrict__ off,
     int count) {
   __shared__ float4 sp[kGroupWarps][32];

@@ -10,6 +10,10 @@
 namespace npme {
 
 constexpr int kGroupWarps = 4;  // warps per CTA of the FP32 direct sum
+#ifndef NPME_GROUP_MIN_BLOCKS
+#define NPME_GROUP_MIN_BLOCKS 5
+#endif
+constexpr int kGroupMinBlocks = NPME_GROUP_MIN_BLOCKS;  // resident CTAs asked of ptxas
 #ifndef NPME_DIRECT_UNROLL
 #define NPME_DIRECT_UNROLL 8
 #endif
@@ -189,6 +193,186 @@ __device__ __forceinline__ void interp_body(const BrickPoint<T> &pt, const T *__
   }
 }
 
+// Real derivative-match kernels (1/r, r^alpha) of the FP32 direct sum with
+// packed arithmetic: every lane evaluates its target against two sources per
+// step with sm_100's two-wide FP32 instructions (__fadd2_rn / __fmul2_rn /
+// __ffma2_rn), which halves the issued arithmetic of the distance test and
+// of the polynomial.  The staged chunk is laid out in source pairs:
+//   sp[p]      = (-x_2p, -x_2p+1, -y_2p, -y_2p+1)
+//   sp[16 + p] = (-z_2p, -z_2p+1,  q_2p,  q_2p+1)
+// (coordinates negated so that t + (-s) gives t - s exactly), slo the same
+// for the low parts of the rounded differences.  Slots past the chunk hold a
+// far source with charge 0.  Same arithmetic per pair as the scalar body
+// (difference, r^2, hit test, refinement below refine2, polynomial in
+// s = r^2/Rdir^2), except that a refined step refines both of its pairs.
+// kPackedBlock consecutive source-pair steps of the packed direct sum: the
+// differences and distances of all steps first, then the refinement of close
+// pairs (rare, a divergent branch), then the pair kernel of all steps without
+// branches, so that the scheduler can interleave the independent polynomial
+// chains of the block.  Pairs outside the cutoff (and the target itself) get
+// r^2 = Rdir^2 and charge 0.  The whole pair phase is skipped when no lane
+// of the warp has a hit in the block.
+#ifndef NPME_PACKED_BLOCK
+#define NPME_PACKED_BLOCK 4
+#endif
+constexpr int kPackedBlock = NPME_PACKED_BLOCK;
+
+template <int FUNC, int ND>
+__device__ __forceinline__ void packed_block(
+    const PairCoef<float> &k, const float4 *sp, const float4 *slo, int s0, float2 tx2,
+    float2 ty2, float2 tz2, float2 tl2x, float2 tl2y, float2 tl2z, float R2, float refine2,
+    float2 &P0, float2 &N1, float2 &N2, float2 &N3) {
+  constexpr int U = kPackedBlock;
+  float2 x[U], y[U], z[U], r2[U], q[U];
+  float rmin = 3.0e38f;
+  bool any = false;
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const float4 A = sp[s0 + u], B = sp[16 + s0 + u];
+    x[u] = __fadd2_rn(tx2, make_float2(A.x, A.y));
+    y[u] = __fadd2_rn(ty2, make_float2(A.z, A.w));
+    z[u] = __fadd2_rn(tz2, make_float2(B.x, B.y));
+    q[u] = make_float2(B.z, B.w);
+    r2[u] = __ffma2_rn(x[u], x[u], __ffma2_rn(y[u], y[u], __fmul2_rn(z[u], z[u])));
+    rmin = fminf(rmin, fminf(r2[u].x, r2[u].y));
+    any |= (r2[u].x <= R2) | (r2[u].y <= R2);
+  }
+  if (!__any_sync(0xffffffffu, any)) return;
+  if (rmin < refine2) {  // close pair: exact difference from head + residual
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (fminf(r2[u].x, r2[u].y) < refine2) {
+        const float4 LA = slo[s0 + u], LB = slo[16 + s0 + u];
+        x[u] = __fadd2_rn(x[u], __fadd2_rn(tl2x, make_float2(LA.x, LA.y)));
+        y[u] = __fadd2_rn(y[u], __fadd2_rn(tl2y, make_float2(LA.z, LA.w)));
+        z[u] = __fadd2_rn(z[u], __fadd2_rn(tl2z, make_float2(LB.x, LB.y)));
+        const float2 rn = __ffma2_rn(x[u], x[u], __ffma2_rn(y[u], y[u], __fmul2_rn(z[u], z[u])));
+        // keep the hit decision of the unrefined distance
+        r2[u].x = r2[u].x > 0.f && r2[u].x <= R2 ? rn.x : r2[u].x;
+        r2[u].y = r2[u].y > 0.f && r2[u].y <= R2 ? rn.y : r2[u].y;
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const bool h0 = r2[u].x <= R2 && r2[u].x > 0.f, h1 = r2[u].y <= R2 && r2[u].y > 0.f;
+    const float2 rr = make_float2(h0 ? r2[u].x : R2, h1 ? r2[u].y : R2);
+    const float2 qm = make_float2(h0 ? q[u].x : 0.f, h1 ? q[u].y : 0.f);
+    const float2 sv = __fmul2_rn(rr, k.invR2_2);
+    float2 np = k.nar2[ND];  // -f_LR polynomial
+#pragma unroll
+    for (int n = ND - 1; n >= 0; n--) np = __ffma2_rn(np, sv, k.nar2[n]);
+    float2 d = k.br2[ND - 1];  // (1/r) d f_LR / dr polynomial
+#pragma unroll
+    for (int n = ND - 2; n >= 0; n--) d = __ffma2_rn(d, sv, k.br2[n]);
+    float2 f0, t;  // t = -f1
+    if (FUNC == 0) {
+      const float2 ri = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+      f0 = __fadd2_rn(ri, np);                    // 1/r - f_LR
+      t = __ffma2_rn(__fmul2_rn(ri, ri), ri, d);  // 1/r^3 + d
+    } else {
+      // r^alpha = 2^((alpha/2) log2 r^2) on the special-function unit;
+      // 1/r^2 = rsqrt(r^2)^2
+      const float2 e0 = make_float2(exp2f(k.half_alpha * __log2f(rr.x)),
+                                    exp2f(k.half_alpha * __log2f(rr.y)));
+      const float2 ri = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+      f0 = __fadd2_rn(e0, np);
+      // -f1 = d - alpha r^alpha / r^2
+      t = __ffma2_rn(__fmul2_rn(e0, make_float2(-k.alpha, -k.alpha)), __fmul2_rn(ri, ri), d);
+    }
+    const float2 gq = __fmul2_rn(t, qm);
+    P0 = __ffma2_rn(f0, qm, P0);
+    N1 = __ffma2_rn(gq, x[u], N1);
+    N2 = __ffma2_rn(gq, y[u], N2);
+    N3 = __ffma2_rn(gq, z[u], N3);
+  }
+}
+
+template <int FUNC, int ND>
+__device__ __forceinline__ void direct_group_packed(
+    const PairCoef<float> &k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
+    const int4 G, const double4 c, const int2 *__restrict__ segs,
+    const uint32_t *__restrict__ perm, float refine2, double fself_r, double *__restrict__ V,
+    float4 *sp, float4 *slo, int lane) {
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  // idle lanes sit far outside the cutoff
+  float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f;
+  if (active) {
+    const double4 p = gpos[ti];
+    const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+    tx = (float)dx, ty = (float)dy, tz = (float)dz;
+    tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
+  }
+  const float2 tx2 = make_float2(tx, tx), ty2 = make_float2(ty, ty), tz2 = make_float2(tz, tz);
+  const float2 tl2x = make_float2(tlx, tlx), tl2y = make_float2(tly, tly),
+               tl2z = make_float2(tlz, tlz);
+  const float R2 = k.R2;
+  double acc[4] = {0, 0, 0, 0};
+  float *sa = reinterpret_cast<float *>(sp), *la = reinterpret_cast<float *>(slo);
+  const int slot = (lane >> 1) * 4 + (lane & 1);
+
+  // register prefetch of the next chunk: lane l holds source l of the chunk
+  int seg = G.z, off = 0, pcnt = 0;
+  double px = 0, py = 0, pz = 0;
+  float pq = 0.f;
+#define NPME_PREFETCH_P(SG, OF)                                \
+  {                                                            \
+    const int2 S_ = segs[SG];                                  \
+    pcnt = min(32, S_.y - (OF));                               \
+    if (lane < pcnt) {                                         \
+      const long j_ = (long)S_.x + (OF) + lane;                \
+      const double4 p_ = gpos[j_];                             \
+      px = p_.x, py = p_.y, pz = p_.z;                         \
+      pq = qg[j_];                                             \
+    }                                                          \
+  }
+  if (seg < G.w) NPME_PREFETCH_P(seg, 0);
+  while (seg < G.w) {
+    __syncwarp();
+    {
+      float hx = 1e18f, hy = 1e18f, hz = 1e18f, q = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+      if (lane < pcnt) {
+        const double dx = px - c.x, dy = py - c.y, dz = pz - c.z;
+        hx = (float)dx, hy = (float)dy, hz = (float)dz;
+        lx = (float)(dx - (double)hx), ly = (float)(dy - (double)hy), lz = (float)(dz - (double)hz);
+        q = pq;
+      }
+      sa[slot] = -hx;
+      sa[slot + 2] = -hy;
+      sa[64 + slot] = -hz;
+      sa[64 + slot + 2] = q;
+      la[slot] = -lx;
+      la[slot + 2] = -ly;
+      la[64 + slot] = -lz;
+    }
+    __syncwarp();
+    const int npair = (pcnt + 1) >> 1;
+    off += 32;
+    if (off >= segs[seg].y) {
+      seg++;
+      off = 0;
+    }
+    if (seg < G.w) NPME_PREFETCH_P(seg, off);
+    float2 P0 = make_float2(0.f, 0.f), N1 = P0, N2 = P0, N3 = P0;  // N*: minus the gradient
+    // blocks of kPackedBlock steps; slots past the chunk hold far sources, so
+    // the step count is rounded up to whole blocks
+    for (int s0 = 0; s0 < npair; s0 += kPackedBlock)
+      packed_block<FUNC, ND>(k, sp, slo, s0, tx2, ty2, tz2, tl2x, tl2y, tl2z, R2, refine2, P0,
+                             N1, N2, N3);
+    acc[0] += (double)P0.x + (double)P0.y;
+    acc[1] -= (double)N1.x + (double)N1.y;
+    acc[2] -= (double)N2.x + (double)N2.y;
+    acc[3] -= (double)N3.x + (double)N3.y;
+  }
+#undef NPME_PREFETCH_P
+  if (active) {
+    const long o = perm[ti];
+    acc[0] -= fself_r * (double)qg[ti];  // src/Interface.cpp:2061-2062
+    reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+  }
+}
+
 // FP32 direct sum of one warp group (see direct.cu for the scheme).  sp and
 // slo are this warp's 32-entry shared staging arrays.
 template <bool CPLX, int FUNC, int SPLIT, int ND>
@@ -197,6 +381,13 @@ __device__ __forceinline__ void direct_group_body(
     const int4 G, const double4 c, const int2 *__restrict__ segs,
     const uint32_t *__restrict__ perm, float refine2, double fself_r, double fself_i,
     double *__restrict__ V, float4 *sp, float4 *slo, int lane) {
+#if !defined(NPME_SCALAR_DIRECT)
+  if constexpr (!CPLX && SPLIT == 0 && ND > 0) {
+    direct_group_packed<FUNC, ND>(k, gpos, qg, G, c, segs, perm, refine2, fself_r, V, sp, slo,
+                                  lane);
+    return;
+  }
+#endif
   const int ti = G.x + lane;
   const bool active = lane < G.y;
   // idle lanes sit far outside the cutoff

@@ -9,6 +9,10 @@ namespace npme {
 
 constexpr int kMaxDeriv = 15;  // derivative-match order supported on device
 
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+
 // Pair-kernel constants, passed by value to the kernels.  Polynomial
 // coefficients are stored in the scaled variable s = r^2 / Rdir^2:
 //   f_LR(r) = sum_n ar[n] s^n,   (1/r) d f_LR / dr = sum_n br[n] s^n
@@ -25,11 +29,12 @@ struct PairCoef {
   T k0r, k0i;
   T ar[kMaxDeriv + 1], ai[kMaxDeriv + 1];
   T br[kMaxDeriv + 1], bi[kMaxDeriv + 1];
+  // the real coefficients as equal pairs for the packed (two pairs per
+  // instruction) evaluation: -ar[n] and br[n]; (invR2, invR2)
+  typename Vec2<T>::type nar2[kMaxDeriv + 1], br2[kMaxDeriv + 1];
+  typename Vec2<T>::type invR2_2;
 };
 
-template <typename T> struct Vec2;
-template <> struct Vec2<float> { using type = float2; };
-template <> struct Vec2<double> { using type = double2; };
 template <typename T> struct Vec4;
 template <> struct Vec4<float> { using type = float4; };
 template <> struct Vec4<double> { using type = double4; };

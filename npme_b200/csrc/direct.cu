@@ -43,8 +43,11 @@ PairCoef<T> make_pair_coef(const npme_handle *h) {
     k.ai[i] = (T)(h->a_i[i] * s);
     k.br[i] = (T)(h->b_r[i] * s);
     k.bi[i] = (T)(h->b_i[i] * s);
+    k.nar2[i].x = k.nar2[i].y = -k.ar[i];
+    k.br2[i].x = k.br2[i].y = k.br[i];
     s *= R2;
   }
+  k.invR2_2.x = k.invR2_2.y = k.invR2;
   return k;
 }
 template PairCoef<float> make_pair_coef<float>(const npme_handle *);
@@ -188,7 +191,7 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
 // error that dominates the gradient.
 
 template <bool CPLX, int FUNC, int SPLIT, int ND>
-__global__ void __launch_bounds__(32 * kGroupWarps) direct_groups_kernel(
+__global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) direct_groups_kernel(
     PairCoef<float> k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
     const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
     const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
