@@ -34,7 +34,8 @@ struct BatchSys {
   const double *q;  // caller charges (device)
   double *V;        // caller output (device)
   const BrickPoint<float> *bpts;
-  const uint32_t *cperm;
+  const uint32_t *cperm;  // targets: group order -> caller index
+  const uint32_t *dperm;  // direct-sum sources: source order -> caller index
   float *qb, *qc;
   const int *brick_list, *brick_start;
   int nb2, nb3;
@@ -43,7 +44,7 @@ struct BatchSys {
   const float *G;
   long N1, N2, N3;
   float c1, c2, c3;
-  const double4 *gpos;
+  const double4 *gpos, *spos;
   const int4 *groups;
   const double4 *gcen;
   const int2 *segs;
@@ -70,7 +71,7 @@ __global__ void batch_gather_kernel(const BatchSys *__restrict__ sys,
        u += (long long)gridDim.x * blockDim.x) {
     const int s = find_sys(off, count, u);
     const BatchSys &S = sys[s];
-    gather_body<float, CPLX>(S.q, S.bpts, S.cperm, S.qb, S.qc, (long)(u - off[s]));
+    gather_body<float, CPLX>(S.q, S.bpts, S.dperm, S.qb, S.qc, (long)(u - off[s]));
   }
 }
 
@@ -131,8 +132,8 @@ __global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) batch_direc
   const int s = find_sys(off, count, u);
   const BatchSys &S = sys[s];
   const long g = (long)(u - off[s]);
-  direct_group_body<CPLX, FUNC, SPLIT, ND>(k, S.gpos, S.qc, S.groups[g], S.gcen[g], S.segs,
-                                           S.cperm, S.refine2, S.fself_r, S.fself_i, S.V,
+  direct_group_body<CPLX, FUNC, SPLIT, ND>(k, S.gpos, S.spos, S.qc, S.q, S.groups[g], S.gcen[g],
+                                           S.segs, S.cperm, S.refine2, S.fself_r, S.fself_i, S.V,
                                            sp[wid], slo[wid], lane);
 }
 
@@ -266,6 +267,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     S.V = d_V[f32[k]];
     S.bpts = (const BrickPoint<float> *)h->d_bpts;
     S.cperm = h->d_cperm;
+    S.dperm = h->d_dperm;
     S.qb = (float *)h->d_qb;
     S.qc = (float *)h->d_qc;
     S.brick_list = h->d_brick_list;
@@ -280,6 +282,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     S.c2 = (float)(h->grid.N[1] / h->box[7]);
     S.c3 = (float)(h->grid.N[2] / h->box[8]);
     S.gpos = h->d_gpos;
+    S.spos = h->d_spos;
     S.groups = h->d_groups;
     S.gcen = h->d_gcen;
     S.segs = h->d_segs;

@@ -19,13 +19,14 @@ constexpr int kGroupMinBlocks = NPME_GROUP_MIN_BLOCKS;  // resident CTAs asked o
 #endif
 constexpr int kDirectUnroll = NPME_DIRECT_UNROLL;  // pair-loop unroll factor
 
-// Charges into brick order (spread/interp) and direct-sum order.
+// Charges into brick order (spread/interp) and the direct sum's source
+// order (dperm: source slot -> caller index).
 template <typename T, bool CPLX>
 __device__ __forceinline__ void gather_body(const double *__restrict__ q,
                                             const BrickPoint<T> *__restrict__ bp,
-                                            const uint32_t *__restrict__ cperm,
+                                            const uint32_t *__restrict__ dperm,
                                             T *__restrict__ qb, T *__restrict__ qc, long i) {
-  const uint32_t ob = bp[i].orig, oc = cperm[i];
+  const uint32_t ob = bp[i].orig, oc = dperm[i];
   if (CPLX) {
     qb[2 * i] = (T)q[2 * (long)ob];
     qb[2 * i + 1] = (T)q[2 * (long)ob + 1];
@@ -193,18 +194,6 @@ __device__ __forceinline__ void interp_body(const BrickPoint<T> &pt, const T *__
   }
 }
 
-// Real derivative-match kernels (1/r, r^alpha) of the FP32 direct sum with
-// packed arithmetic: every lane evaluates its target against two sources per
-// step with sm_100's two-wide FP32 instructions (__fadd2_rn / __fmul2_rn /
-// __ffma2_rn), which halves the issued arithmetic of the distance test and
-// of the polynomial.  The staged chunk is laid out in source pairs:
-//   sp[p]      = (-x_2p, -x_2p+1, -y_2p, -y_2p+1)
-//   sp[16 + p] = (-z_2p, -z_2p+1,  q_2p,  q_2p+1)
-// (coordinates negated so that t + (-s) gives t - s exactly), slo the same
-// for the low parts of the rounded differences.  Slots past the chunk hold a
-// far source with charge 0.  Same arithmetic per pair as the scalar body
-// (difference, r^2, hit test, refinement below refine2, polynomial in
-// s = r^2/Rdir^2), except that a refined step refines both of its pairs.
 // kPackedBlock consecutive source-pair steps of the packed direct sum: the
 // differences and distances of all steps first, then the refinement of close
 // pairs (rare, a divergent branch), then the pair kernel of all steps without
@@ -288,12 +277,39 @@ __device__ __forceinline__ void packed_block(
   }
 }
 
+// Position of a lane in the virtual concatenation of a group's source
+// segments (segment index and offset in it), so that a staged chunk of 32
+// sources runs across segment boundaries.
+struct SrcCursor {
+  int seg, off;
+  __device__ __forceinline__ void normalize(const int2 *__restrict__ segs, int end) {
+    while (seg < end) {
+      const int c = segs[seg].y;
+      if (off < c) break;
+      off -= c;
+      seg++;
+    }
+  }
+};
+
+// Real derivative-match kernels (1/r, r^alpha) of the FP32 direct sum with
+// packed arithmetic: every lane evaluates its target against two sources per
+// step with sm_100's two-wide FP32 instructions (__fadd2_rn / __fmul2_rn /
+// __ffma2_rn), which halves the issued arithmetic of the distance test and
+// of the polynomial.  The staged chunk is laid out in source pairs:
+//   sp[p]      = (-x_2p, -x_2p+1, -y_2p, -y_2p+1)
+//   sp[16 + p] = (-z_2p, -z_2p+1,  q_2p,  q_2p+1)
+// (coordinates negated so that t + (-s) gives t - s exactly), slo the same
+// for the low parts of the rounded differences.  Slots past the chunk hold a
+// far source with charge 0.  Same arithmetic per pair as the scalar body
+// (difference, r^2, hit test, refinement below refine2, polynomial in
+// s = r^2/Rdir^2), except that a refined step refines both of its pairs.
 template <int FUNC, int ND>
 __device__ __forceinline__ void direct_group_packed(
-    const PairCoef<float> &k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
-    const int4 G, const double4 c, const int2 *__restrict__ segs,
-    const uint32_t *__restrict__ perm, float refine2, double fself_r, double *__restrict__ V,
-    float4 *sp, float4 *slo, int lane) {
+    const PairCoef<float> &k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller, const int4 G,
+    const double4 c, const int2 *__restrict__ segs, const uint32_t *__restrict__ perm,
+    float refine2, double fself_r, double *__restrict__ V, float4 *sp, float4 *slo, int lane) {
   const int ti = G.x + lane;
   const bool active = lane < G.y;
   // idle lanes sit far outside the cutoff
@@ -313,26 +329,22 @@ __device__ __forceinline__ void direct_group_packed(
   const int slot = (lane >> 1) * 4 + (lane & 1);
 
   // register prefetch of the next chunk: lane l holds source l of the chunk
-  int seg = G.z, off = 0, pcnt = 0;
+  SrcCursor cur{G.z, lane};
+  cur.normalize(segs, G.w);
+  bool pv = cur.seg < G.w;
   double px = 0, py = 0, pz = 0;
   float pq = 0.f;
-#define NPME_PREFETCH_P(SG, OF)                                \
-  {                                                            \
-    const int2 S_ = segs[SG];                                  \
-    pcnt = min(32, S_.y - (OF));                               \
-    if (lane < pcnt) {                                         \
-      const long j_ = (long)S_.x + (OF) + lane;                \
-      const double4 p_ = gpos[j_];                             \
-      px = p_.x, py = p_.y, pz = p_.z;                         \
-      pq = qg[j_];                                             \
-    }                                                          \
+  if (pv) {
+    const long j = (long)segs[cur.seg].x + cur.off;
+    const double4 p = spos[j];
+    px = p.x, py = p.y, pz = p.z, pq = qs[j];
   }
-  if (seg < G.w) NPME_PREFETCH_P(seg, 0);
-  while (seg < G.w) {
+  while (__any_sync(0xffffffffu, pv)) {
+    const int pcnt = __popc(__ballot_sync(0xffffffffu, pv));  // valid lanes form a prefix
     __syncwarp();
     {
       float hx = 1e18f, hy = 1e18f, hz = 1e18f, q = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
-      if (lane < pcnt) {
+      if (pv) {
         const double dx = px - c.x, dy = py - c.y, dz = pz - c.z;
         hx = (float)dx, hy = (float)dy, hz = (float)dz;
         lx = (float)(dx - (double)hx), ly = (float)(dy - (double)hy), lz = (float)(dz - (double)hz);
@@ -347,13 +359,15 @@ __device__ __forceinline__ void direct_group_packed(
       la[64 + slot] = -lz;
     }
     __syncwarp();
-    const int npair = (pcnt + 1) >> 1;
-    off += 32;
-    if (off >= segs[seg].y) {
-      seg++;
-      off = 0;
+    cur.off += 32;
+    cur.normalize(segs, G.w);
+    pv = cur.seg < G.w;
+    if (pv) {
+      const long j = (long)segs[cur.seg].x + cur.off;
+      const double4 p = spos[j];
+      px = p.x, py = p.y, pz = p.z, pq = qs[j];
     }
-    if (seg < G.w) NPME_PREFETCH_P(seg, off);
+    const int npair = (pcnt + 1) >> 1;
     float2 P0 = make_float2(0.f, 0.f), N1 = P0, N2 = P0, N3 = P0;  // N*: minus the gradient
     // blocks of kPackedBlock steps; slots past the chunk hold far sources, so
     // the step count is rounded up to whole blocks
@@ -365,26 +379,29 @@ __device__ __forceinline__ void direct_group_packed(
     acc[2] -= (double)N2.x + (double)N2.y;
     acc[3] -= (double)N3.x + (double)N3.y;
   }
-#undef NPME_PREFETCH_P
   if (active) {
     const long o = perm[ti];
-    acc[0] -= fself_r * (double)qg[ti];  // src/Interface.cpp:2061-2062
+    acc[0] -= fself_r * qcaller[o];  // src/Interface.cpp:2061-2062
     reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
   }
 }
 
-// FP32 direct sum of one warp group (see direct.cu for the scheme).  sp and
-// slo are this warp's 32-entry shared staging arrays.
+// FP32 direct sum of one warp group (see direct.cu for the scheme): targets
+// gpos[G.x, G.x + G.y) in group order, sources spos / qs (charges gathered
+// into source order) over the segments [G.z, G.w); qcaller holds the
+// caller-order charges for the self term.  sp and slo are this warp's
+// 32-entry shared staging arrays.
 template <bool CPLX, int FUNC, int SPLIT, int ND>
 __device__ __forceinline__ void direct_group_body(
-    const PairCoef<float> &k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
-    const int4 G, const double4 c, const int2 *__restrict__ segs,
-    const uint32_t *__restrict__ perm, float refine2, double fself_r, double fself_i,
-    double *__restrict__ V, float4 *sp, float4 *slo, int lane) {
+    const PairCoef<float> &k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller, const int4 G,
+    const double4 c, const int2 *__restrict__ segs, const uint32_t *__restrict__ perm,
+    float refine2, double fself_r, double fself_i, double *__restrict__ V, float4 *sp,
+    float4 *slo, int lane) {
 #if !defined(NPME_SCALAR_DIRECT)
   if constexpr (!CPLX && SPLIT == 0 && ND > 0) {
-    direct_group_packed<FUNC, ND>(k, gpos, qg, G, c, segs, perm, refine2, fself_r, V, sp, slo,
-                                  lane);
+    direct_group_packed<FUNC, ND>(k, gpos, spos, qs, qcaller, G, c, segs, perm, refine2, fself_r,
+                                  V, sp, slo, lane);
     return;
   }
 #endif
@@ -402,29 +419,28 @@ __device__ __forceinline__ void direct_group_body(
   double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
 
   // register prefetch of the next chunk: lane l holds source l of the chunk
-  int seg = G.z, off = 0, pcnt = 0;
+  SrcCursor cur{G.z, lane};
+  cur.normalize(segs, G.w);
+  bool pv = cur.seg < G.w;
   double px = 0, py = 0, pz = 0;
   float pq = 0.f, pqi = 0.f;
-#define NPME_PREFETCH(SG, OF)                                  \
-  {                                                            \
-    const int2 S_ = segs[SG];                                  \
-    pcnt = min(32, S_.y - (OF));                               \
-    if (lane < pcnt) {                                         \
-      const long j_ = (long)S_.x + (OF) + lane;                \
-      const double4 p_ = gpos[j_];                             \
-      px = p_.x, py = p_.y, pz = p_.z;                         \
-      if (CPLX) {                                              \
-        pq = qg[2 * j_];                                       \
-        pqi = qg[2 * j_ + 1];                                  \
-      } else {                                                 \
-        pq = qg[j_];                                           \
-      }                                                        \
+#define NPME_PREFETCH                                          \
+  if (pv) {                                                    \
+    const long j_ = (long)segs[cur.seg].x + cur.off;           \
+    const double4 p_ = spos[j_];                               \
+    px = p_.x, py = p_.y, pz = p_.z;                           \
+    if (CPLX) {                                                \
+      pq = qs[2 * j_];                                         \
+      pqi = qs[2 * j_ + 1];                                    \
+    } else {                                                   \
+      pq = qs[j_];                                             \
     }                                                          \
   }
-  if (seg < G.w) NPME_PREFETCH(seg, 0);
-  while (seg < G.w) {
+  NPME_PREFETCH
+  while (__any_sync(0xffffffffu, pv)) {
+    const int cnt = __popc(__ballot_sync(0xffffffffu, pv));  // valid lanes form a prefix
     __syncwarp();
-    if (lane < pcnt) {
+    if (pv) {
       const double dx = px - c.x, dy = py - c.y, dz = pz - c.z;
       const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
       sp[lane] = make_float4(hx, hy, hz, pq);
@@ -432,13 +448,10 @@ __device__ __forceinline__ void direct_group_body(
                               (float)(dz - (double)hz), pqi);
     }
     __syncwarp();
-    const int cnt = pcnt;
-    off += 32;
-    if (off >= segs[seg].y) {
-      seg++;
-      off = 0;
-    }
-    if (seg < G.w) NPME_PREFETCH(seg, off);
+    cur.off += 32;
+    cur.normalize(segs, G.w);
+    pv = cur.seg < G.w;
+    NPME_PREFETCH
     float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
 #pragma unroll kDirectUnroll
     for (int s = 0; s < cnt; s++) {
@@ -484,14 +497,14 @@ __device__ __forceinline__ void direct_group_body(
   if (active) {
     const long o = perm[ti];
     if (CPLX) {
-      const double qr = qg[2 * (long)ti], qi = qg[2 * (long)ti + 1];
+      const double qr = qcaller[2 * o], qi = qcaller[2 * o + 1];
       acc[0] -= fself_r * qr - fself_i * qi;  // src/Interface.cpp:2909-2910
       acci[0] -= fself_r * qi + fself_i * qr;
       double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
 #pragma unroll
       for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
     } else {
-      acc[0] -= fself_r * (double)qg[ti];  // src/Interface.cpp:2061-2062
+      acc[0] -= fself_r * qcaller[o];  // src/Interface.cpp:2061-2062
       reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
     }
   }

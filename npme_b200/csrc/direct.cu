@@ -175,10 +175,10 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
 // ---------------------------------------------------------------------------
 // FP32 bulk direct sum over warp groups (see build_groups in npme_gpu.cu).
 // One warp owns one group of <= 32 targets (one per lane) and walks the
-// group's source segments in chunks of 32: every lane loads one source
-// (FP64 position), the warp stages the chunk in shared memory as float
-// coordinates relative to the group centre and every lane then sweeps the
-// staged chunk for its target.  The next chunk's loads are issued before the
+// group's source segments in chunks of 32 that run across segment
+// boundaries: every lane loads one source (FP64 position), the warp stages
+// the chunk in shared memory as float coordinates relative to the group
+// centre and every lane then sweeps the staged chunk for its target.  The next chunk's loads are issued before the
 // sweep, so global latency hides behind the arithmetic.  Warps are
 // independent: only __syncwarp, no block barrier.
 //
@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
 
 template <bool CPLX, int FUNC, int SPLIT, int ND>
 __global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) direct_groups_kernel(
-    PairCoef<float> k, const double4 *__restrict__ gpos, const float *__restrict__ qg,
+    PairCoef<float> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller,
     const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
     const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
     float refine2, double fself_r, double fself_i, double *__restrict__ V) {
@@ -201,8 +202,9 @@ __global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) direct_grou
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long g = (long)blockIdx.x * kGroupWarps + wid;
   if (g >= ngroups) return;  // warp-uniform; nothing below synchronises the block
-  direct_group_body<CPLX, FUNC, SPLIT, ND>(k, gpos, qg, groups[g], gcen[g], segs, perm, refine2,
-                                           fself_r, fself_i, V, sp[wid], slo[wid], lane);
+  direct_group_body<CPLX, FUNC, SPLIT, ND>(k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs,
+                                           perm, refine2, fself_r, fself_i, V, sp[wid], slo[wid],
+                                           lane);
 }
 
 
@@ -211,8 +213,9 @@ static void groups_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s
   const long blocks = (h->n_groups + kGroupWarps - 1) / kGroupWarps;
   if (blocks == 0) return;
   direct_groups_kernel<CPLX, FUNC, SPLIT, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
-      make_pair_coef<float>(h), h->d_gpos, (const float *)a.q, h->d_groups, h->d_gcen,
-      h->d_segs, h->d_cperm, h->n_groups, (float)h->refine2, a.fself_r, a.fself_i, a.V);
+      make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller, h->d_groups,
+      h->d_gcen, h->d_segs, h->d_cperm, h->n_groups, (float)h->refine2, a.fself_r, a.fself_i,
+      a.V);
 }
 
 template <bool CPLX, int FUNC, int SPLIT>
@@ -271,8 +274,8 @@ void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   h->launches++;
 }
 
-void launch_direct(npme_handle *h, double *d_V, cudaStream_t s) {
-  DirectArgs a{h->d_qc, h->fself_r, h->fself_i, d_V};
+void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s) {
+  DirectArgs a{h->d_qc, d_q, h->fself_r, h->fself_i, d_V};
   launch_direct_args(h, a, s);
 }
 

@@ -89,7 +89,7 @@ struct npme_handle {
   int *d_brick_start = nullptr;  // [n_bricks + 1]
   int *d_brick_list = nullptr;   // non-empty brick ids
   void *d_cpos = nullptr;        // cell order positions: float4 (local xyz, cell z) or double4
-  uint32_t *d_cperm = nullptr;   // cell order -> caller index
+  uint32_t *d_cperm = nullptr;   // cell order (FP64) / group order (FP32) -> caller index
   int *d_cell_start = nullptr;   // [ncell + 1]
   void *d_qb = nullptr;          // charges in brick order (T or T2)
   void *d_qc = nullptr;          // charges in cell order (T or T2)
@@ -116,7 +116,10 @@ struct npme_handle {
   long n_groups = 0, n_segs = 0;
   double cand_per_point = 0;     // staged source candidates per target point
   double refine2 = 0;            // r^2 below which pair differences are refined
-  double4 *d_gpos = nullptr;     // group order, FP64 positions
+  double4 *d_gpos = nullptr;     // targets in group order, FP64 positions
+  double4 *d_spos = nullptr;     // sources in fine-column order, FP64 positions
+  uint32_t *d_sperm = nullptr;   // source order -> caller index
+  const uint32_t *d_dperm = nullptr;  // gather order of the direct-sum charges (d_sperm or d_cperm)
   int4 *d_groups = nullptr;      // (first point, count, first segment, end segment)
   double4 *d_gcen = nullptr;     // group frame origin (bbox centre)
   int2 *d_segs = nullptr;        // (first point, count)
@@ -145,15 +148,17 @@ void launch_multiply(npme_handle *h, cudaStream_t s);
 void launch_interp(npme_handle *h, double *d_V, cudaStream_t s);
 
 // direct.cu
-// One direct-sum launch: charges already in the direct-sum order (group
-// order for FP32 bulk, cell order for FP64), the self term f_LR(0) q to
-// subtract from V (zero for the bare short-range sum), and the output.
+// One direct-sum launch: charges already in the direct-sum source order
+// (fine-column order for FP32 bulk, cell order for FP64), the caller's
+// charges and the self term f_LR(0) q to subtract from V (zero for the bare
+// short-range sum), and the output.
 struct DirectArgs {
-  const void *q;
+  const void *q;          // charges gathered into the direct-sum source order
+  const double *qcaller;  // caller-order charges (the self term)
   double fself_r, fself_i;
   double *V;
 };
-void launch_direct(npme_handle *h, double *d_V, cudaStream_t s);
+void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
 void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s);
 // caller-order charges (double) -> direct-sum order in the bulk precision
 void launch_gather_direct(npme_handle *h, const double *d_q, void *d_qdst, cudaStream_t s);

@@ -95,7 +95,7 @@ extern "C" int npme_gpu_direct_sum_device_noalloc(npme_handle *h, double *d_V,
   cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
   h->launches = 0;
   npme::launch_gather_direct(h, d_charge, scratch, s);
-  npme::DirectArgs a{scratch, 0.0, 0.0, d_V};
+  npme::DirectArgs a{scratch, d_charge, 0.0, 0.0, d_V};
   npme::launch_direct_args(h, a, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) {

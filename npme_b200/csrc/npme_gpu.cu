@@ -153,6 +153,7 @@ void pool_release(npme_handle *h) {
 // synchronised the handle's streams).
 void release(npme_handle *h) {
   h->pf = h->pi = nullptr;  // shared plans stay in the process-wide cache
+  h->d_dperm = nullptr;
   // every device buffer was obtained through dalloc, which records the
   // address of the pointer field it fills
   for (auto &kv : h->caps) {
@@ -202,16 +203,57 @@ int npme::handle_buffer(npme_handle *h, void **field, size_t bytes) {
 
 namespace {
 
-// Warp groups for the FP32 direct sum.  Points are binned into xy columns of
-// edge ~(32 / density)^(1/3) and sorted by z inside each column; each run of
-// 32 consecutive points of a column is one group (a compact, roughly cubic
-// cluster).  For every group the source segments are the z ranges of the
-// neighbour columns that can hold a point within Rdir of the group's
-// bounding box: |dz| <= sqrt(Rdir^2 - d_xy^2) with d_xy the distance from
-// the bounding box to the column in the xy plane.  Geometry is fixed between
-// CalcV calls (the reference's contract), so this is set-up work.  Returns
-// the group-order permutation in `order`.
-int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &order) {
+// Sorts the points by xy column (nc[0] x nc[1] columns of edge `edge` from
+// `mn`), then by (z, index) inside each column.  Fills the permutation, the
+// column starts and the sorted z.
+void column_sort(const double *coord, size_t n, const double *mn, const int *nc,
+                 const double *edge, std::vector<uint32_t> &order, std::vector<long> &cstart,
+                 std::vector<double> &zs) {
+  const long ncol = (long)nc[0] * nc[1];
+  std::vector<int> col(n);
+  for (size_t i = 0; i < n; i++) {
+    int c0 = std::min(nc[0] - 1, std::max(0, (int)((coord[3 * i] - mn[0]) / edge[0])));
+    int c1 = std::min(nc[1] - 1, std::max(0, (int)((coord[3 * i + 1] - mn[1]) / edge[1])));
+    col[i] = c0 * nc[1] + c1;
+  }
+  // counting sort by column (stable), then each column by (z, index)
+  cstart.assign(ncol + 1, 0);
+  for (size_t i = 0; i < n; i++) cstart[col[i] + 1]++;
+  for (long c = 0; c < ncol; c++) cstart[c + 1] += cstart[c];
+  order.resize(n);
+  {
+    std::vector<long> fill(cstart.begin(), cstart.end() - 1);
+    for (size_t i = 0; i < n; i++) order[fill[col[i]]++] = (uint32_t)i;
+  }
+  zs.resize(n);
+  std::vector<std::pair<double, uint32_t>> zc;
+  for (long c = 0; c < ncol; c++) {
+    const long b = cstart[c], e1 = cstart[c + 1];
+    zc.resize(e1 - b);
+    for (long k = b; k < e1; k++) zc[k - b] = {coord[3 * (size_t)order[k] + 2], order[k]};
+    std::sort(zc.begin(), zc.end());
+    for (long k = b; k < e1; k++) zs[k] = zc[k - b].first, order[k] = zc[k - b].second;
+  }
+}
+
+#ifndef NPME_SOURCE_SPLIT
+#define NPME_SOURCE_SPLIT 2
+#endif
+
+// Warp groups for the FP32 direct sum.  Targets are binned into xy columns
+// of edge e ~ (32 / density)^(1/3) and sorted by z inside each column; each
+// run of 32 consecutive points of a column is one group (a compact, roughly
+// cubic cluster).  Sources are binned the same way into finer columns (edge
+// e / NPME_SOURCE_SPLIT) and sorted by z.  For every group the source
+// segments are the z ranges of the fine columns that can hold a point within
+// Rdir of the group's bounding box: |dz| <= sqrt(Rdir^2 - d_xy^2), d_xy the
+// distance from the bounding box to the column in the xy plane; finer source
+// columns bound that distance more tightly, so fewer sources are staged per
+// group.  Geometry is fixed between CalcV calls (the reference's contract),
+// so this is set-up work.  Returns the group-order permutation of the
+// targets in `order` and the source-order permutation in `sorder`.
+int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &order,
+                 std::vector<uint32_t> &sorder) {
   const size_t n = h->n;
   const double R = h->p.Rdir, R2 = R * R;
   double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
@@ -226,47 +268,26 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   for (int d = 0; d < 3; d++) vol *= std::max(mx[d] - mn[d], 0.25 * R);
   double e = std::cbrt(32.0 * vol / (double)n);
   e = std::max(e, 1e-3 * R);
-  int nc[2];
-  double edge[2];
+  int nc[2], ns[2];
+  double edge[2], sedge[2];
   for (int d = 0; d < 2; d++) {
     const double ext = mx[d] - mn[d];
     nc[d] = std::max(1, std::min((int)std::ceil(ext / e), 1 << 14));
     edge[d] = std::max(ext / nc[d], 1e-12);
+    ns[d] = std::min(nc[d] * NPME_SOURCE_SPLIT, 1 << 15);
+    sedge[d] = std::max(ext / ns[d], 1e-12);
   }
+  std::vector<long> cstart, sstart;
+  std::vector<double> zt, zs;
+  column_sort(coord, n, mn, nc, edge, order, cstart, zt);
+  column_sort(coord, n, mn, ns, sedge, sorder, sstart, zs);
   const long ncol = (long)nc[0] * nc[1];
-  std::vector<int> col(n);
-  for (size_t i = 0; i < n; i++) {
-    int c0 = std::min(nc[0] - 1, std::max(0, (int)((coord[3 * i] - mn[0]) / edge[0])));
-    int c1 = std::min(nc[1] - 1, std::max(0, (int)((coord[3 * i + 1] - mn[1]) / edge[1])));
-    col[i] = c0 * nc[1] + c1;
-  }
-  // counting sort by column (stable), then each column by (z, index)
-  std::vector<long> cstart(ncol + 1, 0);
-  for (size_t i = 0; i < n; i++) cstart[col[i] + 1]++;
-  for (long c = 0; c < ncol; c++) cstart[c + 1] += cstart[c];
-  order.resize(n);
-  {
-    std::vector<long> fill(cstart.begin(), cstart.end() - 1);
-    for (size_t i = 0; i < n; i++) order[fill[col[i]]++] = (uint32_t)i;
-  }
-  std::vector<double> zs(n);
-  {
-    std::vector<std::pair<double, uint32_t>> zc;
-    for (long c = 0; c < ncol; c++) {
-      const long b = cstart[c], e1 = cstart[c + 1];
-      zc.resize(e1 - b);
-      for (long k = b; k < e1; k++) zc[k - b] = {coord[3 * (size_t)order[k] + 2], order[k]};
-      std::sort(zc.begin(), zc.end());
-      for (long k = b; k < e1; k++) zs[k] = zc[k - b].first, order[k] = zc[k - b].second;
-    }
-  }
 
   std::vector<int4> groups;
   std::vector<double4> cen;
   std::vector<int2> segs;
   double cand = 0;
   for (long c = 0; c < ncol; c++) {
-    const int c0 = (int)(c / nc[1]), c1 = (int)(c % nc[1]);
     for (long p0 = cstart[c]; p0 < cstart[c + 1]; p0 += 32) {
       const long p1 = std::min(p0 + 32, cstart[c + 1]);
       double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
@@ -277,19 +298,23 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
           bh[d] = std::max(bh[d], x);
         }
       const int seg0 = (int)segs.size();
-      const int r0 = (int)std::min<double>(nc[0], std::ceil(R / edge[0]) + 1);
-      const int r1 = (int)std::min<double>(nc[1], std::ceil(R / edge[1]) + 1);
-      for (int s0 = std::max(0, c0 - r0); s0 <= std::min(nc[0] - 1, c0 + r0); s0++) {
-        const double lo0 = mn[0] + s0 * edge[0], hi0 = lo0 + edge[0];
+      // fine columns whose xy extent can come within R of the bounding box
+      int lo[2], hi[2];
+      for (int d = 0; d < 2; d++) {
+        lo[d] = (int)std::max(0.0, std::floor((bl[d] - R - mn[d]) / sedge[d]));
+        hi[d] = (int)std::min((double)(ns[d] - 1), std::floor((bh[d] + R - mn[d]) / sedge[d]));
+      }
+      for (int s0 = lo[0]; s0 <= hi[0]; s0++) {
+        const double lo0 = mn[0] + s0 * sedge[0], hi0 = lo0 + sedge[0];
         const double dx = std::max(0.0, std::max(lo0 - bh[0], bl[0] - hi0));
-        for (int s1 = std::max(0, c1 - r1); s1 <= std::min(nc[1] - 1, c1 + r1); s1++) {
-          const double lo1 = mn[1] + s1 * edge[1], hi1 = lo1 + edge[1];
+        for (int s1 = lo[1]; s1 <= hi[1]; s1++) {
+          const double lo1 = mn[1] + s1 * sedge[1], hi1 = lo1 + sedge[1];
           const double dy = std::max(0.0, std::max(lo1 - bh[1], bl[1] - hi1));
           const double d2 = dx * dx + dy * dy;
           if (d2 > R2) continue;
           const double hz = std::sqrt(R2 - d2);
-          const long sc = (long)s0 * nc[1] + s1;
-          const double *zb = zs.data() + cstart[sc], *ze = zs.data() + cstart[sc + 1];
+          const long sc = (long)s0 * ns[1] + s1;
+          const double *zb = zs.data() + sstart[sc], *ze = zs.data() + sstart[sc + 1];
           const long a = std::lower_bound(zb, ze, bl[2] - hz) - zs.data();
           const long b = std::upper_bound(zb, ze, bh[2] + hz) - zs.data();
           if (b > a) {
@@ -303,10 +328,12 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
                                  0.5 * (bl[2] + bh[2]), 0.0));
     }
   }
-  std::vector<double4> gpos(n);
+  std::vector<double4> gpos(n), spos(n);
   for (size_t k = 0; k < n; k++) {
     const double *x = coord + 3 * (size_t)order[k];
     gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
+    const double *y = coord + 3 * (size_t)sorder[k];
+    spos[k] = make_double4(y[0], y[1], y[2], 0.0);
   }
   h->n_groups = (long)groups.size();
   h->n_segs = (long)segs.size();
@@ -316,10 +343,15 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   h->refine2 = (0.25 * e) * (0.25 * e);
   int rc;
   if ((rc = dalloc(h, &h->d_gpos, sizeof(double4) * n))) return rc;
+  if ((rc = dalloc(h, &h->d_spos, sizeof(double4) * n))) return rc;
+  if ((rc = dalloc(h, &h->d_sperm, sizeof(uint32_t) * n))) return rc;
   if ((rc = dalloc(h, &h->d_groups, sizeof(int4) * groups.size()))) return rc;
   if ((rc = dalloc(h, &h->d_gcen, sizeof(double4) * cen.size()))) return rc;
   if ((rc = dalloc(h, &h->d_segs, sizeof(int2) * std::max<size_t>(1, segs.size())))) return rc;
   CK(cudaMemcpyAsync(h->d_gpos, gpos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_spos, spos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_sperm, sorder.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
+                     h->stream));
   CK(cudaMemcpyAsync(h->d_groups, groups.data(), sizeof(int4) * groups.size(),
                      cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_gcen, cen.data(), sizeof(double4) * cen.size(), cudaMemcpyHostToDevice,
@@ -405,8 +437,10 @@ int upload_points(npme_handle *h, const double *coord) {
 
   const int C = h->complex_kernel ? 2 : 1;
   int rc;
-  // the FP32 direct sum walks warp groups: charges are gathered in group order
-  if (h->use_groups && (rc = build_groups(h, coord, cperm))) return rc;
+  // the FP32 direct sum walks warp groups: targets in group order, sources
+  // (and their gathered charges) in fine-column order
+  std::vector<uint32_t> sperm;
+  if (h->use_groups && (rc = build_groups(h, coord, cperm, sperm))) return rc;
   if ((rc = dalloc(h, &h->d_coord, sizeof(double) * 3 * n))) return rc;
   if ((rc = dalloc(h, (BrickPoint<T> **)&h->d_bpts, sizeof(BrickPoint<T>) * n))) return rc;
   if ((rc = dalloc(h, &h->d_brick_start, sizeof(int) * (nbt + 1)))) return rc;
@@ -432,6 +466,8 @@ int upload_points(npme_handle *h, const double *coord) {
                      h->stream));
   CK(cudaMemcpyAsync(h->d_cell_start, cstart.data(), sizeof(int) * (ncell + 1),
                      cudaMemcpyHostToDevice, h->stream));
+  // charges of the direct sum are gathered into its source order
+  h->d_dperm = h->use_groups ? h->d_sperm : h->d_cperm;
 
   // --- grids ---
   const long *N = g.N;
@@ -687,7 +723,7 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   CK(cudaEventRecord(h->ev_fork, s));
   CK(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
   tmark(h, 8, h->stream2);
-  npme::launch_direct(h, d_V, h->stream2);
+  npme::launch_direct(h, d_charge, d_V, h->stream2);
   tmark(h, 9, h->stream2);
   CK(cudaEventRecord(h->ev_join, h->stream2));
   CK(cudaMemsetAsync(h->d_grid, 0, gbytes, s));
@@ -801,7 +837,7 @@ int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_char
   cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
   h->launches = 0;
   npme::launch_gather_direct(h, d_charge, h->d_qc, s);
-  npme::DirectArgs a{h->d_qc, 0.0, 0.0, d_V};
+  npme::DirectArgs a{h->d_qc, d_charge, 0.0, 0.0, d_V};
   npme::launch_direct_args(h, a, s);
   CK(cudaGetLastError());
   return NPME_OK;

@@ -294,16 +294,16 @@ int build_kernel_transform(npme_handle *h) {
 }
 
 // ---------------------------------------------------------------------------
-// Per-call charge gather into brick order (spread/interp) and cell order
-// (direct sum), converted to the bulk precision.
+// Per-call charge gather into brick order (spread/interp) and the direct
+// sum's source order, converted to the bulk precision.
 
 template <typename T, bool CPLX>
 __global__ void gather_kernel(const double *__restrict__ q, const BrickPoint<T> *__restrict__ bp,
-                              const uint32_t *__restrict__ cperm, T *__restrict__ qb,
+                              const uint32_t *__restrict__ dperm, T *__restrict__ qb,
                               T *__restrict__ qc, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
        i += (long)gridDim.x * blockDim.x)
-    gather_body<T, CPLX>(q, bp, cperm, qb, qc, i);
+    gather_body<T, CPLX>(q, bp, dperm, qb, qc, i);
 }
 
 void launch_gather_charges(npme_handle *h, const double *d_q, cudaStream_t s) {
@@ -312,20 +312,20 @@ void launch_gather_charges(npme_handle *h, const double *d_q, cudaStream_t s) {
   if (h->fp32) {
     if (h->complex_kernel)
       gather_kernel<float, true><<<blocks, threads, 0, s>>>(
-          d_q, (const BrickPoint<float> *)h->d_bpts, h->d_cperm, (float *)h->d_qb,
+          d_q, (const BrickPoint<float> *)h->d_bpts, h->d_dperm, (float *)h->d_qb,
           (float *)h->d_qc, (long)h->n);
     else
       gather_kernel<float, false><<<blocks, threads, 0, s>>>(
-          d_q, (const BrickPoint<float> *)h->d_bpts, h->d_cperm, (float *)h->d_qb,
+          d_q, (const BrickPoint<float> *)h->d_bpts, h->d_dperm, (float *)h->d_qb,
           (float *)h->d_qc, (long)h->n);
   } else {
     if (h->complex_kernel)
       gather_kernel<double, true><<<blocks, threads, 0, s>>>(
-          d_q, (const BrickPoint<double> *)h->d_bpts, h->d_cperm, (double *)h->d_qb,
+          d_q, (const BrickPoint<double> *)h->d_bpts, h->d_dperm, (double *)h->d_qb,
           (double *)h->d_qc, (long)h->n);
     else
       gather_kernel<double, false><<<blocks, threads, 0, s>>>(
-          d_q, (const BrickPoint<double> *)h->d_bpts, h->d_cperm, (double *)h->d_qb,
+          d_q, (const BrickPoint<double> *)h->d_bpts, h->d_dperm, (double *)h->d_qb,
           (double *)h->d_qc, (long)h->n);
   }
   h->launches++;
@@ -354,14 +354,14 @@ void launch_gather_direct(npme_handle *h, const double *d_q, void *d_qdst, cudaS
   const long n = (long)h->n;
   if (h->fp32) {
     if (h->complex_kernel)
-      gather_one_kernel<float, true><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (float *)d_qdst, n);
+      gather_one_kernel<float, true><<<blocks, threads, 0, s>>>(d_q, h->d_dperm, (float *)d_qdst, n);
     else
-      gather_one_kernel<float, false><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (float *)d_qdst, n);
+      gather_one_kernel<float, false><<<blocks, threads, 0, s>>>(d_q, h->d_dperm, (float *)d_qdst, n);
   } else {
     if (h->complex_kernel)
-      gather_one_kernel<double, true><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (double *)d_qdst, n);
+      gather_one_kernel<double, true><<<blocks, threads, 0, s>>>(d_q, h->d_dperm, (double *)d_qdst, n);
     else
-      gather_one_kernel<double, false><<<blocks, threads, 0, s>>>(d_q, h->d_cperm, (double *)d_qdst, n);
+      gather_one_kernel<double, false><<<blocks, threads, 0, s>>>(d_q, h->d_dperm, (double *)d_qdst, n);
   }
   h->launches++;
 }
