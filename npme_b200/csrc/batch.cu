@@ -111,13 +111,13 @@ template <int P, bool CPLX>
 __global__ void __launch_bounds__(256) batch_interp_kernel(const BatchSys *__restrict__ sys,
                                                            const long long *__restrict__ off,
                                                            int count) {
-  const long long total = off[count];
-  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total;
-       u += (long long)gridDim.x * blockDim.x) {
-    const int s = find_sys(off, count, u);
-    const BatchSys &S = sys[s];
-    interp_body<float, P, CPLX>(S.bpts[u - off[s]], S.grid, S.V, S.N2, S.N3, S.c1, S.c2, S.c3);
-  }
+  extern __shared__ unsigned char smem_raw[];
+  const long long u = blockIdx.x;
+  const int s = find_sys(off, count, u);
+  const BatchSys &S = sys[s];
+  interp_brick_body<float, P, CPLX>(S.brick_list[u - off[s]], S.brick_start, S.bpts, S.grid, S.V,
+                                    S.nb2, S.nb3, S.N1, S.N2, S.N3, S.c1, S.c2, S.c3,
+                                    reinterpret_cast<float *>(smem_raw));
 }
 
 template <bool CPLX, int FUNC, int SPLIT, int ND>
@@ -165,8 +165,7 @@ int bfail(npme_batch *b, int code, const std::string &m) {
 struct Class {
   std::vector<int> members;  // indices into the batch's FP32 handle list
   std::vector<long long> off;   // prefix of the class's work units
-  std::vector<long long> poff;  // spread classes: prefix of points (interpolation)
-  size_t desc_at = 0, off_at = 0, poff_at = 0;  // byte offsets in the descriptor block
+  size_t desc_at = 0, off_at = 0;  // byte offsets in the descriptor block
 };
 
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -329,15 +328,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   };
   for (auto &kv : gath) lay(kv.second, units_gather);
   for (auto &kv : mult) lay(kv.second, units_mult);
-  for (auto &kv : spr) {
-    lay(kv.second, units_spread);
-    Class &c = kv.second;
-    c.poff.assign(c.members.size() + 1, 0);
-    for (size_t t = 0; t < c.members.size(); t++)
-      c.poff[t + 1] = c.poff[t] + (long long)hs[f32[c.members[t]]]->n;
-    c.poff_at = bytes;
-    bytes = align16(bytes + sizeof(long long) * c.poff.size());
-  }
+  for (auto &kv : spr) lay(kv.second, units_spread);  // spread and interpolation: bricks
   for (auto &kv : dir) lay(kv.second, units_dir);
 
   // the pinned staging buffer is reused: wait for the previous batch's copy
@@ -365,8 +356,6 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     BatchSys *dd = (BatchSys *)(b->h_pinned + c->desc_at);
     for (size_t t = 0; t < c->members.size(); t++) dd[t] = desc[c->members[t]];
     memcpy(b->h_pinned + c->off_at, c->off.data(), sizeof(long long) * c->off.size());
-    if (!c->poff.empty())
-      memcpy(b->h_pinned + c->poff_at, c->poff.data(), sizeof(long long) * c->poff.size());
   }
   cudaMemcpyAsync(b->d_block, b->h_pinned, bytes, cudaMemcpyHostToDevice, s);
   auto D = [&](const Class &c) { return (const BatchSys *)(b->d_block + c.desc_at); };
@@ -472,12 +461,17 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     Class &c = kv.second;
     const int P = kv.first.first;
     const bool cx = kv.first.second;
-    const long long np = c.poff.back();
-    if (np == 0) continue;
-    const long long *po = (const long long *)(b->d_block + c.poff_at);
-    const unsigned g = grid_of(np, 256, 148 * 32);
+    const long long nb = c.off.back();
+    if (nb == 0) continue;
     const int cnt = (int)c.members.size();
-#define NPME_BI(PP, CX) batch_interp_kernel<PP, CX><<<g, 256, 0, s>>>(D(c), po, cnt)
+#define NPME_BI(PP, CX)                                                                    \
+  {                                                                                        \
+    constexpr int TL = kBrick + PP - 1;                                                    \
+    const size_t smem = sizeof(float) * TL * TL * TL * (CX ? 2 : 1);                       \
+    auto kern = batch_interp_kernel<PP, CX>;                                               \
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+    kern<<<(unsigned)nb, 256, smem, s>>>(D(c), O(c), cnt);                                 \
+  }
 #define NPME_BI_P(CX)                   \
   switch (P) {                          \
     case 4: NPME_BI(4, CX); break;      \

@@ -38,6 +38,19 @@ __device__ __forceinline__ void gather_body(const double *__restrict__ q,
   }
 }
 
+// Points of a brick are stored sorted by the shared-memory bank of their
+// stencil origin in the brick's tile (set-up, npme_gpu.cu).  Virtual warp vw
+// of a brick with nb points takes the points at positions lane * W + vw of
+// that order (W = ceil(nb / 32) virtual warps), so the 32 lanes of a warp
+// hold points of 32 different banks as long as no bank holds more than W
+// points: the shared-memory accesses of a stencil step are then free of bank
+// conflicts and of colliding atomics.
+__device__ __forceinline__ int brick_point(int nb, int vw, int lane) {
+  const int W = (nb + 31) >> 5;
+  const int p = lane * W + vw;
+  return p < nb ? p : -1;
+}
+
 // Spread of one brick by the whole CTA (src/RecSumQ.cpp:184-314): the
 // brick's points accumulate their p^3 stencils into the shared tile of
 // (kBrick + P - 1)^3 grid points, which is then added to the global grid.
@@ -53,8 +66,12 @@ __device__ __forceinline__ void spread_brick_body(int brick, const int *__restri
   const int b3 = brick % nb3, b2 = (brick / nb3) % nb2, b1 = brick / (nb3 * nb2);
   for (int t = threadIdx.x; t < TV * C; t += blockDim.x) tile[t] = T(0);
   __syncthreads();
-  const int beg = brick_start[brick], end = brick_start[brick + 1];
-  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+  const int beg = brick_start[brick], nbp = brick_start[brick + 1] - beg;
+  const int nvw = (nbp + 31) >> 5, lane = threadIdx.x & 31;
+  for (int vw = threadIdx.x >> 5; vw < nvw; vw += blockDim.x >> 5) {
+    const int pi = brick_point(nbp, vw, lane);
+    if (pi < 0) continue;
+    const int i = beg + pi;
     const BrickPoint<T> pt = bp[i];
     T w1[P], w2[P], w3[P], dummy[P];
     bspline_weights<T, P, false>(pt.u[0], w1, dummy);
@@ -63,7 +80,7 @@ __device__ __forceinline__ void spread_brick_body(int brick, const int *__restri
     const int l1 = (int)(pt.g0 >> 20) - b1 * kBrick;
     const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
     const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
-    T qr = q[C * (long)i], qi = CPLX ? q[2 * (long)i + 1] : T(0);
+    const T qr = q[C * (long)i], qi = CPLX ? q[2 * (long)i + 1] : T(0);
 #pragma unroll
     for (int t1 = 0; t1 < P; t1++) {
 #pragma unroll
@@ -86,13 +103,10 @@ __device__ __forceinline__ void spread_brick_body(int brick, const int *__restri
     if (g1 + i1 >= N1) continue;
     if (g2 + i2 >= N2 || g3 + i3 >= N3) continue;  // beyond the box: always zero
     const long gi = ((g1 + i1) * N2 + (g2 + i2)) * N3 + (g3 + i3);
-    if (CPLX) {
-      const T vr = tile[2 * t], vi = tile[2 * t + 1];
-      if (vr != T(0)) atomicAdd(grid + 2 * gi, vr);
-      if (vi != T(0)) atomicAdd(grid + 2 * gi + 1, vi);
-    } else {
-      const T v = tile[t];
-      if (v != T(0)) atomicAdd(grid + gi, v);
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      const T v = tile[C * t + c];
+      if (v != T(0)) atomicAdd(grid + C * gi + c, v);
     }
   }
 }
@@ -129,68 +143,99 @@ __device__ __forceinline__ void multiply_cplx_body(typename Vec2<T>::type *__res
   X[idx] = o;
 }
 
-// Interpolation of one point (src/RecSumV.cpp:201-306): V += sum theta B B B,
-// grad += (N/L) sum theta dB ..., added into the caller-order output.
+// Interpolation of one brick by the whole CTA (src/RecSumV.cpp:201-306):
+// the brick's theta tile of (kBrick + P - 1)^3 grid points is read into
+// shared memory once, then every point gathers its p^3 stencil from the
+// tile: V += sum theta B1 B2 B3, grad += (N/L) sum theta dB ..., added into
+// the caller-order output.
 template <typename T, int P, bool CPLX>
-__device__ __forceinline__ void interp_body(const BrickPoint<T> &pt, const T *__restrict__ theta,
-                                            double *__restrict__ V, long N2, long N3, T c1, T c2,
-                                            T c3) {
+__device__ __forceinline__ void interp_brick_body(int brick, const int *__restrict__ brick_start,
+                                                  const BrickPoint<T> *__restrict__ bp,
+                                                  const T *__restrict__ theta,
+                                                  double *__restrict__ V, int nb2, int nb3,
+                                                  long N1, long N2, long N3, T c1, T c2, T c3,
+                                                  T *tile) {
+  constexpr int TL = kBrick + P - 1;
+  constexpr int TV = TL * TL * TL;
   constexpr int C = CPLX ? 2 : 1;
-  T w1[P], w2[P], w3[P], d1[P], d2[P], d3[P];
-  bspline_weights<T, P, true>(pt.u[0], w1, d1);
-  bspline_weights<T, P, true>(pt.u[1], w2, d2);
-  bspline_weights<T, P, true>(pt.u[2], w3, d3);
-  const long g1 = pt.g0 >> 20, g2 = (pt.g0 >> 10) & 1023u, g3 = pt.g0 & 1023u;
-  T v[4] = {0, 0, 0, 0}, vi[4] = {0, 0, 0, 0};
+  const int b3 = brick % nb3, b2 = (brick / nb3) % nb2, b1 = brick / (nb3 * nb2);
+  const long g1 = (long)b1 * kBrick, g2 = (long)b2 * kBrick, g3 = (long)b3 * kBrick;
+  for (int t = threadIdx.x; t < TV; t += blockDim.x) {
+    const int i3 = t % TL, i2 = (t / TL) % TL, i1 = t / (TL * TL);
+    T vr = T(0), vi = T(0);
+    if (g1 + i1 < N1 && g2 + i2 < N2 && g3 + i3 < N3) {
+      const long gi = ((g1 + i1) * N2 + (g2 + i2)) * N3 + (g3 + i3);
+      vr = theta[C * gi];
+      if (CPLX) vi = theta[C * gi + 1];
+    }
+    tile[C * t] = vr;
+    if (CPLX) tile[C * t + 1] = vi;
+  }
+  __syncthreads();
+  const int beg = brick_start[brick], nbp = brick_start[brick + 1] - beg;
+  const int nvw = (nbp + 31) >> 5, lane = threadIdx.x & 31;
+  for (int vw = threadIdx.x >> 5; vw < nvw; vw += blockDim.x >> 5) {
+    const int pi = brick_point(nbp, vw, lane);
+    if (pi < 0) continue;
+    const BrickPoint<T> pt = bp[beg + pi];
+    T w1[P], w2[P], w3[P], d1[P], d2[P], d3[P];
+    bspline_weights<T, P, true>(pt.u[0], w1, d1);
+    bspline_weights<T, P, true>(pt.u[1], w2, d2);
+    bspline_weights<T, P, true>(pt.u[2], w3, d3);
+    const int l1 = (int)(pt.g0 >> 20) - b1 * kBrick;
+    const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
+    const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
+    T v[4] = {0, 0, 0, 0}, vi[4] = {0, 0, 0, 0};
 #pragma unroll
-  for (int t1 = 0; t1 < P; t1++) {
+    for (int t1 = 0; t1 < P; t1++) {
 #pragma unroll
-    for (int t2 = 0; t2 < P; t2++) {
-      const T *row = theta + C * (((g1 + t1) * N2 + (g2 + t2)) * N3 + g3);
-      T tb = 0, td = 0, tbi = 0, tdi = 0;
+      for (int t2 = 0; t2 < P; t2++) {
+        const T *row = tile + C * (((l1 + t1) * TL + (l2 + t2)) * TL + l3);
+        T tb = 0, td = 0, tbi = 0, tdi = 0;
 #pragma unroll
-      for (int t3 = 0; t3 < P; t3++) {
-        const T th = __ldg(row + C * t3);
-        tb = fma(th, w3[t3], tb);
-        td = fma(th, d3[t3], td);
+        for (int t3 = 0; t3 < P; t3++) {
+          const T th = row[C * t3];
+          tb = fma(th, w3[t3], tb);
+          td = fma(th, d3[t3], td);
+          if (CPLX) {
+            const T thi = row[C * t3 + 1];
+            tbi = fma(thi, w3[t3], tbi);
+            tdi = fma(thi, d3[t3], tdi);
+          }
+        }
+        const T A1 = w1[t1] * w2[t2], A2 = d1[t1] * w2[t2], A3 = w1[t1] * d2[t2];
+        v[0] = fma(A1, tb, v[0]);
+        v[1] = fma(A2, tb, v[1]);
+        v[2] = fma(A3, tb, v[2]);
+        v[3] = fma(A1, td, v[3]);
         if (CPLX) {
-          const T thi = __ldg(row + C * t3 + 1);
-          tbi = fma(thi, w3[t3], tbi);
-          tdi = fma(thi, d3[t3], tdi);
+          vi[0] = fma(A1, tbi, vi[0]);
+          vi[1] = fma(A2, tbi, vi[1]);
+          vi[2] = fma(A3, tbi, vi[2]);
+          vi[3] = fma(A1, tdi, vi[3]);
         }
       }
-      const T A1 = w1[t1] * w2[t2], A2 = d1[t1] * w2[t2], A3 = w1[t1] * d2[t2];
-      v[0] = fma(A1, tb, v[0]);
-      v[1] = fma(A2, tb, v[1]);
-      v[2] = fma(A3, tb, v[2]);
-      v[3] = fma(A1, td, v[3]);
-      if (CPLX) {
-        vi[0] = fma(A1, tbi, vi[0]);
-        vi[1] = fma(A2, tbi, vi[1]);
-        vi[2] = fma(A3, tbi, vi[2]);
-        vi[3] = fma(A1, tdi, vi[3]);
-      }
     }
-  }
-  const T sc[4] = {T(1), c1, c2, c3};
-  const long o = pt.orig;
-  if (CPLX) {
-    double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+    const T sc[4] = {T(1), c1, c2, c3};
+    const long o = pt.orig;
+    if (CPLX) {
+      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      double2 a = Vo[m];
-      a.x += (double)(v[m] * sc[m]);
-      a.y += (double)(vi[m] * sc[m]);
-      Vo[m] = a;
+      for (int m = 0; m < 4; m++) {
+        double2 a = Vo[m];
+        a.x += (double)(v[m] * sc[m]);
+        a.y += (double)(vi[m] * sc[m]);
+        Vo[m] = a;
+      }
+    } else {
+      double4 *Vo = reinterpret_cast<double4 *>(V) + o;
+      double4 a = *Vo;
+      a.x += (double)v[0];
+      a.y += (double)(v[1] * c1);
+      a.z += (double)(v[2] * c2);
+      a.w += (double)(v[3] * c3);
+      *Vo = a;
     }
-  } else {
-    double4 *Vo = reinterpret_cast<double4 *>(V) + o;
-    double4 a = *Vo;
-    a.x += (double)v[0];
-    a.y += (double)(v[1] * c1);
-    a.z += (double)(v[2] * c2);
-    a.w += (double)(v[3] * c3);
-    *Vo = a;
   }
 }
 

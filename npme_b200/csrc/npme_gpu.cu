@@ -402,6 +402,36 @@ int upload_points(npme_handle *h, const double *coord) {
   std::vector<int> blist;
   for (long b = 0; b < nbt; b++)
     if (bstart[b + 1] > bstart[b]) blist.push_back((int)b);
+  // inside a brick, points sorted by the shared-memory bank of their stencil
+  // origin in the brick's tile (the kernels give the lanes of a warp points
+  // of different banks; see brick_point in bodies.cuh)
+  {
+    const int TL = npme::kBrick + P - 1;
+    const int words = (int)(sizeof(T) / 4) * (h->complex_kernel ? 2 : 1);
+    const int nkeys = 32 / words;
+    std::vector<BrickPoint<T>> tmp;
+    int cnt[32];
+    for (const int b : blist) {
+      const int beg = bstart[b], end = bstart[b + 1];
+      const long b3 = b % g.nb[2], b2 = (b / g.nb[2]) % g.nb[1], b1 = b / (g.nb[2] * g.nb[1]);
+      auto key = [&](const BrickPoint<T> &pt) {
+        const long l1 = (long)(pt.g0 >> 20) - b1 * npme::kBrick;
+        const long l2 = (long)((pt.g0 >> 10) & 1023u) - b2 * npme::kBrick;
+        const long l3 = (long)(pt.g0 & 1023u) - b3 * npme::kBrick;
+        return (int)(((l1 * TL + l2) * TL + l3) % nkeys);
+      };
+      tmp.assign(sorted.begin() + beg, sorted.begin() + end);
+      std::fill(cnt, cnt + 32, 0);
+      for (const auto &pt : tmp) cnt[key(pt)]++;
+      int acc = beg;
+      for (int k = 0; k < nkeys; k++) {
+        const int c = cnt[k];
+        cnt[k] = acc;
+        acc += c;
+      }
+      for (const auto &pt : tmp) sorted[cnt[key(pt)]++] = pt;
+    }
+  }
   h->n_bricks = nbt;
   h->n_nonempty = (long)blist.size();
 

@@ -473,28 +473,31 @@ void launch_multiply(npme_handle *h, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // Interpolation (src/RecSumV.cpp:201-306, 308-434): V += sum theta B1 B2 B3,
 // dV/dx_d += (N_d / L_d) sum theta dB_d ..., real kernels keep the real part
-// (src/RecSumV.cpp:395-398).  One thread per point in brick order; V is
-// accumulated into the caller-order output, which already holds the direct
-// sum.
+// (src/RecSumV.cpp:395-398).  One CTA per non-empty brick, which reads the
+// brick's theta tile into shared memory; V is accumulated into the
+// caller-order output, which already holds the direct sum.
 
 template <typename T, int P, bool CPLX>
 __global__ void __launch_bounds__(256) interp_kernel(
+    const int *__restrict__ brick_list, const int *__restrict__ brick_start,
     const BrickPoint<T> *__restrict__ bp, const T *__restrict__ theta, double *__restrict__ V,
-    long n, long N2, long N3, T c1, T c2, T c3) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x)
-    interp_body<T, P, CPLX>(bp[i], theta, V, N2, N3, c1, c2, c3);
+    int nb2, int nb3, long N1, long N2, long N3, T c1, T c2, T c3) {
+  extern __shared__ unsigned char smem_raw[];
+  interp_brick_body<T, P, CPLX>(brick_list[blockIdx.x], brick_start, bp, theta, V, nb2, nb3, N1,
+                                N2, N3, c1, c2, c3, reinterpret_cast<T *>(smem_raw));
 }
 
 template <typename T, bool CPLX, int P>
 static void interp_dispatch(npme_handle *h, double *d_V, cudaStream_t s) {
-  const int threads = 256;
-  const int blocks = (int)std::min<long>((h->n + threads - 1) / threads, 148 * 32);
+  constexpr int TL = kBrick + P - 1;
+  const size_t smem = sizeof(T) * TL * TL * TL * (CPLX ? 2 : 1);
   const double *L = h->box + 6;
-  interp_kernel<T, P, CPLX><<<blocks, threads, 0, s>>>(
-      (const BrickPoint<T> *)h->d_bpts, (const T *)h->d_grid, d_V, (long)h->n, h->grid.N[1],
-      h->grid.N[2], (T)(h->grid.N[0] / L[0]), (T)(h->grid.N[1] / L[1]),
-      (T)(h->grid.N[2] / L[2]));
+  auto kern = interp_kernel<T, P, CPLX>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<(unsigned)h->n_nonempty, 256, smem, s>>>(
+      h->d_brick_list, h->d_brick_start, (const BrickPoint<T> *)h->d_bpts, (const T *)h->d_grid,
+      d_V, (int)h->grid.nb[1], (int)h->grid.nb[2], h->grid.N[0], h->grid.N[1], h->grid.N[2],
+      (T)(h->grid.N[0] / L[0]), (T)(h->grid.N[1] / L[1]), (T)(h->grid.N[2] / L[2]));
 }
 
 template <typename T, bool CPLX>
@@ -509,6 +512,7 @@ static void interp_order(npme_handle *h, double *d_V, cudaStream_t s) {
 }
 
 void launch_interp(npme_handle *h, double *d_V, cudaStream_t s) {
+  if (h->n_nonempty == 0) return;
   if (h->fp32) {
     if (h->complex_kernel) interp_order<float, true>(h, d_V, s);
     else interp_order<float, false>(h, d_V, s);
