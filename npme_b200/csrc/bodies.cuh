@@ -292,26 +292,25 @@ __device__ __forceinline__ void packed_block(
     const bool h0 = r2[u].x <= R2 && r2[u].x > 0.f, h1 = r2[u].y <= R2 && r2[u].y > 0.f;
     const float2 rr = make_float2(h0 ? r2[u].x : R2, h1 ? r2[u].y : R2);
     const float2 qm = make_float2(h0 ? q[u].x : 0.f, h1 ? q[u].y : 0.f);
-    const float2 sv = __fmul2_rn(rr, k.invR2_2);
-    float2 np = k.nar2[ND];  // -f_LR polynomial
+    const float2 sv = rr;    // scaled coordinates: r^2 = s
+    float2 np = k.nar2[ND];  // -Rdir^(-alpha) f_LR polynomial
 #pragma unroll
     for (int n = ND - 1; n >= 0; n--) np = __ffma2_rn(np, sv, k.nar2[n]);
-    float2 d = k.br2[ND - 1];  // (1/r) d f_LR / dr polynomial
+    float2 d = k.br2[ND - 1];  // Rdir^(2-alpha) (1/r) d f_LR / dr polynomial
 #pragma unroll
     for (int n = ND - 2; n >= 0; n--) d = __ffma2_rn(d, sv, k.br2[n]);
     float2 f0, t;  // t = -f1
     if (FUNC == 0) {
       const float2 ri = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
-      f0 = __fadd2_rn(ri, np);                    // 1/r - f_LR
-      t = __ffma2_rn(__fmul2_rn(ri, ri), ri, d);  // 1/r^3 + d
+      f0 = __fadd2_rn(ri, np);                    // Rdir (1/r - f_LR)
+      t = __ffma2_rn(__fmul2_rn(ri, ri), ri, d);  // -Rdir^3 f1
     } else {
-      // r^alpha = 2^((alpha/2) log2 r^2) on the special-function unit;
-      // 1/r^2 = rsqrt(r^2)^2
+      // s^(alpha/2) = 2^((alpha/2) log2 s) on the special-function unit;
+      // 1/s = rsqrt(s)^2
       const float2 e0 = make_float2(exp2f(k.half_alpha * __log2f(rr.x)),
                                     exp2f(k.half_alpha * __log2f(rr.y)));
       const float2 ri = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
       f0 = __fadd2_rn(e0, np);
-      // -f1 = d - alpha r^alpha / r^2
       t = __ffma2_rn(__fmul2_rn(e0, make_float2(-k.alpha, -k.alpha)), __fmul2_rn(ri, ri), d);
     }
     const float2 gq = __fmul2_rn(t, qm);
@@ -359,16 +358,18 @@ __device__ __forceinline__ void direct_group_packed(
   const bool active = lane < G.y;
   // idle lanes sit far outside the cutoff
   float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f;
+  const double ir = k.invR;  // coordinates in units of Rdir
   if (active) {
     const double4 p = gpos[ti];
-    const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+    const double dx = (p.x - c.x) * ir, dy = (p.y - c.y) * ir, dz = (p.z - c.z) * ir;
     tx = (float)dx, ty = (float)dy, tz = (float)dz;
     tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
   }
   const float2 tx2 = make_float2(tx, tx), ty2 = make_float2(ty, ty), tz2 = make_float2(tz, tz);
   const float2 tl2x = make_float2(tlx, tlx), tl2y = make_float2(tly, tly),
                tl2z = make_float2(tlz, tlz);
-  const float R2 = k.R2;
+  const float R2 = 1.f;
+  refine2 = (float)((double)refine2 * ir * ir);
   double acc[4] = {0, 0, 0, 0};
   float *sa = reinterpret_cast<float *>(sp), *la = reinterpret_cast<float *>(slo);
   const int slot = (lane >> 1) * 4 + (lane & 1);
@@ -390,7 +391,7 @@ __device__ __forceinline__ void direct_group_packed(
     {
       float hx = 1e18f, hy = 1e18f, hz = 1e18f, q = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
       if (pv) {
-        const double dx = px - c.x, dy = py - c.y, dz = pz - c.z;
+        const double dx = (px - c.x) * ir, dy = (py - c.y) * ir, dz = (pz - c.z) * ir;
         hx = (float)dx, hy = (float)dy, hz = (float)dz;
         lx = (float)(dx - (double)hx), ly = (float)(dy - (double)hy), lz = (float)(dz - (double)hz);
         q = pq;
@@ -426,8 +427,10 @@ __device__ __forceinline__ void direct_group_packed(
   }
   if (active) {
     const long o = perm[ti];
-    acc[0] -= fself_r * qcaller[o];  // src/Interface.cpp:2061-2062
-    reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+    const double vs = k.vscale, gs = k.gscale;
+    // V -= f_LR(0) q (src/Interface.cpp:2061-2062)
+    reinterpret_cast<double4 *>(V)[o] =
+        make_double4(vs * acc[0] - fself_r * qcaller[o], gs * acc[1], gs * acc[2], gs * acc[3]);
   }
 }
 

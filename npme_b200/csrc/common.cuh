@@ -29,10 +29,16 @@ struct PairCoef {
   T k0r, k0i;
   T ar[kMaxDeriv + 1], ai[kMaxDeriv + 1];
   T br[kMaxDeriv + 1], bi[kMaxDeriv + 1];
-  // the real coefficients as equal pairs for the packed (two pairs per
-  // instruction) evaluation: -ar[n] and br[n]; (invR2, invR2)
+  // Packed (two pairs per instruction) evaluation of the real kernels
+  // works in coordinates scaled by 1/Rdir, so r^2 is s itself.  With
+  // alpha = -1 for 1/r it accumulates
+  //   f0' = s^(alpha/2) - Rdir^(-alpha) f_LR  = Rdir^(-alpha) f0,
+  //   t'  = Rdir^(2-alpha) d - alpha s^(alpha/2) / s = -Rdir^(2-alpha) f1,
+  // so V = vscale sum q f0' and grad V = -gscale sum q t' x' with
+  // vscale = Rdir^alpha, gscale = Rdir^(alpha-1).  Coefficient pairs:
+  // nar2[n] = -Rdir^(-alpha) ar[n], br2[n] = Rdir^(2-alpha) br[n].
   typename Vec2<T>::type nar2[kMaxDeriv + 1], br2[kMaxDeriv + 1];
-  typename Vec2<T>::type invR2_2;
+  double invR, vscale, gscale;
 };
 
 template <typename T> struct Vec4;

@@ -43,11 +43,17 @@ PairCoef<T> make_pair_coef(const npme_handle *h) {
     k.ai[i] = (T)(h->a_i[i] * s);
     k.br[i] = (T)(h->b_r[i] * s);
     k.bi[i] = (T)(h->b_i[i] * s);
-    k.nar2[i].x = k.nar2[i].y = -k.ar[i];
-    k.br2[i].x = k.br2[i].y = k.br[i];
+    const double al = h->p.funcType == NPME_FUNC_RALPHA ? h->p.alpha : -1.0;
+    k.nar2[i].x = k.nar2[i].y = (T)(-h->a_r[i] * s * std::pow(R, -al));
+    k.br2[i].x = k.br2[i].y = (T)(h->b_r[i] * s * std::pow(R, 2.0 - al));
     s *= R2;
   }
-  k.invR2_2.x = k.invR2_2.y = k.invR2;
+  {
+    const double al = h->p.funcType == NPME_FUNC_RALPHA ? h->p.alpha : -1.0;
+    k.invR = 1.0 / R;
+    k.vscale = std::pow(R, al);
+    k.gscale = std::pow(R, al - 1.0);
+  }
   return k;
 }
 template PairCoef<float> make_pair_coef<float>(const npme_handle *);

@@ -328,6 +328,23 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
                                  0.5 * (bl[2] + bh[2]), 0.0));
     }
   }
+  // heaviest groups first, so the last wave of the launch holds the light ones
+  {
+    std::vector<long> work(groups.size());
+    for (size_t g = 0; g < groups.size(); g++) {
+      long c = 0;
+      for (int t = groups[g].z; t < groups[g].w; t++) c += segs[t].y;
+      work[g] = c;
+    }
+    std::vector<uint32_t> go(groups.size());
+    for (size_t g = 0; g < go.size(); g++) go[g] = (uint32_t)g;
+    std::stable_sort(go.begin(), go.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
+    std::vector<int4> g2(groups.size());
+    std::vector<double4> c2(cen.size());
+    for (size_t g = 0; g < go.size(); g++) g2[g] = groups[go[g]], c2[g] = cen[go[g]];
+    groups.swap(g2);
+    cen.swap(c2);
+  }
   std::vector<double4> gpos(n), spos(n);
   for (size_t k = 0; k < n; k++) {
     const double *x = coord + 3 * (size_t)order[k];
