@@ -247,7 +247,7 @@ __device__ __forceinline__ void interp_brick_body(int brick, const int *__restri
 // r^2 = Rdir^2 and charge 0.  The whole pair phase is skipped when no lane
 // of the warp has a hit in the block.
 #ifndef NPME_PACKED_BLOCK
-#define NPME_PACKED_BLOCK 4
+#define NPME_PACKED_BLOCK 2
 #endif
 constexpr int kPackedBlock = NPME_PACKED_BLOCK;
 
@@ -257,42 +257,46 @@ __device__ __forceinline__ void packed_block(
     float2 ty2, float2 tz2, float2 tl2x, float2 tl2y, float2 tl2z, float R2, float refine2,
     float2 &P0, float2 &N1, float2 &N2, float2 &N3) {
   constexpr int U = kPackedBlock;
-  float2 x[U], y[U], z[U], r2[U], q[U];
+  // rr: r^2 of the pairs inside the cutoff, R2 for the others (and for the
+  // target itself); qm: their charges, 0 for the others.  A pair is inside
+  // iff 0 < r^2 <= R2, i.e. iff bits(r^2) - 1 < bits(R2) as unsigned
+  // integers (r^2 >= 0).
+  float2 x[U], y[U], z[U], rr[U], qm[U];
   float rmin = 3.0e38f;
   bool any = false;
+  const unsigned rb = __float_as_uint(R2);
 #pragma unroll
   for (int u = 0; u < U; u++) {
     const float4 A = sp[s0 + u], B = sp[16 + s0 + u];
     x[u] = __fadd2_rn(tx2, make_float2(A.x, A.y));
     y[u] = __fadd2_rn(ty2, make_float2(A.z, A.w));
     z[u] = __fadd2_rn(tz2, make_float2(B.x, B.y));
-    q[u] = make_float2(B.z, B.w);
-    r2[u] = __ffma2_rn(x[u], x[u], __ffma2_rn(y[u], y[u], __fmul2_rn(z[u], z[u])));
-    rmin = fminf(rmin, fminf(r2[u].x, r2[u].y));
-    any |= (r2[u].x <= R2) | (r2[u].y <= R2);
+    const float2 r2 = __ffma2_rn(x[u], x[u], __ffma2_rn(y[u], y[u], __fmul2_rn(z[u], z[u])));
+    const bool h0 = __float_as_uint(r2.x) - 1u < rb, h1 = __float_as_uint(r2.y) - 1u < rb;
+    rr[u] = make_float2(h0 ? r2.x : R2, h1 ? r2.y : R2);
+    qm[u] = make_float2(h0 ? B.z : 0.f, h1 ? B.w : 0.f);
+    rmin = fminf(rmin, fminf(rr[u].x, rr[u].y));
+    any |= h0 | h1;
   }
   if (!__any_sync(0xffffffffu, any)) return;
   if (rmin < refine2) {  // close pair: exact difference from head + residual
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      if (fminf(r2[u].x, r2[u].y) < refine2) {
+      if (fminf(rr[u].x, rr[u].y) < refine2) {
         const float4 LA = slo[s0 + u], LB = slo[16 + s0 + u];
         x[u] = __fadd2_rn(x[u], __fadd2_rn(tl2x, make_float2(LA.x, LA.y)));
         y[u] = __fadd2_rn(y[u], __fadd2_rn(tl2y, make_float2(LA.z, LA.w)));
         z[u] = __fadd2_rn(z[u], __fadd2_rn(tl2z, make_float2(LB.x, LB.y)));
         const float2 rn = __ffma2_rn(x[u], x[u], __ffma2_rn(y[u], y[u], __fmul2_rn(z[u], z[u])));
-        // keep the hit decision of the unrefined distance
-        r2[u].x = r2[u].x > 0.f && r2[u].x <= R2 ? rn.x : r2[u].x;
-        r2[u].y = r2[u].y > 0.f && r2[u].y <= R2 ? rn.y : r2[u].y;
+        // the hit decision stays that of the unrefined distance
+        rr[u].x = rr[u].x < R2 ? rn.x : rr[u].x;
+        rr[u].y = rr[u].y < R2 ? rn.y : rr[u].y;
       }
     }
   }
 #pragma unroll
   for (int u = 0; u < U; u++) {
-    const bool h0 = r2[u].x <= R2 && r2[u].x > 0.f, h1 = r2[u].y <= R2 && r2[u].y > 0.f;
-    const float2 rr = make_float2(h0 ? r2[u].x : R2, h1 ? r2[u].y : R2);
-    const float2 qm = make_float2(h0 ? q[u].x : 0.f, h1 ? q[u].y : 0.f);
-    const float2 sv = rr;    // scaled coordinates: r^2 = s
+    const float2 sv = rr[u];  // scaled coordinates: r^2 = s
     float2 np = k.nar2[ND];  // -Rdir^(-alpha) f_LR polynomial
 #pragma unroll
     for (int n = ND - 1; n >= 0; n--) np = __ffma2_rn(np, sv, k.nar2[n]);
@@ -301,20 +305,20 @@ __device__ __forceinline__ void packed_block(
     for (int n = ND - 2; n >= 0; n--) d = __ffma2_rn(d, sv, k.br2[n]);
     float2 f0, t;  // t = -f1
     if (FUNC == 0) {
-      const float2 ri = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+      const float2 ri = make_float2(rsqrtf(sv.x), rsqrtf(sv.y));
       f0 = __fadd2_rn(ri, np);                    // Rdir (1/r - f_LR)
       t = __ffma2_rn(__fmul2_rn(ri, ri), ri, d);  // -Rdir^3 f1
     } else {
       // s^(alpha/2) = 2^((alpha/2) log2 s) on the special-function unit;
       // 1/s = rsqrt(s)^2
-      const float2 e0 = make_float2(exp2f(k.half_alpha * __log2f(rr.x)),
-                                    exp2f(k.half_alpha * __log2f(rr.y)));
-      const float2 ri = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+      const float2 e0 = make_float2(exp2f(k.half_alpha * __log2f(sv.x)),
+                                    exp2f(k.half_alpha * __log2f(sv.y)));
+      const float2 ri = make_float2(rsqrtf(sv.x), rsqrtf(sv.y));
       f0 = __fadd2_rn(e0, np);
       t = __ffma2_rn(__fmul2_rn(e0, make_float2(-k.alpha, -k.alpha)), __fmul2_rn(ri, ri), d);
     }
-    const float2 gq = __fmul2_rn(t, qm);
-    P0 = __ffma2_rn(f0, qm, P0);
+    const float2 gq = __fmul2_rn(t, qm[u]);
+    P0 = __ffma2_rn(f0, qm[u], P0);
     N1 = __ffma2_rn(gq, x[u], N1);
     N2 = __ffma2_rn(gq, y[u], N2);
     N3 = __ffma2_rn(gq, z[u], N3);
