@@ -251,6 +251,26 @@ int npme_gpu_calcv_exact_real(npme_handle *h, double *V, size_t n,
 int npme_gpu_calcv_exact_complex(npme_handle *h, double *V, size_t n,
                                  const double *charge, const double *coord);
 
+/* CalcV_exact (FP64, full kernel, no self term) at m of the set-up points:
+ * row t of V (4 doubles, or 4 complex) is the point targets[t], summed over
+ * all n charges (charge: n or 2n doubles).  No counterpart in the
+ * reference; the grid chooser measures errors with it. */
+int npme_gpu_calcv_exact_subset(npme_handle *h, double *V, size_t m,
+                                const unsigned int *targets, const double *charge);
+
+/* FFT box for a solve that names none, the job of the reference's
+ * NPME_AddMissingKeywords (src/Interface.cpp:256-432), which predicts it
+ * with its RSEM error model (src/EstimateParm.cpp).  Here the error is
+ * measured instead: starting from a coarse box, the box is refined until the
+ * RMS absolute potential error against the exact sum, over up to 4096
+ * sampled points, is <= tol (the reference's tol: an absolute RMS error of
+ * V), or the FFT arrays would exceed maxFFTmemGB.  p gives every other
+ * parameter (its N1..N3 are ignored); on return *out = p with N1..N3 set and
+ * *err the measured error.  Uses the GPU (a few solves of the system). */
+int npme_gpu_choose_grid(const npme_params *p, size_t n, const double *coord,
+                         const double *charge, double tol, double maxFFTmemGB,
+                         npme_params *out, double *err);
+
 /* Number of unordered point pairs with r <= Rdir in the set-up geometry
  * (the work of the direct sum), counted on the device with the cell list. */
 int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs);

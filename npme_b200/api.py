@@ -101,6 +101,7 @@ EXPORTS = (
     "npme_gpu_server_default_config", "npme_gpu_server_create", "npme_gpu_submit",
     "npme_gpu_poll", "npme_gpu_wait", "npme_gpu_ticket_info", "npme_gpu_release_ticket",
     "npme_gpu_server_stats", "npme_gpu_server_destroy",
+    "npme_gpu_calcv_exact_subset", "npme_gpu_choose_grid",
 )
 VOID_EXPORTS = ("npme_gpu_default_params", "npme_gpu_server_default_config")
 
@@ -265,6 +266,16 @@ class Solver:
             self.h, ctypes.c_void_p(V_ptr), ctypes.c_void_p(q_ptr),
             ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 
+    def calcv_exact_subset(self, targets, q):
+        """Exact FP64 sum at the set-up points `targets` (indices) from all
+        charges; row t of the result is point targets[t]."""
+        t = np.ascontiguousarray(targets, dtype=np.uint32)
+        qb = self._q(q)
+        V = np.empty((t.size, 8 if self.complex else 4), dtype=np.float64)
+        self._check(self.L.npme_gpu_calcv_exact_subset(
+            self.h, _dp(V), t.size, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), _dp(qb)))
+        return V.view(np.complex128) if self.complex else V
+
     def count_pairs(self):
         """Unordered pairs with r <= Rdir (direct-sum work)."""
         c = ctypes.c_ulonglong()
@@ -348,6 +359,24 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def choose_grid(params, coord, q, tol, max_fft_gb=10.0):
+    """FFT box meeting an RMS absolute potential error `tol`, by measurement
+    (npme_gpu_choose_grid).  Returns (params with N1..N3 set, error)."""
+    L = load_library()
+    c = np.ascontiguousarray(coord, dtype=np.float64).reshape(-1, 3)
+    cplx = params.funcType == FUNC["helmholtz"]
+    qb = (np.ascontiguousarray(q, dtype=np.complex128).view(np.float64) if cplx
+          else np.ascontiguousarray(q, dtype=np.float64))
+    out = Params()
+    err = ctypes.c_double()
+    rc = L.npme_gpu_choose_grid(ctypes.byref(params), c.shape[0], _dp(c), _dp(qb),
+                                ctypes.c_double(tol), ctypes.c_double(max_fft_gb),
+                                ctypes.byref(out), ctypes.byref(err))
+    if rc:
+        raise _err(L, None, rc)
+    return out, err.value
 
 
 class NativeServer:

@@ -18,7 +18,10 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libnpme_gpu.so")
 SOURCES = ["npme_gpu.cu", "recsum.cu", "direct.cu", "noalloc.cu", "batch.cu", "fft.cu",
-           "server.cu"]
+           "server.cu", "choose.cu"]
+APPS = os.path.join(HERE, "apps")
+BIN = os.path.join(HERE, "bin")
+APPS_SRC = ["npme", "compareV", "makeRandomBox"]
 HEADERS = ["common.cuh", "bodies.cuh", "internal.h",
            os.path.join("..", "..", "include", "npme_gpu.h")]
 
@@ -74,7 +77,26 @@ def build(force=False, verbose=False):
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + p.stderr[-4000:])
+    build_apps(force)
     return LIB
+
+
+def build_apps(force=False):
+    """Command-line tools of the reference (npme, compareV, makeRandomBox)
+    over the C ABI, into npme_b200/bin/ (rpath to the library)."""
+    os.makedirs(BIN, exist_ok=True)
+    cxx = shutil.which("g++") or "g++"
+    hdrs = [os.path.join(APPS, "npme_io.h"), os.path.join(HERE, "..", "include", "npme_gpu.h")]
+    for app in APPS_SRC:
+        src = os.path.join(APPS, app + ".cpp")
+        exe = os.path.join(BIN, app)
+        if not force and not _stale(exe, [src, LIB] + hdrs):
+            continue
+        cmd = [cxx, "-std=c++17", "-O2", "-o", exe, src, "-L" + HERE, "-lnpme_gpu",
+               "-Wl,-rpath,$ORIGIN/.."]
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError("app build failed:\n" + " ".join(cmd) + "\n" + p.stderr[-4000:])
 
 
 if __name__ == "__main__":

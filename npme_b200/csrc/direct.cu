@@ -360,12 +360,15 @@ template <int FUNC>
 __global__ void __launch_bounds__(kExactBS) exact_kernel(const double *__restrict__ coord,
                                                           const double *__restrict__ q, long n,
                                                           double alpha, double k0r, double k0i,
-                                                          double *__restrict__ V) {
+                                                          const uint32_t *__restrict__ tidx,
+                                                          long nt, double *__restrict__ V) {
   constexpr bool CPLX = FUNC == 2;
   __shared__ double4 sp[kExactBS];
   __shared__ double2 sq[kExactBS];
-  const long i = blockIdx.x * (long)kExactBS + threadIdx.x;
-  const bool active = i < n;
+  // output row t holds target tidx[t] (every point when tidx is null)
+  const long t = blockIdx.x * (long)kExactBS + threadIdx.x;
+  const bool active = t < nt;
+  const long i = active ? (tidx ? (long)tidx[t] : t) : -1;
   double xi = 0, yi = 0, zi = 0;
   if (active) xi = coord[3 * i], yi = coord[3 * i + 1], zi = coord[3 * i + 2];
   double a[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
@@ -416,28 +419,30 @@ __global__ void __launch_bounds__(kExactBS) exact_kernel(const double *__restric
   }
   if (active) {
     if (CPLX) {
-      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * i;
+      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * t;
       for (int m = 0; m < 4; m++) Vo[m] = make_double2(a[m], ai[m]);
     } else {
-      reinterpret_cast<double4 *>(V)[i] = make_double4(a[0], a[1], a[2], a[3]);
+      reinterpret_cast<double4 *>(V)[t] = make_double4(a[0], a[1], a[2], a[3]);
     }
   }
 }
 
-void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s) {
+void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s,
+                  const uint32_t *d_tidx, long nt) {
   const long n = (long)h->n;
-  const int blocks = (int)((n + kExactBS - 1) / kExactBS);
+  if (!d_tidx) nt = n;
+  const int blocks = (int)((nt + kExactBS - 1) / kExactBS);
   if (blocks == 0) return;
   const int f = h->p.funcType;
   if (f == 0)
     exact_kernel<0><<<blocks, kExactBS, 0, s>>>(h->d_coord, d_q, n, h->p.alpha, h->p.k0_r,
-                                                 h->p.k0_i, d_V);
+                                                 h->p.k0_i, d_tidx, nt, d_V);
   else if (f == 1)
     exact_kernel<1><<<blocks, kExactBS, 0, s>>>(h->d_coord, d_q, n, h->p.alpha, h->p.k0_r,
-                                                 h->p.k0_i, d_V);
+                                                 h->p.k0_i, d_tidx, nt, d_V);
   else
     exact_kernel<2><<<blocks, kExactBS, 0, s>>>(h->d_coord, d_q, n, h->p.alpha, h->p.k0_r,
-                                                 h->p.k0_i, d_V);
+                                                 h->p.k0_i, d_tidx, nt, d_V);
   h->launches++;
 }
 

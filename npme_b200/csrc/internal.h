@@ -101,6 +101,7 @@ struct npme_handle {
   double *d_V = nullptr;         // staging for host output (4n or 8n doubles)
   double *d_V_exact = nullptr;
   int *d_err = nullptr;          // device error flag
+  uint32_t *d_tidx = nullptr;    // target list of the exact subset sum
   size_t dev_bytes = 0;
   std::map<void *, size_t> caps;  // pointer field -> capacity of its buffer
   // kernel-transform construction scratch (kept to reuse across set-ups)
@@ -134,6 +135,9 @@ namespace npme {
 
 // npme_gpu.cu: capacity-tracked device buffer owned by the handle
 int handle_buffer(npme_handle *h, void **field, size_t bytes);
+// PME-corrected half extent X of a box of half extent X0 for an N-point FFT
+// axis (src/RecSumSupportFunctions.cpp:137-147)
+double compact_extent(double X0, double del, long order, long N);
 
 // fft.cu
 int prepare_plans(npme_handle *h);
@@ -162,7 +166,10 @@ void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t 
 void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s);
 // caller-order charges (double) -> direct-sum order in the bulk precision
 void launch_gather_direct(npme_handle *h, const double *d_q, void *d_qdst, cudaStream_t s);
-void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
+// exact O(N^2) sum; with d_tidx, only for the nt targets listed (output row t
+// = target d_tidx[t])
+void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s,
+                  const uint32_t *d_tidx = nullptr, long nt = 0);
 void launch_count_pairs(npme_handle *h, unsigned long long *d_count, cudaStream_t s);
 template <typename T>
 PairCoef<T> make_pair_coef(const npme_handle *h);

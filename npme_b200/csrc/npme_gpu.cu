@@ -197,6 +197,10 @@ int dalloc(npme_handle *h, P **ptr, size_t bytes) {
 
 }  // namespace
 
+double npme::compact_extent(double X0, double del, long order, long N) {
+  return min_x_compact(X0, del, order, N);
+}
+
 int npme::handle_buffer(npme_handle *h, void **field, size_t bytes) {
   return dalloc(h, field, bytes);
 }
@@ -859,6 +863,31 @@ static int exact_host(npme_handle *h, double *V, size_t n, const double *charge,
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(V, h->d_V, sizeof(double) * 4 * C * n, cudaMemcpyDeviceToHost,
                      h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return NPME_OK;
+}
+
+int npme_gpu_calcv_exact_subset(npme_handle *h, double *V, size_t m,
+                                const unsigned int *targets, const double *charge) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!h->ready) return fail(h, NPME_ESTATE, "calcv_exact_subset before setup");
+  if (!V || !targets || !charge) return fail(h, NPME_EINVAL, "null buffer");
+  if (m == 0) return NPME_OK;
+  if (m > h->n) return fail(h, NPME_EINVAL, "more targets than points");
+  for (size_t t = 0; t < m; t++)
+    if (targets[t] >= h->n) return fail(h, NPME_EINVAL, "target index out of range");
+  CK(cudaSetDevice(h->device));
+  const int C = h->complex_kernel ? 2 : 1;
+  int rc;
+  if ((rc = dalloc(h, &h->d_tidx, sizeof(uint32_t) * m))) return rc;
+  CK(cudaMemcpyAsync(h->d_tidx, targets, sizeof(uint32_t) * m, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->d_q_in, charge, sizeof(double) * C * h->n, cudaMemcpyHostToDevice,
+                     h->stream));
+  h->launches = 0;
+  npme::launch_exact(h, h->d_q_in, h->d_V, h->stream, h->d_tidx, (long)m);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(V, h->d_V, sizeof(double) * 4 * C * m, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return NPME_OK;
 }
