@@ -11,7 +11,7 @@ namespace npme {
 
 constexpr int kGroupWarps = 4;  // warps per CTA of the FP32 direct sum
 #ifndef NPME_GROUP_MIN_BLOCKS
-#define NPME_GROUP_MIN_BLOCKS 5
+#define NPME_GROUP_MIN_BLOCKS 1
 #endif
 constexpr int kGroupMinBlocks = NPME_GROUP_MIN_BLOCKS;  // resident CTAs asked of ptxas
 #ifndef NPME_DIRECT_UNROLL
