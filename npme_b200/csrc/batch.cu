@@ -437,6 +437,10 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
 #undef NPME_BS
     b->launches++;
   }
+  {  // launch errors are checked before cuFFT runs
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return bfail(b, NPME_ECUDA, std::string("batch: ") + cudaGetErrorString(e));
+  }
   // 4. forward transforms
   for (int k = 0; k < m; k++) {
     npme_handle *h = hs[f32[k]];
@@ -449,6 +453,10 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     if (kv.first) batch_multiply_kernel<true><<<g, 256, 0, s>>>(D(c), O(c), (int)c.members.size());
     else batch_multiply_kernel<false><<<g, 256, 0, s>>>(D(c), O(c), (int)c.members.size());
     b->launches++;
+  }
+  {  // launch errors are checked before cuFFT runs
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return bfail(b, NPME_ECUDA, std::string("batch: ") + cudaGetErrorString(e));
   }
   // 6. inverse transforms
   for (int k = 0; k < m; k++) {

@@ -769,21 +769,25 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
                         (size_t)h->grid.N[0] * h->grid.N[1] * h->grid.N[2];
   tmark(h, 0, s);
   npme::launch_gather_charges(h, d_charge, s);
+  CK(cudaGetLastError());  // launch errors are checked before cuFFT runs
   tmark(h, 1, s);
   // the direct sum runs on stream2, overlapped with the reciprocal sum
   CK(cudaEventRecord(h->ev_fork, s));
   CK(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
   tmark(h, 8, h->stream2);
   npme::launch_direct(h, d_charge, d_V, h->stream2);
+  CK(cudaGetLastError());
   tmark(h, 9, h->stream2);
   CK(cudaEventRecord(h->ev_join, h->stream2));
   CK(cudaMemsetAsync(h->d_grid, 0, gbytes, s));
   npme::launch_spread(h, s);
+  CK(cudaGetLastError());
   tmark(h, 2, s);
   int frc = npme::fft_forward(h, s);
   if (frc) return frc;
   tmark(h, 3, s);
   npme::launch_multiply(h, s);
+  CK(cudaGetLastError());
   tmark(h, 4, s);
   if ((frc = npme::fft_inverse(h, s))) return frc;
   tmark(h, 5, s);
