@@ -438,6 +438,78 @@ __device__ __forceinline__ void direct_group_packed(
   }
 }
 
+// sin and cos of x on the special-function unit after a Cody-Waite
+// reduction to [-pi, pi] (2 pi split as 6.28125 + 1.9353071795864769e-3, the
+// first part exact in 8 bits so n * 6.28125 is exact for |n| < 2^16).
+__device__ __forceinline__ float2 sincos_sfu(float x) {
+  const float n = rintf(x * 0.15915494309189535f);
+  float y = fmaf(-n, 6.28125f, x);
+  y = fmaf(-n, 1.9353071795864769e-3f, y);
+  return make_float2(__cosf(y), __sinf(y));
+}
+
+// Helmholtz DM kernel exp(i k0 r)/r of the FP32 direct sum with packed
+// complex arithmetic: one source per lane per step, the (re, im) parts of
+// exp(i k0 r)/r, of the DM polynomials and of the charge products in
+// FP32x2 instructions, sin / cos on the special-function unit.  Same staged
+// chunk as the scalar body (sp: x, y, z, Re q; slo: low parts, Im q); pairs
+// outside the cutoff get r^2 = Rdir^2 and charge 0, the rare close pairs
+// are refined as in the scalar body.
+template <int ND>
+__device__ __forceinline__ void helmholtz_steps(const PairCoef<float> &k, const float4 *sp,
+                                                const float4 *slo, int cnt, float tx, float ty,
+                                                float tz, float tlx, float tly, float tlz,
+                                                float refine2, float2 &Pv, float2 &Gx,
+                                                float2 &Gy, float2 &Gz) {
+  const float R2 = k.R2;
+  const unsigned rb = __float_as_uint(R2);
+  const float2 ik = make_float2(-k.k0i, k.k0r);  // i k0
+#pragma unroll 4
+  for (int s = 0; s < cnt; s++) {
+    const float4 src = sp[s];
+    float x = tx - src.x, y = ty - src.y, z = tz - src.z;
+    float r2 = fmaf(x, x, fmaf(y, y, z * z));
+    const bool hit = __float_as_uint(r2) - 1u < rb;  // 0 < r2 <= R2
+    if (hit && r2 < refine2) {  // close pair: exact difference from head + residual
+      const float4 lo = slo[s];
+      x += tlx - lo.x;
+      y += tly - lo.y;
+      z += tlz - lo.z;
+      r2 = fmaf(x, x, fmaf(y, y, z * z));
+    }
+    const float rr = hit ? r2 : R2;
+    const float4 lo = slo[s];
+    const float2 q = hit ? make_float2(src.w, lo.w) : make_float2(0.f, 0.f);
+    const float ri = rsqrtf(rr), r = rr * ri;
+    const float2 cs = sincos_sfu(k.k0r * r);
+    const float damp = k.k0i != 0.f ? __expf(-k.k0i * r) * ri : ri;
+    const float2 E = __fmul2_rn(cs, make_float2(damp, damp));  // exp(i k0 r) / r
+    // E1 = (i k0 E - E / r) / r, the radial derivative over r
+    const float2 IK = __ffma2_rn(make_float2(ik.x, ik.x), E,
+                                 __fmul2_rn(make_float2(-ik.y, ik.y), make_float2(E.y, E.x)));
+    const float ri2 = ri * ri;
+    const float2 E1 = __ffma2_rn(E, make_float2(-ri2, -ri2), __fmul2_rn(IK, make_float2(ri, ri)));
+    const float sv = rr * k.invR2;
+    const float2 s2 = make_float2(sv, sv);
+    float2 P = k.nac2[ND];
+#pragma unroll
+    for (int n = ND - 1; n >= 0; n--) P = __ffma2_rn(P, s2, k.nac2[n]);
+    float2 D = k.nbc2[ND - 1];
+#pragma unroll
+    for (int n = ND - 2; n >= 0; n--) D = __ffma2_rn(D, s2, k.nbc2[n]);
+    const float2 F0 = __fadd2_rn(E, P), F1 = __fadd2_rn(E1, D);
+    const float2 qs = make_float2(q.y, q.x);
+    // V += F0 q, G = F1 q (complex products)
+    Pv = __ffma2_rn(make_float2(F0.x, F0.x), q, Pv);
+    Pv = __ffma2_rn(make_float2(-F0.y, F0.y), qs, Pv);
+    const float2 G = __ffma2_rn(make_float2(-F1.y, F1.y), qs,
+                                __fmul2_rn(make_float2(F1.x, F1.x), q));
+    Gx = __ffma2_rn(G, make_float2(x, x), Gx);
+    Gy = __ffma2_rn(G, make_float2(y, y), Gy);
+    Gz = __ffma2_rn(G, make_float2(z, z), Gz);
+  }
+}
+
 // FP32 direct sum of one warp group (see direct.cu for the scheme): targets
 // gpos[G.x, G.x + G.y) in group order, sources spos / qs (charges gathered
 // into source order) over the segments [G.z, G.w); qcaller holds the
@@ -505,6 +577,13 @@ __device__ __forceinline__ void direct_group_body(
     pv = cur.seg < G.w;
     NPME_PREFETCH
     float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
+#if !defined(NPME_SCALAR_DIRECT)
+    if constexpr (CPLX && SPLIT == 0 && ND > 0) {
+      float2 Pv = make_float2(0.f, 0.f), Gx = Pv, Gy = Pv, Gz = Pv;
+      helmholtz_steps<ND>(k, sp, slo, cnt, tx, ty, tz, tlx, tly, tlz, refine2, Pv, Gx, Gy, Gz);
+      p0 = Pv.x, p0i = Pv.y, p1 = Gx.x, p1i = Gx.y, p2 = Gy.x, p2i = Gy.y, p3 = Gz.x, p3i = Gz.y;
+    } else
+#endif
 #pragma unroll kDirectUnroll
     for (int s = 0; s < cnt; s++) {
       const float4 src = sp[s];

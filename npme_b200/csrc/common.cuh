@@ -39,6 +39,8 @@ struct PairCoef {
   // nar2[n] = -Rdir^(-alpha) ar[n], br2[n] = Rdir^(2-alpha) br[n].
   typename Vec2<T>::type nar2[kMaxDeriv + 1], br2[kMaxDeriv + 1];
   double invR, vscale, gscale;
+  // Helmholtz packed evaluation: (re, im) pairs of -ar/-ai and -br/-bi
+  typename Vec2<T>::type nac2[kMaxDeriv + 1], nbc2[kMaxDeriv + 1];
 };
 
 template <typename T> struct Vec4;

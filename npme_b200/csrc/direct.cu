@@ -44,6 +44,8 @@ PairCoef<T> make_pair_coef(const npme_handle *h) {
     k.br[i] = (T)(h->b_r[i] * s);
     k.bi[i] = (T)(h->b_i[i] * s);
     const double al = h->p.funcType == NPME_FUNC_RALPHA ? h->p.alpha : -1.0;
+    k.nac2[i].x = (T)(-h->a_r[i] * s), k.nac2[i].y = (T)(-h->a_i[i] * s);
+    k.nbc2[i].x = (T)(-h->b_r[i] * s), k.nbc2[i].y = (T)(-h->b_i[i] * s);
     k.nar2[i].x = k.nar2[i].y = (T)(-h->a_r[i] * s * std::pow(R, -al));
     k.br2[i].x = k.br2[i].y = (T)(h->b_r[i] * s * std::pow(R, 2.0 - al));
     s *= R2;
