@@ -54,8 +54,10 @@ typedef enum {
   NPME_ESTATE = 6    /* call out of order (e.g. calcv before setup) */
 } npme_status;
 
-/* funcType keyword: "Laplace", "Ralpha", "Helmholtz" */
-enum { NPME_FUNC_LAPLACE = 0, NPME_FUNC_RALPHA = 1, NPME_FUNC_HELMHOLTZ = 2 };
+/* funcType keyword: "Laplace", "Ralpha", "Helmholtz"; NPME_FUNC_USER: a
+ * caller-defined real kernel (npme_gpu_set_user_kernel) */
+enum { NPME_FUNC_LAPLACE = 0, NPME_FUNC_RALPHA = 1, NPME_FUNC_HELMHOLTZ = 2,
+       NPME_FUNC_USER = 3 };
 /* EwaldSplit keyword: "DerivMatch", "LaplaceOrig" */
 enum { NPME_SPLIT_DERIVMATCH = 0, NPME_SPLIT_LAPLACE_ORIG = 1 };
 /* Arithmetic of the bulk work.  FP64: everything in double ("plain").
@@ -119,6 +121,25 @@ int npme_gpu_create(const npme_params *p, npme_handle **out);
  * it lets a server reuse one handle for requests with different
  * parameters.  On error the old parameters stay in force. */
 int npme_gpu_set_params(npme_handle *h, const npme_params *p);
+
+/* Caller-defined real kernels: the reference's generic interface
+ * (NPME_InterfaceReal_GenFunc with NPME_KfuncReal functors for f, f_LR and
+ * f_SR, src/Interface.h:302-304, src/KernelFunction.h:25-65).  On the GPU
+ * the functors are device code: a caller writes a functor type in CUDA and
+ * lets include/npme_user_kernel.cuh instantiate the three kernel-dependent
+ * launches for it (direct sum, long-range sampling for the kernel
+ * transform, exact sum); npme_user::ops<Functor>() returns this table.  The
+ * handle must have funcType NPME_FUNC_USER; set the table before setup.
+ * fself = f_LR(0), subtracted as the self term. */
+typedef struct {
+  double fself;
+  int (*direct)(npme_handle *h, const void *args, void *stream);
+  int (*sample_lr)(npme_handle *h, int M1, int M2, int M3, const double *ax,
+                   const double *ay, const double *az, void *out, void *stream);
+  int (*exact)(npme_handle *h, const double *d_charge, double *d_V, void *stream,
+               const unsigned int *d_targets, long n_targets);
+} npme_user_ops;
+int npme_gpu_set_user_kernel(npme_handle *h, const npme_user_ops *ops);
 
 /* SetUp / ResetCoord: bins and sorts the points, builds the kernel transform,
  * the FFT plans and all work buffers.  coord is a host pointer. */

@@ -1,0 +1,172 @@
+// Caller-defined real kernels for npme_b200 (the GPU form of the reference's
+// NPME_InterfaceReal_GenFunc with NPME_KfuncReal functors for f, f_LR and
+// f_SR, src/Interface.h:302-304, src/KernelFunction.h:25-65).
+//
+// The reference calls virtual C++ functors on the host.  Here the kernel is
+// device code, so the caller writes a functor type in CUDA and compiles this
+// header with nvcc (-std=c++17 -gencode arch=compute_100a,code=sm_100a, -I to
+// this directory and to npme_b200/csrc), linking -lnpme_gpu:
+//
+//   struct Yukawa {                      // f = exp(-kappa r) / r
+//     // full kernel f and (1/r) df/dr at r^2 > 0 (exact sum, FP64)
+//     __host__ __device__ static void full(double r2, double &f0, double &f1);
+//     // smooth long-range part f_LR at r^2 >= 0 (kernel transform, FP64);
+//     // pairs beyond Rdir are left to it, so f_LR should equal f there
+//     __host__ __device__ static double lr(double r2);
+//     // short-range part f - f_LR and its (1/r) d/dr for 0 < r^2 <= Rdir^2,
+//     // in the bulk precision T (float or double)
+//     template <typename T> __device__ static T sr(T r2, T &f1);
+//   };
+//
+//   npme_params p;  npme_gpu_default_params(&p);
+//   p.funcType = NPME_FUNC_USER;  p.Rdir = ...;  p.N1 = ...;
+//   npme_handle *h;  npme_gpu_create(&p, &h);
+//   npme_user_ops ops = npme_user::ops<Yukawa>();
+//   npme_gpu_set_user_kernel(h, &ops);
+//   npme_gpu_setup(h, n, coord);   npme_gpu_calcv_real(h, V, n, q, coord);
+//
+// The spreading, FFTs, kernel multiply and interpolation are the library's;
+// this header instantiates the three kernel-dependent launches: the direct
+// sum (FP32 warp-group body or FP64 cell-list body with the functor's sr),
+// the sampling of f_LR for the kernel transform and the exact sum.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "npme_gpu.h"
+#include "bodies.cuh"
+
+namespace npme_user {
+
+template <class K>
+struct Pair {
+  template <typename T>
+  __device__ static T sr(T r2, T &f1) {
+    return K::template sr<T>(r2, f1);
+  }
+};
+
+template <class K>
+struct LR {
+  __device__ double2 operator()(double r2) const { return make_double2(K::lr(r2), 0.0); }
+};
+
+template <class K>
+__global__ void __launch_bounds__(32 * npme::kGroupWarps) groups_kernel(
+    npme::PairCoef<float> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    float refine2, double fself, double *__restrict__ V) {
+  __shared__ float4 sp[npme::kGroupWarps][32];
+  __shared__ float4 slo[npme::kGroupWarps][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * npme::kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  npme::direct_group_body<false, NPME_FUNC_USER, 0, 0, Pair<K>>(
+      k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, refine2, fself, 0.0, V, sp[wid],
+      slo[wid], lane);
+}
+
+template <class K>
+__global__ void sample_kernel(int M1, int M2, int M3, const double *__restrict__ ax,
+                              const double *__restrict__ ay, const double *__restrict__ az,
+                              double2 *out) {
+  const long total = (long)M1 * M2 * M3;
+  const LR<K> lr{};
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x)
+    out[idx] = npme::fhat_sample_body(lr, idx, M1, M2, M3, ax, ay, az);
+}
+
+constexpr int kExactTile = 128;
+
+// Exact FP64 sum with the full kernel; output row t is target tidx[t] (every
+// point when tidx is null).
+template <class K>
+__global__ void __launch_bounds__(kExactTile) exact_kernel(const double *__restrict__ coord,
+                                                           const double *__restrict__ q, long n,
+                                                           const unsigned int *__restrict__ tidx,
+                                                           long nt, double *__restrict__ V) {
+  __shared__ double4 sp[kExactTile];
+  const long t = blockIdx.x * (long)kExactTile + threadIdx.x;
+  const bool active = t < nt;
+  const long i = active ? (tidx ? (long)tidx[t] : t) : -1;
+  double xi = 0, yi = 0, zi = 0;
+  if (active) xi = coord[3 * i], yi = coord[3 * i + 1], zi = coord[3 * i + 2];
+  double a[4] = {0, 0, 0, 0};
+  for (long j0 = 0; j0 < n; j0 += kExactTile) {
+    __syncthreads();
+    const long j = j0 + threadIdx.x;
+    if (j < n) sp[threadIdx.x] = make_double4(coord[3 * j], coord[3 * j + 1], coord[3 * j + 2], q[j]);
+    __syncthreads();
+    const int cnt = (int)min((long)kExactTile, n - j0);
+    for (int s = 0; s < cnt; s++) {
+      if (j0 + s == i) continue;
+      const double x = xi - sp[s].x, y = yi - sp[s].y, z = zi - sp[s].z;
+      double f0, f1;
+      K::full(x * x + y * y + z * z, f0, f1);
+      a[0] += f0 * sp[s].w;
+      a[1] += f1 * sp[s].w * x;
+      a[2] += f1 * sp[s].w * y;
+      a[3] += f1 * sp[s].w * z;
+    }
+  }
+  if (active) reinterpret_cast<double4 *>(V)[t] = make_double4(a[0], a[1], a[2], a[3]);
+}
+
+template <class K>
+int direct(npme_handle *h, const void *args, void *stream) {
+  const npme::DirectArgs &a = *static_cast<const npme::DirectArgs *>(args);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->use_groups) {
+    const long blocks = (h->n_groups + npme::kGroupWarps - 1) / npme::kGroupWarps;
+    if (blocks == 0) return NPME_OK;
+    groups_kernel<K><<<(unsigned)blocks, 32 * npme::kGroupWarps, 0, s>>>(
+        npme::make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
+        h->d_groups, h->d_gcen, h->d_segs, h->d_cperm, h->n_groups, (float)h->refine2,
+        a.fself_r, a.V);
+  } else {
+    const npme::CellGeom &c = h->cells;
+    const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
+    npme::direct_kernel<double, false, NPME_FUNC_USER, 0, 0, Pair<K>>
+        <<<ncell, npme::kDirectBS, 0, s>>>(
+            npme::make_pair_coef<double>(h), (const double4 *)h->d_cpos, (const double *)a.q,
+            h->d_cell_start, h->d_cperm, c.nc[0], c.nc[1], c.nc[2], c.edge[0], c.edge[1],
+            c.edge[2], c.reach, a.fself_r, 0.0, a.V);
+  }
+  return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+}
+
+template <class K>
+int sample_lr(npme_handle *, int M1, int M2, int M3, const double *ax, const double *ay,
+              const double *az, void *out, void *stream) {
+  sample_kernel<K><<<148 * 8, 256, 0, (cudaStream_t)stream>>>(M1, M2, M3, ax, ay, az,
+                                                             (double2 *)out);
+  return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+}
+
+template <class K>
+int exact(npme_handle *h, const double *d_q, double *d_V, void *stream,
+          const unsigned int *d_tidx, long nt) {
+  const long n = (long)h->n;
+  if (!d_tidx) nt = n;
+  const int blocks = (int)((nt + kExactTile - 1) / kExactTile);
+  if (blocks == 0) return NPME_OK;
+  exact_kernel<K><<<blocks, kExactTile, 0, (cudaStream_t)stream>>>(h->d_coord, d_q, n, d_tidx, nt,
+                                                                    d_V);
+  return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+}
+
+// The launch table of functor K for npme_gpu_set_user_kernel.
+template <class K>
+npme_user_ops ops() {
+  npme_user_ops o;
+  o.fself = K::lr(0.0);
+  o.direct = &direct<K>;
+  o.sample_lr = &sample_lr<K>;
+  o.exact = &exact<K>;
+  return o;
+}
+
+}  // namespace npme_user

@@ -14,7 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EBUSY, ESTATE = range(7)
-FUNC = {"laplace": 0, "ralpha": 1, "helmholtz": 2}
+FUNC = {"laplace": 0, "ralpha": 1, "helmholtz": 2, "user": 3}
 SPLIT = {"dm": 0, "derivmatch": 0, "orig": 1, "laplaceorig": 1}
 PREC_FP64, PREC_FP32 = 0, 1
 
@@ -59,6 +59,13 @@ class Info(ctypes.Structure):
     ]
 
 
+class UserOps(ctypes.Structure):
+    """npme_user_ops: the launch table of a caller-defined kernel, filled by
+    npme_user::ops<Functor>() in the caller's CUDA code."""
+    _fields_ = [("fself", ctypes.c_double), ("direct", ctypes.c_void_p),
+                ("sample_lr", ctypes.c_void_p), ("exact", ctypes.c_void_p)]
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("setup_threads", ctypes.c_int),
                 ("max_batch", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
@@ -101,7 +108,7 @@ EXPORTS = (
     "npme_gpu_server_default_config", "npme_gpu_server_create", "npme_gpu_submit",
     "npme_gpu_poll", "npme_gpu_wait", "npme_gpu_ticket_info", "npme_gpu_release_ticket",
     "npme_gpu_server_stats", "npme_gpu_server_destroy",
-    "npme_gpu_calcv_exact_subset", "npme_gpu_choose_grid",
+    "npme_gpu_calcv_exact_subset", "npme_gpu_choose_grid", "npme_gpu_set_user_kernel",
 )
 VOID_EXPORTS = ("npme_gpu_default_params", "npme_gpu_server_default_config")
 
@@ -215,6 +222,12 @@ class Solver:
         self.p = params
         self.complex = params.funcType == FUNC["helmholtz"]
         self.n = 0
+        return self
+
+    def set_user_kernel(self, ops):
+        """Launch table (UserOps) of a caller-defined kernel; funcType "user"."""
+        self._check(self.L.npme_gpu_set_user_kernel(self.h, ctypes.byref(ops)))
+        self._user_ops = ops
         return self
 
     def setup(self, coord):

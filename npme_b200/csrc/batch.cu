@@ -242,14 +242,15 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   cudaStream_t s = (cudaStream_t)stream;
   b->launches = 0;
 
-  // FP64 (plain) members take their ordinary path in stream order
+  // FP64 (plain) and caller-defined-kernel members take their ordinary path
+  // in stream order
   std::vector<int> f32;
   for (int i = 0; i < count; i++) {
-    if (hs[i]->fp32) {
+    if (hs[i]->fp32 && !hs[i]->user_kernel) {
       f32.push_back(i);
     } else {
       const int rc = npme_gpu_calcv_device(hs[i], d_V[i], d_q[i], stream);
-      if (rc) return bfail(b, rc, "batch member (fp64): " + hs[i]->err);
+      if (rc) return bfail(b, rc, "batch member: " + hs[i]->err);
       b->launches += hs[i]->launches;
     }
   }

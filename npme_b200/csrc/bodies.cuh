@@ -143,6 +143,31 @@ __device__ __forceinline__ void multiply_cplx_body(typename Vec2<T>::type *__res
   X[idx] = o;
 }
 
+// One element of the windowed eight-image sum that samples f_LR on the
+// compact octant for the kernel transform (src/RecSumGrid.cpp:45-282): per
+// axis the two image coordinates x1, x2 and window values T1, T2 are stored
+// as ax[0..M) = x1, ax[M..2M) = x2, ax[2M..3M) = T1, ax[3M..4M) = T2.  LR is
+// a functor double2 operator()(double r2) returning f_LR (re, im).
+template <class LR>
+__device__ __forceinline__ double2 fhat_sample_body(const LR &lr, long idx, int M1, int M2,
+                                                    int M3, const double *__restrict__ ax,
+                                                    const double *__restrict__ ay,
+                                                    const double *__restrict__ az) {
+  const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
+  double sr = 0, si = 0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int s1 = c >> 2, s2 = (c >> 1) & 1, s3 = c & 1;
+    const double x = ax[s1 * M1 + i1], y = ay[s2 * M2 + i2], z = az[s3 * M3 + i3];
+    const double t = ax[(2 + s1) * M1 + i1] * ay[(2 + s2) * M2 + i2] * az[(2 + s3) * M3 + i3];
+    if (t == 0.0) continue;
+    const double2 f = lr(x * x + y * y + z * z);
+    sr += t * f.x;
+    si += t * f.y;
+  }
+  return make_double2(sr, si);
+}
+
 // Interpolation of one brick by the whole CTA (src/RecSumV.cpp:201-306):
 // the brick's theta tile of (kBrick + P - 1)^3 grid points is read into
 // shared memory once, then every point gathers its p^3 stencil from the
@@ -515,7 +540,7 @@ __device__ __forceinline__ void helmholtz_steps(const PairCoef<float> &k, const 
 // into source order) over the segments [G.z, G.w); qcaller holds the
 // caller-order charges for the self term.  sp and slo are this warp's
 // 32-entry shared staging arrays.
-template <bool CPLX, int FUNC, int SPLIT, int ND>
+template <bool CPLX, int FUNC, int SPLIT, int ND, class PK = BuiltinPair>
 __device__ __forceinline__ void direct_group_body(
     const PairCoef<float> &k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
     const float *__restrict__ qs, const double *__restrict__ qcaller, const int4 G,
@@ -523,7 +548,7 @@ __device__ __forceinline__ void direct_group_body(
     float refine2, double fself_r, double fself_i, double *__restrict__ V, float4 *sp,
     float4 *slo, int lane) {
 #if !defined(NPME_SCALAR_DIRECT)
-  if constexpr (!CPLX && SPLIT == 0 && ND > 0) {
+  if constexpr (!CPLX && SPLIT == 0 && ND > 0 && std::is_same<PK, BuiltinPair>::value) {
     direct_group_packed<FUNC, ND>(k, gpos, spos, qs, qcaller, G, c, segs, perm, refine2, fself_r,
                                   V, sp, slo, lane);
     return;
@@ -578,7 +603,7 @@ __device__ __forceinline__ void direct_group_body(
     NPME_PREFETCH
     float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
 #if !defined(NPME_SCALAR_DIRECT)
-    if constexpr (CPLX && SPLIT == 0 && ND > 0) {
+    if constexpr (CPLX && SPLIT == 0 && ND > 0 && std::is_same<PK, BuiltinPair>::value) {
       float2 Pv = make_float2(0.f, 0.f), Gx = Pv, Gy = Pv, Gz = Pv;
       helmholtz_steps<ND>(k, sp, slo, cnt, tx, ty, tz, tlx, tly, tlz, refine2, Pv, Gx, Gy, Gz);
       p0 = Pv.x, p0i = Pv.y, p1 = Gx.x, p1i = Gx.y, p2 = Gy.x, p2i = Gy.y, p3 = Gz.x, p3i = Gz.y;
@@ -599,7 +624,7 @@ __device__ __forceinline__ void direct_group_body(
         }
         if (!CPLX) {
           float f1;
-          const float f0 = pair_sr_real<float, FUNC, SPLIT, ND>(k, r2, f1);
+          const float f0 = pair_sr<float, FUNC, SPLIT, ND, PK>(k, r2, f1);
           const float gq = f1 * src.w;
           p0 = fmaf(f0, src.w, p0);
           p1 = fmaf(gq, x, p1);
@@ -637,6 +662,129 @@ __device__ __forceinline__ void direct_group_body(
     } else {
       acc[0] -= fself_r * qcaller[o];  // src/Interface.cpp:2061-2062
       reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain cell-list direct sum (the FP64 port of the reference's direct sum,
+// src/PotentialLaplace.cpp:201-719): one CTA per cell of edge >= Rdir / nNeigh,
+// the neighbour columns staged through shared memory in tiles of kDirectBS.
+constexpr int kDirectBS = 64;
+
+template <typename T, bool CPLX, int FUNC, int SPLIT, int ND, class PK = BuiltinPair>
+__global__ void __launch_bounds__(kDirectBS) direct_kernel(
+    PairCoef<T> k, const typename Vec4<T>::type *__restrict__ cpos, const T *__restrict__ qc,
+    const int *__restrict__ cell_start, const uint32_t *__restrict__ cperm, int nc0, int nc1,
+    int nc2, T e0, T e1, T e2, int reach, double fself_r, double fself_i,
+    double *__restrict__ V) {
+  using V4 = typename Vec4<T>::type;
+  __shared__ V4 sp[kDirectBS];
+  __shared__ T sq[kDirectBS * (CPLX ? 2 : 1)];
+  const int cell = blockIdx.x;
+  const int cz = cell % nc2, cy = (cell / nc2) % nc1, cx = cell / (nc2 * nc1);
+  const int tbeg = cell_start[cell], tend = cell_start[cell + 1];
+  const T R2 = k.R2;
+  const double e0d = e0, e1d = e1, e2d = e2;
+  for (int t0 = tbeg; t0 < tend; t0 += kDirectBS) {
+    const int i = t0 + threadIdx.x;
+    const bool active = i < tend;
+    V4 ti = active ? cpos[i] : V4{0, 0, 0, 0};
+    double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
+    for (int dx = -reach; dx <= reach; dx++) {
+      const int sx = cx + dx;
+      if (sx < 0 || sx >= nc0) continue;
+      const double mx = (double)(abs(dx) > 0 ? abs(dx) - 1 : 0) * e0d;
+      for (int dy = -reach; dy <= reach; dy++) {
+        const int sy = cy + dy;
+        if (sy < 0 || sy >= nc1) continue;
+        const double my = (double)(abs(dy) > 0 ? abs(dy) - 1 : 0) * e1d;
+        const double rem = (double)R2 - mx * mx - my * my;
+        if (rem < 0) continue;
+        // cells with |dz| - 1 <= sqrt(rem) / e2 can hold a source within Rdir
+        const int zr = min(reach, 1 + (int)floor(sqrt(rem) / e2d));
+        const int z0 = max(cz - zr, 0), z1 = min(cz + zr, nc2 - 1);
+        const int colbase = (sx * nc1 + sy) * nc2;
+        const int jb = cell_start[colbase + z0], je = cell_start[colbase + z1 + 1];
+        const T ox = (T)dx * e0, oy = (T)dy * e1;
+        for (int j0 = jb; j0 < je; j0 += kDirectBS) {
+          __syncthreads();
+          const int j = j0 + threadIdx.x;
+          if (j < je) {
+            V4 s = cpos[j];
+            s.x += ox;
+            s.y += oy;
+            s.z += (s.w - (T)cz) * e2;
+            sp[threadIdx.x] = s;
+            if (CPLX) {
+              sq[2 * threadIdx.x] = qc[2 * (long)j];
+              sq[2 * threadIdx.x + 1] = qc[2 * (long)j + 1];
+            } else {
+              sq[threadIdx.x] = qc[j];
+            }
+          }
+          __syncthreads();
+          const int cnt = min(kDirectBS, je - j0);
+          T p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
+          const int self = i - j0;  // staged slot of the target itself, if present
+          for (int s = 0; s < cnt; s++) {
+            const V4 src = sp[s];
+            const T x = ti.x - src.x, y = ti.y - src.y, z = ti.z - src.z;
+            const T r2 = fma(x, x, fma(y, y, z * z));
+            if (r2 <= R2 && s != self) {
+              if (!CPLX) {
+                T f1;
+                const T f0 = pair_sr<T, FUNC, SPLIT, ND, PK>(k, r2, f1);
+                const T qj = sq[s];
+                const T g = f1 * qj;
+                p0 = fma(f0, qj, p0);
+                p1 = fma(g, x, p1);
+                p2 = fma(g, y, p2);
+                p3 = fma(g, z, p3);
+              } else {
+                T f0r, f0i, f1r, f1i;
+                pair_sr_helmholtz<T, ND>(k, r2, f0r, f0i, f1r, f1i);
+                const T qr = sq[2 * s], qi = sq[2 * s + 1];
+                // f0 q and (f1 q) * (x, y, z), complex
+                p0 = fma(f0r, qr, fma(-f0i, qi, p0));
+                p0i = fma(f0r, qi, fma(f0i, qr, p0i));
+                const T gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
+                p1 = fma(gr, x, p1);
+                p2 = fma(gr, y, p2);
+                p3 = fma(gr, z, p3);
+                p1i = fma(gi, x, p1i);
+                p2i = fma(gi, y, p2i);
+                p3i = fma(gi, z, p3i);
+              }
+            }
+          }
+          acc[0] += (double)p0;
+          acc[1] += (double)p1;
+          acc[2] += (double)p2;
+          acc[3] += (double)p3;
+          if (CPLX) {
+            acci[0] += (double)p0i;
+            acci[1] += (double)p1i;
+            acci[2] += (double)p2i;
+            acci[3] += (double)p3i;
+          }
+        }
+      }
+    }
+    if (active) {
+      const long o = cperm[i];
+      if (CPLX) {
+        const double qr = qc[2 * (long)i], qi = qc[2 * (long)i + 1];
+        // V -= f_LR(0) q (src/Interface.cpp:2909-2910)
+        acc[0] -= fself_r * qr - fself_i * qi;
+        acci[0] -= fself_r * qi + fself_i * qr;
+        double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+#pragma unroll
+        for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
+      } else {
+        acc[0] -= fself_r * (double)qc[i];  // src/Interface.cpp:2061-2062
+        reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+      }
     }
   }
 }

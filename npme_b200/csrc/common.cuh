@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace npme {
 
 constexpr int kMaxDeriv = 15;  // derivative-match order supported on device
@@ -180,6 +182,19 @@ __device__ __forceinline__ void pair_sr_helmholtz(const PairCoef<T> &k, T r2, T 
   f0i = ei - pi;
   f1r = e1r - dr;
   f1i = e1i - di;
+}
+
+// Pair-kernel policy of the direct sums: the built-in kernels selected by
+// (FUNC, SPLIT, ND), or a caller's functor type U (include/npme_user_kernel.cuh)
+// with  template <typename T> __device__ static T sr(T r2, T &f1).
+struct BuiltinPair {};
+
+template <typename T, int FUNC, int SPLIT, int ND, class PK>
+__device__ __forceinline__ T pair_sr(const PairCoef<T> &k, T r2, T &f1) {
+  if constexpr (std::is_same<PK, BuiltinPair>::value)
+    return pair_sr_real<T, FUNC, SPLIT, ND>(k, r2, f1);
+  else
+    return PK::template sr<T>(r2, f1);
 }
 
 }  // namespace npme

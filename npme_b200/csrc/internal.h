@@ -62,6 +62,8 @@ struct npme_handle {
   npme_params p;
   int device = 0;
   bool complex_kernel = false;
+  bool user_kernel = false;  // funcType NPME_FUNC_USER: launches from uops
+  npme_user_ops uops = {};
   bool fp32 = true;
   bool ready = false;
   std::string err;

@@ -538,7 +538,9 @@ int upload_points(npme_handle *h, const double *coord) {
 
 int check_params(npme_handle *h, const npme_params &p) {
   if (!(p.Rdir > 0)) return fail(h, NPME_EINVAL, "Rdir must be > 0");
-  if (p.funcType < 0 || p.funcType > 2) return fail(h, NPME_EINVAL, "unknown funcType");
+  if (p.funcType < 0 || p.funcType > 3) return fail(h, NPME_EINVAL, "unknown funcType");
+  if (p.funcType == NPME_FUNC_USER && p.EwaldSplit != NPME_SPLIT_DERIVMATCH)
+    return fail(h, NPME_EINVAL, "a user kernel brings its own split (EwaldSplit DerivMatch)");
   if (p.EwaldSplit < 0 || p.EwaldSplit > 1) return fail(h, NPME_EINVAL, "unknown EwaldSplit");
   if (p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG && p.funcType != NPME_FUNC_LAPLACE)
     return fail(h, NPME_EINVAL, "EwaldSplit LaplaceOrig requires funcType Laplace");
@@ -567,12 +569,16 @@ int check_params(npme_handle *h, const npme_params &p) {
 int apply_params(npme_handle *h) {
   h->complex_kernel = h->p.funcType == NPME_FUNC_HELMHOLTZ;
   h->fp32 = h->p.precision == NPME_PREC_FP32;
+  h->user_kernel = h->p.funcType == NPME_FUNC_USER;
   memset(h->a_r, 0, sizeof(h->a_r));
   memset(h->a_i, 0, sizeof(h->a_i));
   memset(h->b_r, 0, sizeof(h->b_r));
   memset(h->b_i, 0, sizeof(h->b_i));
   h->beta = 0;
-  if (h->p.EwaldSplit == NPME_SPLIT_DERIVMATCH) {
+  if (h->user_kernel) {  // the caller's functors define the split
+    h->fself_r = h->uops.direct ? h->uops.fself : 0.0;
+    h->fself_i = 0;
+  } else if (h->p.EwaldSplit == NPME_SPLIT_DERIVMATCH) {
     std::complex<double> a[32], b[32];
     dm_coefficients(h->p, a, b);
     for (int i = 0; i <= h->p.nDeriv; i++) {
@@ -683,8 +689,23 @@ int npme_gpu_set_params(npme_handle *h, const npme_params *p) {
   return NPME_OK;
 }
 
+int npme_gpu_set_user_kernel(npme_handle *h, const npme_user_ops *ops) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!ops || !ops->direct || !ops->sample_lr || !ops->exact)
+    return fail(h, NPME_EINVAL, "incomplete user kernel table");
+  if (!h->user_kernel) return fail(h, NPME_EINVAL, "the handle's funcType is not NPME_FUNC_USER");
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->stream2) cudaStreamSynchronize(h->stream2);
+  h->uops = *ops;
+  h->fself_r = ops->fself, h->fself_i = 0;
+  h->ready = false;  // the kernel transform depends on f_LR: set up again
+  return NPME_OK;
+}
+
 int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
   if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (h->user_kernel && !h->uops.direct)
+    return fail(h, NPME_ESTATE, "user kernel: npme_gpu_set_user_kernel before setup");
   if (!coord && n) return fail(h, NPME_EINVAL, "null coord");
   if (n == 0) return fail(h, NPME_EINVAL, "nCharge must be > 0");
   if (n >= (size_t)1 << 31) return fail(h, NPME_EINVAL, "nCharge must be < 2^31");

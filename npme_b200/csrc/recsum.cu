@@ -60,28 +60,20 @@ __device__ double2 lr_eval(const LRKernel &k, double r2) {
   return make_double2(pr, pi);
 }
 
+struct BuiltinLR {
+  LRKernel k;
+  __device__ double2 operator()(double r2) const { return lr_eval(k, r2); }
+};
+
 __global__ void sample_fhat_kernel(LRKernel k, int M1, int M2, int M3,
                                    const double *__restrict__ ax,  // 4*M per axis: x1,x2,T1,T2
                                    const double *__restrict__ ay,
                                    const double *__restrict__ az, double2 *out) {
   const long total = (long)M1 * M2 * M3;
+  const BuiltinLR lr{k};
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x) {
-    const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
-    double sr = 0, si = 0;
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const int s1 = c >> 2, s2 = (c >> 1) & 1, s3 = c & 1;
-      const double x = ax[s1 * M1 + i1], y = ay[s2 * M2 + i2], z = az[s3 * M3 + i3];
-      const double t = ax[(2 + s1) * M1 + i1] * ay[(2 + s2) * M2 + i2] *
-                       az[(2 + s3) * M3 + i3];
-      if (t == 0.0) continue;
-      const double2 f = lr_eval(k, x * x + y * y + z * z);
-      sr += t * f.x;
-      si += t * f.y;
-    }
-    out[idx] = make_double2(sr, si);
-  }
+       idx += (long)gridDim.x * blockDim.x)
+    out[idx] = fhat_sample_body(lr, idx, M1, M2, M3, ax, ay, az);
 }
 
 // out[k] = f[0] + (-1)^k f[M-1] + 2 sum_{j=1}^{M-2} f[j] cos(2 pi j k / N)
@@ -258,8 +250,14 @@ int build_kernel_transform(npme_handle *h) {
                     h->stream);
   }
   const int threads = 256, blocks = 148 * 8;
-  sample_fhat_kernel<<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, h->d_fax[0], h->d_fax[1],
-                                                        h->d_fax[2], h->d_ft0);
+  if (h->user_kernel) {
+    if ((rc = h->uops.sample_lr(h, M1, M2, M3, h->d_fax[0], h->d_fax[1], h->d_fax[2], h->d_ft0,
+                                h->stream)))
+      return rc;
+  } else {
+    sample_fhat_kernel<<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, h->d_fax[0],
+                                                          h->d_fax[1], h->d_fax[2], h->d_ft0);
+  }
   double2 *src = h->d_ft0, *dst = h->d_ft1;
   for (int d = 0; d < 3; d++) {
     dct1_axis_kernel<<<blocks, threads, 0, h->stream>>>(src, dst, M1, M2, M3, d, (int)N[d],

@@ -1,0 +1,48 @@
+// Caller-defined kernels for the tests, instantiated through
+// include/npme_user_kernel.cuh and exported as C functions that fill the
+// launch table:
+//   GaussScreened  f = exp(-a r^2) / r, split with erf(beta r):
+//                  f_LR = f erf(beta r) (smooth: even in r), f_SR = f erfc(beta r)
+//   CoulombErf     a = 0: 1/r with the original Ewald split
+// (A plain Yukawa exp(-kappa r)/r split this way would leave f_LR with a
+// term linear in r at the origin, which the grid does not resolve.)
+#include <cmath>
+
+#include "npme_user_kernel.cuh"
+
+namespace {
+
+constexpr double kBeta = 0.475;
+constexpr double kTwoOverSqrtPi = 1.1283791670955126;
+
+template <int A_MICRO>
+struct GaussScreened {
+  static constexpr double kA = A_MICRO * 1e-6;
+  __host__ __device__ static void full(double r2, double &f0, double &f1) {
+    const double r = sqrt(r2), e = exp(-kA * r2);
+    f0 = e / r;
+    f1 = -e * (2.0 * kA * r2 + 1.0) / (r2 * r);
+  }
+  __host__ __device__ static double lr(double r2) {
+    if (r2 == 0.0) return kBeta * kTwoOverSqrtPi;
+    const double r = sqrt(r2);
+    return exp(-kA * r2) * erf(kBeta * r) / r;
+  }
+  template <typename T>
+  __device__ static T sr(T r2, T &f1) {
+    const T r = sqrt(r2), ri = T(1) / r;
+    const T f0 = exp(-T(kA) * r2) * erfc(T(kBeta) * r) * ri;
+    const T g = T(kTwoOverSqrtPi * kBeta) * exp(-T(kA + kBeta * kBeta) * r2) * ri;
+    f1 = (-(T(2 * kA) * r + ri) * f0 - g) * ri;
+    return f0;
+  }
+};
+
+using Screened = GaussScreened<20000>;  // a = 0.02
+using CoulombErf = GaussScreened<0>;
+
+}  // namespace
+
+extern "C" void screened_ops(npme_user_ops *out) { *out = npme_user::ops<Screened>(); }
+extern "C" void coulomb_erf_ops(npme_user_ops *out) { *out = npme_user::ops<CoulombErf>(); }
+extern "C" double user_kernel_beta() { return kBeta; }
