@@ -184,7 +184,7 @@ def run_reference_arm(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_of(w, "fp64", 1),
+            "config": config_of(w, args.precision, args.gpus),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": f"full workload ({w.n} points), {args.steps} CalcV "
                                        f"calls after one SetUp ({setup_s and round(setup_s, 3)} s)"
