@@ -11,6 +11,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -287,50 +288,114 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   column_sort(coord, n, mn, ns, sedge, sorder, sstart, zs);
   const long ncol = (long)nc[0] * nc[1];
 
+  // Per coarse column: the fine columns that can hold a source within R of
+  // the column's points, each with a pair of cursors into its z-sorted
+  // sources.  The groups of a column come in increasing z, so the cursors
+  // only creep forward (a few steps per group, either direction as the
+  // window half-height varies) instead of a binary search per group and
+  // column, and the column's source z values stay in cache.  Coarse columns
+  // are independent: large systems split them over host threads, each
+  // filling its own lists, concatenated in column order afterwards.
+  struct Part {
+    std::vector<int4> groups;
+    std::vector<double4> cen;
+    std::vector<int2> segs;
+    double cand = 0;
+  };
+  auto build_part = [&](long c_begin, long c_end, Part &out) {
+    std::vector<long> nb_col, pa, pb;
+    std::vector<int> nb_s0, nb_s1;
+    std::vector<double> dxv, dyv;
+    for (long c = c_begin; c < c_end; c++) {
+      if (cstart[c] == cstart[c + 1]) continue;
+      double cl[2] = {1e300, 1e300}, ch[2] = {-1e300, -1e300};
+      for (long k = cstart[c]; k < cstart[c + 1]; k++)
+        for (int d = 0; d < 2; d++) {
+          const double x = coord[3 * (size_t)order[k] + d];
+          cl[d] = std::min(cl[d], x);
+          ch[d] = std::max(ch[d], x);
+        }
+      int lo[2], hi[2];
+      for (int d = 0; d < 2; d++) {
+        lo[d] = (int)std::max(0.0, std::floor((cl[d] - R - mn[d]) / sedge[d]));
+        hi[d] = (int)std::min((double)(ns[d] - 1), std::floor((ch[d] + R - mn[d]) / sedge[d]));
+      }
+      nb_col.clear(), nb_s0.clear(), nb_s1.clear();
+      for (int s0 = lo[0]; s0 <= hi[0]; s0++)
+        for (int s1 = lo[1]; s1 <= hi[1]; s1++) {
+          const long sc = (long)s0 * ns[1] + s1;
+          if (sstart[sc] == sstart[sc + 1]) continue;
+          nb_col.push_back(sc), nb_s0.push_back(s0 - lo[0]), nb_s1.push_back(s1 - lo[1]);
+        }
+      pa.assign(nb_col.size(), 0), pb.assign(nb_col.size(), 0);
+      for (size_t t = 0; t < nb_col.size(); t++) pa[t] = pb[t] = sstart[nb_col[t]];
+      dxv.resize(hi[0] - lo[0] + 1), dyv.resize(hi[1] - lo[1] + 1);
+      for (long p0 = cstart[c]; p0 < cstart[c + 1]; p0 += 32) {
+        const long p1 = std::min(p0 + 32, cstart[c + 1]);
+        double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
+        for (long k = p0; k < p1; k++)
+          for (int d = 0; d < 3; d++) {
+            const double x = coord[3 * (size_t)order[k] + d];
+            bl[d] = std::min(bl[d], x);
+            bh[d] = std::max(bh[d], x);
+          }
+        // squared xy distances from the bounding box to each fine column
+        for (size_t u = 0; u < dxv.size(); u++) {
+          const double l0 = mn[0] + (lo[0] + (long)u) * sedge[0], h0 = l0 + sedge[0];
+          const double d = std::max(0.0, std::max(l0 - bh[0], bl[0] - h0));
+          dxv[u] = d * d;
+        }
+        for (size_t u = 0; u < dyv.size(); u++) {
+          const double l1 = mn[1] + (lo[1] + (long)u) * sedge[1], h1 = l1 + sedge[1];
+          const double d = std::max(0.0, std::max(l1 - bh[1], bl[1] - h1));
+          dyv[u] = d * d;
+        }
+        const int seg0 = (int)out.segs.size();
+        for (size_t t = 0; t < nb_col.size(); t++) {
+          const double d2 = dxv[nb_s0[t]] + dyv[nb_s1[t]];
+          if (d2 > R2) continue;
+          const double hz = std::sqrt(R2 - d2), zlo = bl[2] - hz, zhi = bh[2] + hz;
+          const long zb = sstart[nb_col[t]], ze = sstart[nb_col[t] + 1];
+          long a = pa[t], b = pb[t];
+          // a: first source with z >= zlo; b: first source with z > zhi
+          while (a < ze && zs[a] < zlo) a++;
+          while (a > zb && zs[a - 1] >= zlo) a--;
+          while (b < ze && zs[b] <= zhi) b++;
+          while (b > zb && zs[b - 1] > zhi) b--;
+          pa[t] = a, pb[t] = b;
+          if (b > a) {
+            out.segs.push_back(make_int2((int)a, (int)(b - a)));
+            out.cand += (double)(b - a) * (double)(p1 - p0);
+          }
+        }
+        out.groups.push_back(make_int4((int)p0, (int)(p1 - p0), seg0, (int)out.segs.size()));
+        out.cen.push_back(make_double4(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]),
+                                       0.5 * (bl[2] + bh[2]), 0.0));
+      }
+    }
+  };
+  const int nthreads =
+      n < 50000 ? 1 : (int)std::min<long>(16, std::max(1u, std::thread::hardware_concurrency()));
+  std::vector<Part> parts(nthreads);
+  if (nthreads == 1) {
+    build_part(0, ncol, parts[0]);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; t++)
+      pool.emplace_back(build_part, ncol * t / nthreads, ncol * (t + 1) / nthreads,
+                        std::ref(parts[t]));
+    for (auto &th : pool) th.join();
+  }
   std::vector<int4> groups;
   std::vector<double4> cen;
   std::vector<int2> segs;
   double cand = 0;
-  for (long c = 0; c < ncol; c++) {
-    for (long p0 = cstart[c]; p0 < cstart[c + 1]; p0 += 32) {
-      const long p1 = std::min(p0 + 32, cstart[c + 1]);
-      double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
-      for (long k = p0; k < p1; k++)
-        for (int d = 0; d < 3; d++) {
-          const double x = coord[3 * (size_t)order[k] + d];
-          bl[d] = std::min(bl[d], x);
-          bh[d] = std::max(bh[d], x);
-        }
-      const int seg0 = (int)segs.size();
-      // fine columns whose xy extent can come within R of the bounding box
-      int lo[2], hi[2];
-      for (int d = 0; d < 2; d++) {
-        lo[d] = (int)std::max(0.0, std::floor((bl[d] - R - mn[d]) / sedge[d]));
-        hi[d] = (int)std::min((double)(ns[d] - 1), std::floor((bh[d] + R - mn[d]) / sedge[d]));
-      }
-      for (int s0 = lo[0]; s0 <= hi[0]; s0++) {
-        const double lo0 = mn[0] + s0 * sedge[0], hi0 = lo0 + sedge[0];
-        const double dx = std::max(0.0, std::max(lo0 - bh[0], bl[0] - hi0));
-        for (int s1 = lo[1]; s1 <= hi[1]; s1++) {
-          const double lo1 = mn[1] + s1 * sedge[1], hi1 = lo1 + sedge[1];
-          const double dy = std::max(0.0, std::max(lo1 - bh[1], bl[1] - hi1));
-          const double d2 = dx * dx + dy * dy;
-          if (d2 > R2) continue;
-          const double hz = std::sqrt(R2 - d2);
-          const long sc = (long)s0 * ns[1] + s1;
-          const double *zb = zs.data() + sstart[sc], *ze = zs.data() + sstart[sc + 1];
-          const long a = std::lower_bound(zb, ze, bl[2] - hz) - zs.data();
-          const long b = std::upper_bound(zb, ze, bh[2] + hz) - zs.data();
-          if (b > a) {
-            segs.push_back(make_int2((int)a, (int)(b - a)));
-            cand += (double)(b - a) * (double)(p1 - p0);
-          }
-        }
-      }
-      groups.push_back(make_int4((int)p0, (int)(p1 - p0), seg0, (int)segs.size()));
-      cen.push_back(make_double4(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]),
-                                 0.5 * (bl[2] + bh[2]), 0.0));
-    }
+  for (Part &pt : parts) {
+    const int base = (int)segs.size();
+    for (int4 g : pt.groups) groups.push_back(make_int4(g.x, g.y, g.z + base, g.w + base));
+    cen.insert(cen.end(), pt.cen.begin(), pt.cen.end());
+    segs.insert(segs.end(), pt.segs.begin(), pt.segs.end());
+    cand += pt.cand;
   }
   // heaviest groups first, so the last wave of the launch holds the light ones
   {
