@@ -5,6 +5,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -208,6 +209,17 @@ int npme::handle_buffer(npme_handle *h, void **field, size_t bytes) {
 
 namespace {
 
+// Host threads for the set-up of an n-point system: the machine's cores
+// shared among the set-ups running at the same time (a serving process runs
+// several on its own threads), one for small systems.
+std::atomic<int> g_active_setups{0};
+
+int setup_threads(size_t n) {
+  if (n < 50000) return 1;
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  return std::max(1, std::min(16, hw / std::max(1, g_active_setups.load())));
+}
+
 // Sorts the points by xy column (nc[0] x nc[1] columns of edge `edge` from
 // `mn`), then by (z, index) inside each column.  Fills the permutation, the
 // column starts and the sorted z.
@@ -231,13 +243,23 @@ void column_sort(const double *coord, size_t n, const double *mn, const int *nc,
     for (size_t i = 0; i < n; i++) order[fill[col[i]]++] = (uint32_t)i;
   }
   zs.resize(n);
-  std::vector<std::pair<double, uint32_t>> zc;
-  for (long c = 0; c < ncol; c++) {
-    const long b = cstart[c], e1 = cstart[c + 1];
-    zc.resize(e1 - b);
-    for (long k = b; k < e1; k++) zc[k - b] = {coord[3 * (size_t)order[k] + 2], order[k]};
-    std::sort(zc.begin(), zc.end());
-    for (long k = b; k < e1; k++) zs[k] = zc[k - b].first, order[k] = zc[k - b].second;
+  auto sort_columns = [&](long c0, long c1) {
+    std::vector<std::pair<double, uint32_t>> zc;
+    for (long c = c0; c < c1; c++) {
+      const long b = cstart[c], e1 = cstart[c + 1];
+      zc.resize(e1 - b);
+      for (long k = b; k < e1; k++) zc[k - b] = {coord[3 * (size_t)order[k] + 2], order[k]};
+      std::sort(zc.begin(), zc.end());
+      for (long k = b; k < e1; k++) zs[k] = zc[k - b].first, order[k] = zc[k - b].second;
+    }
+  };
+  const int nt = setup_threads(n);
+  if (nt == 1) {
+    sort_columns(0, ncol);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; t++) pool.emplace_back(sort_columns, ncol * t / nt, ncol * (t + 1) / nt);
+    for (auto &th : pool) th.join();
   }
 }
 
@@ -374,8 +396,7 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
       }
     }
   };
-  const int nthreads =
-      n < 50000 ? 1 : (int)std::min<long>(16, std::max(1u, std::thread::hardware_concurrency()));
+  const int nthreads = setup_threads(n);
   std::vector<Part> parts(nthreads);
   if (nthreads == 1) {
     build_part(0, ncol, parts[0]);
@@ -767,7 +788,16 @@ int npme_gpu_set_user_kernel(npme_handle *h, const npme_user_ops *ops) {
   return NPME_OK;
 }
 
+static int setup_impl(npme_handle *h, size_t n, const double *coord);
+
 int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
+  g_active_setups++;
+  const int rc = setup_impl(h, n, coord);
+  g_active_setups--;
+  return rc;
+}
+
+static int setup_impl(npme_handle *h, size_t n, const double *coord) {
   if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
   if (h->user_kernel && !h->uops.direct)
     return fail(h, NPME_ESTATE, "user kernel: npme_gpu_set_user_kernel before setup");
