@@ -276,7 +276,7 @@ __device__ __forceinline__ void interp_brick_body(int brick, const int *__restri
 #endif
 constexpr int kPackedBlock = NPME_PACKED_BLOCK;
 
-template <int FUNC, int ND>
+template <int FUNC, int ND, bool REFINE>
 __device__ __forceinline__ void packed_block(
     const PairCoef<float> &k, const float4 *sp, const float4 *slo, int s0, float2 tx2,
     float2 ty2, float2 tz2, float2 tl2x, float2 tl2y, float2 tl2z, float R2, float refine2,
@@ -300,11 +300,11 @@ __device__ __forceinline__ void packed_block(
     const bool h0 = __float_as_uint(r2.x) - 1u < rb, h1 = __float_as_uint(r2.y) - 1u < rb;
     rr[u] = make_float2(h0 ? r2.x : R2, h1 ? r2.y : R2);
     qm[u] = make_float2(h0 ? B.z : 0.f, h1 ? B.w : 0.f);
-    rmin = fminf(rmin, fminf(rr[u].x, rr[u].y));
+    if (REFINE) rmin = fminf(rmin, fminf(rr[u].x, rr[u].y));
     any |= h0 | h1;
   }
   if (!__any_sync(0xffffffffu, any)) return;
-  if (rmin < refine2) {  // close pair: exact difference from head + residual
+  if (REFINE && rmin < refine2) {  // close pair: exact difference from head + residual
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (fminf(rr[u].x, rr[u].y) < refine2) {
@@ -403,6 +403,12 @@ __device__ __forceinline__ void direct_group_packed(
   float *sa = reinterpret_cast<float *>(sp), *la = reinterpret_cast<float *>(slo);
   const int slot = (lane >> 1) * 4 + (lane & 1);
 
+  // A pair closer than sqrt(refine2) needs its source within the group's
+  // half-diagonal (c.w) plus sqrt(refine2) of the centre; chunks with no
+  // such source skip the refinement bookkeeping.
+  const double rfs = sqrt((double)refine2) + c.w * ir;
+  const double near2 = rfs * rfs;
+  bool near = false;
   // register prefetch of the next chunk: lane l holds source l of the chunk
   SrcCursor cur{G.z, lane};
   cur.normalize(segs, G.w);
@@ -419,11 +425,13 @@ __device__ __forceinline__ void direct_group_packed(
     __syncwarp();
     {
       float hx = 1e18f, hy = 1e18f, hz = 1e18f, q = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+      near = false;
       if (pv) {
         const double dx = (px - c.x) * ir, dy = (py - c.y) * ir, dz = (pz - c.z) * ir;
         hx = (float)dx, hy = (float)dy, hz = (float)dz;
         lx = (float)(dx - (double)hx), ly = (float)(dy - (double)hy), lz = (float)(dz - (double)hz);
         q = pq;
+        near = dx * dx + dy * dy + dz * dz < near2;
       }
       sa[slot] = -hx;
       sa[slot + 2] = -hy;
@@ -446,9 +454,15 @@ __device__ __forceinline__ void direct_group_packed(
     float2 P0 = make_float2(0.f, 0.f), N1 = P0, N2 = P0, N3 = P0;  // N*: minus the gradient
     // blocks of kPackedBlock steps; slots past the chunk hold far sources, so
     // the step count is rounded up to whole blocks
-    for (int s0 = 0; s0 < npair; s0 += kPackedBlock)
-      packed_block<FUNC, ND>(k, sp, slo, s0, tx2, ty2, tz2, tl2x, tl2y, tl2z, R2, refine2, P0,
-                             N1, N2, N3);
+    if (__any_sync(0xffffffffu, near)) {
+      for (int s0 = 0; s0 < npair; s0 += kPackedBlock)
+        packed_block<FUNC, ND, true>(k, sp, slo, s0, tx2, ty2, tz2, tl2x, tl2y, tl2z, R2, refine2,
+                                     P0, N1, N2, N3);
+    } else {
+      for (int s0 = 0; s0 < npair; s0 += kPackedBlock)
+        packed_block<FUNC, ND, false>(k, sp, slo, s0, tx2, ty2, tz2, tl2x, tl2y, tl2z, R2,
+                                      refine2, P0, N1, N2, N3);
+    }
     acc[0] += (double)P0.x + (double)P0.y;
     acc[1] -= (double)N1.x + (double)N1.y;
     acc[2] -= (double)N2.x + (double)N2.y;

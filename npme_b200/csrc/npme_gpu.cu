@@ -391,8 +391,11 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
           }
         }
         out.groups.push_back(make_int4((int)p0, (int)(p1 - p0), seg0, (int)out.segs.size()));
-        out.cen.push_back(make_double4(0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]),
-                                       0.5 * (bl[2] + bh[2]), 0.0));
+        // centre and half-diagonal of the bounding box
+        out.cen.push_back(make_double4(
+            0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]),
+            0.5 * std::sqrt((bh[0] - bl[0]) * (bh[0] - bl[0]) + (bh[1] - bl[1]) * (bh[1] - bl[1]) +
+                            (bh[2] - bl[2]) * (bh[2] - bl[2]))));
       }
     }
   };
