@@ -83,9 +83,8 @@ __global__ void __launch_bounds__(256) batch_spread_kernel(const BatchSys *__res
   const long long u = blockIdx.x;
   const int s = find_sys(off, count, u);
   const BatchSys &S = sys[s];
-  spread_brick_body<float, P, CPLX>(S.brick_list[u - off[s]], S.brick_start, S.bpts, S.qb,
-                                    S.grid, S.nb2, S.nb3, S.N1, S.N2, S.N3,
-                                    reinterpret_cast<float *>(smem_raw));
+  spread_brick_fixed<P, CPLX>(S.brick_list[u - off[s]], S.brick_start, S.bpts, S.qb, S.grid,
+                              S.nb2, S.nb3, S.N1, S.N2, S.N3, reinterpret_cast<int *>(smem_raw));
 }
 
 template <bool CPLX>
@@ -420,7 +419,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
 #define NPME_BS(PP, CX)                                                                    \
   {                                                                                        \
     constexpr int TL = kBrick + PP - 1;                                                    \
-    const size_t smem = sizeof(float) * TL * TL * TL * (CX ? 2 : 1);                       \
+    const size_t smem = 2 * sizeof(int) * TL * TL * TL * (CX ? 2 : 1);                     \
     auto kern = batch_spread_kernel<PP, CX>;                                               \
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
     kern<<<(unsigned)nb, 256, smem, s>>>(D(c), O(c), cnt);                                 \

@@ -111,6 +111,98 @@ __device__ __forceinline__ void spread_brick_body(int brick, const int *__restri
   }
 }
 
+// FP32 spreading with two native 32-bit integer shared atomics per
+// contribution instead of one floating-point shared atomic (which the
+// hardware does not have and executes as a compare-and-swap loop; a probe
+// ran 3.5x faster with integer atomics).  Each contribution v = c q is
+// scaled by S = 2^k, k = 30 - ceil(log2(n_brick max|q|)), so the high words
+// round(v S) of all contributions to a tile point cannot exceed 2^30 in sum;
+// the low words round((v S - hi) 2^L) carry L = 30 - ceil(log2 n_brick)
+// more bits.  The integer sums are exact and independent of the order of
+// the atomics; each tile value hi + lo 2^-L is rounded once, to float, when
+// it is added to the grid.  Same points, weights and tile as
+// spread_brick_body.
+template <int P, bool CPLX>
+__device__ __forceinline__ void spread_brick_fixed(int brick, const int *__restrict__ brick_start,
+                                                   const BrickPoint<float> *__restrict__ bp,
+                                                   const float *__restrict__ q,
+                                                   float *__restrict__ grid, int nb2, int nb3,
+                                                   long N1, long N2, long N3, int *tile) {
+  constexpr int TL = kBrick + P - 1;
+  constexpr int TV = TL * TL * TL;
+  constexpr int C = CPLX ? 2 : 1;
+  __shared__ float s_max[32];
+  int *thi = tile, *tlo = tile + TV * C;
+  const int b3 = brick % nb3, b2 = (brick / nb3) % nb2, b1 = brick / (nb3 * nb2);
+  for (int t = threadIdx.x; t < 2 * TV * C; t += blockDim.x) tile[t] = 0;
+  const int beg = brick_start[brick], nbp = brick_start[brick + 1] - beg;
+  float m = 0.f;
+  for (int i = threadIdx.x; i < nbp * C; i += blockDim.x) m = fmaxf(m, fabsf(q[C * (long)beg + i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  if (lane == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  m = s_max[0];
+  for (int w = 1; w < nw; w++) m = fmaxf(m, s_max[w]);
+  if (m == 0.f) return;  // nothing to spread (the whole CTA returns)
+  const int lnb = 32 - __clz(max(nbp - 1, 1));  // ceil(log2(nbp)), nbp >= 2
+  const int k = max(-120, min(120, 30 - (ilogbf(m) + 1) - lnb));
+  const int L = 30 - lnb;
+  const float S = ldexpf(1.f, k), SL = ldexpf(1.f, L);
+  const int nvw = (nbp + 31) >> 5;
+  for (int vw = threadIdx.x >> 5; vw < nvw; vw += nw) {
+    const int pi = brick_point(nbp, vw, lane);
+    if (pi < 0) continue;
+    const int i = beg + pi;
+    const BrickPoint<float> pt = bp[i];
+    float w1[P], w2[P], w3[P], dummy[P];
+    bspline_weights<float, P, false>(pt.u[0], w1, dummy);
+    bspline_weights<float, P, false>(pt.u[1], w2, dummy);
+    bspline_weights<float, P, false>(pt.u[2], w3, dummy);
+    const int l1 = (int)(pt.g0 >> 20) - b1 * kBrick;
+    const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
+    const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
+    const float qr = q[C * (long)i] * S, qi = CPLX ? q[2 * (long)i + 1] * S : 0.f;
+#pragma unroll
+    for (int t1 = 0; t1 < P; t1++) {
+#pragma unroll
+      for (int t2 = 0; t2 < P; t2++) {
+        const float c12 = w1[t1] * w2[t2];
+        const int row = C * (((l1 + t1) * TL + (l2 + t2)) * TL + l3);
+#pragma unroll
+        for (int t3 = 0; t3 < P; t3++) {
+          const float c = c12 * w3[t3];
+#pragma unroll
+          for (int part = 0; part < C; part++) {
+            const float v = c * (part ? qi : qr);
+            const float h = rintf(v);
+            atomicAdd(thi + row + C * t3 + part, (int)h);
+            atomicAdd(tlo + row + C * t3 + part, __float2int_rn((v - h) * SL));
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const float invS = ldexpf(1.f, -k), invSL = ldexpf(1.f, -L);
+  const long g1 = (long)b1 * kBrick, g2 = (long)b2 * kBrick, g3 = (long)b3 * kBrick;
+  for (int t = threadIdx.x; t < TV; t += blockDim.x) {
+    const int i3 = t % TL, i2 = (t / TL) % TL, i1 = t / (TL * TL);
+    if (g1 + i1 >= N1) continue;
+    if (g2 + i2 >= N2 || g3 + i3 >= N3) continue;  // beyond the box: always zero
+    const long gi = ((g1 + i1) * N2 + (g2 + i2)) * N3 + (g3 + i3);
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      const int hv = thi[C * t + c], lv = tlo[C * t + c];
+      if (hv != 0 || lv != 0) {
+        const double v = ((double)hv + (double)lv * (double)invSL) * (double)invS;
+        atomicAdd(grid + C * gi + c, (float)v);
+      }
+    }
+  }
+}
+
 // X(k) *= G(|k1|, |k2|, k3) on the R2C half spectrum (src/RecSumV.cpp:639-707).
 template <typename T>
 __device__ __forceinline__ void multiply_real_body(typename Vec2<T>::type *__restrict__ X,

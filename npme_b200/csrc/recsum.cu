@@ -368,9 +368,10 @@ void launch_gather_direct(npme_handle *h, const double *d_q, void *d_qdst, cudaS
 // Spread (src/RecSumQ.cpp:184-314): Q[g] += q B1 B2 B3.  One CTA per
 // non-empty brick of kBrick^3 stencil origins.  The CTA accumulates its
 // points' stencils into a shared-memory tile of (kBrick + P - 1)^3 grid
-// points with shared atomics, then adds the tile to the global grid (global
-// atomics only where tiles of neighbouring bricks overlap: one add per tile
-// point instead of one per stencil point).  Complex charges are spread
+// points with shared atomics (FP32: 64-bit fixed point in two native
+// 32-bit integer atomics, spread_brick_fixed), then adds the tile to the
+// global grid (global atomics only where tiles of neighbouring bricks
+// overlap: one add per tile point instead of one per stencil point).  Complex charges are spread
 // without conjugation; with the cyclic convolution used here that gives the
 // reference's theta for conj(q) spreading (src/RecSumQ.cpp:337) because the
 // reference conjugates twice (src/RecSumV.cpp:672).
@@ -381,14 +382,19 @@ __global__ void __launch_bounds__(256) spread_kernel(
     const BrickPoint<T> *__restrict__ bp, const T *__restrict__ q, T *__restrict__ grid,
     int nb2, int nb3, long N1, long N2, long N3) {
   extern __shared__ unsigned char smem_raw[];
-  spread_brick_body<T, P, CPLX>(brick_list[blockIdx.x], brick_start, bp, q, grid, nb2, nb3, N1,
-                                N2, N3, reinterpret_cast<T *>(smem_raw));
+  if constexpr (std::is_same<T, float>::value)
+    spread_brick_fixed<P, CPLX>(brick_list[blockIdx.x], brick_start, bp, q, grid, nb2, nb3, N1,
+                                N2, N3, reinterpret_cast<int *>(smem_raw));
+  else
+    spread_brick_body<T, P, CPLX>(brick_list[blockIdx.x], brick_start, bp, q, grid, nb2, nb3, N1,
+                                  N2, N3, reinterpret_cast<T *>(smem_raw));
 }
 
 template <typename T, bool CPLX, int P>
 static void spread_dispatch(npme_handle *h, cudaStream_t s) {
   constexpr int TL = kBrick + P - 1;
-  const size_t smem = sizeof(T) * TL * TL * TL * (CPLX ? 2 : 1);
+  // FP32: two int words per tile value; FP64: one double
+  const size_t smem = (sizeof(T) == 4 ? 8 : sizeof(T)) * TL * TL * TL * (CPLX ? 2 : 1);
   auto kern = spread_kernel<T, P, CPLX>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<(unsigned)h->n_nonempty, 256, smem, s>>>(
