@@ -214,10 +214,14 @@ namespace {
 // several on its own threads), one for small systems.
 std::atomic<int> g_active_setups{0};
 
+#ifndef NPME_SETUP_THREADS_MAX
+#define NPME_SETUP_THREADS_MAX 16
+#endif
+
 int setup_threads(size_t n) {
   if (n < 50000) return 1;
   const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-  return std::max(1, std::min(16, hw / std::max(1, g_active_setups.load())));
+  return std::max(1, std::min(NPME_SETUP_THREADS_MAX, hw / std::max(1, g_active_setups.load())));
 }
 
 // Sorts the points by xy column (nc[0] x nc[1] columns of edge `edge` from

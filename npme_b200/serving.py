@@ -116,6 +116,27 @@ class Server:
     def close(self):
         self.srv.close()
 
+    def warm_plans(self, requests):
+        """Solves a tiny system once per (kernel kind, FFT box) the requests
+        will use, so that cuFFT plans (and any kernels cuFFT compiles on
+        first use) exist before the first real request: a server does this
+        at start-up for the sizes it serves."""
+        import npme_b200
+        seen = set()
+        g = np.random.Generator(np.random.Philox(0))
+        for r in requests:
+            p = params_for(r, self.precision, self.device)
+            key = (r.kernel == "helmholtz", p.N1, p.N2, p.N3)
+            if key in seen:
+                continue
+            seen.add(key)
+            c = g.random((64, 3)) * 4.0
+            q = (g.uniform(-1, 1, 64) + 1j * g.uniform(-1, 1, 64)) if key[0] \
+                else g.uniform(-1, 1, 64)
+            with npme_b200.Solver(p) as s:
+                s.setup(c).calcv(q)
+        return len(seen)
+
     def run(self, requests, realtime=True):
         """Serves `requests` (sorted by arrival).  With realtime=False every
         request is available at t = 0 (offline batched throughput)."""
