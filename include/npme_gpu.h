@@ -55,7 +55,7 @@ typedef enum {
 } npme_status;
 
 /* funcType keyword: "Laplace", "Ralpha", "Helmholtz"; NPME_FUNC_USER: a
- * caller-defined real kernel (npme_gpu_set_user_kernel) */
+ * caller-defined kernel (npme_gpu_set_user_kernel) */
 enum { NPME_FUNC_LAPLACE = 0, NPME_FUNC_RALPHA = 1, NPME_FUNC_HELMHOLTZ = 2,
        NPME_FUNC_USER = 3 };
 /* EwaldSplit keyword: "DerivMatch", "LaplaceOrig" */
@@ -130,9 +130,11 @@ int npme_gpu_set_params(npme_handle *h, const npme_params *p);
  * launches for it (direct sum, long-range sampling for the kernel
  * transform, exact sum); npme_user::ops<Functor>() returns this table.  The
  * handle must have funcType NPME_FUNC_USER; set the table before setup.
- * fself = f_LR(0), subtracted as the self term. */
+ * fself = f_LR(0), subtracted as the self term.  Real and complex kernels
+ * (the reference's NPME_KfuncReal and NPME_KfuncComplex). */
 typedef struct {
-  double fself;
+  double fself, fself_i;  /* f_LR(0) (imaginary part for complex kernels) */
+  int complex_kernel;     /* 1: complex kernel (complex charges and V) */
   int (*direct)(npme_handle *h, const void *args, void *stream);
   int (*sample_lr)(npme_handle *h, int M1, int M2, int M3, const double *ax,
                    const double *ay, const double *az, void *out, void *stream);

@@ -1,4 +1,4 @@
-// Caller-defined real kernels for npme_b200 (the GPU form of the reference's
+// Caller-defined kernels for npme_b200 (the GPU form of the reference's
 // NPME_InterfaceReal_GenFunc with NPME_KfuncReal functors for f, f_LR and
 // f_SR, src/Interface.h:302-304, src/KernelFunction.h:25-65).
 //
@@ -18,6 +18,16 @@
 //     template <typename T> __device__ static T sr(T r2, T &f1);
 //   };
 //
+//   A complex kernel (the reference's NPME_KfuncComplex) declares
+//     static constexpr bool kComplex = true;
+//   and provides instead
+//     __host__ __device__ static void full_c(double r2, double &f0r, double &f0i,
+//                                            double &f1r, double &f1i);
+//     __host__ __device__ static double2 lr_c(double r2);
+//     template <typename T> __device__ static void sr_c(T r2, T &f0r, T &f0i,
+//                                                       T &f1r, T &f1i);
+//   (charges and V complex, as for Helmholtz).
+//
 //   npme_params p;  npme_gpu_default_params(&p);
 //   p.funcType = NPME_FUNC_USER;  p.Rdir = ...;  p.N1 = ...;
 //   npme_handle *h;  npme_gpu_create(&p, &h);
@@ -33,22 +43,51 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "npme_gpu.h"
 #include "bodies.cuh"
 
 namespace npme_user {
 
+// Complex kernels declare  static constexpr bool kComplex = true  and
+// provide full_c / lr_c / sr_c (see the header comment); real kernels need
+// not declare kComplex.
+template <class K, class = void>
+struct is_complex : std::false_type {};
+template <class K>
+struct is_complex<K, std::void_t<decltype(K::kComplex)>>
+    : std::integral_constant<bool, K::kComplex> {};
+
+// The pair-kernel policy handed to the library's direct-sum bodies; both
+// entries exist so that either body compiles, only K's kind is ever called.
 template <class K>
 struct Pair {
   template <typename T>
   __device__ static T sr(T r2, T &f1) {
-    return K::template sr<T>(r2, f1);
+    if constexpr (is_complex<K>::value) {
+      f1 = T(0);
+      return T(0);
+    } else {
+      return K::template sr<T>(r2, f1);
+    }
+  }
+  template <typename T>
+  __device__ static void sr_c(T r2, T &f0r, T &f0i, T &f1r, T &f1i) {
+    if constexpr (is_complex<K>::value) {
+      K::template sr_c<T>(r2, f0r, f0i, f1r, f1i);
+    } else {
+      f0r = f0i = f1r = f1i = T(0);
+    }
   }
 };
 
 template <class K>
 struct LR {
-  __device__ double2 operator()(double r2) const { return make_double2(K::lr(r2), 0.0); }
+  __device__ double2 operator()(double r2) const {
+    if constexpr (is_complex<K>::value) return K::lr_c(r2);
+    else return make_double2(K::lr(r2), 0.0);
+  }
 };
 
 template <class K>
@@ -57,15 +96,15 @@ __global__ void __launch_bounds__(32 * npme::kGroupWarps) groups_kernel(
     const float *__restrict__ qs, const double *__restrict__ qcaller,
     const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
     const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
-    float refine2, double fself, double *__restrict__ V) {
+    float refine2, double fself, double fself_i, double *__restrict__ V) {
   __shared__ float4 sp[npme::kGroupWarps][32];
   __shared__ float4 slo[npme::kGroupWarps][32];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long g = (long)blockIdx.x * npme::kGroupWarps + wid;
   if (g >= ngroups) return;  // warp-uniform
-  npme::direct_group_body<false, NPME_FUNC_USER, 0, 0, Pair<K>>(
-      k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, refine2, fself, 0.0, V, sp[wid],
-      slo[wid], lane);
+  npme::direct_group_body<is_complex<K>::value, NPME_FUNC_USER, 0, 0, Pair<K>>(
+      k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, refine2, fself, fself_i, V,
+      sp[wid], slo[wid], lane);
 }
 
 template <class K>
@@ -115,6 +154,48 @@ __global__ void __launch_bounds__(kExactTile) exact_kernel(const double *__restr
   if (active) reinterpret_cast<double4 *>(V)[t] = make_double4(a[0], a[1], a[2], a[3]);
 }
 
+// The same for complex kernels and charges (V rows of four complex values).
+template <class K>
+__global__ void __launch_bounds__(kExactTile) exact_kernel_c(const double *__restrict__ coord,
+                                                             const double *__restrict__ q, long n,
+                                                             const unsigned int *__restrict__ tidx,
+                                                             long nt, double *__restrict__ V) {
+  __shared__ double4 sp[kExactTile];
+  __shared__ double2 sq[kExactTile];
+  const long t = blockIdx.x * (long)kExactTile + threadIdx.x;
+  const bool active = t < nt;
+  const long i = active ? (tidx ? (long)tidx[t] : t) : -1;
+  double xi = 0, yi = 0, zi = 0;
+  if (active) xi = coord[3 * i], yi = coord[3 * i + 1], zi = coord[3 * i + 2];
+  double a[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+  for (long j0 = 0; j0 < n; j0 += kExactTile) {
+    __syncthreads();
+    const long j = j0 + threadIdx.x;
+    if (j < n) {
+      sp[threadIdx.x] = make_double4(coord[3 * j], coord[3 * j + 1], coord[3 * j + 2], 0.0);
+      sq[threadIdx.x] = make_double2(q[2 * j], q[2 * j + 1]);
+    }
+    __syncthreads();
+    const int cnt = (int)min((long)kExactTile, n - j0);
+    for (int s = 0; s < cnt; s++) {
+      if (j0 + s == i) continue;
+      const double x = xi - sp[s].x, y = yi - sp[s].y, z = zi - sp[s].z;
+      double f0r, f0i, f1r, f1i;
+      K::full_c(x * x + y * y + z * z, f0r, f0i, f1r, f1i);
+      const double qr = sq[s].x, qi = sq[s].y;
+      a[0] += f0r * qr - f0i * qi;
+      ai[0] += f0r * qi + f0i * qr;
+      const double gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
+      a[1] += gr * x, a[2] += gr * y, a[3] += gr * z;
+      ai[1] += gi * x, ai[2] += gi * y, ai[3] += gi * z;
+    }
+  }
+  if (active) {
+    double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * t;
+    for (int m = 0; m < 4; m++) Vo[m] = make_double2(a[m], ai[m]);
+  }
+}
+
 template <class K>
 int direct(npme_handle *h, const void *args, void *stream) {
   const npme::DirectArgs &a = *static_cast<const npme::DirectArgs *>(args);
@@ -125,15 +206,15 @@ int direct(npme_handle *h, const void *args, void *stream) {
     groups_kernel<K><<<(unsigned)blocks, 32 * npme::kGroupWarps, 0, s>>>(
         npme::make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
         h->d_groups, h->d_gcen, h->d_segs, h->d_cperm, h->n_groups, (float)h->refine2,
-        a.fself_r, a.V);
+        a.fself_r, a.fself_i, a.V);
   } else {
     const npme::CellGeom &c = h->cells;
     const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
-    npme::direct_kernel<double, false, NPME_FUNC_USER, 0, 0, Pair<K>>
+    npme::direct_kernel<double, is_complex<K>::value, NPME_FUNC_USER, 0, 0, Pair<K>>
         <<<ncell, npme::kDirectBS, 0, s>>>(
             npme::make_pair_coef<double>(h), (const double4 *)h->d_cpos, (const double *)a.q,
             h->d_cell_start, h->d_cperm, c.nc[0], c.nc[1], c.nc[2], c.edge[0], c.edge[1],
-            c.edge[2], c.reach, a.fself_r, 0.0, a.V);
+            c.edge[2], c.reach, a.fself_r, a.fself_i, a.V);
   }
   return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
 }
@@ -153,8 +234,12 @@ int exact(npme_handle *h, const double *d_q, double *d_V, void *stream,
   if (!d_tidx) nt = n;
   const int blocks = (int)((nt + kExactTile - 1) / kExactTile);
   if (blocks == 0) return NPME_OK;
-  exact_kernel<K><<<blocks, kExactTile, 0, (cudaStream_t)stream>>>(h->d_coord, d_q, n, d_tidx, nt,
-                                                                    d_V);
+  if constexpr (is_complex<K>::value)
+    exact_kernel_c<K><<<blocks, kExactTile, 0, (cudaStream_t)stream>>>(h->d_coord, d_q, n, d_tidx,
+                                                                        nt, d_V);
+  else
+    exact_kernel<K><<<blocks, kExactTile, 0, (cudaStream_t)stream>>>(h->d_coord, d_q, n, d_tidx,
+                                                                      nt, d_V);
   return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
 }
 
@@ -162,7 +247,12 @@ int exact(npme_handle *h, const double *d_q, double *d_V, void *stream,
 template <class K>
 npme_user_ops ops() {
   npme_user_ops o;
-  o.fself = K::lr(0.0);
+  if constexpr (is_complex<K>::value) {
+    const double2 f = K::lr_c(0.0);
+    o.fself = f.x, o.fself_i = f.y, o.complex_kernel = 1;
+  } else {
+    o.fself = K::lr(0.0), o.fself_i = 0.0, o.complex_kernel = 0;
+  }
   o.direct = &direct<K>;
   o.sample_lr = &sample_lr<K>;
   o.exact = &exact<K>;

@@ -62,7 +62,8 @@ class Info(ctypes.Structure):
 class UserOps(ctypes.Structure):
     """npme_user_ops: the launch table of a caller-defined kernel, filled by
     npme_user::ops<Functor>() in the caller's CUDA code."""
-    _fields_ = [("fself", ctypes.c_double), ("direct", ctypes.c_void_p),
+    _fields_ = [("fself", ctypes.c_double), ("fself_i", ctypes.c_double),
+                ("complex_kernel", ctypes.c_int), ("direct", ctypes.c_void_p),
                 ("sample_lr", ctypes.c_void_p), ("exact", ctypes.c_void_p)]
 
 
@@ -228,6 +229,7 @@ class Solver:
         """Launch table (UserOps) of a caller-defined kernel; funcType "user"."""
         self._check(self.L.npme_gpu_set_user_kernel(self.h, ctypes.byref(ops)))
         self._user_ops = ops
+        self.complex = bool(ops.complex_kernel)
         return self
 
     def setup(self, coord):

@@ -738,7 +738,7 @@ __device__ __forceinline__ void direct_group_body(
           p3 = fmaf(gq, z, p3);
         } else {
           float f0r, f0i, f1r, f1i;
-          pair_sr_helmholtz<float, ND>(k, r2, f0r, f0i, f1r, f1i);
+          pair_sr_cplx<float, ND, PK>(k, r2, f0r, f0i, f1r, f1i);
           const float qr = src.w, qi = slo[s].w;
           p0 = fmaf(f0r, qr, fmaf(-f0i, qi, p0));
           p0i = fmaf(f0r, qi, fmaf(f0i, qr, p0i));
@@ -849,7 +849,7 @@ __global__ void __launch_bounds__(kDirectBS) direct_kernel(
                 p3 = fma(g, z, p3);
               } else {
                 T f0r, f0i, f1r, f1i;
-                pair_sr_helmholtz<T, ND>(k, r2, f0r, f0i, f1r, f1i);
+                pair_sr_cplx<T, ND, PK>(k, r2, f0r, f0i, f1r, f1i);
                 const T qr = sq[2 * s], qi = sq[2 * s + 1];
                 // f0 q and (f1 q) * (x, y, z), complex
                 p0 = fma(f0r, qr, fma(-f0i, qi, p0));

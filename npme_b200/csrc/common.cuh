@@ -197,4 +197,16 @@ __device__ __forceinline__ T pair_sr(const PairCoef<T> &k, T r2, T &f1) {
     return PK::template sr<T>(r2, f1);
 }
 
+// Complex kernels: the built-in Helmholtz kernel, or a caller's functor with
+//   template <typename T> __device__ static void sr_c(T r2, T &f0r, T &f0i,
+//                                                     T &f1r, T &f1i).
+template <typename T, int ND, class PK>
+__device__ __forceinline__ void pair_sr_cplx(const PairCoef<T> &k, T r2, T &f0r, T &f0i, T &f1r,
+                                             T &f1i) {
+  if constexpr (std::is_same<PK, BuiltinPair>::value)
+    pair_sr_helmholtz<T, ND>(k, r2, f0r, f0i, f1r, f1i);
+  else
+    PK::template sr_c<T>(r2, f0r, f0i, f1r, f1i);
+}
+
 }  // namespace npme

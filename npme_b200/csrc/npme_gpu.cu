@@ -660,9 +660,10 @@ int check_params(npme_handle *h, const npme_params &p) {
 // Derived state of the parameters: kernel kind, precision and the splitting
 // coefficients (host FP64).
 int apply_params(npme_handle *h) {
-  h->complex_kernel = h->p.funcType == NPME_FUNC_HELMHOLTZ;
-  h->fp32 = h->p.precision == NPME_PREC_FP32;
   h->user_kernel = h->p.funcType == NPME_FUNC_USER;
+  h->complex_kernel = h->user_kernel ? h->uops.complex_kernel != 0
+                                     : h->p.funcType == NPME_FUNC_HELMHOLTZ;
+  h->fp32 = h->p.precision == NPME_PREC_FP32;
   memset(h->a_r, 0, sizeof(h->a_r));
   memset(h->a_i, 0, sizeof(h->a_i));
   memset(h->b_r, 0, sizeof(h->b_r));
@@ -670,7 +671,7 @@ int apply_params(npme_handle *h) {
   h->beta = 0;
   if (h->user_kernel) {  // the caller's functors define the split
     h->fself_r = h->uops.direct ? h->uops.fself : 0.0;
-    h->fself_i = 0;
+    h->fself_i = h->uops.direct ? h->uops.fself_i : 0.0;
   } else if (h->p.EwaldSplit == NPME_SPLIT_DERIVMATCH) {
     std::complex<double> a[32], b[32];
     dm_coefficients(h->p, a, b);
@@ -790,7 +791,8 @@ int npme_gpu_set_user_kernel(npme_handle *h, const npme_user_ops *ops) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->stream2) cudaStreamSynchronize(h->stream2);
   h->uops = *ops;
-  h->fself_r = ops->fself, h->fself_i = 0;
+  h->fself_r = ops->fself, h->fself_i = ops->fself_i;
+  h->complex_kernel = ops->complex_kernel != 0;
   h->ready = false;  // the kernel transform depends on f_LR: set up again
   return NPME_OK;
 }

@@ -109,3 +109,31 @@ def test_user_erf_coulomb_equals_builtin_original_ewald(user_lib):
         Ve = sb.calcv_exact(q)
     print("user erf vs builtin orig", rel(Vu, Vb), "builtin vs exact", rel(Vb[:, 0], Ve[:, 0]))
     assert rel(Vu, Vb) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_complex_user_kernel_matches_its_exact_sum(user_lib, precision):
+    """exp(i k r)/r as a complex functor (the reference's NPME_KfuncComplex)."""
+    import npme_b200
+    from npme_b200 import api
+    L = ctypes.CDLL(user_lib)
+    ops = api.UserOps()
+    L.wave_erf_ops(ctypes.byref(ops))
+    assert ops.complex_kernel == 1 and abs(ops.fself_i - 0.5) < 1e-15
+    c, _ = _system()
+    g = np.random.Generator(np.random.Philox(43))
+    q = g.uniform(-1, 1, c.shape[0]) + 1j * g.uniform(-1, 1, c.shape[0])
+    p = api.make_params("user", "dm", Rdir=8.0, order=8, grid=(64, 64, 64), precision=precision)
+    with npme_b200.Solver(p) as s:
+        V = s.set_user_kernel(ops).setup(c).calcv(q)
+        Ve = s.calcv_exact(q)
+    i = 123
+    d = c[i] - np.delete(c, i, axis=0)
+    r = np.linalg.norm(d, axis=1)
+    want = np.sum(np.delete(q, i) * np.exp(0.5j * r) / r)
+    assert abs(Ve[i, 0] - want) < 1e-12 * abs(want) + 1e-12
+    print(precision, "complex user kernel rel err V", rel(V[:, 0], Ve[:, 0]),
+          "grad", rel(V[:, 1:], Ve[:, 1:]))
+    assert rel(V[:, 0], Ve[:, 0]) < 1e-4
+    assert rel(V[:, 1:], Ve[:, 1:]) < 1e-4
