@@ -23,11 +23,11 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # seconds per unit on one B200 (FP32 bulk), from the 1M-point benchmark
-# stage times: direct 7.0 ms for 1e6 x 5.6e3 staged candidates, spread +
-# interpolation 0.62 ms for 1e6 x 216 stencil points, FFT pair 0.18 ms for
+# stage times: direct 4.9 ms for 1e6 x 4.57e3 modelled candidates, spread +
+# interpolation 0.30 ms for 1e6 x 216 stencil points, FFT pair 0.18 ms for
 # 256^3 x log2(256^3)
-T_CANDIDATE = 1.25e-12
-T_STENCIL = 2.9e-12
+T_CANDIDATE = 1.07e-12
+T_STENCIL = 1.39e-12
 T_FFT = 4.5e-13
 T_FIXED = 60e-6  # launches and set-up kernels per solve
 
