@@ -115,10 +115,10 @@ __device__ __forceinline__ void spread_brick_body(int brick, const int *__restri
 // contribution instead of one floating-point shared atomic (which the
 // hardware does not have and executes as a compare-and-swap loop; a probe
 // ran 3.5x faster with integer atomics).  Each contribution v = c q is
-// scaled by S = 2^k, k = 30 - ceil(log2(n_brick max|q|)), so the high words
-// round(v S) of all contributions to a tile point cannot exceed 2^30 in sum;
-// the low words round((v S - hi) 2^L) carry L = 30 - ceil(log2 n_brick)
-// more bits.  The integer sums are exact and independent of the order of
+// scaled by S = 2^k so that |v S| <= 2^B, B = min(21, 30 - ceil(log2
+// n_brick)): the high words round(v S) of all contributions to a tile point
+// cannot exceed 2^30 in sum, and the low words round((v S - hi) 2^B) carry
+// B more bits.  The integer sums are exact and independent of the order of
 // the atomics; each tile value hi + lo 2^-L is rounded once, to float, when
 // it is added to the grid.  Same points, weights and tile as
 // spread_brick_body.
@@ -147,8 +147,11 @@ __device__ __forceinline__ void spread_brick_fixed(int brick, const int *__restr
   for (int w = 1; w < nw; w++) m = fmaxf(m, s_max[w]);
   if (m == 0.f) return;  // nothing to spread (the whole CTA returns)
   const int lnb = 32 - __clz(max(nbp - 1, 1));  // ceil(log2(nbp)), nbp >= 2
-  const int k = max(-120, min(120, 30 - (ilogbf(m) + 1) - lnb));
-  const int L = 30 - lnb;
+  // bits per contribution: sums of nbp of them stay below 2^30, and single
+  // words below 2^22 so that a float converts to int by the add-magic trick
+  const int B = min(21, 30 - lnb);
+  const int k = max(-120, min(120, B - (ilogbf(m) + 1)));
+  const int L = B;
   const float S = ldexpf(1.f, k), SL = ldexpf(1.f, L);
   const int nvw = (nbp + 31) >> 5;
   for (int vw = threadIdx.x >> 5; vw < nvw; vw += nw) {
@@ -175,10 +178,15 @@ __device__ __forceinline__ void spread_brick_fixed(int brick, const int *__restr
           const float c = c12 * w3[t3];
 #pragma unroll
           for (int part = 0; part < C; part++) {
+            // |v| <= 2^21: adding 1.5 * 2^23 rounds v to an integer held in
+            // the low mantissa bits (no conversion instruction needed)
+            constexpr float kMagic = 12582912.f;
             const float v = c * (part ? qi : qr);
-            const float h = rintf(v);
-            atomicAdd(thi + row + C * t3 + part, (int)h);
-            atomicAdd(tlo + row + C * t3 + part, __float2int_rn((v - h) * SL));
+            const float vm = v + kMagic;
+            const float r = v - (vm - kMagic);  // exact remainder, |r| <= 1/2
+            atomicAdd(thi + row + C * t3 + part, __float_as_int(vm) - 0x4B400000);
+            atomicAdd(tlo + row + C * t3 + part,
+                      __float_as_int(fmaf(r, SL, kMagic)) - 0x4B400000);
           }
         }
       }
