@@ -37,7 +37,7 @@
 //
 // The spreading, FFTs, kernel multiply and interpolation are the library's;
 // this header instantiates the three kernel-dependent launches: the direct
-// sum (FP32 warp-group body or FP64 cell-list body with the functor's sr),
+// sum (FP32 or FP64 warp-group body with the functor's sr),
 // the sampling of f_LR for the kernel transform and the exact sum.
 #pragma once
 
@@ -105,6 +105,24 @@ __global__ void __launch_bounds__(32 * npme::kGroupWarps) groups_kernel(
   npme::direct_group_body<is_complex<K>::value, NPME_FUNC_USER, 0, 0, Pair<K>>(
       k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, refine2, fself, fself_i, V,
       sp[wid], slo[wid], lane);
+}
+
+template <class K>
+__global__ void __launch_bounds__(32 * npme::kGroupWarps) groups64_kernel(
+    npme::PairCoef<double> k, const double4 *__restrict__ gpos,
+    const double4 *__restrict__ spos, const double *__restrict__ qs,
+    const double *__restrict__ qcaller, const int4 *__restrict__ groups,
+    const double4 *__restrict__ gcen, const int2 *__restrict__ segs,
+    const uint32_t *__restrict__ perm, long ngroups, double fself, double fself_i,
+    double *__restrict__ V) {
+  __shared__ double4 sp[npme::kGroupWarps][32];
+  __shared__ double sqi[npme::kGroupWarps][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * npme::kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  npme::direct_group_fp64<is_complex<K>::value, NPME_FUNC_USER, 0, 0, Pair<K>>(
+      k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, fself, fself_i, V, sp[wid],
+      sqi[wid], lane);
 }
 
 template <class K>
@@ -200,7 +218,7 @@ template <class K>
 int direct(npme_handle *h, const void *args, void *stream) {
   const npme::DirectArgs &a = *static_cast<const npme::DirectArgs *>(args);
   cudaStream_t s = (cudaStream_t)stream;
-  if (h->use_groups) {
+  if (h->fp32) {
     const long blocks = (h->n_groups + npme::kGroupWarps - 1) / npme::kGroupWarps;
     if (blocks == 0) return NPME_OK;
     groups_kernel<K><<<(unsigned)blocks, 32 * npme::kGroupWarps, 0, s>>>(
@@ -208,13 +226,11 @@ int direct(npme_handle *h, const void *args, void *stream) {
         h->d_groups, h->d_gcen, h->d_segs, h->d_cperm, h->n_groups, (float)h->refine2,
         a.fself_r, a.fself_i, a.V);
   } else {
-    const npme::CellGeom &c = h->cells;
-    const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
-    npme::direct_kernel<double, is_complex<K>::value, NPME_FUNC_USER, 0, 0, Pair<K>>
-        <<<ncell, npme::kDirectBS, 0, s>>>(
-            npme::make_pair_coef<double>(h), (const double4 *)h->d_cpos, (const double *)a.q,
-            h->d_cell_start, h->d_cperm, c.nc[0], c.nc[1], c.nc[2], c.edge[0], c.edge[1],
-            c.edge[2], c.reach, a.fself_r, a.fself_i, a.V);
+    const long blocks = (h->n_groups + npme::kGroupWarps - 1) / npme::kGroupWarps;
+    if (blocks == 0) return NPME_OK;
+    groups64_kernel<K><<<(unsigned)blocks, 32 * npme::kGroupWarps, 0, s>>>(
+        npme::make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
+        h->d_groups, h->d_gcen, h->d_segs, h->d_cperm, h->n_groups, a.fself_r, a.fself_i, a.V);
   }
   return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
 }

@@ -780,127 +780,100 @@ __device__ __forceinline__ void direct_group_body(
   }
 }
 
-// ---------------------------------------------------------------------------
-// Plain cell-list direct sum (the FP64 port of the reference's direct sum,
-// src/PotentialLaplace.cpp:201-719): one CTA per cell of edge >= Rdir / nNeigh,
-// the neighbour columns staged through shared memory in tiles of kDirectBS.
-constexpr int kDirectBS = 64;
-
-template <typename T, bool CPLX, int FUNC, int SPLIT, int ND, class PK = BuiltinPair>
-__global__ void __launch_bounds__(kDirectBS) direct_kernel(
-    PairCoef<T> k, const typename Vec4<T>::type *__restrict__ cpos, const T *__restrict__ qc,
-    const int *__restrict__ cell_start, const uint32_t *__restrict__ cperm, int nc0, int nc1,
-    int nc2, T e0, T e1, T e2, int reach, double fself_r, double fself_i,
-    double *__restrict__ V) {
-  using V4 = typename Vec4<T>::type;
-  __shared__ V4 sp[kDirectBS];
-  __shared__ T sq[kDirectBS * (CPLX ? 2 : 1)];
-  const int cell = blockIdx.x;
-  const int cz = cell % nc2, cy = (cell / nc2) % nc1, cx = cell / (nc2 * nc1);
-  const int tbeg = cell_start[cell], tend = cell_start[cell + 1];
-  const T R2 = k.R2;
-  const double e0d = e0, e1d = e1, e2d = e2;
-  for (int t0 = tbeg; t0 < tend; t0 += kDirectBS) {
-    const int i = t0 + threadIdx.x;
-    const bool active = i < tend;
-    V4 ti = active ? cpos[i] : V4{0, 0, 0, 0};
-    double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
-    for (int dx = -reach; dx <= reach; dx++) {
-      const int sx = cx + dx;
-      if (sx < 0 || sx >= nc0) continue;
-      const double mx = (double)(abs(dx) > 0 ? abs(dx) - 1 : 0) * e0d;
-      for (int dy = -reach; dy <= reach; dy++) {
-        const int sy = cy + dy;
-        if (sy < 0 || sy >= nc1) continue;
-        const double my = (double)(abs(dy) > 0 ? abs(dy) - 1 : 0) * e1d;
-        const double rem = (double)R2 - mx * mx - my * my;
-        if (rem < 0) continue;
-        // cells with |dz| - 1 <= sqrt(rem) / e2 can hold a source within Rdir
-        const int zr = min(reach, 1 + (int)floor(sqrt(rem) / e2d));
-        const int z0 = max(cz - zr, 0), z1 = min(cz + zr, nc2 - 1);
-        const int colbase = (sx * nc1 + sy) * nc2;
-        const int jb = cell_start[colbase + z0], je = cell_start[colbase + z1 + 1];
-        const T ox = (T)dx * e0, oy = (T)dy * e1;
-        for (int j0 = jb; j0 < je; j0 += kDirectBS) {
-          __syncthreads();
-          const int j = j0 + threadIdx.x;
-          if (j < je) {
-            V4 s = cpos[j];
-            s.x += ox;
-            s.y += oy;
-            s.z += (s.w - (T)cz) * e2;
-            sp[threadIdx.x] = s;
-            if (CPLX) {
-              sq[2 * threadIdx.x] = qc[2 * (long)j];
-              sq[2 * threadIdx.x + 1] = qc[2 * (long)j + 1];
-            } else {
-              sq[threadIdx.x] = qc[j];
-            }
-          }
-          __syncthreads();
-          const int cnt = min(kDirectBS, je - j0);
-          T p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
-          const int self = i - j0;  // staged slot of the target itself, if present
-          for (int s = 0; s < cnt; s++) {
-            const V4 src = sp[s];
-            const T x = ti.x - src.x, y = ti.y - src.y, z = ti.z - src.z;
-            const T r2 = fma(x, x, fma(y, y, z * z));
-            if (r2 <= R2 && s != self) {
-              if (!CPLX) {
-                T f1;
-                const T f0 = pair_sr<T, FUNC, SPLIT, ND, PK>(k, r2, f1);
-                const T qj = sq[s];
-                const T g = f1 * qj;
-                p0 = fma(f0, qj, p0);
-                p1 = fma(g, x, p1);
-                p2 = fma(g, y, p2);
-                p3 = fma(g, z, p3);
-              } else {
-                T f0r, f0i, f1r, f1i;
-                pair_sr_cplx<T, ND, PK>(k, r2, f0r, f0i, f1r, f1i);
-                const T qr = sq[2 * s], qi = sq[2 * s + 1];
-                // f0 q and (f1 q) * (x, y, z), complex
-                p0 = fma(f0r, qr, fma(-f0i, qi, p0));
-                p0i = fma(f0r, qi, fma(f0i, qr, p0i));
-                const T gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
-                p1 = fma(gr, x, p1);
-                p2 = fma(gr, y, p2);
-                p3 = fma(gr, z, p3);
-                p1i = fma(gi, x, p1i);
-                p2i = fma(gi, y, p2i);
-                p3i = fma(gi, z, p3i);
-              }
-            }
-          }
-          acc[0] += (double)p0;
-          acc[1] += (double)p1;
-          acc[2] += (double)p2;
-          acc[3] += (double)p3;
-          if (CPLX) {
-            acci[0] += (double)p0i;
-            acci[1] += (double)p1i;
-            acci[2] += (double)p2i;
-            acci[3] += (double)p3i;
-          }
+// FP64 direct sum of one warp group (the plain precision): the same groups
+// and source segments as the FP32 body, every difference and pair kernel in
+// double, no head/residual split needed.  sp holds 32 (x, y, z, Re q)
+// entries relative to the group centre, sqi the imaginary parts.
+template <bool CPLX, int FUNC, int SPLIT, int ND, class PK = BuiltinPair>
+__device__ __forceinline__ void direct_group_fp64(
+    const PairCoef<double> &k, const double4 *__restrict__ gpos,
+    const double4 *__restrict__ spos, const double *__restrict__ qs,
+    const double *__restrict__ qcaller, const int4 G, const double4 c,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, double fself_r,
+    double fself_i, double *__restrict__ V, double4 *sp, double *sqi, int lane) {
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  double tx = 1e150, ty = 1e150, tz = 1e150;  // idle lanes sit far outside the cutoff
+  if (active) {
+    const double4 p = gpos[ti];
+    tx = p.x - c.x, ty = p.y - c.y, tz = p.z - c.z;
+  }
+  const double R2 = k.R2;
+  double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
+  SrcCursor cur{G.z, lane};
+  cur.normalize(segs, G.w);
+  bool pv = cur.seg < G.w;
+  double4 pp = make_double4(0, 0, 0, 0);
+  double pqi = 0;
+#define NPME_PREFETCH64                                     \
+  if (pv) {                                                 \
+    const long j_ = (long)segs[cur.seg].x + cur.off;        \
+    const double4 p_ = spos[j_];                            \
+    pp = make_double4(p_.x - c.x, p_.y - c.y, p_.z - c.z,   \
+                      CPLX ? qs[2 * j_] : qs[j_]);          \
+    if (CPLX) pqi = qs[2 * j_ + 1];                         \
+  }
+  NPME_PREFETCH64
+  while (__any_sync(0xffffffffu, pv)) {
+    const int cnt = __popc(__ballot_sync(0xffffffffu, pv));  // valid lanes form a prefix
+    __syncwarp();
+    if (pv) {
+      sp[lane] = pp;
+      if (CPLX) sqi[lane] = pqi;
+    }
+    __syncwarp();
+    cur.off += 32;
+    cur.normalize(segs, G.w);
+    pv = cur.seg < G.w;
+    NPME_PREFETCH64
+#pragma unroll 4
+    for (int s = 0; s < cnt; s++) {
+      const double4 src = sp[s];
+      const double x = tx - src.x, y = ty - src.y, z = tz - src.z;
+      const double r2 = fma(x, x, fma(y, y, z * z));
+      if (r2 <= R2 && r2 > 0.0) {
+        if (!CPLX) {
+          double f1;
+          const double f0 = pair_sr<double, FUNC, SPLIT, ND, PK>(k, r2, f1);
+          const double gq = f1 * src.w;
+          acc[0] = fma(f0, src.w, acc[0]);
+          acc[1] = fma(gq, x, acc[1]);
+          acc[2] = fma(gq, y, acc[2]);
+          acc[3] = fma(gq, z, acc[3]);
+        } else {
+          double f0r, f0i, f1r, f1i;
+          pair_sr_cplx<double, ND, PK>(k, r2, f0r, f0i, f1r, f1i);
+          const double qr = src.w, qi = sqi[s];
+          acc[0] = fma(f0r, qr, fma(-f0i, qi, acc[0]));
+          acci[0] = fma(f0r, qi, fma(f0i, qr, acci[0]));
+          const double gr = f1r * qr - f1i * qi, gi = f1r * qi + f1i * qr;
+          acc[1] = fma(gr, x, acc[1]);
+          acc[2] = fma(gr, y, acc[2]);
+          acc[3] = fma(gr, z, acc[3]);
+          acci[1] = fma(gi, x, acci[1]);
+          acci[2] = fma(gi, y, acci[2]);
+          acci[3] = fma(gi, z, acci[3]);
         }
       }
     }
-    if (active) {
-      const long o = cperm[i];
-      if (CPLX) {
-        const double qr = qc[2 * (long)i], qi = qc[2 * (long)i + 1];
-        // V -= f_LR(0) q (src/Interface.cpp:2909-2910)
-        acc[0] -= fself_r * qr - fself_i * qi;
-        acci[0] -= fself_r * qi + fself_i * qr;
-        double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+  }
+#undef NPME_PREFETCH64
+  if (active) {
+    const long o = perm[ti];
+    if (CPLX) {
+      const double qr = qcaller[2 * o], qi = qcaller[2 * o + 1];
+      acc[0] -= fself_r * qr - fself_i * qi;  // src/Interface.cpp:2909-2910
+      acci[0] -= fself_r * qi + fself_i * qr;
+      double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
 #pragma unroll
-        for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
-      } else {
-        acc[0] -= fself_r * (double)qc[i];  // src/Interface.cpp:2061-2062
-        reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
-      }
+      for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
+    } else {
+      acc[0] -= fself_r * qcaller[o];  // src/Interface.cpp:2061-2062
+      reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
     }
   }
 }
+
+constexpr int kDirectBS = 64;  // tile of the cell-list pair count (direct.cu)
 
 }  // namespace npme

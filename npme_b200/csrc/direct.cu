@@ -1,16 +1,13 @@
-// Short-range direct sum over a cell list, and the exact O(N^2) sum.
+// Short-range direct sum over warp groups, the cell-list pair count and the
+// exact O(N^2) sum.
 //
 // Direct sum (src/PotentialLaplace.cpp:201-264 and the pair kernels cited in
 // common.cuh): V_i = sum_{j != i, r_ij <= Rdir} q_j f_SR(r_ij),
-// dV_i/dx = sum q_j f1_SR(r_ij) (x_i - x_j).  Points are sorted by cell
-// (edge >= Rdir/nNeigh, row-major, z fastest), so the cells of one (x, y)
-// neighbour column with consecutive z are one contiguous range.  One CTA owns
-// one target cell; source ranges are staged through shared memory with their
-// cell offset applied (coordinates are kept relative to the point's own cell,
-// so float arithmetic keeps ~1e-7 relative resolution whatever the box size).
-// Each thread accumulates its target over a staged tile in the bulk
-// precision and adds the tile total to a double accumulator.  No atomics: the
-// result is deterministic and each output row is written once.
+// dV_i/dx = sum q_j f1_SR(r_ij) (x_i - x_j).  Targets are grouped by 32 in
+// z-sorted coarse columns and every group owns a list of source segments
+// (build_groups in npme_gpu.cu); one warp walks one group in both
+// precisions.  Each lane accumulates its target in double and writes its
+// output row once: no atomics, deterministic results.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -62,7 +59,7 @@ template PairCoef<float> make_pair_coef<float>(const npme_handle *);
 template PairCoef<double> make_pair_coef<double>(const npme_handle *);
 
 // ---------------------------------------------------------------------------
-// FP32 bulk direct sum over warp groups (see build_groups in npme_gpu.cu).
+// FP32 bulk direct sum over warp groups.
 // One warp owns one group of <= 32 targets (one per lane) and walks the
 // group's source segments in chunks of 32 that run across segment
 // boundaries: every lane loads one source (FP64 position), the warp stages
@@ -107,8 +104,42 @@ static void groups_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s
       a.V);
 }
 
+template <bool CPLX, int FUNC, int SPLIT, int ND>
+__global__ void __launch_bounds__(32 * kGroupWarps) direct_groups64_kernel(
+    PairCoef<double> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const double *__restrict__ qs, const double *__restrict__ qcaller,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    double fself_r, double fself_i, double *__restrict__ V) {
+  __shared__ double4 sp[kGroupWarps][32];
+  __shared__ double sqi[kGroupWarps][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  direct_group_fp64<CPLX, FUNC, SPLIT, ND>(k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs,
+                                           perm, fself_r, fself_i, V, sp[wid], sqi[wid], lane);
+}
+
+template <bool CPLX, int FUNC, int SPLIT, int ND>
+static void groups64_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  const long blocks = (h->n_groups + kGroupWarps - 1) / kGroupWarps;
+  if (blocks == 0) return;
+  direct_groups64_kernel<CPLX, FUNC, SPLIT, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
+      make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
+      h->d_groups, h->d_gcen, h->d_segs, h->d_cperm, h->n_groups, a.fself_r, a.fself_i, a.V);
+}
+
 template <bool CPLX, int FUNC, int SPLIT>
 static void groups_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  if (!h->fp32) {
+    switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
+      case 3: groups64_launch_nd<CPLX, FUNC, SPLIT, 3>(h, a, s); break;
+      case 6: groups64_launch_nd<CPLX, FUNC, SPLIT, 6>(h, a, s); break;
+      case 8: groups64_launch_nd<CPLX, FUNC, SPLIT, 8>(h, a, s); break;
+      default: groups64_launch_nd<CPLX, FUNC, SPLIT, 0>(h, a, s); break;
+    }
+    return;
+  }
   switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
     case 3: groups_launch_nd<CPLX, FUNC, SPLIT, 3>(h, a, s); break;
     case 6: groups_launch_nd<CPLX, FUNC, SPLIT, 6>(h, a, s); break;
@@ -117,50 +148,15 @@ static void groups_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   }
 }
 
-template <typename T, bool CPLX, int FUNC, int SPLIT, int ND>
-static void direct_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
-  const CellGeom &c = h->cells;
-  const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
-  direct_kernel<T, CPLX, FUNC, SPLIT, ND><<<ncell, kDirectBS, 0, s>>>(
-      make_pair_coef<T>(h), (const typename Vec4<T>::type *)h->d_cpos, (const T *)a.q,
-      h->d_cell_start, h->d_cperm, c.nc[0], c.nc[1], c.nc[2], (T)c.edge[0], (T)c.edge[1],
-      (T)c.edge[2], c.reach, a.fself_r, a.fself_i, a.V);
-}
-
-// Dispatch on the derivative-match degree: the reference's defaults (3, 6, 8
-// for B-spline orders 4, 6, 8) get fully unrolled polynomials.
-template <typename T, bool CPLX, int FUNC, int SPLIT>
-static void direct_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
-  switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
-    case 3: direct_launch_nd<T, CPLX, FUNC, SPLIT, 3>(h, a, s); break;
-    case 6: direct_launch_nd<T, CPLX, FUNC, SPLIT, 6>(h, a, s); break;
-    case 8: direct_launch_nd<T, CPLX, FUNC, SPLIT, 8>(h, a, s); break;
-    default: direct_launch_nd<T, CPLX, FUNC, SPLIT, 0>(h, a, s); break;
-  }
-}
-
-template <typename T>
-static void direct_prec(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
-  const int f = h->p.funcType, sp = h->p.EwaldSplit;
-  if (f == NPME_FUNC_HELMHOLTZ) direct_launch<T, true, 2, 0>(h, a, s);
-  else if (sp == NPME_SPLIT_LAPLACE_ORIG) direct_launch<T, false, 0, 1>(h, a, s);
-  else if (f == NPME_FUNC_RALPHA) direct_launch<T, false, 1, 0>(h, a, s);
-  else direct_launch<T, false, 0, 0>(h, a, s);
-}
-
 void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   if (h->user_kernel) {
     h->uops.direct(h, &a, s);
-  } else if (h->use_groups) {
+  } else {  // both precisions walk warp groups
     const int f = h->p.funcType, sp = h->p.EwaldSplit;
     if (f == NPME_FUNC_HELMHOLTZ) groups_launch<true, 2, 0>(h, a, s);
     else if (sp == NPME_SPLIT_LAPLACE_ORIG) groups_launch<false, 0, 1>(h, a, s);
     else if (f == NPME_FUNC_RALPHA) groups_launch<false, 1, 0>(h, a, s);
     else groups_launch<false, 0, 0>(h, a, s);
-  } else if (h->fp32) {
-    direct_prec<float>(h, a, s);
-  } else {
-    direct_prec<double>(h, a, s);
   }
   h->launches++;
 }

@@ -581,7 +581,7 @@ int upload_points(npme_handle *h, const double *coord) {
 
   const int C = h->complex_kernel ? 2 : 1;
   int rc;
-  // the FP32 direct sum walks warp groups: targets in group order, sources
+  // the direct sum walks warp groups: targets in group order, sources
   // (and their gathered charges) in fine-column order
   std::vector<uint32_t> sperm;
   if (h->use_groups && (rc = build_groups(h, coord, cperm, sperm))) return rc;
@@ -859,9 +859,8 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
   }
   if (ncells > (1L << 30)) return fail(h, NPME_EINVAL, "too many direct-sum cells");
   h->cells.reach = p.nNeigh;
-  // FP32 bulk mode uses the warp-group direct sum; FP64 keeps the plain
-  // cell-list port
-  h->use_groups = h->fp32;
+  // both precisions walk warp groups; the cell list above serves the pair count
+  h->use_groups = true;
   int rc = h->fp32 ? upload_points<float>(h, coord) : upload_points<double>(h, coord);
   if (rc) {
     release(h);
