@@ -426,10 +426,12 @@ def main():
             fp_peak /= 2
         achieved = (pairs * flops_pair / (st["direct"] / 1e3) / 1e12
                     if pairs and st["direct"] > 0 else None)
-        roofline = {"kernel": "direct_kernel", "bound": "fp32" if args.precision == "fp32" else "fp64",
+        dk = ("direct_sym_kernel" if info0.get("pairsOnce") else
+              "direct_groups_kernel" if args.precision == "fp32" else "direct_groups64_kernel")
+        roofline = {"kernel": dk, "bound": "fp32" if args.precision == "fp32" else "fp64",
                     "achieved": achieved, "peak": fp_peak, "unit": "TFLOP/s",
                     "frac": (achieved / fp_peak) if achieved else None,
-                    "traffic": profile_traffic("direct_kernel"),
+                    "traffic": profile_traffic(dk),
                     "peak_source": "nominal 148 SM x 128 lanes x 2 flop at the sampled median "
                                    "SM clock (MEASURED_PEAKS.json has no FP32 figure)",
                     "work": f"{pairs} unordered pairs within Rdir x {flops_pair} flop"}

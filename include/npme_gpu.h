@@ -101,8 +101,11 @@ typedef struct {
   float stage_ms[8];    /* last calcv with timing on: gather, spread, fft,
                            multiply, ifft, direct, interp, total */
   int launches;         /* kernels launched by the last calcv */
-  long nGroups;         /* FP32 direct sum: warp groups of <= 32 points */
-  double candidatesPerPoint; /* FP32 direct sum: staged sources per target */
+  long nGroups;         /* direct sum: warp groups of <= 32 points */
+  double candidatesPerPoint; /* direct sum: staged sources per target */
+  int pairsOnce;        /* 1: the direct sum evaluates every pair once, for
+                           both of its points (FP32 real DM kernels) */
+  double pairsOnceCandidatesPerPoint; /* half-shell sources per target */
 } npme_info;
 
 typedef struct npme_handle npme_handle;

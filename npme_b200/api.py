@@ -56,6 +56,7 @@ class Info(ctypes.Structure):
         ("nNonEmptyBricks", ctypes.c_long), ("deviceBytes", ctypes.c_size_t),
         ("stage_ms", ctypes.c_float * 8), ("launches", ctypes.c_int),
         ("nGroups", ctypes.c_long), ("candidatesPerPoint", ctypes.c_double),
+        ("pairsOnce", ctypes.c_int), ("pairsOnceCandidatesPerPoint", ctypes.c_double),
     ]
 
 
@@ -312,6 +313,8 @@ class Solver:
             "nNonEmptyBricks": i.nNonEmptyBricks, "deviceBytes": i.deviceBytes,
             "stage_ms": dict(zip(STAGES, list(i.stage_ms))), "launches": i.launches,
             "nGroups": i.nGroups, "candidatesPerPoint": i.candidatesPerPoint,
+            "pairsOnce": bool(i.pairsOnce),
+            "pairsOnceCandidatesPerPoint": i.pairsOnceCandidatesPerPoint,
         }
 
     def close(self):

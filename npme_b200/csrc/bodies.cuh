@@ -376,6 +376,57 @@ __device__ __forceinline__ void interp_brick_body(int brick, const int *__restri
 #endif
 constexpr int kPackedBlock = NPME_PACKED_BLOCK;
 
+// Real DM pair kernel in the scaled frame (coordinates in units of Rdir,
+// s = r^2): f0 = Rdir^(-alpha)... scaled f_SR and t = -(scaled f1) for two
+// squared distances at once.  1/r: f0 = 1/r - P(s), t = 1/r^3 + D(s);
+// r^alpha: f0 = s^(alpha/2) - P(s), t = -alpha s^(alpha/2) / s + D(s), with
+// P, D the DM polynomials (src/KernelFunctionLaplace.cpp:394-436,
+// src/KernelFunctionRalpha.cpp:342-384).
+template <int FUNC, int ND>
+__device__ __forceinline__ void dm_eval2(const PairCoef<float> &k, float2 sv, float2 &f0,
+                                         float2 &t) {
+  float2 np = k.nar2[ND];  // -Rdir^(-alpha) f_LR polynomial
+#pragma unroll
+  for (int n = ND - 1; n >= 0; n--) np = __ffma2_rn(np, sv, k.nar2[n]);
+  float2 d = k.br2[ND - 1];  // Rdir^(2-alpha) (1/r) d f_LR / dr polynomial
+#pragma unroll
+  for (int n = ND - 2; n >= 0; n--) d = __ffma2_rn(d, sv, k.br2[n]);
+  if (FUNC == 0) {
+    const float2 ri = make_float2(rsqrtf(sv.x), rsqrtf(sv.y));
+    f0 = __fadd2_rn(ri, np);                    // Rdir (1/r - f_LR)
+    t = __ffma2_rn(__fmul2_rn(ri, ri), ri, d);  // -Rdir^3 f1
+  } else {
+    // s^(alpha/2) = 2^((alpha/2) log2 s) on the special-function unit;
+    // 1/s = rsqrt(s)^2
+    const float2 e0 = make_float2(exp2f(k.half_alpha * __log2f(sv.x)),
+                                  exp2f(k.half_alpha * __log2f(sv.y)));
+    const float2 ri = make_float2(rsqrtf(sv.x), rsqrtf(sv.y));
+    f0 = __fadd2_rn(e0, np);
+    t = __ffma2_rn(__fmul2_rn(e0, make_float2(-k.alpha, -k.alpha)), __fmul2_rn(ri, ri), d);
+  }
+}
+
+// The same pair kernel for one squared distance.
+template <int FUNC, int ND>
+__device__ __forceinline__ void dm_eval1(const PairCoef<float> &k, float sv, float &f0,
+                                         float &t) {
+  float np = k.nar2[ND].x;
+#pragma unroll
+  for (int n = ND - 1; n >= 0; n--) np = fmaf(np, sv, k.nar2[n].x);
+  float d = k.br2[ND - 1].x;
+#pragma unroll
+  for (int n = ND - 2; n >= 0; n--) d = fmaf(d, sv, k.br2[n].x);
+  const float ri = rsqrtf(sv);
+  if (FUNC == 0) {
+    f0 = ri + np;
+    t = fmaf(ri * ri, ri, d);
+  } else {
+    const float e0 = exp2f(k.half_alpha * __log2f(sv));
+    f0 = e0 + np;
+    t = fmaf(e0 * -k.alpha, ri * ri, d);
+  }
+}
+
 template <int FUNC, int ND, bool REFINE>
 __device__ __forceinline__ void packed_block(
     const PairCoef<float> &k, const float4 *sp, const float4 *slo, int s0, float2 tx2,
@@ -421,27 +472,8 @@ __device__ __forceinline__ void packed_block(
   }
 #pragma unroll
   for (int u = 0; u < U; u++) {
-    const float2 sv = rr[u];  // scaled coordinates: r^2 = s
-    float2 np = k.nar2[ND];  // -Rdir^(-alpha) f_LR polynomial
-#pragma unroll
-    for (int n = ND - 1; n >= 0; n--) np = __ffma2_rn(np, sv, k.nar2[n]);
-    float2 d = k.br2[ND - 1];  // Rdir^(2-alpha) (1/r) d f_LR / dr polynomial
-#pragma unroll
-    for (int n = ND - 2; n >= 0; n--) d = __ffma2_rn(d, sv, k.br2[n]);
     float2 f0, t;  // t = -f1
-    if (FUNC == 0) {
-      const float2 ri = make_float2(rsqrtf(sv.x), rsqrtf(sv.y));
-      f0 = __fadd2_rn(ri, np);                    // Rdir (1/r - f_LR)
-      t = __ffma2_rn(__fmul2_rn(ri, ri), ri, d);  // -Rdir^3 f1
-    } else {
-      // s^(alpha/2) = 2^((alpha/2) log2 s) on the special-function unit;
-      // 1/s = rsqrt(s)^2
-      const float2 e0 = make_float2(exp2f(k.half_alpha * __log2f(sv.x)),
-                                    exp2f(k.half_alpha * __log2f(sv.y)));
-      const float2 ri = make_float2(rsqrtf(sv.x), rsqrtf(sv.y));
-      f0 = __fadd2_rn(e0, np);
-      t = __ffma2_rn(__fmul2_rn(e0, make_float2(-k.alpha, -k.alpha)), __fmul2_rn(ri, ri), d);
-    }
+    dm_eval2<FUNC, ND>(k, rr[u], f0, t);
     const float2 gq = __fmul2_rn(t, qm[u]);
     P0 = __ffma2_rn(f0, qm[u], P0);
     N1 = __ffma2_rn(gq, x[u], N1);
@@ -570,6 +602,227 @@ __device__ __forceinline__ void direct_group_packed(
   }
   if (active) {
     const long o = perm[ti];
+    const double vs = k.vscale, gs = k.gscale;
+    // V -= f_LR(0) q (src/Interface.cpp:2061-2062)
+    reinterpret_cast<double4 *>(V)[o] =
+        make_double4(vs * acc[0] - fself_r * qcaller[o], gs * acc[1], gs * acc[2], gs * acc[3]);
+  }
+}
+
+// One block of kPackedBlock steps of the Newton's-third-law sweep (below):
+// lane l holds the source pair (a, b) of a 64-source chunk in registers and
+// meets target (l + k) mod 32 of the group at step k, read from the group's
+// target tile in shared memory.  Every pair is evaluated once and gives both
+// sides: the target-side sums (aV, aX, aY, aZ) travel with their target,
+// one lane down per step (__shfl_sync from lane + 1), and the source-side
+// sums (SV, SX, SY, SZ, packed for a and b) stay in the lane.  Source
+// coordinates are held negated (sx2 = -x_s) as in the staged layout of the
+// one-sided body; misses get r^2 = 1 (Rdir^2) and charge 0 on both sides.
+template <int FUNC, int ND, bool REFINE>
+__device__ __forceinline__ void sym_block(
+    const PairCoef<float> &k, const float4 *tsm, const float4 *tlo, int lane, int k0,
+    float2 sx2, float2 sy2, float2 sz2, float2 q2, float2 lx2, float2 ly2, float2 lz2,
+    float refine2, float &aV, float &aX, float &aY, float &aZ, float2 &SV, float2 &SX,
+    float2 &SY, float2 &SZ) {
+  constexpr int U = kPackedBlock;
+  const unsigned FULL = 0xffffffffu;
+  const unsigned rb = __float_as_uint(1.f);
+  float2 x[U], y[U], z[U], rr[U], qm[U], qt[U];
+  int tt[U];
+  float rmin = 3.0e38f;
+  bool any = false;
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    tt[u] = (lane + k0 + u) & 31;
+    const float4 T = tsm[tt[u]];
+    x[u] = __fadd2_rn(make_float2(T.x, T.x), sx2);
+    y[u] = __fadd2_rn(make_float2(T.y, T.y), sy2);
+    z[u] = __fadd2_rn(make_float2(T.z, T.z), sz2);
+    const float2 r2 = __ffma2_rn(x[u], x[u], __ffma2_rn(y[u], y[u], __fmul2_rn(z[u], z[u])));
+    const bool h0 = __float_as_uint(r2.x) - 1u < rb, h1 = __float_as_uint(r2.y) - 1u < rb;
+    rr[u] = make_float2(h0 ? r2.x : 1.f, h1 ? r2.y : 1.f);
+    qm[u] = make_float2(h0 ? q2.x : 0.f, h1 ? q2.y : 0.f);
+    qt[u] = make_float2(h0 ? T.w : 0.f, h1 ? T.w : 0.f);
+    if (REFINE) rmin = fminf(rmin, fminf(rr[u].x, rr[u].y));
+    any |= h0 | h1;
+  }
+  if (!__any_sync(FULL, any)) {  // no pair of the block inside the cutoff
+    const int src = (lane + U) & 31;
+    aV = __shfl_sync(FULL, aV, src);
+    aX = __shfl_sync(FULL, aX, src);
+    aY = __shfl_sync(FULL, aY, src);
+    aZ = __shfl_sync(FULL, aZ, src);
+    return;
+  }
+  if (REFINE && rmin < refine2) {  // close pair: exact difference from head + residual
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (fminf(rr[u].x, rr[u].y) < refine2) {
+        const float4 L = tlo[tt[u]];
+        x[u] = __fadd2_rn(x[u], __fadd2_rn(make_float2(L.x, L.x), lx2));
+        y[u] = __fadd2_rn(y[u], __fadd2_rn(make_float2(L.y, L.y), ly2));
+        z[u] = __fadd2_rn(z[u], __fadd2_rn(make_float2(L.z, L.z), lz2));
+        const float2 rn = __ffma2_rn(x[u], x[u], __ffma2_rn(y[u], y[u], __fmul2_rn(z[u], z[u])));
+        // the hit decision stays that of the unrefined distance
+        rr[u].x = rr[u].x < 1.f ? rn.x : rr[u].x;
+        rr[u].y = rr[u].y < 1.f ? rn.y : rr[u].y;
+      }
+    }
+  }
+  const int src = (lane + 1) & 31;
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    float2 f0, t;  // t = -f1
+    dm_eval2<FUNC, ND>(k, rr[u], f0, t);
+    const float2 gq = __fmul2_rn(t, qm[u]), gs = __fmul2_rn(t, qt[u]);
+    aV = fmaf(f0.x, qm[u].x, fmaf(f0.y, qm[u].y, aV));
+    aX = fmaf(gq.x, x[u].x, fmaf(gq.y, x[u].y, aX));
+    aY = fmaf(gq.x, y[u].x, fmaf(gq.y, y[u].y, aY));
+    aZ = fmaf(gq.x, z[u].x, fmaf(gq.y, z[u].y, aZ));
+    SV = __ffma2_rn(f0, qt[u], SV);
+    SX = __ffma2_rn(gs, x[u], SX);
+    SY = __ffma2_rn(gs, y[u], SY);
+    SZ = __ffma2_rn(gs, z[u], SZ);
+    aV = __shfl_sync(FULL, aV, src);
+    aX = __shfl_sync(FULL, aX, src);
+    aY = __shfl_sync(FULL, aY, src);
+    aZ = __shfl_sync(FULL, aZ, src);
+  }
+}
+
+// Real derivative-match kernels (1/r, r^alpha) of the FP32 direct sum with
+// every unordered pair evaluated once (Newton's third law, as the
+// reference's own cell-pair loops do: src/PotentialLaplace.cpp:145-197,
+// :3447-3610).  The group walks its half-shell source segments: sources
+// whose point lies in a later coarse column, or later in the group's own
+// column, than the group's targets (build_groups); the pairs inside the
+// group are the first phase, from both sides with target-side sums only.
+// Target-side sums accumulate per chunk in FP32 and across chunks in FP64,
+// as in the one-sided body; the source-side sums of a chunk are added to
+// vsrc (source order, FP32, scaled frame) with one vector atomic per source
+// and folded into V by merge_source_kernel.
+template <int FUNC, int ND>
+__device__ __forceinline__ void direct_group_sym(
+    const PairCoef<float> &k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller, const int4 G,
+    const double4 c, const int2 *__restrict__ segs, const uint32_t *__restrict__ perm,
+    float refine2, double fself_r, double *__restrict__ V, float4 *__restrict__ vsrc,
+    float4 *tsm, float4 *tlo, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  // idle lanes sit far outside the cutoff with charge 0
+  float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f, tq = 0.f;
+  const double ir = k.invR;  // coordinates in units of Rdir
+  long o = 0;
+  if (active) {
+    const double4 p = gpos[ti];
+    o = perm[ti];
+    const double dx = (p.x - c.x) * ir, dy = (p.y - c.y) * ir, dz = (p.z - c.z) * ir;
+    tx = (float)dx, ty = (float)dy, tz = (float)dz;
+    tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
+    tq = (float)qcaller[o];
+  }
+  tsm[lane] = make_float4(tx, ty, tz, tq);
+  tlo[lane] = make_float4(tlx, tly, tlz, 0.f);
+  __syncwarp();
+  refine2 = (float)((double)refine2 * ir * ir);
+  const unsigned rb = __float_as_uint(1.f);
+  double acc[4] = {0, 0, 0, 0};
+
+  // pairs inside the group, from both sides; the differences are always
+  // refined (head difference + residual difference)
+  {
+    float aV = 0.f, aX = 0.f, aY = 0.f, aZ = 0.f;
+    for (int s = 0; s < G.y; s++) {
+      const float4 S = tsm[s], L = tlo[s];
+      const float x = (tx - S.x) + (tlx - L.x), y = (ty - S.y) + (tly - L.y),
+                  z = (tz - S.z) + (tlz - L.z);
+      const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+      const bool hit = __float_as_uint(r2) - 1u < rb;  // 0 < r^2 <= 1, not the target itself
+      float f0, t;
+      dm_eval1<FUNC, ND>(k, hit ? r2 : 1.f, f0, t);
+      const float q = hit ? S.w : 0.f, g = t * q;
+      aV = fmaf(f0, q, aV);
+      aX = fmaf(g, x, aX);
+      aY = fmaf(g, y, aY);
+      aZ = fmaf(g, z, aZ);
+    }
+    acc[0] += (double)aV;
+    acc[1] -= (double)aX;
+    acc[2] -= (double)aY;
+    acc[3] -= (double)aZ;
+  }
+
+  // half-shell segments in chunks of 64 sources: lane l holds positions l
+  // and l + 32 of the chunk (register prefetch of the next chunk)
+  const double rfs = sqrt((double)refine2) + c.w * ir;
+  const double near2 = rfs * rfs;
+  SrcCursor ca{G.z, lane};
+  ca.normalize(segs, G.w);
+  SrcCursor cb{ca.seg, ca.off + 32};
+  cb.normalize(segs, G.w);
+  bool va = ca.seg < G.w, vb = cb.seg < G.w;
+  long ja = -1, jb = -1;
+  double4 pa = make_double4(0, 0, 0, 0), pb = pa;
+  float qa = 0.f, qb = 0.f;
+  if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], qa = qs[ja];
+  if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], qb = qs[jb];
+  while (__any_sync(FULL, va)) {
+    // this chunk's sources, relative to the group centre; empty slots far
+    // away (on the other side from idle targets) with charge 0
+    float hxa = -1e18f, hya = -1e18f, hza = -1e18f, lxa = 0.f, lya = 0.f, lza = 0.f;
+    float hxb = -1e18f, hyb = -1e18f, hzb = -1e18f, lxb = 0.f, lyb = 0.f, lzb = 0.f;
+    bool near = false;
+    const long ka = va ? ja : -1, kb = vb ? jb : -1;
+    float q0 = 0.f, q1 = 0.f;
+    if (va) {
+      const double dx = (pa.x - c.x) * ir, dy = (pa.y - c.y) * ir, dz = (pa.z - c.z) * ir;
+      hxa = (float)dx, hya = (float)dy, hza = (float)dz;
+      lxa = (float)(dx - (double)hxa), lya = (float)(dy - (double)hya), lza = (float)(dz - (double)hza);
+      q0 = qa;
+      near = dx * dx + dy * dy + dz * dz < near2;
+    }
+    if (vb) {
+      const double dx = (pb.x - c.x) * ir, dy = (pb.y - c.y) * ir, dz = (pb.z - c.z) * ir;
+      hxb = (float)dx, hyb = (float)dy, hzb = (float)dz;
+      lxb = (float)(dx - (double)hxb), lyb = (float)(dy - (double)hyb), lzb = (float)(dz - (double)hzb);
+      q1 = qb;
+      near = near || dx * dx + dy * dy + dz * dz < near2;
+    }
+    const float2 sx2 = make_float2(-hxa, -hxb), sy2 = make_float2(-hya, -hyb),
+                 sz2 = make_float2(-hza, -hzb), q2 = make_float2(q0, q1);
+    const float2 lx2 = make_float2(-lxa, -lxb), ly2 = make_float2(-lya, -lyb),
+                 lz2 = make_float2(-lza, -lzb);
+    // prefetch the next chunk
+    ca.off += 64;
+    ca.normalize(segs, G.w);
+    cb.off += 64;
+    cb.normalize(segs, G.w);
+    va = ca.seg < G.w, vb = cb.seg < G.w;
+    if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], qa = qs[ja];
+    if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], qb = qs[jb];
+
+    float aV = 0.f, aX = 0.f, aY = 0.f, aZ = 0.f;
+    float2 SV = make_float2(0.f, 0.f), SX = SV, SY = SV, SZ = SV;
+    if (__any_sync(FULL, near)) {
+      for (int k0 = 0; k0 < 32; k0 += kPackedBlock)
+        sym_block<FUNC, ND, true>(k, tsm, tlo, lane, k0, sx2, sy2, sz2, q2, lx2, ly2, lz2,
+                                  refine2, aV, aX, aY, aZ, SV, SX, SY, SZ);
+    } else {
+      for (int k0 = 0; k0 < 32; k0 += kPackedBlock)
+        sym_block<FUNC, ND, false>(k, tsm, tlo, lane, k0, sx2, sy2, sz2, q2, lx2, ly2, lz2,
+                                   refine2, aV, aX, aY, aZ, SV, SX, SY, SZ);
+    }
+    // after 32 steps every target's sums are back in its own lane
+    acc[0] += (double)aV;
+    acc[1] -= (double)aX;
+    acc[2] -= (double)aY;
+    acc[3] -= (double)aZ;
+    if (ka >= 0) atomicAdd(vsrc + ka, make_float4(SV.x, SX.x, SY.x, SZ.x));
+    if (kb >= 0) atomicAdd(vsrc + kb, make_float4(SV.y, SX.y, SY.y, SZ.y));
+  }
+  if (active) {
     const double vs = k.vscale, gs = k.gscale;
     // V -= f_LR(0) q (src/Interface.cpp:2061-2062)
     reinterpret_cast<double4 *>(V)[o] =

@@ -104,6 +104,78 @@ static void groups_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s
       a.V);
 }
 
+// FP32 real-DM direct sum with every pair evaluated once (direct_group_sym),
+// then the source-side sums folded into V.
+template <int FUNC, int ND>
+__global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) direct_sym_kernel(
+    PairCoef<float> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    float refine2, double fself_r, double *__restrict__ V, float4 *__restrict__ vsrc) {
+  __shared__ float4 tsm[kGroupWarps][32];  // group targets (x, y, z, q), heads
+  __shared__ float4 tlo[kGroupWarps][32];  // residuals of the target coordinates
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform; nothing below synchronises the block
+  direct_group_sym<FUNC, ND>(k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm,
+                             refine2, fself_r, V, vsrc, tsm[wid], tlo[wid], lane);
+}
+
+// V[caller(s)] += scale * vsrc[s], then vsrc[s] = 0 for the next call.
+__global__ void merge_source_kernel(float4 *__restrict__ vsrc, const uint32_t *__restrict__ sperm,
+                                    long n, double vs, double gs, double *__restrict__ V) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 a = vsrc[s];
+  vsrc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+  double4 *o = reinterpret_cast<double4 *>(V) + sperm[s];
+  double4 v = *o;
+  v.x += vs * (double)a.x;
+  v.y += gs * (double)a.y;
+  v.z += gs * (double)a.z;
+  v.w += gs * (double)a.w;
+  *o = v;
+}
+
+template <int FUNC, int ND>
+static void sym_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  const long blocks = (h->n_hgroups + kGroupWarps - 1) / kGroupWarps;
+  if (blocks == 0) return;
+  const PairCoef<float> k = make_pair_coef<float>(h);
+  direct_sym_kernel<FUNC, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
+      k, h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller, h->d_hgroups, h->d_hcen,
+      h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2, a.fself_r, a.V, h->d_vsrc);
+  const long n = (long)h->n;
+  merge_source_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->d_vsrc, h->d_sperm, n,
+                                                                    k.vscale, k.gscale, a.V);
+  h->launches++;
+}
+
+// The pair-once form applies to the FP32 real DM kernels with a tabulated
+// derivative order; everything else walks the full segments.
+bool pairs_once(const npme_handle *h) {
+  if (!h->use_sym || h->user_kernel || !h->fp32 || h->n_hgroups == 0) return false;
+  if (h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) return false;
+  const int f = h->p.funcType, nd = h->p.nDeriv;
+  return (f == NPME_FUNC_LAPLACE || f == NPME_FUNC_RALPHA) && (nd == 3 || nd == 6 || nd == 8);
+}
+
+static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  if (!pairs_once(h)) return false;
+  const int f = h->p.funcType, nd = h->p.nDeriv;
+  if (f == NPME_FUNC_LAPLACE) {
+    if (nd == 3) sym_launch_nd<0, 3>(h, a, s);
+    else if (nd == 6) sym_launch_nd<0, 6>(h, a, s);
+    else sym_launch_nd<0, 8>(h, a, s);
+  } else {
+    if (nd == 3) sym_launch_nd<1, 3>(h, a, s);
+    else if (nd == 6) sym_launch_nd<1, 6>(h, a, s);
+    else sym_launch_nd<1, 8>(h, a, s);
+  }
+  return true;
+}
+
 template <bool CPLX, int FUNC, int SPLIT, int ND>
 __global__ void __launch_bounds__(32 * kGroupWarps) direct_groups64_kernel(
     PairCoef<double> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
@@ -151,7 +223,7 @@ static void groups_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
 void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   if (h->user_kernel) {
     h->uops.direct(h, &a, s);
-  } else {  // both precisions walk warp groups
+  } else if (!sym_launch(h, a, s)) {  // both precisions walk warp groups
     const int f = h->p.funcType, sp = h->p.EwaldSplit;
     if (f == NPME_FUNC_HELMHOLTZ) groups_launch<true, 2, 0>(h, a, s);
     else if (sp == NPME_SPLIT_LAPLACE_ORIG) groups_launch<false, 0, 1>(h, a, s);

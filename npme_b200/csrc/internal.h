@@ -126,6 +126,16 @@ struct npme_handle {
   int4 *d_groups = nullptr;      // (first point, count, first segment, end segment)
   double4 *d_gcen = nullptr;     // group frame origin (bbox centre)
   int2 *d_segs = nullptr;        // (first point, count)
+  // FP32 real-DM direct sum with every pair evaluated once: the same groups
+  // with their half-shell segments (sources in later coarse columns, or later
+  // in the group's own column), ordered by their own work
+  bool use_sym = true;
+  long n_hgroups = 0, n_hsegs = 0;
+  double hcand_per_point = 0;    // half-shell candidates per target point
+  int4 *d_hgroups = nullptr;
+  double4 *d_hcen = nullptr;
+  int2 *d_hsegs = nullptr;
+  float4 *d_vsrc = nullptr;      // source-side sums (source order, scaled frame), kept zero
 
   npme::Timing timing;
   bool timing_pending = false;
@@ -164,6 +174,9 @@ struct DirectArgs {
   double fself_r, fself_i;
   double *V;
 };
+// true when the direct sum takes the pair-once form (FP32 real DM kernels
+// with the half-shell lists built)
+bool pairs_once(const npme_handle *h);
 void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
 void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s);
 // caller-order charges (double) -> direct-sum order in the bulk precision

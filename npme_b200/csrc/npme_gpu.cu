@@ -8,6 +8,7 @@
 #include <atomic>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -166,6 +167,7 @@ void release(npme_handle *h) {
   if (!h->caps.empty()) cudaStreamSynchronize(h->stream);
   h->caps.clear();
   h->n_groups = h->n_segs = 0;
+  h->n_hgroups = h->n_hsegs = 0;
   h->dev_bytes = 0;
   h->ready = false;
 }
@@ -224,19 +226,12 @@ int setup_threads(size_t n) {
   return std::max(1, std::min(NPME_SETUP_THREADS_MAX, hw / std::max(1, g_active_setups.load())));
 }
 
-// Sorts the points by xy column (nc[0] x nc[1] columns of edge `edge` from
-// `mn`), then by (z, index) inside each column.  Fills the permutation, the
-// column starts and the sorted z.
-void column_sort(const double *coord, size_t n, const double *mn, const int *nc,
-                 const double *edge, std::vector<uint32_t> &order, std::vector<long> &cstart,
+// Sorts the points by xy column (`col`, ncol columns), then by (z, index)
+// inside each column.  Fills the permutation, the column starts and the
+// sorted z.
+void column_sort(const double *coord, size_t n, long ncol, const std::vector<int> &col,
+                 std::vector<uint32_t> &order, std::vector<long> &cstart,
                  std::vector<double> &zs) {
-  const long ncol = (long)nc[0] * nc[1];
-  std::vector<int> col(n);
-  for (size_t i = 0; i < n; i++) {
-    int c0 = std::min(nc[0] - 1, std::max(0, (int)((coord[3 * i] - mn[0]) / edge[0])));
-    int c1 = std::min(nc[1] - 1, std::max(0, (int)((coord[3 * i + 1] - mn[1]) / edge[1])));
-    col[i] = c0 * nc[1] + c1;
-  }
   // counting sort by column (stable), then each column by (z, index)
   cstart.assign(ncol + 1, 0);
   for (size_t i = 0; i < n; i++) cstart[col[i] + 1]++;
@@ -299,20 +294,44 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   for (int d = 0; d < 3; d++) vol *= std::max(mx[d] - mn[d], 0.25 * R);
   double e = std::cbrt(32.0 * vol / (double)n);
   e = std::max(e, 1e-3 * R);
+  constexpr int S = NPME_SOURCE_SPLIT;
   int nc[2], ns[2];
   double edge[2], sedge[2];
   for (int d = 0; d < 2; d++) {
     const double ext = mx[d] - mn[d];
     nc[d] = std::max(1, std::min((int)std::ceil(ext / e), 1 << 14));
     edge[d] = std::max(ext / nc[d], 1e-12);
-    ns[d] = std::min(nc[d] * NPME_SOURCE_SPLIT, 1 << 15);
-    sedge[d] = std::max(ext / ns[d], 1e-12);
+    ns[d] = nc[d] * S;
+    sedge[d] = edge[d] / S;
+  }
+  // every fine column lies inside one coarse column: a point's fine column
+  // is its coarse column's sub-column
+  std::vector<int> ccol(n), scol(n);
+  for (size_t i = 0; i < n; i++) {
+    int cs[2], ss[2];
+    for (int d = 0; d < 2; d++) {
+      const double u = coord[3 * i + d] - mn[d];
+      cs[d] = std::min(nc[d] - 1, std::max(0, (int)(u / edge[d])));
+      ss[d] = cs[d] * S + std::min(S - 1, std::max(0, (int)((u - cs[d] * edge[d]) / sedge[d])));
+    }
+    ccol[i] = cs[0] * nc[1] + cs[1];
+    scol[i] = ss[0] * ns[1] + ss[1];
   }
   std::vector<long> cstart, sstart;
   std::vector<double> zt, zs;
-  column_sort(coord, n, mn, nc, edge, order, cstart, zt);
-  column_sort(coord, n, mn, ns, sedge, sorder, sstart, zs);
   const long ncol = (long)nc[0] * nc[1];
+  column_sort(coord, n, ncol, ccol, order, cstart, zt);
+  column_sort(coord, n, (long)ns[0] * ns[1], scol, sorder, sstart, zs);
+  // position of each source in the coarse (group) order: increasing inside
+  // a fine column, since both orders sort a column by (z, index)
+  const bool half = h->fp32;
+  std::vector<uint32_t> fcpos;
+  if (half) {
+    std::vector<uint32_t> cpos(n);
+    for (size_t k = 0; k < n; k++) cpos[order[k]] = (uint32_t)k;
+    fcpos.resize(n);
+    for (size_t k = 0; k < n; k++) fcpos[k] = cpos[sorder[k]];
+  }
 
   // Per coarse column: the fine columns that can hold a source within R of
   // the column's points, each with a pair of cursors into its z-sorted
@@ -323,13 +342,13 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   // are independent: large systems split them over host threads, each
   // filling its own lists, concatenated in column order afterwards.
   struct Part {
-    std::vector<int4> groups;
+    std::vector<int4> groups, hgroups;
     std::vector<double4> cen;
-    std::vector<int2> segs;
-    double cand = 0;
+    std::vector<int2> segs, hsegs;
+    double cand = 0, hcand = 0;
   };
   auto build_part = [&](long c_begin, long c_end, Part &out) {
-    std::vector<long> nb_col, pa, pb;
+    std::vector<long> nb_col, nb_cc, pa, pb;
     std::vector<int> nb_s0, nb_s1;
     std::vector<double> dxv, dyv;
     for (long c = c_begin; c < c_end; c++) {
@@ -346,12 +365,13 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
         lo[d] = (int)std::max(0.0, std::floor((cl[d] - R - mn[d]) / sedge[d]));
         hi[d] = (int)std::min((double)(ns[d] - 1), std::floor((ch[d] + R - mn[d]) / sedge[d]));
       }
-      nb_col.clear(), nb_s0.clear(), nb_s1.clear();
+      nb_col.clear(), nb_cc.clear(), nb_s0.clear(), nb_s1.clear();
       for (int s0 = lo[0]; s0 <= hi[0]; s0++)
         for (int s1 = lo[1]; s1 <= hi[1]; s1++) {
           const long sc = (long)s0 * ns[1] + s1;
           if (sstart[sc] == sstart[sc + 1]) continue;
           nb_col.push_back(sc), nb_s0.push_back(s0 - lo[0]), nb_s1.push_back(s1 - lo[1]);
+          nb_cc.push_back((long)(s0 / S) * nc[1] + s1 / S);
         }
       pa.assign(nb_col.size(), 0), pb.assign(nb_col.size(), 0);
       for (size_t t = 0; t < nb_col.size(); t++) pa[t] = pb[t] = sstart[nb_col[t]];
@@ -376,7 +396,7 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
           const double d = std::max(0.0, std::max(l1 - bh[1], bl[1] - h1));
           dyv[u] = d * d;
         }
-        const int seg0 = (int)out.segs.size();
+        const int seg0 = (int)out.segs.size(), hseg0 = (int)out.hsegs.size();
         for (size_t t = 0; t < nb_col.size(); t++) {
           const double d2 = dxv[nb_s0[t]] + dyv[nb_s1[t]];
           if (d2 > R2) continue;
@@ -393,8 +413,23 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
             out.segs.push_back(make_int2((int)a, (int)(b - a)));
             out.cand += (double)(b - a) * (double)(p1 - p0);
           }
+          // half shell: later coarse columns whole, the group's own column
+          // from the first point after the group
+          if (half && b > a && nb_cc[t] >= c) {
+            long a2 = a;
+            if (nb_cc[t] == c)
+              a2 = std::lower_bound(fcpos.begin() + a, fcpos.begin() + b, (uint32_t)p1) -
+                   fcpos.begin();
+            if (b > a2) {
+              out.hsegs.push_back(make_int2((int)a2, (int)(b - a2)));
+              out.hcand += (double)(b - a2) * (double)(p1 - p0);
+            }
+          }
         }
         out.groups.push_back(make_int4((int)p0, (int)(p1 - p0), seg0, (int)out.segs.size()));
+        if (half)
+          out.hgroups.push_back(
+              make_int4((int)p0, (int)(p1 - p0), hseg0, (int)out.hsegs.size()));
         // centre and half-diagonal of the bounding box
         out.cen.push_back(make_double4(
             0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]),
@@ -414,34 +449,41 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
                         std::ref(parts[t]));
     for (auto &th : pool) th.join();
   }
-  std::vector<int4> groups;
+  std::vector<int4> groups, hgroups;
   std::vector<double4> cen;
-  std::vector<int2> segs;
-  double cand = 0;
+  std::vector<int2> segs, hsegs;
+  double cand = 0, hcand = 0;
   for (Part &pt : parts) {
-    const int base = (int)segs.size();
+    const int base = (int)segs.size(), hbase = (int)hsegs.size();
     for (int4 g : pt.groups) groups.push_back(make_int4(g.x, g.y, g.z + base, g.w + base));
+    for (int4 g : pt.hgroups) hgroups.push_back(make_int4(g.x, g.y, g.z + hbase, g.w + hbase));
     cen.insert(cen.end(), pt.cen.begin(), pt.cen.end());
     segs.insert(segs.end(), pt.segs.begin(), pt.segs.end());
-    cand += pt.cand;
+    hsegs.insert(hsegs.end(), pt.hsegs.begin(), pt.hsegs.end());
+    cand += pt.cand, hcand += pt.hcand;
   }
-  // heaviest groups first, so the last wave of the launch holds the light ones
-  {
-    std::vector<long> work(groups.size());
-    for (size_t g = 0; g < groups.size(); g++) {
+  // heaviest groups first, so the last wave of the launch holds the light
+  // ones (each list by its own work)
+  auto by_work = [](std::vector<int4> &gl, const std::vector<int2> &sl,
+                    const std::vector<double4> &cin, std::vector<double4> &cout) {
+    std::vector<long> work(gl.size());
+    for (size_t g = 0; g < gl.size(); g++) {
       long c = 0;
-      for (int t = groups[g].z; t < groups[g].w; t++) c += segs[t].y;
+      for (int t = gl[g].z; t < gl[g].w; t++) c += sl[t].y;
       work[g] = c;
     }
-    std::vector<uint32_t> go(groups.size());
+    std::vector<uint32_t> go(gl.size());
     for (size_t g = 0; g < go.size(); g++) go[g] = (uint32_t)g;
     std::stable_sort(go.begin(), go.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
-    std::vector<int4> g2(groups.size());
-    std::vector<double4> c2(cen.size());
-    for (size_t g = 0; g < go.size(); g++) g2[g] = groups[go[g]], c2[g] = cen[go[g]];
-    groups.swap(g2);
-    cen.swap(c2);
-  }
+    std::vector<int4> g2(gl.size());
+    cout.resize(gl.size());
+    for (size_t g = 0; g < go.size(); g++) g2[g] = gl[go[g]], cout[g] = cin[go[g]];
+    gl.swap(g2);
+  };
+  std::vector<double4> gcen, hcen;
+  by_work(groups, segs, cen, gcen);
+  if (half) by_work(hgroups, hsegs, cen, hcen);
+  cen.swap(gcen);
   std::vector<double4> gpos(n), spos(n);
   for (size_t k = 0; k < n; k++) {
     const double *x = coord + 3 * (size_t)order[k];
@@ -452,6 +494,9 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   h->n_groups = (long)groups.size();
   h->n_segs = (long)segs.size();
   h->cand_per_point = cand / (double)n;
+  h->n_hgroups = (long)hgroups.size();
+  h->n_hsegs = (long)hsegs.size();
+  h->hcand_per_point = hcand / (double)n;
   // heads of offsets up to ~the group half-diagonal carry ~6e-8 e absolute
   // error; below r = e/4 the relative error would exceed ~1e-6, so refine
   h->refine2 = (0.25 * e) * (0.25 * e);
@@ -473,6 +518,20 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   if (!segs.empty())
     CK(cudaMemcpyAsync(h->d_segs, segs.data(), sizeof(int2) * segs.size(), cudaMemcpyHostToDevice,
                        h->stream));
+  if (half) {
+    if ((rc = dalloc(h, &h->d_hgroups, sizeof(int4) * hgroups.size()))) return rc;
+    if ((rc = dalloc(h, &h->d_hcen, sizeof(double4) * hcen.size()))) return rc;
+    if ((rc = dalloc(h, &h->d_hsegs, sizeof(int2) * std::max<size_t>(1, hsegs.size())))) return rc;
+    if ((rc = dalloc(h, &h->d_vsrc, sizeof(float4) * n))) return rc;
+    CK(cudaMemcpyAsync(h->d_hgroups, hgroups.data(), sizeof(int4) * hgroups.size(),
+                       cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_hcen, hcen.data(), sizeof(double4) * hcen.size(),
+                       cudaMemcpyHostToDevice, h->stream));
+    if (!hsegs.empty())
+      CK(cudaMemcpyAsync(h->d_hsegs, hsegs.data(), sizeof(int2) * hsegs.size(),
+                         cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * n, h->stream));
+  }
   return NPME_OK;
 }
 
@@ -861,6 +920,11 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
   h->cells.reach = p.nNeigh;
   // both precisions walk warp groups; the cell list above serves the pair count
   h->use_groups = true;
+  // FP32 real DM kernels evaluate every pair once unless NPME_PAIRS_ONCE=0
+  {
+    const char *e = std::getenv("NPME_PAIRS_ONCE");
+    h->use_sym = !(e && e[0] == '0');
+  }
   int rc = h->fp32 ? upload_points<float>(h, coord) : upload_points<double>(h, coord);
   if (rc) {
     release(h);
@@ -1091,6 +1155,8 @@ int npme_gpu_get_info(const npme_handle *hc, npme_info *info) {
   info->launches = h->launches;
   info->nGroups = h->n_groups;
   info->candidatesPerPoint = h->cand_per_point;
+  info->pairsOnce = npme::pairs_once(h) ? 1 : 0;
+  info->pairsOnceCandidatesPerPoint = h->hcand_per_point;
   return NPME_OK;
 }
 

@@ -220,6 +220,51 @@ def test_direct_sum_entry_point_matches_oracle(name, prec):
     assert rel(V[:, 1:], Vo[:, 1:]) < tol[1]
 
 
+def _direct_fp32(w, c, q, torch):
+    with npme_b200.Solver(api.params_from_workload(w, precision="fp32")) as s:
+        s.setup(c)
+        dq = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        dV = torch.zeros((len(q), 4), dtype=torch.float64, device="cuda")
+        st = torch.cuda.Stream()
+        s.direct_sum_device(dV.data_ptr(), dq.data_ptr(), st.cuda_stream)
+        st.synchronize()
+        return dV.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["laplace_dm_4k", "ralpha_dm_small", "laplace_dm_order8"])
+def test_pairs_once_matches_both_sides(name, monkeypatch):
+    # FP32 real DM kernels evaluate every pair once, for both of its points
+    # (NPME_PAIRS_ONCE=0 selects the one-sided walk); the two agree to FP32
+    # rounding and both match the oracle
+    torch = pytest.importorskip("torch")
+    w = SMALL[name]
+    c, q = w.generate()
+    Vo = ob.direct(ob.params_from_workload(w), c, q)
+    got = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("NPME_PAIRS_ONCE", mode)
+        got[mode] = _direct_fp32(w, c, q, torch)
+    assert rel(got["1"], got["0"]) < 1e-6
+    for V in got.values():
+        assert rel(V[:, 0], Vo[:, 0]) < FP32_V_TOL
+        assert rel(V[:, 1:], Vo[:, 1:]) < FP32_G_TOL
+
+
+def test_pairs_once_on_a_lattice():
+    # a cubic lattice: many points share z (ties in the column order that
+    # splits the half shell) and sit on column boundaries
+    torch = pytest.importorskip("torch")
+    w = SMALL["laplace_dm_4k"]
+    g = np.arange(16) * 1.25
+    c = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[: w.n].copy()
+    q = np.random.default_rng(5).uniform(-1.0, 1.0, w.n)
+    q -= q.mean()
+    Vo = ob.direct(ob.params_from_workload(w), c, q)
+    V = _direct_fp32(w, c, q, torch)
+    assert rel(V[:, 0], Vo[:, 0]) < FP32_V_TOL
+    assert rel(V[:, 1:], Vo[:, 1:]) < FP32_G_TOL
+
+
 # ---------------------------------------------------------------------------
 # full benchmark sizes: size-independent properties
 

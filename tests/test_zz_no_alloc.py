@@ -18,8 +18,10 @@ from tests.golden.make_golden import SMALL
 pytestmark = pytest.mark.gpu
 
 # same bound as the FP64 parity tests; the two entry points run the same
-# kernels on the same gathered charges, so they agree far below it
-TOL = 1e-12
+# kernels on the same gathered charges, so they agree far below it.  The FP32
+# real DM kernels add the source side of each pair with float atomics, whose
+# order (and so the last bits of the sums) varies from call to call.
+TOL = {"fp64": 1e-12, "fp32": 1e-7}
 
 
 def _run(s, fn, dq, n, cplx, torch):
@@ -48,8 +50,8 @@ def test_noalloc_matches_direct_sum_twice(name, prec):
         other = _run(s, s.direct_sum_device_noalloc, dq2, w.n, cplx, torch)
         second = _run(s, s.direct_sum_device_noalloc, dq, w.n, cplx, torch)
     assert np.all(np.isfinite(first)) and np.all(np.isfinite(second))
-    assert rel(first, ref) < TOL
-    assert rel(second, ref) < TOL
+    assert rel(first, ref) < TOL[prec]
+    assert rel(second, ref) < TOL[prec]
     assert rel(other, -2.0 * ref) < 1e-6
 
 
