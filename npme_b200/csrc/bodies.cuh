@@ -609,7 +609,7 @@ __device__ __forceinline__ void direct_group_packed(
   }
 }
 
-// One block of kPackedBlock steps of the Newton's-third-law sweep (below):
+// One block of steps of the Newton's-third-law sweep (below):
 // lane l holds the source pair (a, b) of a 64-source chunk in registers and
 // meets target (l + k) mod 32 of the group at step k, read from the group's
 // target tile in shared memory.  Every pair is evaluated once and gives both
@@ -618,13 +618,22 @@ __device__ __forceinline__ void direct_group_packed(
 // sums (SV, SX, SY, SZ, packed for a and b) stay in the lane.  Source
 // coordinates are held negated (sx2 = -x_s) as in the staged layout of the
 // one-sided body; misses get r^2 = 1 (Rdir^2) and charge 0 on both sides.
+#ifndef NPME_SYM_BLOCK
+#define NPME_SYM_BLOCK 0
+#endif
+// steps per block of the pair-once sweep (measured: 2 for 1/r, 4 for r^alpha)
+template <int FUNC>
+constexpr int sym_block_steps() {
+  return NPME_SYM_BLOCK > 0 ? NPME_SYM_BLOCK : (FUNC == 1 ? 4 : 2);
+}
+
 template <int FUNC, int ND, bool REFINE>
 __device__ __forceinline__ void sym_block(
     const PairCoef<float> &k, const float4 *tsm, const float4 *tlo, int lane, int k0,
     float2 sx2, float2 sy2, float2 sz2, float2 q2, float2 lx2, float2 ly2, float2 lz2,
     float refine2, float &aV, float &aX, float &aY, float &aZ, float2 &SV, float2 &SX,
     float2 &SY, float2 &SZ) {
-  constexpr int U = kPackedBlock;
+  constexpr int U = sym_block_steps<FUNC>();
   const unsigned FULL = 0xffffffffu;
   const unsigned rb = __float_as_uint(1.f);
   float2 x[U], y[U], z[U], rr[U], qm[U], qt[U];
@@ -806,11 +815,11 @@ __device__ __forceinline__ void direct_group_sym(
     float aV = 0.f, aX = 0.f, aY = 0.f, aZ = 0.f;
     float2 SV = make_float2(0.f, 0.f), SX = SV, SY = SV, SZ = SV;
     if (__any_sync(FULL, near)) {
-      for (int k0 = 0; k0 < 32; k0 += kPackedBlock)
+      for (int k0 = 0; k0 < 32; k0 += sym_block_steps<FUNC>())
         sym_block<FUNC, ND, true>(k, tsm, tlo, lane, k0, sx2, sy2, sz2, q2, lx2, ly2, lz2,
                                   refine2, aV, aX, aY, aZ, SV, SX, SY, SZ);
     } else {
-      for (int k0 = 0; k0 < 32; k0 += kPackedBlock)
+      for (int k0 = 0; k0 < 32; k0 += sym_block_steps<FUNC>())
         sym_block<FUNC, ND, false>(k, tsm, tlo, lane, k0, sx2, sy2, sz2, q2, lx2, ly2, lz2,
                                    refine2, aV, aX, aY, aZ, SV, SX, SY, SZ);
     }
