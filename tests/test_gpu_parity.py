@@ -228,6 +228,7 @@ def _direct_fp32(w, c, q, torch):
         st = torch.cuda.Stream()
         s.direct_sum_device(dV.data_ptr(), dq.data_ptr(), st.cuda_stream)
         st.synchronize()
+        _direct_fp32.pairs_once = s.info()["pairsOnce"]
         return dV.cpu().numpy()
 
 
@@ -244,6 +245,7 @@ def test_pairs_once_matches_both_sides(name, monkeypatch):
     for mode in ("0", "1"):
         monkeypatch.setenv("NPME_PAIRS_ONCE", mode)
         got[mode] = _direct_fp32(w, c, q, torch)
+        assert _direct_fp32.pairs_once == (mode == "1")
     assert rel(got["1"], got["0"]) < 1e-6
     for V in got.values():
         assert rel(V[:, 0], Vo[:, 0]) < FP32_V_TOL
