@@ -1136,6 +1136,137 @@ __device__ __forceinline__ void direct_group_fp64(
   }
 }
 
+// FP64 direct sum of one warp group with every unordered pair evaluated once
+// (the FP64 counterpart of direct_group_sym, for the real kernels): the
+// group's targets (x, y, z, q) sit in shared memory, each lane holds two
+// sources of a 64-source chunk of the half-shell segments, target (l + k)
+// mod 32 meets lane l at step k and its sums rotate one lane down per step;
+// the source-side sums of a chunk go to vsrc ([n][4] doubles, source order)
+// with one FP64 atomic per component.  Pairs inside the group are a first,
+// one-sided pass.  Same pair arithmetic as direct_group_fp64.
+template <int FUNC, int SPLIT, int ND, class PK = BuiltinPair>
+__device__ __forceinline__ void direct_group_sym64(
+    const PairCoef<double> &k, const double4 *__restrict__ gpos,
+    const double4 *__restrict__ spos, const double *__restrict__ qs,
+    const double *__restrict__ qcaller, const int4 G, const double4 c,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, double fself_r,
+    double *__restrict__ V, double *__restrict__ vsrc, double4 *tsm, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  double tx = 1e150, ty = 1e150, tz = 1e150, tq = 0.0;  // idle lanes: far away, no charge
+  long o = 0;
+  if (active) {
+    const double4 p = gpos[ti];
+    o = perm[ti];
+    tx = p.x - c.x, ty = p.y - c.y, tz = p.z - c.z;
+    tq = qcaller[o];
+  }
+  tsm[lane] = make_double4(tx, ty, tz, tq);
+  __syncwarp();
+  const double R2 = k.R2;
+  double acc[4] = {0, 0, 0, 0};
+  // pairs inside the group, target side only (each is met from both ends)
+  for (int s = 0; s < G.y; s++) {
+    const double4 S = tsm[s];
+    const double x = tx - S.x, y = ty - S.y, z = tz - S.z;
+    const double r2 = fma(x, x, fma(y, y, z * z));
+    if (r2 <= R2 && r2 > 0.0) {
+      double f1;
+      const double f0 = pair_sr<double, FUNC, SPLIT, ND, PK>(k, r2, f1);
+      const double gq = f1 * S.w;
+      acc[0] = fma(f0, S.w, acc[0]);
+      acc[1] = fma(gq, x, acc[1]);
+      acc[2] = fma(gq, y, acc[2]);
+      acc[3] = fma(gq, z, acc[3]);
+    }
+  }
+  // half-shell segments in chunks of 64 sources (register prefetch)
+  SrcCursor ca{G.z, lane};
+  ca.normalize(segs, G.w);
+  SrcCursor cb{ca.seg, ca.off + 32};
+  cb.normalize(segs, G.w);
+  bool va = ca.seg < G.w, vb = cb.seg < G.w;
+  long ja = -1, jb = -1;
+  double4 pa = make_double4(0, 0, 0, 0), pb = pa;
+  if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], pa.w = qs[ja];
+  if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], pb.w = qs[jb];
+  while (__any_sync(FULL, va)) {
+    // empty slots far away on the other side from idle targets, no charge
+    double4 A = make_double4(-1e150, -1e150, -1e150, 0.0), B = A;
+    if (va) A = make_double4(pa.x - c.x, pa.y - c.y, pa.z - c.z, pa.w);
+    if (vb) B = make_double4(pb.x - c.x, pb.y - c.y, pb.z - c.z, pb.w);
+    const long ka = va ? ja : -1, kb = vb ? jb : -1;
+    ca.off += 64;
+    ca.normalize(segs, G.w);
+    cb.off += 64;
+    cb.normalize(segs, G.w);
+    va = ca.seg < G.w, vb = cb.seg < G.w;
+    if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], pa.w = qs[ja];
+    if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], pb.w = qs[jb];
+
+    double aV = 0, aX = 0, aY = 0, aZ = 0;           // target side, rotating
+    double sa[4] = {0, 0, 0, 0}, sb[4] = {0, 0, 0, 0};  // source side
+    const int src = (lane + 1) & 31;
+#pragma unroll 2
+    for (int kk = 0; kk < 32; kk++) {
+      const double4 T = tsm[(lane + kk) & 31];
+      {
+        const double x = T.x - A.x, y = T.y - A.y, z = T.z - A.z;
+        const double r2 = fma(x, x, fma(y, y, z * z));
+        if (r2 <= R2 && r2 > 0.0) {
+          double f1;
+          const double f0 = pair_sr<double, FUNC, SPLIT, ND, PK>(k, r2, f1);
+          const double gq = f1 * A.w, gs = f1 * T.w;
+          aV = fma(f0, A.w, aV);
+          aX = fma(gq, x, aX);
+          aY = fma(gq, y, aY);
+          aZ = fma(gq, z, aZ);
+          sa[0] = fma(f0, T.w, sa[0]);
+          sa[1] = fma(-gs, x, sa[1]);
+          sa[2] = fma(-gs, y, sa[2]);
+          sa[3] = fma(-gs, z, sa[3]);
+        }
+      }
+      {
+        const double x = T.x - B.x, y = T.y - B.y, z = T.z - B.z;
+        const double r2 = fma(x, x, fma(y, y, z * z));
+        if (r2 <= R2 && r2 > 0.0) {
+          double f1;
+          const double f0 = pair_sr<double, FUNC, SPLIT, ND, PK>(k, r2, f1);
+          const double gq = f1 * B.w, gs = f1 * T.w;
+          aV = fma(f0, B.w, aV);
+          aX = fma(gq, x, aX);
+          aY = fma(gq, y, aY);
+          aZ = fma(gq, z, aZ);
+          sb[0] = fma(f0, T.w, sb[0]);
+          sb[1] = fma(-gs, x, sb[1]);
+          sb[2] = fma(-gs, y, sb[2]);
+          sb[3] = fma(-gs, z, sb[3]);
+        }
+      }
+      aV = __shfl_sync(FULL, aV, src);
+      aX = __shfl_sync(FULL, aX, src);
+      aY = __shfl_sync(FULL, aY, src);
+      aZ = __shfl_sync(FULL, aZ, src);
+    }
+    acc[0] += aV;
+    acc[1] += aX;
+    acc[2] += aY;
+    acc[3] += aZ;
+    if (ka >= 0)
+#pragma unroll
+      for (int m = 0; m < 4; m++) atomicAdd(vsrc + 4 * ka + m, sa[m]);
+    if (kb >= 0)
+#pragma unroll
+      for (int m = 0; m < 4; m++) atomicAdd(vsrc + 4 * kb + m, sb[m]);
+  }
+  if (active) {
+    acc[0] -= fself_r * qcaller[o];  // src/Interface.cpp:2061-2062
+    reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+  }
+}
+
 constexpr int kDirectBS = 64;  // tile of the cell-list pair count (direct.cu)
 
 }  // namespace npme

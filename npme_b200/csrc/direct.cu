@@ -152,18 +152,81 @@ static void sym_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   h->launches++;
 }
 
-// The pair-once form applies to the FP32 real DM kernels with a tabulated
-// derivative order; everything else walks the full segments.
+// FP64 form for the real built-in kernels (DM and original Ewald).
+template <int FUNC, int SPLIT, int ND>
+__global__ void __launch_bounds__(32 * kGroupWarps) direct_sym64_kernel(
+    PairCoef<double> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const double *__restrict__ qs, const double *__restrict__ qcaller,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    double fself_r, double *__restrict__ V, double *__restrict__ vsrc) {
+  __shared__ double4 tsm[kGroupWarps][32];  // group targets (x, y, z, q)
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  direct_group_sym64<FUNC, SPLIT, ND>(k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm,
+                                      fself_r, V, vsrc, tsm[wid], lane);
+}
+
+// V[caller(s)][m] += vsrc[s][m], then vsrc[s] = 0 for the next call.
+__global__ void merge_source64_kernel(double4 *__restrict__ vsrc,
+                                      const uint32_t *__restrict__ sperm, long n,
+                                      double *__restrict__ V) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const double4 a = vsrc[s];
+  vsrc[s] = make_double4(0, 0, 0, 0);
+  double4 *o = reinterpret_cast<double4 *>(V) + sperm[s];
+  double4 v = *o;
+  v.x += a.x, v.y += a.y, v.z += a.z, v.w += a.w;
+  *o = v;
+}
+
+template <int FUNC, int SPLIT, int ND>
+static void sym64_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  const long blocks = (h->n_hgroups + kGroupWarps - 1) / kGroupWarps;
+  if (blocks == 0) return;
+  direct_sym64_kernel<FUNC, SPLIT, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
+      make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
+      h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, a.fself_r, a.V,
+      h->d_vsrc64);
+  const long n = (long)h->n;
+  merge_source64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      reinterpret_cast<double4 *>(h->d_vsrc64), h->d_sperm, n, a.V);
+  h->launches++;
+}
+
+template <int FUNC, int SPLIT>
+static void sym64_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  switch (SPLIT == 1 ? 0 : h->p.nDeriv) {
+    case 3: sym64_launch_nd<FUNC, SPLIT, 3>(h, a, s); break;
+    case 6: sym64_launch_nd<FUNC, SPLIT, 6>(h, a, s); break;
+    case 8: sym64_launch_nd<FUNC, SPLIT, 8>(h, a, s); break;
+    default: sym64_launch_nd<FUNC, SPLIT, 0>(h, a, s); break;
+  }
+}
+
+// The pair-once form applies to the real built-in kernels: in FP32 the DM
+// kernels with a tabulated derivative order, in FP64 also the original
+// Ewald split and any order; everything else walks the full segments.
 bool pairs_once(const npme_handle *h) {
-  if (!h->use_sym || h->user_kernel || !h->fp32 || h->n_hgroups == 0) return false;
-  if (h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) return false;
+  if (!h->use_sym || h->user_kernel || h->n_hgroups == 0) return false;
   const int f = h->p.funcType, nd = h->p.nDeriv;
-  return (f == NPME_FUNC_LAPLACE || f == NPME_FUNC_RALPHA) && (nd == 3 || nd == 6 || nd == 8);
+  if (f != NPME_FUNC_LAPLACE && f != NPME_FUNC_RALPHA) return false;
+  if (!h->fp32) return true;
+  if (h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) return false;
+  return nd == 3 || nd == 6 || nd == 8;
 }
 
 static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   if (!pairs_once(h)) return false;
   const int f = h->p.funcType, nd = h->p.nDeriv;
+  if (!h->fp32) {
+    if (h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) sym64_launch<0, 1>(h, a, s);
+    else if (f == NPME_FUNC_RALPHA) sym64_launch<1, 0>(h, a, s);
+    else sym64_launch<0, 0>(h, a, s);
+    return true;
+  }
   if (f == NPME_FUNC_LAPLACE) {
     if (nd == 3) sym_launch_nd<0, 3>(h, a, s);
     else if (nd == 6) sym_launch_nd<0, 6>(h, a, s);

@@ -126,7 +126,7 @@ struct npme_handle {
   int4 *d_groups = nullptr;      // (first point, count, first segment, end segment)
   double4 *d_gcen = nullptr;     // group frame origin (bbox centre)
   int2 *d_segs = nullptr;        // (first point, count)
-  // FP32 real-DM direct sum with every pair evaluated once: the same groups
+  // real-kernel direct sum with every pair evaluated once: the same groups
   // with their half-shell segments (sources in later coarse columns, or later
   // in the group's own column), ordered by their own work
   bool use_sym = true;
@@ -135,7 +135,8 @@ struct npme_handle {
   int4 *d_hgroups = nullptr;
   double4 *d_hcen = nullptr;
   int2 *d_hsegs = nullptr;
-  float4 *d_vsrc = nullptr;      // source-side sums (source order, scaled frame), kept zero
+  float4 *d_vsrc = nullptr;      // FP32: source-side sums (source order, scaled frame), kept zero
+  double *d_vsrc64 = nullptr;    // FP64: source-side sums [n][4] (source order), kept zero
 
   npme::Timing timing;
   bool timing_pending = false;

@@ -324,7 +324,7 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
   column_sort(coord, n, (long)ns[0] * ns[1], scol, sorder, sstart, zs);
   // position of each source in the coarse (group) order: increasing inside
   // a fine column, since both orders sort a column by (z, index)
-  const bool half = h->fp32;
+  const bool half = true;
   std::vector<uint32_t> fcpos;
   if (half) {
     std::vector<uint32_t> cpos(n);
@@ -522,7 +522,13 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
     if ((rc = dalloc(h, &h->d_hgroups, sizeof(int4) * hgroups.size()))) return rc;
     if ((rc = dalloc(h, &h->d_hcen, sizeof(double4) * hcen.size()))) return rc;
     if ((rc = dalloc(h, &h->d_hsegs, sizeof(int2) * std::max<size_t>(1, hsegs.size())))) return rc;
-    if ((rc = dalloc(h, &h->d_vsrc, sizeof(float4) * n))) return rc;
+    if (h->fp32) {
+      if ((rc = dalloc(h, &h->d_vsrc, sizeof(float4) * n))) return rc;
+      CK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * n, h->stream));
+    } else {
+      if ((rc = dalloc(h, &h->d_vsrc64, sizeof(double) * 4 * n))) return rc;
+      CK(cudaMemsetAsync(h->d_vsrc64, 0, sizeof(double) * 4 * n, h->stream));
+    }
     CK(cudaMemcpyAsync(h->d_hgroups, hgroups.data(), sizeof(int4) * hgroups.size(),
                        cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_hcen, hcen.data(), sizeof(double4) * hcen.size(),
@@ -530,7 +536,6 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
     if (!hsegs.empty())
       CK(cudaMemcpyAsync(h->d_hsegs, hsegs.data(), sizeof(int2) * hsegs.size(),
                          cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * n, h->stream));
   }
   return NPME_OK;
 }

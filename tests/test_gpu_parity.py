@@ -267,6 +267,32 @@ def test_pairs_once_on_a_lattice():
     assert rel(V[:, 1:], Vo[:, 1:]) < FP32_G_TOL
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_clustered_points(prec):
+    # two dense blobs and a sparse background: columns of very different
+    # height, groups that are thin slabs, segments of very different length
+    torch = pytest.importorskip("torch")
+    w = SMALL["laplace_dm_4k"]
+    g = np.random.default_rng(11)
+    c = np.concatenate([g.normal([6.0, 6.0, 6.0], 0.8, (1800, 3)),
+                        g.normal([14.0, 13.0, 12.0], 1.5, (1600, 3)),
+                        g.uniform(0.0, 20.0, (w.n - 3400, 3))])
+    q = g.uniform(-1.0, 1.0, w.n)
+    q -= q.mean()
+    Vo = ob.direct(ob.params_from_workload(w), c, q)
+    with npme_b200.Solver(api.params_from_workload(w, precision=prec)) as s:
+        s.setup(c)
+        dq = torch.from_numpy(q).cuda()
+        dV = torch.zeros((w.n, 4), dtype=torch.float64, device="cuda")
+        st = torch.cuda.Stream()
+        s.direct_sum_device(dV.data_ptr(), dq.data_ptr(), st.cuda_stream)
+        st.synchronize()
+        V = dV.cpu().numpy()
+    tol = (FP64_TOL, FP64_TOL) if prec == "fp64" else (FP32_V_TOL, FP32_G_TOL)
+    assert rel(V[:, 0], Vo[:, 0]) < tol[0]
+    assert rel(V[:, 1:], Vo[:, 1:]) < tol[1]
+
+
 # ---------------------------------------------------------------------------
 # full benchmark sizes: size-independent properties
 
