@@ -849,6 +849,35 @@ __device__ __forceinline__ float2 sincos_sfu(float x) {
   return make_float2(__cosf(y), __sinf(y));
 }
 
+// Helmholtz DM pair kernel at squared distance rr (FP32, complex as float2):
+// F0 = exp(i k0 r)/r - f_LR (the DM polynomial in s = rr / Rdir^2, held
+// negated in nac2) and F1 = (1/r) dF0/dr, with sin / cos on the
+// special-function unit (src/KernelFunctionHelmholtz.cpp:506-563).
+template <int ND>
+__device__ __forceinline__ void helm_eval(const PairCoef<float> &k, float rr, float2 &F0,
+                                          float2 &F1) {
+  const float2 ik = make_float2(-k.k0i, k.k0r);  // i k0
+  const float ri = rsqrtf(rr), r = rr * ri;
+  const float2 cs = sincos_sfu(k.k0r * r);
+  const float damp = k.k0i != 0.f ? __expf(-k.k0i * r) * ri : ri;
+  const float2 E = __fmul2_rn(cs, make_float2(damp, damp));  // exp(i k0 r) / r
+  // E1 = (i k0 E - E / r) / r, the radial derivative over r
+  const float2 IK = __ffma2_rn(make_float2(ik.x, ik.x), E,
+                               __fmul2_rn(make_float2(-ik.y, ik.y), make_float2(E.y, E.x)));
+  const float ri2 = ri * ri;
+  const float2 E1 = __ffma2_rn(E, make_float2(-ri2, -ri2), __fmul2_rn(IK, make_float2(ri, ri)));
+  const float sv = rr * k.invR2;
+  const float2 s2 = make_float2(sv, sv);
+  float2 P = k.nac2[ND];
+#pragma unroll
+  for (int n = ND - 1; n >= 0; n--) P = __ffma2_rn(P, s2, k.nac2[n]);
+  float2 D = k.nbc2[ND - 1];
+#pragma unroll
+  for (int n = ND - 2; n >= 0; n--) D = __ffma2_rn(D, s2, k.nbc2[n]);
+  F0 = __fadd2_rn(E, P);
+  F1 = __fadd2_rn(E1, D);
+}
+
 // Helmholtz DM kernel exp(i k0 r)/r of the FP32 direct sum with packed
 // complex arithmetic: one source per lane per step, the (re, im) parts of
 // exp(i k0 r)/r, of the DM polynomials and of the charge products in
@@ -864,7 +893,6 @@ __device__ __forceinline__ void helmholtz_steps(const PairCoef<float> &k, const 
                                                 float2 &Gy, float2 &Gz) {
   const float R2 = k.R2;
   const unsigned rb = __float_as_uint(R2);
-  const float2 ik = make_float2(-k.k0i, k.k0r);  // i k0
 #pragma unroll 4
   for (int s = 0; s < cnt; s++) {
     const float4 src = sp[s];
@@ -881,24 +909,8 @@ __device__ __forceinline__ void helmholtz_steps(const PairCoef<float> &k, const 
     const float rr = hit ? r2 : R2;
     const float4 lo = slo[s];
     const float2 q = hit ? make_float2(src.w, lo.w) : make_float2(0.f, 0.f);
-    const float ri = rsqrtf(rr), r = rr * ri;
-    const float2 cs = sincos_sfu(k.k0r * r);
-    const float damp = k.k0i != 0.f ? __expf(-k.k0i * r) * ri : ri;
-    const float2 E = __fmul2_rn(cs, make_float2(damp, damp));  // exp(i k0 r) / r
-    // E1 = (i k0 E - E / r) / r, the radial derivative over r
-    const float2 IK = __ffma2_rn(make_float2(ik.x, ik.x), E,
-                                 __fmul2_rn(make_float2(-ik.y, ik.y), make_float2(E.y, E.x)));
-    const float ri2 = ri * ri;
-    const float2 E1 = __ffma2_rn(E, make_float2(-ri2, -ri2), __fmul2_rn(IK, make_float2(ri, ri)));
-    const float sv = rr * k.invR2;
-    const float2 s2 = make_float2(sv, sv);
-    float2 P = k.nac2[ND];
-#pragma unroll
-    for (int n = ND - 1; n >= 0; n--) P = __ffma2_rn(P, s2, k.nac2[n]);
-    float2 D = k.nbc2[ND - 1];
-#pragma unroll
-    for (int n = ND - 2; n >= 0; n--) D = __ffma2_rn(D, s2, k.nbc2[n]);
-    const float2 F0 = __fadd2_rn(E, P), F1 = __fadd2_rn(E1, D);
+    float2 F0, F1;
+    helm_eval<ND>(k, rr, F0, F1);
     const float2 qs = make_float2(q.y, q.x);
     // V += F0 q, G = F1 q (complex products)
     Pv = __ffma2_rn(make_float2(F0.x, F0.x), q, Pv);
@@ -908,6 +920,182 @@ __device__ __forceinline__ void helmholtz_steps(const PairCoef<float> &k, const 
     Gx = __ffma2_rn(G, make_float2(x, x), Gx);
     Gy = __ffma2_rn(G, make_float2(y, y), Gy);
     Gz = __ffma2_rn(G, make_float2(z, z), Gz);
+  }
+}
+
+// complex a * b + c and a * b on float2 (re, im)
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+  c = __ffma2_rn(make_float2(a.x, a.x), b, c);
+  return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), c);
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x),
+                    __fmul2_rn(make_float2(a.x, a.x), b));
+}
+
+// Helmholtz DM kernel of the FP32 direct sum with every unordered pair
+// evaluated once (the complex counterpart of direct_group_sym): the group's
+// targets sit in shared memory (th = heads and Re q, tl = residuals and Im
+// q), each lane holds two sources of a 64-source chunk of the half-shell
+// segments, target (l + k) mod 32 meets lane l at step k and its complex sums
+// (V, dV/dx, dV/dy, dV/dz) rotate one lane down per step; the source-side
+// sums of a chunk go to vsrc as two float4 per source (V re, V im, x re,
+// x im; y re, y im, z re, z im) with vector atomics.  Coordinates are
+// unscaled offsets from the group centre, close pairs refined as in the
+// one-sided body; pairs inside the group are a first, one-sided pass.
+template <int ND>
+__device__ __forceinline__ void direct_group_sym_helm(
+    const PairCoef<float> &k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller, const int4 G,
+    const double4 c, const int2 *__restrict__ segs, const uint32_t *__restrict__ perm,
+    float refine2, double fself_r, double fself_i, double *__restrict__ V,
+    float4 *__restrict__ vsrc, float4 *th, float4 *tl, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f;
+  float2 tq = make_float2(0.f, 0.f);
+  long o = 0;
+  if (active) {
+    const double4 p = gpos[ti];
+    o = perm[ti];
+    const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+    tx = (float)dx, ty = (float)dy, tz = (float)dz;
+    tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
+    tq = make_float2((float)qcaller[2 * o], (float)qcaller[2 * o + 1]);
+  }
+  th[lane] = make_float4(tx, ty, tz, tq.x);
+  tl[lane] = make_float4(tlx, tly, tlz, tq.y);
+  __syncwarp();
+  const float R2 = k.R2;
+  const unsigned rb = __float_as_uint(R2);
+  double acc[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
+
+  // pairs inside the group, target side only, differences always refined
+  {
+    float2 Pv = make_float2(0.f, 0.f), Gx = Pv, Gy = Pv, Gz = Pv;
+    for (int s = 0; s < G.y; s++) {
+      const float4 S = th[s], L = tl[s];
+      const float x = (tx - S.x) + (tlx - L.x), y = (ty - S.y) + (tly - L.y),
+                  z = (tz - S.z) + (tlz - L.z);
+      const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+      if (__float_as_uint(r2) - 1u < rb) {  // 0 < r^2 <= R2
+        float2 F0, F1;
+        helm_eval<ND>(k, r2, F0, F1);
+        const float2 q = make_float2(S.w, L.w), g = cmul(F1, q);
+        Pv = cfma(F0, q, Pv);
+        Gx = __ffma2_rn(g, make_float2(x, x), Gx);
+        Gy = __ffma2_rn(g, make_float2(y, y), Gy);
+        Gz = __ffma2_rn(g, make_float2(z, z), Gz);
+      }
+    }
+    acc[0] += Pv.x, acci[0] += Pv.y, acc[1] += Gx.x, acci[1] += Gx.y;
+    acc[2] += Gy.x, acci[2] += Gy.y, acc[3] += Gz.x, acci[3] += Gz.y;
+  }
+
+  SrcCursor ca{G.z, lane};
+  ca.normalize(segs, G.w);
+  SrcCursor cb{ca.seg, ca.off + 32};
+  cb.normalize(segs, G.w);
+  bool va = ca.seg < G.w, vb = cb.seg < G.w;
+  long ja = -1, jb = -1;
+  double4 pa = make_double4(0, 0, 0, 0), pb = pa;
+  float2 qa = make_float2(0.f, 0.f), qb = qa;
+  if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], qa = make_float2(qs[2 * ja], qs[2 * ja + 1]);
+  if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], qb = make_float2(qs[2 * jb], qs[2 * jb + 1]);
+  while (__any_sync(FULL, va)) {
+    // this chunk's two sources of the lane; empty slots far away on the
+    // other side from idle targets, with charge 0
+    float sx[2] = {-1e18f, -1e18f}, sy[2] = {-1e18f, -1e18f}, sz[2] = {-1e18f, -1e18f};
+    float lx[2] = {0.f, 0.f}, ly[2] = {0.f, 0.f}, lz[2] = {0.f, 0.f};
+    float2 sq[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    const long kidx[2] = {va ? ja : -1, vb ? jb : -1};
+    if (va) {
+      const double dx = pa.x - c.x, dy = pa.y - c.y, dz = pa.z - c.z;
+      sx[0] = (float)dx, sy[0] = (float)dy, sz[0] = (float)dz;
+      lx[0] = (float)(dx - (double)sx[0]), ly[0] = (float)(dy - (double)sy[0]);
+      lz[0] = (float)(dz - (double)sz[0]);
+      sq[0] = qa;
+    }
+    if (vb) {
+      const double dx = pb.x - c.x, dy = pb.y - c.y, dz = pb.z - c.z;
+      sx[1] = (float)dx, sy[1] = (float)dy, sz[1] = (float)dz;
+      lx[1] = (float)(dx - (double)sx[1]), ly[1] = (float)(dy - (double)sy[1]);
+      lz[1] = (float)(dz - (double)sz[1]);
+      sq[1] = qb;
+    }
+    ca.off += 64;
+    ca.normalize(segs, G.w);
+    cb.off += 64;
+    cb.normalize(segs, G.w);
+    va = ca.seg < G.w, vb = cb.seg < G.w;
+    if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], qa = make_float2(qs[2 * ja], qs[2 * ja + 1]);
+    if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], qb = make_float2(qs[2 * jb], qs[2 * jb + 1]);
+
+    float2 Pv = make_float2(0.f, 0.f), Gx = Pv, Gy = Pv, Gz = Pv;  // target side, rotating
+    float2 SV[2], SX[2], SY[2], SZ[2];                              // source side
+#pragma unroll
+    for (int u = 0; u < 2; u++) SV[u] = SX[u] = SY[u] = SZ[u] = make_float2(0.f, 0.f);
+    const int src = (lane + 1) & 31;
+    for (int kk = 0; kk < 32; kk++) {
+      const int tt = (lane + kk) & 31;
+      const float4 T = th[tt], L = tl[tt];
+      float x[2], y[2], z[2], rr[2];
+      bool hit[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        x[u] = T.x - sx[u], y[u] = T.y - sy[u], z[u] = T.z - sz[u];
+        float r2 = fmaf(x[u], x[u], fmaf(y[u], y[u], z[u] * z[u]));
+        hit[u] = __float_as_uint(r2) - 1u < rb;
+        if (hit[u] && r2 < refine2) {  // close pair: exact difference from head + residual
+          x[u] += L.x - lx[u];
+          y[u] += L.y - ly[u];
+          z[u] += L.z - lz[u];
+          r2 = fmaf(x[u], x[u], fmaf(y[u], y[u], z[u] * z[u]));
+        }
+        rr[u] = hit[u] ? r2 : R2;
+      }
+      if (__any_sync(FULL, hit[0] | hit[1])) {
+        const float2 qt = make_float2(T.w, L.w);
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          float2 F0, F1;
+          helm_eval<ND>(k, rr[u], F0, F1);
+          const float2 qm = hit[u] ? sq[u] : make_float2(0.f, 0.f);
+          const float2 qn = hit[u] ? qt : make_float2(0.f, 0.f);
+          const float2 g = cmul(F1, qm), gs = cmul(F1, qn);
+          Pv = cfma(F0, qm, Pv);
+          Gx = __ffma2_rn(g, make_float2(x[u], x[u]), Gx);
+          Gy = __ffma2_rn(g, make_float2(y[u], y[u]), Gy);
+          Gz = __ffma2_rn(g, make_float2(z[u], z[u]), Gz);
+          SV[u] = cfma(F0, qn, SV[u]);
+          SX[u] = __ffma2_rn(gs, make_float2(-x[u], -x[u]), SX[u]);
+          SY[u] = __ffma2_rn(gs, make_float2(-y[u], -y[u]), SY[u]);
+          SZ[u] = __ffma2_rn(gs, make_float2(-z[u], -z[u]), SZ[u]);
+        }
+      }
+      Pv.x = __shfl_sync(FULL, Pv.x, src), Pv.y = __shfl_sync(FULL, Pv.y, src);
+      Gx.x = __shfl_sync(FULL, Gx.x, src), Gx.y = __shfl_sync(FULL, Gx.y, src);
+      Gy.x = __shfl_sync(FULL, Gy.x, src), Gy.y = __shfl_sync(FULL, Gy.y, src);
+      Gz.x = __shfl_sync(FULL, Gz.x, src), Gz.y = __shfl_sync(FULL, Gz.y, src);
+    }
+    acc[0] += Pv.x, acci[0] += Pv.y, acc[1] += Gx.x, acci[1] += Gx.y;
+    acc[2] += Gy.x, acci[2] += Gy.y, acc[3] += Gz.x, acci[3] += Gz.y;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      if (kidx[u] >= 0) {
+        atomicAdd(vsrc + 2 * kidx[u], make_float4(SV[u].x, SV[u].y, SX[u].x, SX[u].y));
+        atomicAdd(vsrc + 2 * kidx[u] + 1, make_float4(SY[u].x, SY[u].y, SZ[u].x, SZ[u].y));
+      }
+    }
+  }
+  if (active) {
+    const double qr = qcaller[2 * o], qi = qcaller[2 * o + 1];
+    acc[0] -= fself_r * qr - fself_i * qi;  // src/Interface.cpp:2909-2910
+    acci[0] -= fself_r * qi + fself_i * qr;
+    double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
+#pragma unroll
+    for (int m = 0; m < 4; m++) Vo[m] = make_double2(acc[m], acci[m]);
   }
 }
 

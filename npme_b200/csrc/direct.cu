@@ -1,5 +1,6 @@
-// Short-range direct sum over warp groups, the cell-list pair count and the
-// exact O(N^2) sum.
+// Short-range direct sum over warp groups (every pair once for the built-in
+// kernels, one-sided otherwise), the cell-list pair count and the exact
+// O(N^2) sum.
 //
 // Direct sum (src/PotentialLaplace.cpp:201-264 and the pair kernels cited in
 // common.cuh): V_i = sum_{j != i, r_ij <= Rdir} q_j f_SR(r_ij),
@@ -138,6 +139,53 @@ __global__ void merge_source_kernel(float4 *__restrict__ vsrc, const uint32_t *_
   *o = v;
 }
 
+// FP32 Helmholtz DM form (direct_group_sym_helm).
+template <int ND>
+__global__ void __launch_bounds__(32 * kGroupWarps) direct_sym_helm_kernel(
+    PairCoef<float> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    float refine2, double fself_r, double fself_i, double *__restrict__ V,
+    float4 *__restrict__ vsrc) {
+  __shared__ float4 th[kGroupWarps][32];  // group targets: heads, Re q
+  __shared__ float4 tl[kGroupWarps][32];  // residuals, Im q
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  direct_group_sym_helm<ND>(k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, refine2,
+                            fself_r, fself_i, V, vsrc, th[wid], tl[wid], lane);
+}
+
+// Complex V[caller(s)][0..3] += vsrc[2s], vsrc[2s + 1] (re, im pairs), then zero.
+__global__ void merge_source_cplx_kernel(float4 *__restrict__ vsrc,
+                                         const uint32_t *__restrict__ sperm, long n,
+                                         double *__restrict__ V) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 a = vsrc[2 * s], b = vsrc[2 * s + 1];
+  vsrc[2 * s] = vsrc[2 * s + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+  double4 *o = reinterpret_cast<double4 *>(V) + 2 * (long)sperm[s];
+  double4 u = o[0], w = o[1];
+  u.x += a.x, u.y += a.y, u.z += a.z, u.w += a.w;
+  w.x += b.x, w.y += b.y, w.z += b.z, w.w += b.w;
+  o[0] = u, o[1] = w;
+}
+
+template <int ND>
+static void sym_helm_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  const long blocks = (h->n_hgroups + kGroupWarps - 1) / kGroupWarps;
+  if (blocks == 0) return;
+  direct_sym_helm_kernel<ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
+      make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
+      h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2,
+      a.fself_r, a.fself_i, a.V, h->d_vsrc);
+  const long n = (long)h->n;
+  merge_source_cplx_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->d_vsrc, h->d_sperm, n,
+                                                                        a.V);
+  h->launches++;
+}
+
 template <int FUNC, int ND>
 static void sym_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   const long blocks = (h->n_hgroups + kGroupWarps - 1) / kGroupWarps;
@@ -206,21 +254,31 @@ static void sym64_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   }
 }
 
-// The pair-once form applies to the real built-in kernels: in FP32 the DM
-// kernels with a tabulated derivative order, in FP64 also the original
-// Ewald split and any order; everything else walks the full segments.
+// The pair-once form applies to the built-in kernels: in FP32 the DM kernels
+// (1/r, r^alpha, Helmholtz) with a tabulated derivative order, in FP64 the
+// real kernels, original Ewald split and any order included; everything else
+// (FP32 original Ewald, FP64 Helmholtz, caller-defined kernels) walks the
+// full segments.
 bool pairs_once(const npme_handle *h) {
   if (!h->use_sym || h->user_kernel || h->n_hgroups == 0) return false;
   const int f = h->p.funcType, nd = h->p.nDeriv;
+  const bool tabulated = nd == 3 || nd == 6 || nd == 8;
+  if (f == NPME_FUNC_HELMHOLTZ) return h->fp32 && tabulated;
   if (f != NPME_FUNC_LAPLACE && f != NPME_FUNC_RALPHA) return false;
   if (!h->fp32) return true;
   if (h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) return false;
-  return nd == 3 || nd == 6 || nd == 8;
+  return tabulated;
 }
 
 static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   if (!pairs_once(h)) return false;
   const int f = h->p.funcType, nd = h->p.nDeriv;
+  if (f == NPME_FUNC_HELMHOLTZ) {
+    if (nd == 3) sym_helm_launch_nd<3>(h, a, s);
+    else if (nd == 6) sym_helm_launch_nd<6>(h, a, s);
+    else sym_helm_launch_nd<8>(h, a, s);
+    return true;
+  }
   if (!h->fp32) {
     if (h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) sym64_launch<0, 1>(h, a, s);
     else if (f == NPME_FUNC_RALPHA) sym64_launch<1, 0>(h, a, s);

@@ -135,7 +135,7 @@ struct npme_handle {
   int4 *d_hgroups = nullptr;
   double4 *d_hcen = nullptr;
   int2 *d_hsegs = nullptr;
-  float4 *d_vsrc = nullptr;      // FP32: source-side sums (source order, scaled frame), kept zero
+  float4 *d_vsrc = nullptr;      // FP32: source-side sums (source order; two float4 if complex), kept zero
   double *d_vsrc64 = nullptr;    // FP64: source-side sums [n][4] (source order), kept zero
 
   npme::Timing timing;

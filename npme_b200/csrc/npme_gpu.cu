@@ -523,8 +523,9 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
     if ((rc = dalloc(h, &h->d_hcen, sizeof(double4) * hcen.size()))) return rc;
     if ((rc = dalloc(h, &h->d_hsegs, sizeof(int2) * std::max<size_t>(1, hsegs.size())))) return rc;
     if (h->fp32) {
-      if ((rc = dalloc(h, &h->d_vsrc, sizeof(float4) * n))) return rc;
-      CK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * n, h->stream));
+      const size_t nv = (h->complex_kernel ? 2 : 1) * n;  // float4 per source (two if complex)
+      if ((rc = dalloc(h, &h->d_vsrc, sizeof(float4) * nv))) return rc;
+      CK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * nv, h->stream));
     } else {
       if ((rc = dalloc(h, &h->d_vsrc64, sizeof(double) * 4 * n))) return rc;
       CK(cudaMemsetAsync(h->d_vsrc64, 0, sizeof(double) * 4 * n, h->stream));

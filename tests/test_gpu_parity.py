@@ -220,36 +220,42 @@ def test_direct_sum_entry_point_matches_oracle(name, prec):
     assert rel(V[:, 1:], Vo[:, 1:]) < tol[1]
 
 
-def _direct_fp32(w, c, q, torch):
-    with npme_b200.Solver(api.params_from_workload(w, precision="fp32")) as s:
+def _direct(w, c, q, torch, prec="fp32"):
+    cplx = np.iscomplexobj(q)
+    with npme_b200.Solver(api.params_from_workload(w, precision=prec)) as s:
         s.setup(c)
         dq = torch.from_numpy(np.ascontiguousarray(q)).cuda()
-        dV = torch.zeros((len(q), 4), dtype=torch.float64, device="cuda")
+        dV = torch.zeros((len(q), 8 if cplx else 4), dtype=torch.float64, device="cuda")
         st = torch.cuda.Stream()
         s.direct_sum_device(dV.data_ptr(), dq.data_ptr(), st.cuda_stream)
         st.synchronize()
-        _direct_fp32.pairs_once = s.info()["pairsOnce"]
-        return dV.cpu().numpy()
+        _direct.pairs_once = s.info()["pairsOnce"]
+        V = dV.cpu().numpy()
+    return V.view(np.complex128) if cplx else V
 
 
-@pytest.mark.parametrize("name", ["laplace_dm_4k", "ralpha_dm_small", "laplace_dm_order8"])
-def test_pairs_once_matches_both_sides(name, monkeypatch):
-    # FP32 real DM kernels evaluate every pair once, for both of its points
-    # (NPME_PAIRS_ONCE=0 selects the one-sided walk); the two agree to FP32
-    # rounding and both match the oracle
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("name", ["laplace_dm_4k", "ralpha_dm_small", "laplace_dm_order8",
+                                  "helmholtz_dm_small", "laplace_orig_small"])
+def test_pairs_once_matches_both_sides(name, prec, monkeypatch):
+    # the built-in kernels evaluate every pair once, for both of its points
+    # (NPME_PAIRS_ONCE=0 selects the one-sided walk): FP32 DM kernels, FP64
+    # real kernels; the two forms agree to rounding and both match the oracle
     torch = pytest.importorskip("torch")
     w = SMALL[name]
     c, q = w.generate()
     Vo = ob.direct(ob.params_from_workload(w), c, q)
+    expect = (w.split == "dm") if prec == "fp32" else not np.iscomplexobj(q)
     got = {}
     for mode in ("0", "1"):
         monkeypatch.setenv("NPME_PAIRS_ONCE", mode)
-        got[mode] = _direct_fp32(w, c, q, torch)
-        assert _direct_fp32.pairs_once == (mode == "1")
-    assert rel(got["1"], got["0"]) < 1e-6
+        got[mode] = _direct(w, c, q, torch, prec)
+        assert _direct.pairs_once == (mode == "1" and expect)
+    tol = (FP64_TOL, FP64_TOL) if prec == "fp64" else (FP32_V_TOL, FP32_G_TOL)
+    assert rel(got["1"], got["0"]) < (1e-13 if prec == "fp64" else 1e-6)
     for V in got.values():
-        assert rel(V[:, 0], Vo[:, 0]) < FP32_V_TOL
-        assert rel(V[:, 1:], Vo[:, 1:]) < FP32_G_TOL
+        assert rel(V[:, 0], Vo[:, 0]) < tol[0]
+        assert rel(V[:, 1:], Vo[:, 1:]) < tol[1]
 
 
 def test_pairs_once_on_a_lattice():
@@ -262,7 +268,7 @@ def test_pairs_once_on_a_lattice():
     q = np.random.default_rng(5).uniform(-1.0, 1.0, w.n)
     q -= q.mean()
     Vo = ob.direct(ob.params_from_workload(w), c, q)
-    V = _direct_fp32(w, c, q, torch)
+    V = _direct(w, c, q, torch)
     assert rel(V[:, 0], Vo[:, 0]) < FP32_V_TOL
     assert rel(V[:, 1:], Vo[:, 1:]) < FP32_G_TOL
 
