@@ -358,7 +358,9 @@ def main():
 
     # end to end through the C ABI with pinned host buffers
     qh = torch.from_numpy(q).pin_memory().numpy()
-    Vh = torch.empty((w.n, 4), dtype=torch.float64).pin_memory().numpy()
+    cplx = np.iscomplexobj(q)
+    Vh = torch.empty((w.n, 4), dtype=torch.complex128 if cplx else torch.float64)
+    Vh = Vh.pin_memory().numpy()
     for _ in range(2):
         s.calcv(qh, out=Vh)
     e2e_ts = []
@@ -426,8 +428,11 @@ def main():
             fp_peak /= 2
         achieved = (pairs * flops_pair / (st["direct"] / 1e3) / 1e12
                     if pairs and st["direct"] > 0 else None)
-        dk = ("direct_sym_kernel" if info0.get("pairsOnce") else
-              "direct_groups_kernel" if args.precision == "fp32" else "direct_groups64_kernel")
+        if info0.get("pairsOnce"):
+            dk = ("direct_sym64_kernel" if args.precision == "fp64" else
+                  "direct_sym_helm_kernel" if w.func == "helmholtz" else "direct_sym_kernel")
+        else:
+            dk = "direct_groups_kernel" if args.precision == "fp32" else "direct_groups64_kernel"
         roofline = {"kernel": dk, "bound": "fp32" if args.precision == "fp32" else "fp64",
                     "achieved": achieved, "peak": fp_peak, "unit": "TFLOP/s",
                     "frac": (achieved / fp_peak) if achieved else None,
@@ -449,14 +454,18 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": max(3, args.warmup),
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+                "vs_baseline": None,
+                "dtype": ("c64" if cplx else "f32") if args.precision == "fp32"
+                else ("c128" if cplx else "f64"),
                 "data": "synthetic (seeded Philox; points uniform in the box, charges "
-                        "uniform in [-1,1], net zero)",
+                        + ("with re and im uniform in [-1,1])" if cplx else
+                           "uniform in [-1,1], net zero)"),
                 "config": config_of(w, args.precision, world),
                 "e2e": {"value": e2e_value, "unit": UNIT,
                         "h2d_bytes_per_step": int(q.nbytes),
-                        "d2h_bytes_per_step": int(w.n * 4 * 8),
-                        "api": "npme_gpu_calcv_real, pinned host buffers"},
+                        "d2h_bytes_per_step": int(Vh.nbytes),
+                        "api": ("npme_gpu_calcv_complex" if cplx else "npme_gpu_calcv_real")
+                        + ", pinned host buffers"},
                 "roofline": roofline, "stages": stages,
                 "gpu_launches": launches, "clocks": clocks,
                 "setup_seconds": setup_seconds}
