@@ -297,8 +297,9 @@ int npme_gpu_choose_grid(const npme_params *p, size_t n, const double *coord,
                          const double *charge, double tol, double maxFFTmemGB,
                          npme_params *out, double *err);
 
-/* Number of unordered point pairs with r <= Rdir in the set-up geometry
- * (the work of the direct sum), counted on the device with the cell list. */
+/* Number of unordered point pairs with 0 < r <= Rdir in the set-up geometry
+ * (the work of the direct sum), counted on the device in FP64 over the
+ * direct sum's warp groups. */
 int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs);
 
 /* Record per-stage CUDA-event timings for subsequent calcv calls. */

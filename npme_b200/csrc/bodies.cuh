@@ -1455,6 +1455,4 @@ __device__ __forceinline__ void direct_group_sym64(
   }
 }
 
-constexpr int kDirectBS = 64;  // tile of the cell-list pair count (direct.cu)
-
 }  // namespace npme

@@ -1,5 +1,5 @@
 // Short-range direct sum over warp groups (every pair once for the built-in
-// kernels, one-sided otherwise), the cell-list pair count and the exact
+// kernels, one-sided otherwise), the pair count and the exact
 // O(N^2) sum.
 //
 // Direct sum (src/PotentialLaplace.cpp:201-264 and the pair kernels cited in
@@ -359,68 +359,48 @@ void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t 
   launch_direct_args(h, a, s);
 }
 
-// Ordered pairs with r <= Rdir, i != j, using the same cell walk as the
-// direct sum (work accounting for the roofline report).
-template <typename T>
-__global__ void __launch_bounds__(kDirectBS) count_pairs_kernel(
-    const typename Vec4<T>::type *__restrict__ cpos, const int *__restrict__ cell_start,
-    int nc0, int nc1, int nc2, T e0, T e1, T e2, int reach, T R2,
+// Ordered pairs with 0 < r <= Rdir (FP64 distances) over the one-sided group
+// walk, every target of a group against every source of its segments: the
+// work count of the roofline report (set-up only, not on the CalcV path).
+__global__ void __launch_bounds__(32 * kGroupWarps) count_pairs_kernel(
+    const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const int4 *__restrict__ groups, const int2 *__restrict__ segs, long ngroups, double R2,
     unsigned long long *__restrict__ count) {
-  using V4 = typename Vec4<T>::type;
-  __shared__ V4 sp[kDirectBS];
-  const int cell = blockIdx.x;
-  const int cz = cell % nc2, cy = (cell / nc2) % nc1, cx = cell / (nc2 * nc1);
-  const int tbeg = cell_start[cell], tend = cell_start[cell + 1];
+  __shared__ double4 sp[kGroupWarps][32];
+  const unsigned FULL = 0xffffffffu;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  const int4 G = groups[g];
+  const double4 t = lane < G.y ? gpos[G.x + lane] : make_double4(1e150, 1e150, 1e150, 0.0);
   unsigned long long mine = 0;
-  for (int t0 = tbeg; t0 < tend; t0 += kDirectBS) {
-    const int i = t0 + threadIdx.x;
-    const bool active = i < tend;
-    V4 ti = active ? cpos[i] : V4{0, 0, 0, 0};
-    for (int dx = -reach; dx <= reach; dx++) {
-      const int sx = cx + dx;
-      if (sx < 0 || sx >= nc0) continue;
-      for (int dy = -reach; dy <= reach; dy++) {
-        const int sy = cy + dy;
-        if (sy < 0 || sy >= nc1) continue;
-        const int z0 = max(cz - reach, 0), z1 = min(cz + reach, nc2 - 1);
-        const int colbase = (sx * nc1 + sy) * nc2;
-        const int jb = cell_start[colbase + z0], je = cell_start[colbase + z1 + 1];
-        for (int j0 = jb; j0 < je; j0 += kDirectBS) {
-          __syncthreads();
-          const int j = j0 + threadIdx.x;
-          if (j < je) {
-            V4 s = cpos[j];
-            s.x += (T)dx * e0;
-            s.y += (T)dy * e1;
-            s.z += (s.w - (T)cz) * e2;
-            sp[threadIdx.x] = s;
-          }
-          __syncthreads();
-          const int cnt = min(kDirectBS, je - j0);
-          if (active)
-            for (int s = 0; s < cnt; s++) {
-              const T x = ti.x - sp[s].x, y = ti.y - sp[s].y, z = ti.z - sp[s].z;
-              if (x * x + y * y + z * z <= R2 && j0 + s != i) mine++;
-            }
-        }
-      }
+  SrcCursor cur{G.z, lane};
+  cur.normalize(segs, G.w);
+  while (__any_sync(FULL, cur.seg < G.w)) {
+    const bool v = cur.seg < G.w;
+    const int cnt = __popc(__ballot_sync(FULL, v));  // valid lanes form a prefix
+    __syncwarp();
+    if (v) sp[wid][lane] = spos[(long)segs[cur.seg].x + cur.off];
+    __syncwarp();
+    for (int s = 0; s < cnt; s++) {
+      const double4 q = sp[wid][s];
+      const double x = t.x - q.x, y = t.y - q.y, z = t.z - q.z;
+      const double r2 = x * x + y * y + z * z;
+      mine += (r2 <= R2 && r2 > 0.0) ? 1ull : 0ull;
     }
+    cur.off += 32;
+    cur.normalize(segs, G.w);
   }
-  atomicAdd(count, mine);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(FULL, mine, o);
+  if (lane == 0) atomicAdd(count, mine);
 }
 
 void launch_count_pairs(npme_handle *h, unsigned long long *d_count, cudaStream_t s) {
-  const CellGeom &c = h->cells;
-  const int ncell = c.nc[0] * c.nc[1] * c.nc[2];
-  const double R2 = h->p.Rdir * h->p.Rdir;
-  if (h->fp32)
-    count_pairs_kernel<float><<<ncell, kDirectBS, 0, s>>>(
-        (const float4 *)h->d_cpos, h->d_cell_start, c.nc[0], c.nc[1], c.nc[2],
-        (float)c.edge[0], (float)c.edge[1], (float)c.edge[2], c.reach, (float)R2, d_count);
-  else
-    count_pairs_kernel<double><<<ncell, kDirectBS, 0, s>>>(
-        (const double4 *)h->d_cpos, h->d_cell_start, c.nc[0], c.nc[1], c.nc[2], c.edge[0],
-        c.edge[1], c.edge[2], c.reach, R2, d_count);
+  const long blocks = (h->n_groups + kGroupWarps - 1) / kGroupWarps;
+  if (blocks == 0) return;
+  count_pairs_kernel<<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
+      h->d_gpos, h->d_spos, h->d_groups, h->d_segs, h->n_groups, h->p.Rdir * h->p.Rdir, d_count);
 }
 
 // ---------------------------------------------------------------------------

@@ -26,7 +26,8 @@ struct GridGeom {
   int order;
 };
 
-// Geometry of the direct-sum cell list.
+// Cells of edge >= Rdir / nNeigh over the points' bounding box (the
+// reference's cell geometry, reported by npme_gpu_get_info).
 struct CellGeom {
   int nc[3];       // cells per axis
   double origin[3];
@@ -90,11 +91,9 @@ struct npme_handle {
   void *d_bpts = nullptr;        // BrickPoint<T>[n]
   int *d_brick_start = nullptr;  // [n_bricks + 1]
   int *d_brick_list = nullptr;   // non-empty brick ids
-  void *d_cpos = nullptr;        // cell order positions: float4 (local xyz, cell z) or double4
-  uint32_t *d_cperm = nullptr;   // cell order (FP64) / group order (FP32) -> caller index
-  int *d_cell_start = nullptr;   // [ncell + 1]
+  uint32_t *d_cperm = nullptr;   // group order (direct-sum targets) -> caller index
   void *d_qb = nullptr;          // charges in brick order (T or T2)
-  void *d_qc = nullptr;          // charges in cell order (T or T2)
+  void *d_qc = nullptr;          // charges in the direct sum's source order (T or T2)
   void *d_grid = nullptr;        // spread grid, real N1 N2 N3 (or complex)
   void *d_kgrid = nullptr;       // transformed grid N1 N2 (N3/2+1) complex (real kernels)
   void *d_theta = nullptr;       // theta, same layout as d_grid (real kernels)

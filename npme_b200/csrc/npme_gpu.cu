@@ -226,6 +226,23 @@ int setup_threads(size_t n) {
   return std::max(1, std::min(NPME_SETUP_THREADS_MAX, hw / std::max(1, g_active_setups.load())));
 }
 
+// fn(begin, end) over [0, count) split into contiguous ranges, one host
+// thread each; the thread count follows `work` (points handled; default
+// count), the calling thread alone for small systems.
+template <class F>
+void parallel_ranges(size_t count, F fn, size_t work = 0) {
+  const int nt = (int)std::min<size_t>(setup_threads(work ? work : count),
+                                       std::max<size_t>(1, count));
+  if (nt <= 1) {
+    fn((size_t)0, count);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; t++)
+    pool.emplace_back(fn, count * t / nt, count * (t + 1) / nt);
+  for (auto &th : pool) th.join();
+}
+
 // Sorts the points by xy column (`col`, ncol columns), then by (z, index)
 // inside each column.  Fills the permutation, the column starts and the
 // sorted z.
@@ -260,6 +277,19 @@ void column_sort(const double *coord, size_t n, long ncol, const std::vector<int
     for (int t = 0; t < nt; t++) pool.emplace_back(sort_columns, ncol * t / nt, ncol * (t + 1) / nt);
     for (auto &th : pool) th.join();
   }
+}
+
+// gpos[k] = coord[gorder[k]], spos[k] = coord[sorder[k]] (FP64, w unused)
+__global__ void gather_positions_kernel(const double *__restrict__ coord,
+                                        const uint32_t *__restrict__ gorder,
+                                        const uint32_t *__restrict__ sorder, long n,
+                                        double4 *__restrict__ gpos, double4 *__restrict__ spos) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double *x = coord + 3 * (long)gorder[k];
+  gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
+  const double *y = coord + 3 * (long)sorder[k];
+  spos[k] = make_double4(y[0], y[1], y[2], 0.0);
 }
 
 #ifndef NPME_SOURCE_SPLIT
@@ -345,6 +375,7 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
     std::vector<int4> groups, hgroups;
     std::vector<double4> cen;
     std::vector<int2> segs, hsegs;
+    std::vector<long> work, hwork;  // sources staged per group (launch order)
     double cand = 0, hcand = 0;
   };
   auto build_part = [&](long c_begin, long c_end, Part &out) {
@@ -397,6 +428,7 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
           dyv[u] = d * d;
         }
         const int seg0 = (int)out.segs.size(), hseg0 = (int)out.hsegs.size();
+        long gwork = 0, hwork = 0;
         for (size_t t = 0; t < nb_col.size(); t++) {
           const double d2 = dxv[nb_s0[t]] + dyv[nb_s1[t]];
           if (d2 > R2) continue;
@@ -412,6 +444,7 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
           if (b > a) {
             out.segs.push_back(make_int2((int)a, (int)(b - a)));
             out.cand += (double)(b - a) * (double)(p1 - p0);
+            gwork += b - a;
           }
           // half shell: later coarse columns whole, the group's own column
           // from the first point after the group
@@ -423,13 +456,17 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
             if (b > a2) {
               out.hsegs.push_back(make_int2((int)a2, (int)(b - a2)));
               out.hcand += (double)(b - a2) * (double)(p1 - p0);
+              hwork += b - a2;
             }
           }
         }
         out.groups.push_back(make_int4((int)p0, (int)(p1 - p0), seg0, (int)out.segs.size()));
-        if (half)
+        out.work.push_back(gwork);
+        if (half) {
           out.hgroups.push_back(
               make_int4((int)p0, (int)(p1 - p0), hseg0, (int)out.hsegs.size()));
+          out.hwork.push_back(hwork);
+        }
         // centre and half-diagonal of the bounding box
         out.cen.push_back(make_double4(
             0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]),
@@ -449,79 +486,84 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
                         std::ref(parts[t]));
     for (auto &th : pool) th.join();
   }
+  // group records with segment indices made global; the segment lists stay
+  // in their parts and are uploaded part by part (no host concatenation)
   std::vector<int4> groups, hgroups;
   std::vector<double4> cen;
-  std::vector<int2> segs, hsegs;
+  std::vector<long> work, hwork;
+  size_t nsegs = 0, nhsegs = 0;
   double cand = 0, hcand = 0;
   for (Part &pt : parts) {
-    const int base = (int)segs.size(), hbase = (int)hsegs.size();
+    const int base = (int)nsegs, hbase = (int)nhsegs;
     for (int4 g : pt.groups) groups.push_back(make_int4(g.x, g.y, g.z + base, g.w + base));
     for (int4 g : pt.hgroups) hgroups.push_back(make_int4(g.x, g.y, g.z + hbase, g.w + hbase));
     cen.insert(cen.end(), pt.cen.begin(), pt.cen.end());
-    segs.insert(segs.end(), pt.segs.begin(), pt.segs.end());
-    hsegs.insert(hsegs.end(), pt.hsegs.begin(), pt.hsegs.end());
+    work.insert(work.end(), pt.work.begin(), pt.work.end());
+    hwork.insert(hwork.end(), pt.hwork.begin(), pt.hwork.end());
+    nsegs += pt.segs.size(), nhsegs += pt.hsegs.size();
     cand += pt.cand, hcand += pt.hcand;
   }
   // heaviest groups first, so the last wave of the launch holds the light
   // ones (each list by its own work)
-  auto by_work = [](std::vector<int4> &gl, const std::vector<int2> &sl,
+  auto by_work = [](std::vector<int4> &gl, const std::vector<long> &wk,
                     const std::vector<double4> &cin, std::vector<double4> &cout) {
-    std::vector<long> work(gl.size());
-    for (size_t g = 0; g < gl.size(); g++) {
-      long c = 0;
-      for (int t = gl[g].z; t < gl[g].w; t++) c += sl[t].y;
-      work[g] = c;
-    }
     std::vector<uint32_t> go(gl.size());
     for (size_t g = 0; g < go.size(); g++) go[g] = (uint32_t)g;
-    std::stable_sort(go.begin(), go.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
+    std::stable_sort(go.begin(), go.end(), [&](uint32_t a, uint32_t b) { return wk[a] > wk[b]; });
     std::vector<int4> g2(gl.size());
     cout.resize(gl.size());
     for (size_t g = 0; g < go.size(); g++) g2[g] = gl[go[g]], cout[g] = cin[go[g]];
     gl.swap(g2);
   };
   std::vector<double4> gcen, hcen;
-  by_work(groups, segs, cen, gcen);
-  if (half) by_work(hgroups, hsegs, cen, hcen);
+  by_work(groups, work, cen, gcen);
+  if (half) by_work(hgroups, hwork, cen, hcen);
   cen.swap(gcen);
-  std::vector<double4> gpos(n), spos(n);
-  for (size_t k = 0; k < n; k++) {
-    const double *x = coord + 3 * (size_t)order[k];
-    gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
-    const double *y = coord + 3 * (size_t)sorder[k];
-    spos[k] = make_double4(y[0], y[1], y[2], 0.0);
-  }
   h->n_groups = (long)groups.size();
-  h->n_segs = (long)segs.size();
+  h->n_segs = (long)nsegs;
   h->cand_per_point = cand / (double)n;
   h->n_hgroups = (long)hgroups.size();
-  h->n_hsegs = (long)hsegs.size();
+  h->n_hsegs = (long)nhsegs;
   h->hcand_per_point = hcand / (double)n;
   // heads of offsets up to ~the group half-diagonal carry ~6e-8 e absolute
   // error; below r = e/4 the relative error would exceed ~1e-6, so refine
   h->refine2 = (0.25 * e) * (0.25 * e);
   int rc;
+  if ((rc = dalloc(h, &h->d_coord, sizeof(double) * 3 * n))) return rc;
   if ((rc = dalloc(h, &h->d_gpos, sizeof(double4) * n))) return rc;
   if ((rc = dalloc(h, &h->d_spos, sizeof(double4) * n))) return rc;
+  if ((rc = dalloc(h, &h->d_cperm, sizeof(uint32_t) * n))) return rc;
   if ((rc = dalloc(h, &h->d_sperm, sizeof(uint32_t) * n))) return rc;
   if ((rc = dalloc(h, &h->d_groups, sizeof(int4) * groups.size()))) return rc;
   if ((rc = dalloc(h, &h->d_gcen, sizeof(double4) * cen.size()))) return rc;
-  if ((rc = dalloc(h, &h->d_segs, sizeof(int2) * std::max<size_t>(1, segs.size())))) return rc;
-  CK(cudaMemcpyAsync(h->d_gpos, gpos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_spos, spos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+  if ((rc = dalloc(h, &h->d_segs, sizeof(int2) * std::max<size_t>(1, nsegs)))) return rc;
+  // target and source positions are gathered on the device from the
+  // caller's coordinates and the two orders
+  CK(cudaMemcpyAsync(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_cperm, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
+                     h->stream));
   CK(cudaMemcpyAsync(h->d_sperm, sorder.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
                      h->stream));
+  gather_positions_kernel<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
+      h->d_coord, h->d_cperm, h->d_sperm, (long)n, h->d_gpos, h->d_spos);
+  CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h->d_groups, groups.data(), sizeof(int4) * groups.size(),
                      cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_gcen, cen.data(), sizeof(double4) * cen.size(), cudaMemcpyHostToDevice,
                      h->stream));
-  if (!segs.empty())
-    CK(cudaMemcpyAsync(h->d_segs, segs.data(), sizeof(int2) * segs.size(), cudaMemcpyHostToDevice,
-                       h->stream));
+  {
+    size_t off = 0;
+    for (const Part &pt : parts) {
+      if (!pt.segs.empty())
+        CK(cudaMemcpyAsync(h->d_segs + off, pt.segs.data(), sizeof(int2) * pt.segs.size(),
+                           cudaMemcpyHostToDevice, h->stream));
+      off += pt.segs.size();
+    }
+  }
   if (half) {
     if ((rc = dalloc(h, &h->d_hgroups, sizeof(int4) * hgroups.size()))) return rc;
     if ((rc = dalloc(h, &h->d_hcen, sizeof(double4) * hcen.size()))) return rc;
-    if ((rc = dalloc(h, &h->d_hsegs, sizeof(int2) * std::max<size_t>(1, hsegs.size())))) return rc;
+    if ((rc = dalloc(h, &h->d_hsegs, sizeof(int2) * std::max<size_t>(1, nhsegs)))) return rc;
     if (h->fp32) {
       const size_t nv = (h->complex_kernel ? 2 : 1) * n;  // float4 per source (two if complex)
       if ((rc = dalloc(h, &h->d_vsrc, sizeof(float4) * nv))) return rc;
@@ -534,9 +576,13 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
                        cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_hcen, hcen.data(), sizeof(double4) * hcen.size(),
                        cudaMemcpyHostToDevice, h->stream));
-    if (!hsegs.empty())
-      CK(cudaMemcpyAsync(h->d_hsegs, hsegs.data(), sizeof(int2) * hsegs.size(),
-                         cudaMemcpyHostToDevice, h->stream));
+    size_t off = 0;
+    for (const Part &pt : parts) {
+      if (!pt.hsegs.empty())
+        CK(cudaMemcpyAsync(h->d_hsegs + off, pt.hsegs.data(), sizeof(int2) * pt.hsegs.size(),
+                           cudaMemcpyHostToDevice, h->stream));
+      off += pt.hsegs.size();
+    }
   }
   return NPME_OK;
 }
@@ -550,27 +596,39 @@ int upload_points(npme_handle *h, const double *coord) {
   // --- brick order for spread / interpolation ---
   std::vector<BrickPoint<T>> pts(n);
   std::vector<int> bid(n);
-  for (size_t i = 0; i < n; i++) {
-    uint32_t g0[3];
-    T u[3];
-    for (int d = 0; d < 3; d++) {
-      const double w = (double)g.N[d] / L[d] * (coord[3 * i + d] - R[d]);
-      const long ms = start_index(w);
-      const long o = ms + g.N[d] / 4;
-      if (o < 0 || o + P - 1 > g.H[d] - 1)
-        return fail(h, NPME_EINVAL,
-                    "point " + std::to_string(i) + " has a B-spline stencil outside the "
-                    "charge octant (axis " + std::to_string(d) + ")");
-      g0[d] = (uint32_t)o;
-      u[d] = (T)(w + (double)ms);
+  // the first point (lowest index) whose stencil leaves the octant, and its axis
+  std::atomic<long> bad{(long)n};
+  std::atomic<int> bad_axis{0};
+  parallel_ranges(n, [&](size_t i0, size_t i1) {
+    for (size_t i = i0; i < i1; i++) {
+      uint32_t g0[3];
+      T u[3];
+      for (int d = 0; d < 3; d++) {
+        const double w = (double)g.N[d] / L[d] * (coord[3 * i + d] - R[d]);
+        const long ms = start_index(w);
+        const long o = ms + g.N[d] / 4;
+        if (o < 0 || o + P - 1 > g.H[d] - 1) {
+          long cur = bad.load();
+          while ((long)i < cur && !bad.compare_exchange_weak(cur, (long)i)) {
+          }
+          if (bad.load() == (long)i) bad_axis = d;
+          return;
+        }
+        g0[d] = (uint32_t)o;
+        u[d] = (T)(w + (double)ms);
+      }
+      BrickPoint<T> &bp = pts[i];
+      bp.u[0] = u[0], bp.u[1] = u[1], bp.u[2] = u[2];
+      bp.g0 = (g0[0] << 20) | (g0[1] << 10) | g0[2];
+      bp.orig = (uint32_t)i;
+      bid[i] = (int)(((g0[0] / npme::kBrick) * g.nb[1] + g0[1] / npme::kBrick) * g.nb[2] +
+                     g0[2] / npme::kBrick);
     }
-    BrickPoint<T> &bp = pts[i];
-    bp.u[0] = u[0], bp.u[1] = u[1], bp.u[2] = u[2];
-    bp.g0 = (g0[0] << 20) | (g0[1] << 10) | g0[2];
-    bp.orig = (uint32_t)i;
-    bid[i] = (int)(((g0[0] / npme::kBrick) * g.nb[1] + g0[1] / npme::kBrick) * g.nb[2] +
-                   g0[2] / npme::kBrick);
-  }
+  });
+  if (bad.load() < (long)n)
+    return fail(h, NPME_EINVAL,
+                "point " + std::to_string(bad.load()) + " has a B-spline stencil outside the "
+                "charge octant (axis " + std::to_string(bad_axis.load()) + ")");
   const long nbt = g.nb[0] * g.nb[1] * g.nb[2];
   std::vector<int> bstart(nbt + 1, 0);
   for (size_t i = 0; i < n; i++) bstart[bid[i] + 1]++;
@@ -588,9 +646,11 @@ int upload_points(npme_handle *h, const double *coord) {
     const int TL = npme::kBrick + P - 1;
     const int words = (int)(sizeof(T) / 4) * (h->complex_kernel ? 2 : 1);
     const int nkeys = 32 / words;
+    parallel_ranges(blist.size(), [&](size_t k0, size_t k1) {
     std::vector<BrickPoint<T>> tmp;
     int cnt[32];
-    for (const int b : blist) {
+    for (size_t kb = k0; kb < k1; kb++) {
+      const int b = blist[kb];
       const int beg = bstart[b], end = bstart[b + 1];
       const long b3 = b % g.nb[2], b2 = (b / g.nb[2]) % g.nb[1], b1 = b / (g.nb[2] * g.nb[1]);
       auto key = [&](const BrickPoint<T> &pt) {
@@ -610,59 +670,26 @@ int upload_points(npme_handle *h, const double *coord) {
       }
       for (const auto &pt : tmp) sorted[cnt[key(pt)]++] = pt;
     }
+    }, n);
   }
   h->n_bricks = nbt;
   h->n_nonempty = (long)blist.size();
 
-  // --- cell order for the direct sum ---
-  const npme::CellGeom &c = h->cells;
-  const long ncell = (long)c.nc[0] * c.nc[1] * c.nc[2];
-  std::vector<int> cid(n);
-  std::vector<double> loc(3 * n);
-  std::vector<int> cz(n);
-  for (size_t i = 0; i < n; i++) {
-    int ci[3];
-    for (int d = 0; d < 3; d++) {
-      long k = (long)std::floor((coord[3 * i + d] - c.origin[d]) / c.edge[d]);
-      k = std::max(0L, std::min(k, (long)c.nc[d] - 1));
-      ci[d] = (int)k;
-      loc[3 * i + d] = coord[3 * i + d] - (c.origin[d] + k * c.edge[d]);
-    }
-    cz[i] = ci[2];
-    cid[i] = (ci[0] * c.nc[1] + ci[1]) * c.nc[2] + ci[2];
-  }
-  std::vector<int> cstart(ncell + 1, 0);
-  for (size_t i = 0; i < n; i++) cstart[cid[i] + 1]++;
-  for (long b = 0; b < ncell; b++) cstart[b + 1] += cstart[b];
-  std::vector<int> cfill(cstart.begin(), cstart.end() - 1);
-  using V4 = typename npme::Vec4<T>::type;
-  std::vector<V4> cpos(n);
-  std::vector<uint32_t> cperm(n);
-  for (size_t i = 0; i < n; i++) {
-    const int s = cfill[cid[i]]++;
-    cpos[s] = V4{(T)loc[3 * i], (T)loc[3 * i + 1], (T)loc[3 * i + 2], (T)cz[i]};
-    cperm[s] = (uint32_t)i;
-  }
-
+  std::vector<uint32_t> cperm;  // group order -> caller index (build_groups)
   const int C = h->complex_kernel ? 2 : 1;
   int rc;
   // the direct sum walks warp groups: targets in group order, sources
   // (and their gathered charges) in fine-column order
   std::vector<uint32_t> sperm;
-  if (h->use_groups && (rc = build_groups(h, coord, cperm, sperm))) return rc;
-  if ((rc = dalloc(h, &h->d_coord, sizeof(double) * 3 * n))) return rc;
+  if ((rc = build_groups(h, coord, cperm, sperm))) return rc;
   if ((rc = dalloc(h, (BrickPoint<T> **)&h->d_bpts, sizeof(BrickPoint<T>) * n))) return rc;
   if ((rc = dalloc(h, &h->d_brick_start, sizeof(int) * (nbt + 1)))) return rc;
   if ((rc = dalloc(h, &h->d_brick_list, sizeof(int) * std::max<size_t>(1, blist.size()))))
     return rc;
-  if ((rc = dalloc(h, (V4 **)&h->d_cpos, sizeof(V4) * n))) return rc;
-  if ((rc = dalloc(h, &h->d_cperm, sizeof(uint32_t) * n))) return rc;
-  if ((rc = dalloc(h, &h->d_cell_start, sizeof(int) * (ncell + 1)))) return rc;
   if ((rc = dalloc(h, (T **)&h->d_qb, sizeof(T) * C * n))) return rc;
   if ((rc = dalloc(h, (T **)&h->d_qc, sizeof(T) * C * n))) return rc;
   if ((rc = dalloc(h, &h->d_q_in, sizeof(double) * C * n))) return rc;
   if ((rc = dalloc(h, &h->d_V, sizeof(double) * 4 * C * n))) return rc;
-  CK(cudaMemcpyAsync(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_bpts, sorted.data(), sizeof(BrickPoint<T>) * n, cudaMemcpyHostToDevice,
                      h->stream));
   CK(cudaMemcpyAsync(h->d_brick_start, bstart.data(), sizeof(int) * (nbt + 1),
@@ -670,13 +697,8 @@ int upload_points(npme_handle *h, const double *coord) {
   if (!blist.empty())
     CK(cudaMemcpyAsync(h->d_brick_list, blist.data(), sizeof(int) * blist.size(),
                        cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_cpos, cpos.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_cperm, cperm.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
-                     h->stream));
-  CK(cudaMemcpyAsync(h->d_cell_start, cstart.data(), sizeof(int) * (ncell + 1),
-                     cudaMemcpyHostToDevice, h->stream));
   // charges of the direct sum are gathered into its source order
-  h->d_dperm = h->use_groups ? h->d_sperm : h->d_cperm;
+  h->d_dperm = h->d_sperm;
 
   // --- grids ---
   const long *N = g.N;
@@ -924,9 +946,9 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
   }
   if (ncells > (1L << 30)) return fail(h, NPME_EINVAL, "too many direct-sum cells");
   h->cells.reach = p.nNeigh;
-  // both precisions walk warp groups; the cell list above serves the pair count
+  // both precisions walk warp groups
   h->use_groups = true;
-  // FP32 real DM kernels evaluate every pair once unless NPME_PAIRS_ONCE=0
+  // the built-in kernels evaluate every pair once unless NPME_PAIRS_ONCE=0
   {
     const char *e = std::getenv("NPME_PAIRS_ONCE");
     h->use_sym = !(e && e[0] == '0');
