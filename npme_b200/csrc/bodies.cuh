@@ -1324,6 +1324,142 @@ __device__ __forceinline__ void direct_group_fp64(
   }
 }
 
+// FP32 direct sum of one warp group with every unordered pair evaluated once,
+// for the real kernels without a packed body (the original Ewald split and
+// caller-defined kernels): the pair-once walk of direct_group_sym with the
+// scalar pair kernel (pair_sr) of the one-sided body.  Coordinates are
+// unscaled FP32 offsets from the group centre (heads in th with the target
+// charge, residuals in tl), close pairs refined from the residuals; the
+// source-side sums go to vsrc as the gradient itself (merge scale 1).
+template <int FUNC, int SPLIT, int ND, class PK = BuiltinPair>
+__device__ __forceinline__ void direct_group_sym_scalar(
+    const PairCoef<float> &k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller, const int4 G,
+    const double4 c, const int2 *__restrict__ segs, const uint32_t *__restrict__ perm,
+    float refine2, double fself_r, double *__restrict__ V, float4 *__restrict__ vsrc,
+    float4 *th, float4 *tl, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const int ti = G.x + lane;
+  const bool active = lane < G.y;
+  float tx = 1e18f, ty = 1e18f, tz = 1e18f, tlx = 0.f, tly = 0.f, tlz = 0.f, tq = 0.f;
+  long o = 0;
+  if (active) {
+    const double4 p = gpos[ti];
+    o = perm[ti];
+    const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+    tx = (float)dx, ty = (float)dy, tz = (float)dz;
+    tlx = (float)(dx - (double)tx), tly = (float)(dy - (double)ty), tlz = (float)(dz - (double)tz);
+    tq = (float)qcaller[o];
+  }
+  th[lane] = make_float4(tx, ty, tz, tq);
+  tl[lane] = make_float4(tlx, tly, tlz, 0.f);
+  __syncwarp();
+  const float R2 = k.R2;
+  double acc[4] = {0, 0, 0, 0};
+  {  // pairs inside the group, target side only, differences always refined
+    float aV = 0.f, aX = 0.f, aY = 0.f, aZ = 0.f;
+    for (int s = 0; s < G.y; s++) {
+      const float4 S = th[s], L = tl[s];
+      const float x = (tx - S.x) + (tlx - L.x), y = (ty - S.y) + (tly - L.y),
+                  z = (tz - S.z) + (tlz - L.z);
+      const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+      if (r2 <= R2 && r2 > 0.f) {
+        float f1;
+        const float f0 = pair_sr<float, FUNC, SPLIT, ND, PK>(k, r2, f1);
+        const float g = f1 * S.w;
+        aV = fmaf(f0, S.w, aV);
+        aX = fmaf(g, x, aX);
+        aY = fmaf(g, y, aY);
+        aZ = fmaf(g, z, aZ);
+      }
+    }
+    acc[0] += aV, acc[1] += aX, acc[2] += aY, acc[3] += aZ;
+  }
+  SrcCursor ca{G.z, lane};
+  ca.normalize(segs, G.w);
+  SrcCursor cb{ca.seg, ca.off + 32};
+  cb.normalize(segs, G.w);
+  bool va = ca.seg < G.w, vb = cb.seg < G.w;
+  long ja = -1, jb = -1;
+  double4 pa = make_double4(0, 0, 0, 0), pb = pa;
+  float qa = 0.f, qb = 0.f;
+  if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], qa = qs[ja];
+  if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], qb = qs[jb];
+  while (__any_sync(FULL, va)) {
+    // the lane's two sources; empty slots far away on the other side from
+    // idle targets, with charge 0
+    float sx[2] = {-1e18f, -1e18f}, sy[2] = {-1e18f, -1e18f}, sz[2] = {-1e18f, -1e18f};
+    float lx[2] = {0.f, 0.f}, ly[2] = {0.f, 0.f}, lz[2] = {0.f, 0.f}, sq[2] = {0.f, 0.f};
+    const long kidx[2] = {va ? ja : -1, vb ? jb : -1};
+    if (va) {
+      const double dx = pa.x - c.x, dy = pa.y - c.y, dz = pa.z - c.z;
+      sx[0] = (float)dx, sy[0] = (float)dy, sz[0] = (float)dz;
+      lx[0] = (float)(dx - (double)sx[0]), ly[0] = (float)(dy - (double)sy[0]);
+      lz[0] = (float)(dz - (double)sz[0]);
+      sq[0] = qa;
+    }
+    if (vb) {
+      const double dx = pb.x - c.x, dy = pb.y - c.y, dz = pb.z - c.z;
+      sx[1] = (float)dx, sy[1] = (float)dy, sz[1] = (float)dz;
+      lx[1] = (float)(dx - (double)sx[1]), ly[1] = (float)(dy - (double)sy[1]);
+      lz[1] = (float)(dz - (double)sz[1]);
+      sq[1] = qb;
+    }
+    ca.off += 64;
+    ca.normalize(segs, G.w);
+    cb.off += 64;
+    cb.normalize(segs, G.w);
+    va = ca.seg < G.w, vb = cb.seg < G.w;
+    if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], qa = qs[ja];
+    if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], qb = qs[jb];
+
+    float aV = 0.f, aX = 0.f, aY = 0.f, aZ = 0.f;  // target side, rotating
+    float S[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};  // source side
+    const int src = (lane + 1) & 31;
+    for (int kk = 0; kk < 32; kk++) {
+      const int tt = (lane + kk) & 31;
+      const float4 T = th[tt];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        float x = T.x - sx[u], y = T.y - sy[u], z = T.z - sz[u];
+        float r2 = fmaf(x, x, fmaf(y, y, z * z));
+        if (r2 <= R2 && r2 > 0.f) {
+          if (r2 < refine2) {  // close pair: exact difference from head + residual
+            const float4 L = tl[tt];
+            x += L.x - lx[u];
+            y += L.y - ly[u];
+            z += L.z - lz[u];
+            r2 = fmaf(x, x, fmaf(y, y, z * z));
+          }
+          float f1;
+          const float f0 = pair_sr<float, FUNC, SPLIT, ND, PK>(k, r2, f1);
+          const float g = f1 * sq[u], gs = f1 * T.w;
+          aV = fmaf(f0, sq[u], aV);
+          aX = fmaf(g, x, aX);
+          aY = fmaf(g, y, aY);
+          aZ = fmaf(g, z, aZ);
+          S[u][0] = fmaf(f0, T.w, S[u][0]);
+          S[u][1] = fmaf(-gs, x, S[u][1]);
+          S[u][2] = fmaf(-gs, y, S[u][2]);
+          S[u][3] = fmaf(-gs, z, S[u][3]);
+        }
+      }
+      aV = __shfl_sync(FULL, aV, src);
+      aX = __shfl_sync(FULL, aX, src);
+      aY = __shfl_sync(FULL, aY, src);
+      aZ = __shfl_sync(FULL, aZ, src);
+    }
+    acc[0] += aV, acc[1] += aX, acc[2] += aY, acc[3] += aZ;
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+      if (kidx[u] >= 0) atomicAdd(vsrc + kidx[u], make_float4(S[u][0], S[u][1], S[u][2], S[u][3]));
+  }
+  if (active) {
+    acc[0] -= fself_r * qcaller[o];  // src/Interface.cpp:2061-2062
+    reinterpret_cast<double4 *>(V)[o] = make_double4(acc[0], acc[1], acc[2], acc[3]);
+  }
+}
+
 // FP64 direct sum of one warp group with every unordered pair evaluated once
 // (the FP64 counterpart of direct_group_sym, for the real kernels): the
 // group's targets (x, y, z, q) sit in shared memory, each lane holds two

@@ -200,6 +200,24 @@ static void sym_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   h->launches++;
 }
 
+// FP32 form with the scalar pair kernel (original Ewald split).
+template <int FUNC, int SPLIT, int ND>
+__global__ void __launch_bounds__(32 * kGroupWarps) direct_sym_scalar_kernel(
+    PairCoef<float> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    float refine2, double fself_r, double *__restrict__ V, float4 *__restrict__ vsrc) {
+  __shared__ float4 th[kGroupWarps][32];  // group targets: heads, q
+  __shared__ float4 tl[kGroupWarps][32];  // residuals
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  direct_group_sym_scalar<FUNC, SPLIT, ND>(k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs,
+                                           perm, refine2, fself_r, V, vsrc, th[wid], tl[wid],
+                                           lane);
+}
+
 // FP64 form for the real built-in kernels (DM and original Ewald).
 template <int FUNC, int SPLIT, int ND>
 __global__ void __launch_bounds__(32 * kGroupWarps) direct_sym64_kernel(
@@ -255,18 +273,16 @@ static void sym64_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
 }
 
 // The pair-once form applies to the built-in kernels: in FP32 the DM kernels
-// (1/r, r^alpha, Helmholtz) with a tabulated derivative order, in FP64 the
-// real kernels, original Ewald split and any order included; everything else
-// (FP32 original Ewald, FP64 Helmholtz, caller-defined kernels) walks the
-// full segments.
+// (1/r, r^alpha, Helmholtz) with a tabulated derivative order and the
+// original Ewald split, in FP64 the real kernels (any order, original Ewald
+// included); FP64 Helmholtz and caller-defined kernels walk the full segments.
 bool pairs_once(const npme_handle *h) {
   if (!h->use_sym || h->user_kernel || h->n_hgroups == 0) return false;
   const int f = h->p.funcType, nd = h->p.nDeriv;
   const bool tabulated = nd == 3 || nd == 6 || nd == 8;
   if (f == NPME_FUNC_HELMHOLTZ) return h->fp32 && tabulated;
   if (f != NPME_FUNC_LAPLACE && f != NPME_FUNC_RALPHA) return false;
-  if (!h->fp32) return true;
-  if (h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) return false;
+  if (!h->fp32 || h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) return true;
   return tabulated;
 }
 
@@ -277,6 +293,20 @@ static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
     if (nd == 3) sym_helm_launch_nd<3>(h, a, s);
     else if (nd == 6) sym_helm_launch_nd<6>(h, a, s);
     else sym_helm_launch_nd<8>(h, a, s);
+    return true;
+  }
+  if (h->fp32 && h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) {
+    const long blocks = (h->n_hgroups + kGroupWarps - 1) / kGroupWarps;
+    if (blocks > 0) {
+      direct_sym_scalar_kernel<0, 1, 0><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
+          make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
+          h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2,
+          a.fself_r, a.V, h->d_vsrc);
+      const long n = (long)h->n;
+      merge_source_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->d_vsrc, h->d_sperm, n,
+                                                                        1.0, 1.0, a.V);
+      h->launches++;
+    }
     return true;
   }
   if (!h->fp32) {

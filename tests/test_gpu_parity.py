@@ -239,13 +239,14 @@ def _direct(w, c, q, torch, prec="fp32"):
                                   "helmholtz_dm_small", "laplace_orig_small"])
 def test_pairs_once_matches_both_sides(name, prec, monkeypatch):
     # the built-in kernels evaluate every pair once, for both of its points
-    # (NPME_PAIRS_ONCE=0 selects the one-sided walk): FP32 DM kernels, FP64
-    # real kernels; the two forms agree to rounding and both match the oracle
+    # (NPME_PAIRS_ONCE=0 selects the one-sided walk): all of them in FP32,
+    # the real ones in FP64; the two forms agree to rounding and both match
+    # the oracle
     torch = pytest.importorskip("torch")
     w = SMALL[name]
     c, q = w.generate()
     Vo = ob.direct(ob.params_from_workload(w), c, q)
-    expect = (w.split == "dm") if prec == "fp32" else not np.iscomplexobj(q)
+    expect = prec == "fp32" or not np.iscomplexobj(q)
     got = {}
     for mode in ("0", "1"):
         monkeypatch.setenv("NPME_PAIRS_ONCE", mode)
