@@ -37,7 +37,8 @@
 //
 // The spreading, FFTs, kernel multiply and interpolation are the library's;
 // this header instantiates the three kernel-dependent launches: the direct
-// sum (FP32 or FP64 warp-group body with the functor's sr),
+// sum (every pair once for real kernels, the one-sided warp-group body for
+// complex ones, with the functor's sr / sr_c),
 // the sampling of f_LR for the kernel transform and the exact sum.
 #pragma once
 
@@ -123,6 +124,41 @@ __global__ void __launch_bounds__(32 * npme::kGroupWarps) groups64_kernel(
   npme::direct_group_fp64<is_complex<K>::value, NPME_FUNC_USER, 0, 0, Pair<K>>(
       k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, fself, fself_i, V, sp[wid],
       sqi[wid], lane);
+}
+
+// Real kernels: every pair once (the pair-once walk of the built-in kernels)
+template <class K>
+__global__ void __launch_bounds__(32 * npme::kGroupWarps) sym_kernel(
+    npme::PairCoef<float> k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
+    const float *__restrict__ qs, const double *__restrict__ qcaller,
+    const int4 *__restrict__ groups, const double4 *__restrict__ gcen,
+    const int2 *__restrict__ segs, const uint32_t *__restrict__ perm, long ngroups,
+    float refine2, double fself, double *__restrict__ V, float4 *__restrict__ vsrc) {
+  __shared__ float4 th[npme::kGroupWarps][32];
+  __shared__ float4 tl[npme::kGroupWarps][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * npme::kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  npme::direct_group_sym_scalar<NPME_FUNC_USER, 0, 0, Pair<K>>(
+      k, gpos, spos, qs, qcaller, groups[g], gcen[g], segs, perm, refine2, fself, V, vsrc,
+      th[wid], tl[wid], lane);
+}
+
+template <class K>
+__global__ void __launch_bounds__(32 * npme::kGroupWarps) sym64_kernel(
+    npme::PairCoef<double> k, const double4 *__restrict__ gpos,
+    const double4 *__restrict__ spos, const double *__restrict__ qs,
+    const double *__restrict__ qcaller, const int4 *__restrict__ groups,
+    const double4 *__restrict__ gcen, const int2 *__restrict__ segs,
+    const uint32_t *__restrict__ perm, long ngroups, double fself, double *__restrict__ V,
+    double *__restrict__ vsrc) {
+  __shared__ double4 tsm[npme::kGroupWarps][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long g = (long)blockIdx.x * npme::kGroupWarps + wid;
+  if (g >= ngroups) return;  // warp-uniform
+  npme::direct_group_sym64<NPME_FUNC_USER, 0, 0, Pair<K>>(k, gpos, spos, qs, qcaller, groups[g],
+                                                         gcen[g], segs, perm, fself, V, vsrc,
+                                                         tsm[wid], lane);
 }
 
 template <class K>
@@ -218,6 +254,23 @@ template <class K>
 int direct(npme_handle *h, const void *args, void *stream) {
   const npme::DirectArgs &a = *static_cast<const npme::DirectArgs *>(args);
   cudaStream_t s = (cudaStream_t)stream;
+  if (npme::pairs_once(h)) {  // real kernel: the half-shell walk, then the source-side sums
+    const long blocks = (h->n_hgroups + npme::kGroupWarps - 1) / npme::kGroupWarps;
+    if (blocks == 0) return NPME_OK;
+    if (h->fp32)
+      sym_kernel<K><<<(unsigned)blocks, 32 * npme::kGroupWarps, 0, s>>>(
+          npme::make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
+          h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2,
+          a.fself_r, a.V, h->d_vsrc);
+    else
+      sym64_kernel<K><<<(unsigned)blocks, 32 * npme::kGroupWarps, 0, s>>>(
+          npme::make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
+          h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, a.fself_r, a.V,
+          h->d_vsrc64);
+    if (cudaGetLastError() != cudaSuccess) return NPME_ECUDA;
+    npme::launch_merge_source(h, a.V, s, 1.0, 1.0);
+    return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+  }
   if (h->fp32) {
     const long blocks = (h->n_groups + npme::kGroupWarps - 1) / npme::kGroupWarps;
     if (blocks == 0) return NPME_OK;

@@ -180,9 +180,7 @@ static void sym_helm_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t
       make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
       h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2,
       a.fself_r, a.fself_i, a.V, h->d_vsrc);
-  const long n = (long)h->n;
-  merge_source_cplx_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->d_vsrc, h->d_sperm, n,
-                                                                        a.V);
+  launch_merge_source(h, a.V, s, 1.0, 1.0);
   h->launches++;
 }
 
@@ -194,9 +192,7 @@ static void sym_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   direct_sym_kernel<FUNC, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
       k, h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller, h->d_hgroups, h->d_hcen,
       h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2, a.fself_r, a.V, h->d_vsrc);
-  const long n = (long)h->n;
-  merge_source_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->d_vsrc, h->d_sperm, n,
-                                                                    k.vscale, k.gscale, a.V);
+  launch_merge_source(h, a.V, s, k.vscale, k.gscale);
   h->launches++;
 }
 
@@ -256,9 +252,7 @@ static void sym64_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s)
       make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
       h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, a.fself_r, a.V,
       h->d_vsrc64);
-  const long n = (long)h->n;
-  merge_source64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
-      reinterpret_cast<double4 *>(h->d_vsrc64), h->d_sperm, n, a.V);
+  launch_merge_source(h, a.V, s, 1.0, 1.0);
   h->launches++;
 }
 
@@ -272,12 +266,25 @@ static void sym64_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   }
 }
 
+void launch_merge_source(npme_handle *h, double *V, cudaStream_t s, double vs, double gs) {
+  const long n = (long)h->n;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (!h->fp32)
+    merge_source64_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<double4 *>(h->d_vsrc64),
+                                                 h->d_sperm, n, V);
+  else if (h->complex_kernel)
+    merge_source_cplx_kernel<<<blocks, 256, 0, s>>>(h->d_vsrc, h->d_sperm, n, V);
+  else
+    merge_source_kernel<<<blocks, 256, 0, s>>>(h->d_vsrc, h->d_sperm, n, vs, gs, V);
+}
+
 // The pair-once form applies to the built-in kernels: in FP32 the DM kernels
 // (1/r, r^alpha, Helmholtz) with a tabulated derivative order and the
 // original Ewald split, in FP64 the real kernels (any order, original Ewald
 // included); FP64 Helmholtz and caller-defined kernels walk the full segments.
 bool pairs_once(const npme_handle *h) {
-  if (!h->use_sym || h->user_kernel || h->n_hgroups == 0) return false;
+  if (!h->use_sym || h->n_hgroups == 0) return false;
+  if (h->user_kernel) return !h->complex_kernel;  // the functor's scalar pair kernel
   const int f = h->p.funcType, nd = h->p.nDeriv;
   const bool tabulated = nd == 3 || nd == 6 || nd == 8;
   if (f == NPME_FUNC_HELMHOLTZ) return h->fp32 && tabulated;
@@ -302,9 +309,7 @@ static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
           make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
           h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2,
           a.fself_r, a.V, h->d_vsrc);
-      const long n = (long)h->n;
-      merge_source_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->d_vsrc, h->d_sperm, n,
-                                                                        1.0, 1.0, a.V);
+      launch_merge_source(h, a.V, s, 1.0, 1.0);
       h->launches++;
     }
     return true;

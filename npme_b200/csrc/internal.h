@@ -177,6 +177,10 @@ struct DirectArgs {
 // true when the direct sum takes the pair-once form (FP32 real DM kernels
 // with the half-shell lists built)
 bool pairs_once(const npme_handle *h);
+// V[caller(s)] += the source-side sums of the pair-once walk (times vs for
+// the potential, gs for the gradient; FP32 real, FP32 complex or FP64 by the
+// handle), and zeroes them for the next call
+void launch_merge_source(npme_handle *h, double *V, cudaStream_t s, double vs, double gs);
 void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
 void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s);
 // caller-order charges (double) -> direct-sum order in the bulk precision

@@ -89,6 +89,28 @@ def test_user_kernel_matches_its_exact_sum(user_lib, precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_real_user_kernel_pairs_once(user_lib, precision, monkeypatch):
+    """A real caller kernel takes the pair-once walk (every pair evaluated once,
+    for both points); NPME_PAIRS_ONCE=0 gives the one-sided walk, same result."""
+    import npme_b200
+    from npme_b200 import api
+    L = ctypes.CDLL(user_lib)
+    ops = api.UserOps()
+    L.screened_ops(ctypes.byref(ops))
+    c, q = _system()
+    p = api.make_params("user", "dm", Rdir=8.0, order=8, grid=(64, 64, 64), precision=precision)
+    got = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("NPME_PAIRS_ONCE", mode)
+        with npme_b200.Solver(p) as s:
+            s.set_user_kernel(ops).setup(c)
+            got[mode] = s.calcv(q)
+            assert s.info()["pairsOnce"] == (mode == "1")
+    assert rel(got["1"], got["0"]) < (1e-13 if precision == "fp64" else 1e-6)
+
+
+@pytest.mark.gpu
 def test_user_erf_coulomb_equals_builtin_original_ewald(user_lib):
     """1/r with the erf split written as a caller functor gives the library's
     own original-Ewald result (same beta)."""
