@@ -302,7 +302,12 @@ int npme_gpu_choose_grid(const npme_params *p, size_t n, const double *coord,
  * direct sum's warp groups. */
 int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs);
 
-/* Record per-stage CUDA-event timings for subsequent calcv calls. */
+/* Record per-stage CUDA-event timings for subsequent calcv calls (read back
+ * with npme_gpu_get_info).  enable = 1: the direct sum stays beside the
+ * reciprocal chain on the second stream, so the chain's event pairs include
+ * waiting for SMs the direct sum holds; enable = 2: the direct sum starts
+ * after the reciprocal chain, so that every stage's event pair times that
+ * stage alone (the call takes ~1 % longer); 0: off. */
 int npme_gpu_set_timing(npme_handle *h, int enable);
 
 int npme_gpu_get_info(const npme_handle *h, npme_info *info);

@@ -298,8 +298,10 @@ class Solver:
         self._check(self.L.npme_gpu_count_pairs(self.h, ctypes.byref(c)))
         return int(c.value)
 
-    def set_timing(self, on=True):
-        self._check(self.L.npme_gpu_set_timing(self.h, int(bool(on))))
+    def set_timing(self, on=True, serial=False):
+        """Stage timings for later calls; serial=True runs the direct sum after
+        the reciprocal chain so each stage is timed alone."""
+        self._check(self.L.npme_gpu_set_timing(self.h, (2 if serial else 1) if on else 0))
 
     def info(self):
         i = Info()

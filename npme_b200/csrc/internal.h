@@ -46,6 +46,7 @@ struct BrickPoint {
 
 struct Timing {
   bool enabled = false;
+  bool serial = false;  // the direct sum after the reciprocal chain (stage attribution)
   cudaEvent_t ev[10] = {};
 };
 

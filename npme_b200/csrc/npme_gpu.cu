@@ -987,26 +987,34 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   npme::launch_gather_charges(h, d_charge, s);
   CK(cudaGetLastError());  // launch errors are checked before cuFFT runs
   tmark(h, 1, s);
-  // the direct sum runs on stream2, overlapped with the reciprocal sum
-  CK(cudaEventRecord(h->ev_fork, s));
-  CK(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
-  tmark(h, 8, h->stream2);
-  npme::launch_direct(h, d_charge, d_V, h->stream2);
-  CK(cudaGetLastError());
-  tmark(h, 9, h->stream2);
-  CK(cudaEventRecord(h->ev_join, h->stream2));
+  // the direct sum runs on stream2 beside the reciprocal sum; in the serial
+  // timing mode it starts after the reciprocal chain, so that each stage's
+  // events time that stage alone
+  const bool serial = h->timing.enabled && h->timing.serial;
+  auto fork_direct = [&]() -> int {
+    CK(cudaEventRecord(h->ev_fork, s));
+    CK(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
+    tmark(h, 8, h->stream2);
+    npme::launch_direct(h, d_charge, d_V, h->stream2);
+    CK(cudaGetLastError());
+    tmark(h, 9, h->stream2);
+    CK(cudaEventRecord(h->ev_join, h->stream2));
+    return NPME_OK;
+  };
+  int frc;
+  if (!serial && (frc = fork_direct())) return frc;
   CK(cudaMemsetAsync(h->d_grid, 0, gbytes, s));
   npme::launch_spread(h, s);
   CK(cudaGetLastError());
   tmark(h, 2, s);
-  int frc = npme::fft_forward(h, s);
-  if (frc) return frc;
+  if ((frc = npme::fft_forward(h, s))) return frc;
   tmark(h, 3, s);
   npme::launch_multiply(h, s);
   CK(cudaGetLastError());
   tmark(h, 4, s);
   if ((frc = npme::fft_inverse(h, s))) return frc;
   tmark(h, 5, s);
+  if (serial && (frc = fork_direct())) return frc;
   CK(cudaStreamWaitEvent(s, h->ev_join, 0));
   tmark(h, 6, s);
   npme::launch_interp(h, d_V, s);
@@ -1159,7 +1167,9 @@ int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs) {
 
 int npme_gpu_set_timing(npme_handle *h, int enable) {
   if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (enable < 0 || enable > 2) return fail(h, NPME_EINVAL, "timing mode must be 0, 1 or 2");
   h->timing.enabled = enable != 0;
+  h->timing.serial = enable == 2;
   return NPME_OK;
 }
 

@@ -176,6 +176,25 @@ def test_degenerate_planar_and_linear_geometry(prec):
         assert rel(s.setup(c).calcv(q), Vo) < (1e-11 if prec == "fp64" else 1e-5)
 
 
+def test_timing_modes_leave_results_unchanged():
+    # stage timing beside the reciprocal chain (1) and after it (2, serial)
+    w = SMALL["laplace_dm_4k"]
+    c, q = w.generate()
+    with solver(w, "fp32") as s:
+        V0 = s.calcv(q)
+        for serial in (False, True):
+            s.set_timing(True, serial=serial)
+            V = s.calcv(q)
+            st = s.info()["stage_ms"]
+            assert rel(V, V0) < 1e-6
+            assert all(v >= 0.0 for v in st.values()) and st["direct"] > 0.0
+            assert st["total"] >= st["direct"]
+        s.set_timing(False)
+        with pytest.raises(api.NPMEError) as e:
+            s._check(s.L.npme_gpu_set_timing(s.h, 3))
+        assert e.value.code == api.EINVAL
+
+
 def test_call_order_and_argument_errors():
     w = SMALL["laplace_dm_4k"]
     c, q = w.generate()
