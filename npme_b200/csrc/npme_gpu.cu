@@ -503,6 +503,9 @@ int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &ord
     nsegs += pt.segs.size(), nhsegs += pt.hsegs.size();
     cand += pt.cand, hcand += pt.hcand;
   }
+  // group records hold segment indices as int
+  if (nsegs >= ((size_t)1 << 31) || nhsegs >= ((size_t)1 << 31))
+    return fail(h, NPME_EINVAL, "too many direct-sum source segments (2^31)");
   // heaviest groups first, so the last wave of the launch holds the light
   // ones (each list by its own work)
   auto by_work = [](std::vector<int4> &gl, const std::vector<long> &wk,
