@@ -57,6 +57,11 @@ __device__ __forceinline__ float exp_t(float x) { return expf(x); }
 __device__ __forceinline__ double exp_t(double x) { return exp(x); }
 __device__ __forceinline__ float pow_t(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ double pow_t(double x, double y) { return pow(x, y); }
+// x^y for x > 0 as 2^(y log2 x): the r^alpha kernel's power; in FP64 about
+// 5e-16 relative (log2 and exp2 each within an ulp, |y log2 x| < ~8 here),
+// cheaper than pow's special-case handling
+__device__ __forceinline__ float rpow_t(float x, float y) { return powf(x, y); }
+__device__ __forceinline__ double rpow_t(double x, double y) { return exp2(y * log2(x)); }
 __device__ __forceinline__ float erfc_t(float x) { return erfcf(x); }
 __device__ __forceinline__ double erfc_t(double x) { return erfc(x); }
 __device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
@@ -155,7 +160,7 @@ __device__ __forceinline__ T pair_sr_real(const PairCoef<T> &k, T r2, T &f1) {
     f1 = -rinv * rinv * rinv - g1;
     return rinv - g0;
   } else {
-    const T e0 = pow_t(r2, k.half_alpha);
+    const T e0 = rpow_t(r2, k.half_alpha);
     f1 = k.alpha * e0 / r2 - g1;
     return e0 - g0;
   }
