@@ -112,10 +112,10 @@ struct npme_handle {
   double *d_flam[3] = {nullptr, nullptr, nullptr};
   double *d_fcos[3] = {nullptr, nullptr, nullptr};
 
-  // FP32 direct sum: warp groups of <= 32 z-sorted points of one xy column
-  // and, per group, the source segments (neighbour-column z ranges) that can
-  // hold a point within Rdir of the group.  Built once per geometry.
-  bool use_groups = false;
+  // direct sum (both precisions): warp groups of <= 32 z-sorted points of
+  // one xy column and, per group, the source segments (neighbour-column z
+  // ranges) that can hold a point within Rdir of the group.  Built once per
+  // geometry.
   long n_groups = 0, n_segs = 0;
   double cand_per_point = 0;     // staged source candidates per target point
   double refine2 = 0;            // r^2 below which pair differences are refined

@@ -935,9 +935,9 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
     h->grid.nb[d] = (Ns[d] / 2 + npme::kBrick - 1) / npme::kBrick;
   }
   h->grid.order = p.BnOrder;
-  // cells of edge >= Rdir / nNeigh
+  // the reference's cells of edge >= Rdir / nNeigh (reported by
+  // npme_gpu_get_info; the direct sum walks warp groups instead)
   const double target = p.Rdir / p.nNeigh;
-  long ncells = 1;
   for (int d = 0; d < 3; d++) {
     const double ext = mx[d] - mn[d];
     int nc = (int)std::floor(ext / target);
@@ -945,12 +945,8 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
     h->cells.nc[d] = nc;
     h->cells.edge[d] = (nc == 1) ? std::max(ext, target) : ext / nc;
     h->cells.origin[d] = mn[d];
-    ncells *= nc;
   }
-  if (ncells > (1L << 30)) return fail(h, NPME_EINVAL, "too many direct-sum cells");
   h->cells.reach = p.nNeigh;
-  // both precisions walk warp groups
-  h->use_groups = true;
   // the built-in kernels evaluate every pair once unless NPME_PAIRS_ONCE=0
   {
     const char *e = std::getenv("NPME_PAIRS_ONCE");
