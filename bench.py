@@ -419,13 +419,24 @@ def main():
 
             def rr(a, b):
                 return float(np.linalg.norm(a - b) / np.linalg.norm(b))
-            extra["accuracy_vs_exact_fp64"] = {
-                "fp32_bulk": {"rel_rms_V": rr(V32[:, 0], Ve[:, 0]),
-                              "rel_rms_gradV": rr(V32[:, 1:], Ve[:, 1:]),
-                              "max_abs_dV_over_max_V": float(np.abs(V32[:, 0] - Ve[:, 0]).max()
-                                                             / np.abs(Ve[:, 0]).max())},
-                "plain_fp64": {"rel_rms_V": rr(V64[:, 0], Ve[:, 0]),
-                               "rel_rms_gradV": rr(V64[:, 1:], Ve[:, 1:])}}
+
+            def acc(V):
+                dG = np.linalg.norm(V[:, 1:] - Ve[:, 1:], axis=1)
+                # the reference's own relative errors (src/SupportFunctions.cpp:88-119):
+                # RMS error over the mean |V|; for the gradient over the mean of
+                # |V1[4i+p]|, p = 0..2, as its loop takes it (potential, d/dx, d/dy)
+                errV = np.sqrt(np.mean(np.abs(V[:, 0] - Ve[:, 0]) ** 2))
+                errG = np.sqrt(np.mean(np.abs(V[:, 1:] - Ve[:, 1:]) ** 2))
+                return {"rel_rms_V": rr(V[:, 0], Ve[:, 0]),
+                        "rel_rms_gradV": rr(V[:, 1:], Ve[:, 1:]),
+                        "max_abs_dV_over_max_V": float(np.abs(V[:, 0] - Ve[:, 0]).max()
+                                                       / np.abs(Ve[:, 0]).max()),
+                        "max_abs_dgradV_over_max_gradV": float(
+                            dG.max() / np.linalg.norm(Ve[:, 1:], axis=1).max()),
+                        "reference_metric": {
+                            "eps_V": float(errV / np.mean(np.abs(Ve[:, 0]))),
+                            "eps_gradV": float(errG / np.mean(np.abs(Ve[:, :3])))}}
+            extra["accuracy_vs_exact_fp64"] = {"fp32_bulk": acc(V32), "plain_fp64": acc(V64)}
             s64.close()
 
     if rank == 0:
