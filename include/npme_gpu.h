@@ -172,7 +172,12 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge,
  * (src/PotentialLaplace.h:33-44), NPME_PotHelmholtz_SR_DM_DirectSum_V1
  * (src/PotentialHelmholtz.cpp:194) and NPME_PotGenFunc_DirectSum_V1
  * (src/PotentialGenFunc.cpp:140) for the set-up geometry.  Layouts and
- * stream semantics as npme_gpu_calcv_device. */
+ * stream semantics as npme_gpu_calcv_device.  Like the reference's cell-pair
+ * loops it evaluates every pair once for both points (built-in kernels and
+ * real caller kernels; complex caller kernels and FP64 Helmholtz walk each
+ * target's sources), adding the source-side sums with atomics, so repeated
+ * calls can differ in the last bits (NPME_PAIRS_ONCE=0 at set-up: one-sided,
+ * reproducible). */
 int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_charge,
                                void *stream);
 
@@ -186,7 +191,9 @@ int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_char
  * FP64 real) or 524,288 (FP64 complex); larger handles get NPME_EINVAL.  The
  * first call on a device looks the array up (and loads the module): make it
  * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU race.  Output and arguments as npme_gpu_direct_sum_device. */
+ * the GPU race.  The source-side sums of the pair-once walk go to a buffer
+ * of the handle that npme_gpu_setup allocated.  Output and arguments as
+ * npme_gpu_direct_sum_device. */
 int npme_gpu_direct_sum_device_noalloc(npme_handle *h, double *d_V,
                                        const double *d_charge, void *stream);
 
