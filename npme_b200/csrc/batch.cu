@@ -48,6 +48,11 @@ struct BatchSys {
   const int4 *groups;
   const double4 *gcen;
   const int2 *segs;
+  // pair-once walk: half-shell groups and segments, source-side sums
+  const int4 *hgroups;
+  const double4 *hcen;
+  const int2 *hsegs;
+  float4 *vsrc;
   float refine2;
   double fself_r, fself_i;
 };
@@ -134,6 +139,70 @@ __global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) batch_direc
   direct_group_body<CPLX, FUNC, SPLIT, ND>(k, S.gpos, S.spos, S.qc, S.q, S.groups[g], S.gcen[g],
                                            S.segs, S.cperm, S.refine2, S.fself_r, S.fself_i, S.V,
                                            sp[wid], slo[wid], lane);
+}
+
+// Pair-once direct sums of a batch (direct_group_sym and its complex and
+// scalar forms): KIND 0 the packed real DM body, 1 Helmholtz DM, 2 the scalar
+// body of the original Ewald split.
+template <int KIND, int FUNC, int ND>
+__global__ void __launch_bounds__(32 * kGroupWarps) batch_sym_kernel(
+    PairCoef<float> k, const BatchSys *__restrict__ sys, const long long *__restrict__ off,
+    int count) {
+  __shared__ float4 ta[kGroupWarps][32];
+  __shared__ float4 tb[kGroupWarps][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long u = (long long)blockIdx.x * kGroupWarps + wid;
+  if (u >= off[count]) return;  // warp-uniform
+  const int s = find_sys(off, count, u);
+  const BatchSys &S = sys[s];
+  const long g = (long)(u - off[s]);
+  if constexpr (KIND == 0)
+    direct_group_sym<FUNC, ND>(k, S.gpos, S.spos, S.qc, S.q, S.hgroups[g], S.hcen[g], S.hsegs,
+                               S.cperm, S.refine2, S.fself_r, S.V, S.vsrc, ta[wid], tb[wid],
+                               lane);
+  else if constexpr (KIND == 1)
+    direct_group_sym_helm<ND>(k, S.gpos, S.spos, S.qc, S.q, S.hgroups[g], S.hcen[g], S.hsegs,
+                              S.cperm, S.refine2, S.fself_r, S.fself_i, S.V, S.vsrc, ta[wid],
+                              tb[wid], lane);
+  else
+    direct_group_sym_scalar<0, 1, 0>(k, S.gpos, S.spos, S.qc, S.q, S.hgroups[g], S.hcen[g],
+                                     S.hsegs, S.cperm, S.refine2, S.fself_r, S.V, S.vsrc,
+                                     ta[wid], tb[wid], lane);
+}
+
+// V[caller(j)] += the source-side sums of source j (scaled by vs for the
+// potential, gs for the gradient; complex: re, im pairs), then zero them.
+template <bool CPLX>
+__global__ void batch_merge_kernel(const BatchSys *__restrict__ sys,
+                                   const long long *__restrict__ off, int count, double vs,
+                                   double gs) {
+  const long long total = off[count];
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total;
+       u += (long long)gridDim.x * blockDim.x) {
+    const int s = find_sys(off, count, u);
+    const BatchSys &S = sys[s];
+    const long j = (long)(u - off[s]);
+    double4 *o = reinterpret_cast<double4 *>(S.V);
+    if (CPLX) {
+      o += 2 * (long)S.dperm[j];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const float4 a = S.vsrc[2 * j + h];
+        S.vsrc[2 * j + h] = make_float4(0.f, 0.f, 0.f, 0.f);
+        double4 v = o[h];
+        v.x += a.x, v.y += a.y, v.z += a.z, v.w += a.w;
+        o[h] = v;
+      }
+    } else {
+      o += S.dperm[j];
+      const float4 a = S.vsrc[j];
+      S.vsrc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      double4 v = *o;
+      v.x += vs * (double)a.x, v.y += gs * (double)a.y;
+      v.z += gs * (double)a.z, v.w += gs * (double)a.w;
+      *o = v;
+    }
+  }
 }
 
 }  // namespace npme
@@ -285,6 +354,10 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     S.groups = h->d_groups;
     S.gcen = h->d_gcen;
     S.segs = h->d_segs;
+    S.hgroups = h->d_hgroups;
+    S.hcen = h->d_hcen;
+    S.hsegs = h->d_hsegs;
+    S.vsrc = h->d_vsrc;
     S.refine2 = (float)h->refine2;
     S.fself_r = h->fself_r;
     S.fself_i = h->fself_i;
@@ -293,17 +366,18 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   // launch classes
   std::map<int, Class> gath, mult;                           // key: complex
   std::map<std::pair<int, int>, Class> spr;                  // (order, complex)
-  typedef std::tuple<int, int, int, double, double, double, double, double> DKey;
-  std::map<DKey, Class> dir;
+  typedef std::tuple<int, int, int, int, double, double, double, double, double> DKey;
+  std::map<DKey, Class> dir, mrg;  // direct sums; source-side merges of pair-once classes
   for (int k = 0; k < m; k++) {
     const npme_handle *h = hs[f32[k]];
     const int cx = h->complex_kernel ? 1 : 0;
     gath[cx].members.push_back(k);
     mult[cx].members.push_back(k);
     spr[{h->grid.order, cx}].members.push_back(k);
-    dir[DKey(h->p.funcType, h->p.EwaldSplit, h->p.nDeriv, h->p.Rdir, h->p.alpha, h->p.k0_r,
-             h->p.k0_i, h->beta)]
-        .members.push_back(k);
+    const DKey key(pairs_once(h) ? 1 : 0, h->p.funcType, h->p.EwaldSplit, h->p.nDeriv,
+                   h->p.Rdir, h->p.alpha, h->p.k0_r, h->p.k0_i, h->beta);
+    dir[key].members.push_back(k);
+    if (std::get<0>(key)) mrg[key].members.push_back(k);
   }
   auto units_gather = [&](int k) { return (long long)hs[f32[k]]->n; };
   auto units_spread = [&](int k) { return (long long)hs[f32[k]]->n_nonempty; };
@@ -312,7 +386,10 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     const long *N = h->grid.N;
     return (long long)N[0] * N[1] * (h->complex_kernel ? N[2] : N[2] / 2 + 1);
   };
-  auto units_dir = [&](int k) { return (long long)hs[f32[k]]->n_groups; };
+  auto units_dir = [&](int k) {
+    const npme_handle *h = hs[f32[k]];
+    return (long long)(pairs_once(h) ? h->n_hgroups : h->n_groups);
+  };
 
   // descriptor block layout: for every class, its descriptors then offsets
   size_t bytes = 0;
@@ -330,6 +407,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   for (auto &kv : mult) lay(kv.second, units_mult);
   for (auto &kv : spr) lay(kv.second, units_spread);  // spread and interpolation: bricks
   for (auto &kv : dir) lay(kv.second, units_dir);
+  for (auto &kv : mrg) lay(kv.second, units_gather);  // merges: source points
 
   // the pinned staging buffer is reused: wait for the previous batch's copy
   if (b->pending) {
@@ -384,6 +462,33 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     const unsigned g = (unsigned)((ng + kGroupWarps - 1) / kGroupWarps);
     const int cnt = (int)c.members.size();
     const int f = h0->p.funcType, sp = h0->p.EwaldSplit, nd = sp == 1 ? 0 : h0->p.nDeriv;
+    if (std::get<0>(kv.first)) {  // pair-once walk, then the source-side sums
+#define NPME_BSYM(KD, FN, ND) \
+  batch_sym_kernel<KD, FN, ND><<<g, 32 * kGroupWarps, 0, b->stream2>>>(k, D(c), O(c), cnt)
+#define NPME_BSYM_ND(KD, FN)                \
+  switch (nd) {                             \
+    case 3: NPME_BSYM(KD, FN, 3); break;    \
+    case 6: NPME_BSYM(KD, FN, 6); break;    \
+    default: NPME_BSYM(KD, FN, 8); break;   \
+  }
+      if (f == NPME_FUNC_HELMHOLTZ) { NPME_BSYM_ND(1, 2); }
+      else if (sp == NPME_SPLIT_LAPLACE_ORIG) { NPME_BSYM(2, 0, 0); }
+      else if (f == NPME_FUNC_RALPHA) { NPME_BSYM_ND(0, 1); }
+      else { NPME_BSYM_ND(0, 0); }
+#undef NPME_BSYM_ND
+#undef NPME_BSYM
+      b->launches++;
+      const Class &mc = mrg.at(kv.first);
+      const unsigned gm = grid_of(mc.off.back(), 256, 148 * 16);
+      const bool scaled = f != NPME_FUNC_HELMHOLTZ && sp != NPME_SPLIT_LAPLACE_ORIG;
+      if (f == NPME_FUNC_HELMHOLTZ)
+        batch_merge_kernel<true><<<gm, 256, 0, b->stream2>>>(D(mc), O(mc), cnt, 1.0, 1.0);
+      else
+        batch_merge_kernel<false><<<gm, 256, 0, b->stream2>>>(
+            D(mc), O(mc), cnt, scaled ? k.vscale : 1.0, scaled ? k.gscale : 1.0);
+      b->launches++;
+      continue;
+    }
 #define NPME_BD(CX, FN, SL, ND) \
   batch_direct_kernel<CX, FN, SL, ND><<<g, 32 * kGroupWarps, 0, b->stream2>>>(k, D(c), O(c), cnt)
 #define NPME_BD_ND(CX, FN, SL)               \
