@@ -79,6 +79,45 @@ def test_batch_equals_single_system_path():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("pairs_once", ["1", "0"])
+def test_batch_of_fixed_kernels_equals_single_path(pairs_once, monkeypatch):
+    """Batched CalcV of built-in kernels with tabulated derivative orders and
+    of the original Ewald split, with the pair-once walk and without it,
+    against each system solved alone."""
+    torch = pytest.importorskip("torch")
+    import dataclasses
+    from tests.golden.make_golden import SMALL
+    monkeypatch.setenv("NPME_PAIRS_ONCE", pairs_once)
+    names = ["laplace_dm_4k", "laplace_orig_small", "ralpha_dm_small", "helmholtz_dm_small",
+             "laplace_dm_order8"]
+    ws = [dataclasses.replace(SMALL[n], seed=SMALL[n].seed + 3) for n in names]
+    solvers, dq, dV, alone, qs = [], [], [], [], []
+    for w in ws:
+        c, q = w.generate()
+        s = npme_b200.Solver(api.params_from_workload(w, precision="fp32")).setup(c)
+        assert s.info()["pairsOnce"] == (pairs_once == "1")
+        solvers.append(s)
+        alone.append(s.calcv(q))
+        qs.append(q)
+        dq.append(torch.from_numpy(q.view(np.float64) if np.iscomplexobj(q) else q).cuda())
+        dV.append(torch.zeros((w.n, 8 if np.iscomplexobj(q) else 4), dtype=torch.float64,
+                              device="cuda"))
+    b = api.Batch(0)
+    st = torch.cuda.Stream()
+    for _ in range(2):
+        b.calcv(solvers, [x.data_ptr() for x in dV], [x.data_ptr() for x in dq], st.cuda_stream)
+        b.sync()
+        st.synchronize()
+        for w, q, V, ref in zip(ws, qs, dV, alone):
+            got = V.cpu().numpy()
+            got = got.view(np.complex128) if np.iscomplexobj(q) else got
+            assert rel(got, ref) < 1e-6, w.name
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+@pytest.mark.gpu
 def test_served_results_equal_alone_results():
     pytest.importorskip("torch")
     reqs = serving.serving_stream(count=40, n_min=1000, n_max=40_000, seed=13, rate=2000.0)
