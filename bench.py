@@ -30,7 +30,10 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-potentials/s (CalcV, potential + gradient per point)"
 UNIT = "particle-potentials/s"
 
-# algorithmic work per launch ("Roofline accounting")
+# algorithmic flops credited per unordered pair within Rdir, whatever the
+# kernel evaluates (1/r DM: distance, polynomial of order Nder for f and f1,
+# rsqrt, potential and gradient accumulation; r^alpha adds the power;
+# Helmholtz the complex arithmetic)
 DIRECT_FLOPS_PER_PAIR = {"laplace": lambda nd: 29 + 4 * nd,
                          "ralpha": lambda nd: 32 + 4 * nd,
                          "helmholtz": lambda nd: 91 + 8 * nd}
@@ -444,7 +447,7 @@ def main():
         st_alone = {k: v / n_alone for k, v in alone_sum.items()}
         peaks = measured_peaks()
         sm_mhz = clocks.get("sm_mhz") or peaks.get("clocks_under_load", {}).get("sm_mhz_median")
-        # dominant kernel: the direct sum (FP32 pipe); see DESIGN.md
+        # dominant kernel: the direct sum, bound by the FP32 (FP64) pipe
         nd = w.nDeriv
         pairs = info0.get("pairs")
         flops_pair = DIRECT_FLOPS_PER_PAIR[w.func](nd)
