@@ -188,10 +188,10 @@ int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_char
  * nothing: its scratch (the charges gathered into the direct-sum order) is a
  * static 8 MiB device array that every GPU loading the library holds until
  * exit, so at most 2,097,152 points (FP32 real), 1,048,576 (FP32 complex,
- * FP64 real) or 524,288 (FP64 complex); larger handles get NPME_EINVAL.  The
- * first call on a device looks the array up (and loads the module): make it
- * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU race.  The source-side sums of the pair-once walk go to a buffer
+ * FP64 real) or 524,288 (FP64 complex); larger handles get NPME_EINVAL.
+ * npme_gpu_setup loads the array onto its device (while the caller still
+ * allows allocation); each call looks its address up without allocating.
+ * Calls share the array: calls that overlap on the GPU race.  The source-side sums of the pair-once walk go to a buffer
  * of the handle that npme_gpu_setup allocated.  Output and arguments as
  * npme_gpu_direct_sum_device. */
 int npme_gpu_direct_sum_device_noalloc(npme_handle *h, double *d_V,

@@ -267,9 +267,9 @@ int direct(npme_handle *h, const void *args, void *stream) {
           npme::make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
           h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, a.fself_r, a.V,
           h->d_vsrc64);
-    if (cudaGetLastError() != cudaSuccess) return NPME_ECUDA;
+    if (cudaPeekAtLastError() != cudaSuccess) return NPME_ECUDA;
     npme::launch_merge_source(h, a.V, s, 1.0, 1.0);
-    return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+    return cudaPeekAtLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
   }
   if (h->fp32) {
     const long blocks = (h->n_groups + npme::kGroupWarps - 1) / npme::kGroupWarps;
@@ -285,7 +285,7 @@ int direct(npme_handle *h, const void *args, void *stream) {
         npme::make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
         h->d_groups, h->d_gcen, h->d_segs, h->d_cperm, h->n_groups, a.fself_r, a.fself_i, a.V);
   }
-  return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+  return cudaPeekAtLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
 }
 
 template <class K>
@@ -293,7 +293,7 @@ int sample_lr(npme_handle *, int M1, int M2, int M3, const double *ax, const dou
               const double *az, void *out, void *stream) {
   sample_kernel<K><<<148 * 8, 256, 0, (cudaStream_t)stream>>>(M1, M2, M3, ax, ay, az,
                                                              (double2 *)out);
-  return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+  return cudaPeekAtLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
 }
 
 template <class K>
@@ -309,7 +309,7 @@ int exact(npme_handle *h, const double *d_q, double *d_V, void *stream,
   else
     exact_kernel<K><<<blocks, kExactTile, 0, (cudaStream_t)stream>>>(h->d_coord, d_q, n, d_tidx,
                                                                       nt, d_V);
-  return cudaGetLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
+  return cudaPeekAtLastError() == cudaSuccess ? NPME_OK : NPME_ECUDA;
 }
 
 // The launch table of functor K for npme_gpu_set_user_kernel.

@@ -7,8 +7,11 @@
 // dV_i/dx = sum q_j f1_SR(r_ij) (x_i - x_j).  Targets are grouped by 32 in
 // z-sorted coarse columns and every group owns a list of source segments
 // (build_groups in npme_gpu.cu); one warp walks one group in both
-// precisions.  Each lane accumulates its target in double and writes its
-// output row once: no atomics, deterministic results.
+// precisions.  In the pair-once walk the target-side sums stay in registers
+// and each output row is written once, while the source-side sums are added
+// with float (FP32) or double (FP64) atomics into a per-source buffer that a
+// merge kernel folds into V: results are reproducible only up to the order
+// of those atomic additions.  The one-sided walk uses no atomics.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -376,9 +379,10 @@ static void groups_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   }
 }
 
-void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+int launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
+  int rc = NPME_OK;
   if (h->user_kernel) {
-    h->uops.direct(h, &a, s);
+    rc = h->uops.direct(h, &a, s);
   } else if (!sym_launch(h, a, s)) {  // both precisions walk warp groups
     const int f = h->p.funcType, sp = h->p.EwaldSplit;
     if (f == NPME_FUNC_HELMHOLTZ) groups_launch<true, 2, 0>(h, a, s);
@@ -387,11 +391,12 @@ void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
     else groups_launch<false, 0, 0>(h, a, s);
   }
   h->launches++;
+  return rc;
 }
 
-void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s) {
+int launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s) {
   DirectArgs a{h->d_qc, d_q, h->fself_r, h->fself_i, d_V};
-  launch_direct_args(h, a, s);
+  return launch_direct_args(h, a, s);
 }
 
 // Ordered pairs with 0 < r <= Rdir (FP64 distances) over the one-sided group
@@ -516,16 +521,15 @@ __global__ void __launch_bounds__(kExactBS) exact_kernel(const double *__restric
   }
 }
 
-void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s,
-                  const uint32_t *d_tidx, long nt) {
+int launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s,
+                 const uint32_t *d_tidx, long nt) {
   const long n = (long)h->n;
   if (!d_tidx) nt = n;
   const int blocks = (int)((nt + kExactBS - 1) / kExactBS);
-  if (blocks == 0) return;
+  if (blocks == 0) return NPME_OK;
   if (h->user_kernel) {
-    h->uops.exact(h, d_q, d_V, s, d_tidx, nt);
     h->launches++;
-    return;
+    return h->uops.exact(h, d_q, d_V, s, d_tidx, nt);
   }
   const int f = h->p.funcType;
   if (f == 0)
@@ -538,6 +542,7 @@ void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s
     exact_kernel<2><<<blocks, kExactBS, 0, s>>>(h->d_coord, d_q, n, h->p.alpha, h->p.k0_r,
                                                  h->p.k0_i, d_tidx, nt, d_V);
   h->launches++;
+  return NPME_OK;
 }
 
 }  // namespace npme

@@ -175,6 +175,12 @@ struct DirectArgs {
   double fself_r, fself_i;
   double *V;
 };
+// status `code` with `msg` recorded on the handle (or, for a null handle, as
+// the library's last error), as every entry point reports failures
+int record_error(npme_handle *h, int code, const std::string &msg);
+// loads the static scratch of npme_gpu_direct_sum_device_noalloc onto the
+// current device (noalloc.cu)
+int noalloc_preload(std::string &err);
 // true when the direct sum takes the pair-once form (FP32 real DM kernels
 // with the half-shell lists built)
 bool pairs_once(const npme_handle *h);
@@ -182,13 +188,15 @@ bool pairs_once(const npme_handle *h);
 // the potential, gs for the gradient; FP32 real, FP32 complex or FP64 by the
 // handle), and zeroes them for the next call
 void launch_merge_source(npme_handle *h, double *V, cudaStream_t s, double vs, double gs);
-void launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
-void launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s);
+// Both return NPME_OK, or the status a caller-defined kernel's launcher
+// reported (its launch error is not left pending for cudaGetLastError).
+int launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s);
+int launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s);
 // caller-order charges (double) -> direct-sum order in the bulk precision
 void launch_gather_direct(npme_handle *h, const double *d_q, void *d_qdst, cudaStream_t s);
 // exact O(N^2) sum; with d_tidx, only for the nt targets listed (output row t
-// = target d_tidx[t])
-void launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s,
+// = target d_tidx[t]); returns NPME_OK or a caller-defined kernel's status
+int launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s,
                   const uint32_t *d_tidx = nullptr, long nt = 0);
 void launch_count_pairs(npme_handle *h, unsigned long long *d_count, cudaStream_t s);
 template <typename T>

@@ -19,17 +19,20 @@
 // 524,288 (FP64 complex); larger systems are rejected with NPME_EINVAL.
 //
 // In host code g_direct_scratch is only a host-side stand-in for the device
-// symbol, never a device address.  The first call on each device (made with
-// that device current) looks the address up with cudaGetSymbolAddress, which
-// also loads this module onto the device; make that first call before any
-// stream capture.  All calls on a device share the one array and it keeps the
-// last call's contents: the gather overwrites every byte the sum reads, so
-// nothing has to start at zero, but calls whose work overlaps on the GPU (two
-// streams, or two handles) race on the array.  Serialise them.
+// symbol, never a device address.  Every call (with the handle's device
+// current) looks the address up with cudaGetSymbolAddress, which allocates
+// nothing once this module is on the device.  The module, and with it the
+// 8 MiB array, is loaded onto a device when npme_gpu_setup first runs there
+// (CUDA loads modules lazily by default): set-up is the point where the
+// caller still allows allocation, so the first no-allocation call does not
+// make the driver reserve memory.  Looking the address up on every call also
+// keeps it right after cudaDeviceReset or a new primary context.  All calls
+// on a device share the one array and it keeps the last call's contents: the
+// gather overwrites every byte the sum reads, so nothing has to start at
+// zero, but calls whose work overlaps on the GPU (two streams, or two
+// handles) race on the array.  Serialise them.
 #include <cuda_runtime.h>
 
-#include <map>
-#include <mutex>
 #include <string>
 
 #include "internal.h"
@@ -39,16 +42,7 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;
 __device__ __align__(256) unsigned char g_direct_scratch[kNoAllocScratchBytes];
 
-std::mutex g_scratch_mu;
-std::map<int, void *> g_scratch_addr;  // device ordinal -> device address
-
-int scratch_address(int device, void **ptr, std::string &err) {
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  auto it = g_scratch_addr.find(device);
-  if (it != g_scratch_addr.end()) {
-    *ptr = it->second;
-    return NPME_OK;
-  }
+int scratch_address(void **ptr, std::string &err) {
   void *p = nullptr;
   const cudaError_t e = cudaGetSymbolAddress(&p, g_direct_scratch);
   if (e != cudaSuccess || p == nullptr) {
@@ -56,16 +50,24 @@ int scratch_address(int device, void **ptr, std::string &err) {
           cudaGetErrorString(e);
     return NPME_ECUDA;
   }
-  g_scratch_addr[device] = p;
   *ptr = p;
   return NPME_OK;
 }
 
 }  // namespace
 
+namespace npme {
+// Loads this module (and its static array) onto the current device; called by
+// npme_gpu_setup, where allocation is still allowed.
+int noalloc_preload(std::string &err) {
+  void *p = nullptr;
+  return scratch_address(&p, err);
+}
+}  // namespace npme
+
 extern "C" int npme_gpu_direct_sum_device_noalloc(npme_handle *h, double *d_V,
                                                   const double *d_charge, void *stream) {
-  if (!h) return NPME_EINVAL;
+  if (!h) return npme::record_error(nullptr, NPME_EINVAL, "null handle");
   if (!h->ready) {
     h->err = "direct_sum_noalloc before setup";
     return NPME_ESTATE;
@@ -90,13 +92,16 @@ extern "C" int npme_gpu_direct_sum_device_noalloc(npme_handle *h, double *d_V,
     return NPME_ECUDA;
   }
   void *scratch = nullptr;
-  const int rc = scratch_address(h->device, &scratch, h->err);
+  const int rc = scratch_address(&scratch, h->err);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
   h->launches = 0;
   npme::launch_gather_direct(h, d_charge, scratch, s);
   npme::DirectArgs a{scratch, d_charge, 0.0, 0.0, d_V};
-  npme::launch_direct_args(h, a, s);
+  if (npme::launch_direct_args(h, a, s)) {
+    h->err = "direct_sum_noalloc: launch of the caller-defined kernel failed";
+    return NPME_ECUDA;
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     h->err = std::string("direct_sum_noalloc launch: ") + cudaGetErrorString(e);

@@ -209,6 +209,10 @@ int npme::handle_buffer(npme_handle *h, void **field, size_t bytes) {
   return dalloc(h, field, bytes);
 }
 
+int npme::record_error(npme_handle *h, int code, const std::string &msg) {
+  return fail(h, code, msg);
+}
+
 namespace {
 
 // Host threads for the set-up of an n-point system: the machine's cores
@@ -904,6 +908,12 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
   if (n == 0) return fail(h, NPME_EINVAL, "nCharge must be > 0");
   if (n >= (size_t)1 << 31) return fail(h, NPME_EINVAL, "nCharge must be < 2^31");
   CK(cudaSetDevice(h->device));
+  {
+    // load the no-allocation entry point's static scratch now, while the
+    // caller allows allocation (a failure shows up in that entry point)
+    std::string ignored;
+    npme::noalloc_preload(ignored);
+  }
   // A handle that was set up before keeps its buffers (grown when needed),
   // its FFT plans (the FFT box is a handle parameter) and its kernel-transform
   // scratch: only the geometry-dependent state is rebuilt (ResetCoord,
@@ -994,7 +1004,8 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
     CK(cudaEventRecord(h->ev_fork, s));
     CK(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
     tmark(h, 8, h->stream2);
-    npme::launch_direct(h, d_charge, d_V, h->stream2);
+    if (npme::launch_direct(h, d_charge, d_V, h->stream2))
+      return fail(h, NPME_ECUDA, "direct-sum launch of the caller-defined kernel failed");
     CK(cudaGetLastError());
     tmark(h, 9, h->stream2);
     CK(cudaEventRecord(h->ev_join, h->stream2));
@@ -1086,7 +1097,8 @@ static int exact_host(npme_handle *h, double *V, size_t n, const double *charge,
   CK(cudaMemcpyAsync(h->d_q_in, charge, sizeof(double) * C * n, cudaMemcpyHostToDevice,
                      h->stream));
   h->launches = 0;
-  npme::launch_exact(h, h->d_q_in, h->d_V, h->stream);
+  if (npme::launch_exact(h, h->d_q_in, h->d_V, h->stream))
+    return fail(h, NPME_ECUDA, "exact-sum launch of the caller-defined kernel failed");
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(V, h->d_V, sizeof(double) * 4 * C * n, cudaMemcpyDeviceToHost,
                      h->stream));
@@ -1112,7 +1124,8 @@ int npme_gpu_calcv_exact_subset(npme_handle *h, double *V, size_t m,
   CK(cudaMemcpyAsync(h->d_q_in, charge, sizeof(double) * C * h->n, cudaMemcpyHostToDevice,
                      h->stream));
   h->launches = 0;
-  npme::launch_exact(h, h->d_q_in, h->d_V, h->stream, h->d_tidx, (long)m);
+  if (npme::launch_exact(h, h->d_q_in, h->d_V, h->stream, h->d_tidx, (long)m))
+    return fail(h, NPME_ECUDA, "exact-sum launch of the caller-defined kernel failed");
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(V, h->d_V, sizeof(double) * 4 * C * m, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
@@ -1141,7 +1154,8 @@ int npme_gpu_direct_sum_device(npme_handle *h, double *d_V, const double *d_char
   h->launches = 0;
   npme::launch_gather_direct(h, d_charge, h->d_qc, s);
   npme::DirectArgs a{h->d_qc, d_charge, 0.0, 0.0, d_V};
-  npme::launch_direct_args(h, a, s);
+  if (npme::launch_direct_args(h, a, s))
+    return fail(h, NPME_ECUDA, "direct-sum launch of the caller-defined kernel failed");
   CK(cudaGetLastError());
   return NPME_OK;
 }

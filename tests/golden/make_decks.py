@@ -5,6 +5,8 @@ npme_b200/bin/npme without the reference tree.  Only keyword/value pairs are
 kept (the first two words of each line, as the reference's reader does).
 
     python tests/golden/make_decks.py [reference root]
+
+The reference root is the argument, else $NPME_REFERENCE.
 """
 import glob
 import json
@@ -24,7 +26,10 @@ def keywords(path):
     return kv
 
 
-def main(root="/root/reference"):
+def main(root=None):
+    root = root or os.environ.get("NPME_REFERENCE")
+    if not root:
+        sys.exit("give the reference root as an argument or in $NPME_REFERENCE")
     decks = {}
     for d in sorted(glob.glob(os.path.join(root, "test", "0[1-4]_*"))):
         name = os.path.basename(d)

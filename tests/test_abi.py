@@ -64,3 +64,21 @@ def test_order_must_fit_grid():
     with pytest.raises(api.NPMEError) as e:
         npme_b200.Solver(p)
     assert e.value.code == api.EINVAL
+
+
+def test_null_handle_errors_are_recorded():
+    # every entry point reports a null handle through npme_gpu_last_error(NULL)
+    lib = api.load_library()
+    buf = ctypes.create_string_buffer(256)
+    bad = api.make_params("laplace", "dm", 8.0, 6, grid=(64, 64, 64))
+    bad.Rdir = 0.0
+    for f in ("npme_gpu_direct_sum_device", "npme_gpu_direct_sum_device_noalloc",
+              "npme_gpu_calcv_device"):
+        with pytest.raises(api.NPMEError):  # leaves another message behind
+            npme_b200.Solver(bad)
+        lib.npme_gpu_last_error(None, buf, 256)
+        assert b"null handle" not in buf.value
+        rc = getattr(lib, f)(None, None, None, None)
+        assert rc == api.EINVAL, f
+        lib.npme_gpu_last_error(None, buf, 256)
+        assert b"null handle" in buf.value, (f, buf.value)

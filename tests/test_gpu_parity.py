@@ -6,7 +6,9 @@ Tolerances (relative RMS over all points):
   FP64 mode vs reference / oracle:        1e-12 (same algorithm, FP64 throughout)
   FP32 bulk mode vs FP64:                 V 1e-5 (the stated FP32-mode bound),
                                           gradient 3e-5
-  either mode vs the exact O(N^2) sum:    1e-4 at the full sizes (method error)
+  full sizes: FP64 vs the reference's CalcV 1e-10 (required: 1e-6);
+              FP32 bulk vs the exact O(N^2) FP64 sum on 4,096 sampled
+              targets 1e-5
 """
 import dataclasses
 import os
@@ -334,29 +336,76 @@ def test_clustered_points(prec):
 
 
 # ---------------------------------------------------------------------------
-# full benchmark sizes: size-independent properties
+# full benchmark sizes: the reference's own CalcV on identical inputs, the
+# exact O(N^2) FP64 sum on sampled targets, size-independent properties
 
 FULL = [wl.LAPLACE_1M, wl.RALPHA_500K, wl.HELMHOLTZ_250K]
+
+# FP64 mode against the reference's CalcV: the required bound is 1e-6
+# relative RMS; the two compute the same sums in FP64 and agree to ~1e-13,
+# so the test holds them to 1e-10 to catch any real difference.
+FULL_FP64_VS_REF = 1e-10
+# FP32 bulk mode against the exact FP64 sum: the stated FP32-mode bound,
+# 1e-5 relative RMS of V (measured ~4e-7 at 1M, the method's own error)
+FULL_FP32_VS_EXACT = 1e-5
+N_SAMPLE = 4096
+
+
+def exact_numpy(w, c, q, idx):
+    """Exact FP64 potential and gradient at targets idx (no self term), in
+    numpy: the check on the GPU exact kernel's sampled rows."""
+    out = np.zeros((len(idx), 4), np.complex128 if np.iscomplexobj(q) else np.float64)
+    for t, i in enumerate(idx):
+        d = c[i] - c
+        r2 = np.einsum("ij,ij->i", d, d)
+        r2[i] = 1.0
+        r = np.sqrt(r2)
+        if w.func == "laplace":
+            f0 = 1.0 / r
+            f1 = -f0 / r2
+        elif w.func == "ralpha":
+            f0 = r ** w.alpha
+            f1 = w.alpha * f0 / r2
+        else:
+            f0 = np.exp(1j * complex(w.k0) * r) / r
+            f1 = (1j * complex(w.k0) - 1.0 / r) * f0 / r
+        qq = q.copy()
+        qq[i] = 0.0
+        out[t, 0] = np.sum(qq * f0)
+        out[t, 1:] = (qq * f1) @ d
+    return out
 
 
 @pytest.mark.slow
 @pytest.mark.parametrize("w", FULL, ids=lambda w: w.name)
-def test_full_size_fp32_vs_fp64_and_exact(w):
+def test_full_size_matches_reference_and_exact(w):
+    from oracle import refbind as rb
+    if not rb.available(avx=True):
+        pytest.skip("reference build (oracle/_ref) absent")
     c, q = w.generate()
+    rp = rb.make_params(w.func, w.split, w.Rdir, w.order, nDeriv=w.nDeriv, N=w.grid,
+                        alpha=w.alpha, k0=w.k0, vecOption=1)
+    ref = rb.RefSolver(rp, c, avx=True)
+    Vref = ref.calcv(q)
+    ref.close()
+    idx = np.sort(np.random.default_rng(7).choice(w.n, N_SAMPLE, replace=False))
     with solver(w, "fp64") as s64:
         V64 = s64.calcv(q)
-        # exact sum on a sample of targets (oracle, FP64) pins the method error
-        idx = np.random.default_rng(0).choice(w.n, 400, replace=False)
-        Ve = s64.calcv_exact(q) if w.n <= 300_000 else None
+        Ve = s64.calcv_exact_subset(idx.astype(np.uint32), q)
     with solver(w, "fp32") as s32:
         V32 = s32.calcv(q)
-    assert rel(V32[:, 0], V64[:, 0]) < FP32_V_TOL
-    assert rel(V32[:, 1:], V64[:, 1:]) < FP32_G_TOL
-    if Ve is not None:
-        assert rel(V64[:, 0], Ve[:, 0]) < 1e-4
-        assert rel(V32[:, 0], Ve[:, 0]) < 1e-4
+    # the GPU exact rows themselves, against numpy on 32 of the sampled targets
+    sub = np.arange(0, N_SAMPLE, N_SAMPLE // 32)
+    assert rel(Ve[sub], exact_numpy(w, c, q, idx[sub])) < 1e-12
+    # FP64 mode = the reference's NPME result on identical inputs
+    assert rel(V64[:, 0], Vref[:, 0]) < FULL_FP64_VS_REF
+    assert rel(V64[:, 1:], Vref[:, 1:]) < FULL_FP64_VS_REF
+    # FP32 bulk within its stated tolerance of the reference and of the exact sum
+    assert rel(V32[:, 0], Vref[:, 0]) < FP32_V_TOL
+    assert rel(V32[:, 1:], Vref[:, 1:]) < FP32_G_TOL
+    assert rel(V32[idx, 0], Ve[:, 0]) < FULL_FP32_VS_EXACT
+    assert rel(V64[idx, 0], Ve[:, 0]) < FULL_FP32_VS_EXACT  # method error of the config
     # total charge-weighted potential (checksum of checksums) is stable
     e64 = np.sum(np.conj(q) * V64[:, 0])
     e32 = np.sum(np.conj(q) * V32[:, 0])
-    assert abs(e32 - e64) <= 1e-5 * abs(e64)
-    del idx
+    assert abs(e32 - e64) <= 1e-6 * abs(e64)

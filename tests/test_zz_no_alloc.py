@@ -55,6 +55,28 @@ def test_noalloc_matches_direct_sum_twice(name, prec):
     assert rel(other, -2.0 * ref) < 1e-6
 
 
+def test_noalloc_calls_leave_device_memory_unchanged():
+    # free device memory is the same before and after repeated calls: the
+    # entry point takes nothing from the driver (nor from torch's allocator)
+    torch = pytest.importorskip("torch")
+    w = SMALL["laplace_dm_4k"]
+    c, q = w.generate()
+    with npme_b200.Solver(api.params_from_workload(w, precision="fp32")) as s:
+        s.setup(c)
+        dq = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        dV = torch.zeros((w.n, 4), dtype=torch.float64, device="cuda")
+        s.direct_sum_device_noalloc(dV.data_ptr(), dq.data_ptr(), None)
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        torch_bytes0 = torch.cuda.memory_allocated()
+        for _ in range(5):
+            s.direct_sum_device_noalloc(dV.data_ptr(), dq.data_ptr(), None)
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0
+        assert torch.cuda.memory_allocated() == torch_bytes0
+
+
 def test_noalloc_rejects_systems_beyond_the_static_scratch():
     torch = pytest.importorskip("torch")
     # FP64 complex: 16 bytes of scratch per point, 8 MiB hold 524,288 points
