@@ -13,6 +13,14 @@ L2 flushed between steps); `e2e` is the same metric through the C ABI with
 pinned host buffers, host<->device copies included.  With --gpus N under
 torchrun every rank runs an independent replica (a single solve does not
 shard); value = all ranks' points / max-over-ranks time.
+
+After the headline's timed region, rank 0 adds to the same line: the plain
+FP64 port of the same workload (device-timed and end to end), accuracy
+against the exact O(N^2) FP64 sum, the reference's CPU build on the host
+cores, the r^-0.5 (500,000 points) and Helmholtz (250,000 points)
+configurations in both precisions (`other_configs`), and the first 256
+requests of the serving stream served in real time, offline, and by the
+plain FP64 port (`serving_bounded`).  --no-extra drops the last two.
 """
 import argparse
 import json
@@ -49,6 +57,8 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-port line")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other configurations and the bounded serving run")
     return ap.parse_args()
 
 
@@ -197,6 +207,137 @@ def run_reference_arm(args):
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def rel_rms(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def measure_config(w, local, stream, flush, steps, with_cpu=True):
+    """Another configuration on the same GPU, outside the headline's timed
+    region: CalcV device-timed (inputs resident in HBM, L2 flushed between
+    steps) and end to end through the C ABI (pinned host buffers), in FP32
+    bulk and in FP64, with rel-RMS errors of V and grad V against the exact
+    O(N^2) FP64 sum at 4,096 sampled points."""
+    import torch
+    import npme_b200
+    from npme_b200 import api
+    dev = torch.device("cuda", local)
+    c, q = w.generate()
+    cplx = np.iscomplexobj(q)
+    dq = torch.from_numpy(q).to(dev)
+    dV = torch.empty((w.n, 8 if cplx else 4), dtype=torch.float64, device=dev)
+    qh = torch.from_numpy(q).pin_memory().numpy()
+    Vh = torch.empty((w.n, 4), dtype=torch.complex128 if cplx else torch.float64)
+    Vh = Vh.pin_memory().numpy()
+    idx = np.sort(np.random.default_rng(7).choice(w.n, 4096, replace=False)).astype(np.uint32)
+    out = {"workload": w.name, "points": w.n, "box": list(w.box), "kernel": w.func,
+           "alpha": w.alpha, "k0": complex(w.k0).real, "BnOrder": w.order, "grid": list(w.grid),
+           "Rdir": w.Rdir, "steps": steps}
+    Ve = None
+    for prec in ("fp32", "fp64"):
+        s = npme_b200.Solver(api.params_from_workload(w, precision=prec, device=local))
+        t0 = time.perf_counter()
+        s.setup(c)
+        setup_s = time.perf_counter() - t0
+        sptr = stream.cuda_stream
+        for _ in range(3):
+            s.calcv_device(dV.data_ptr(), dq.data_ptr(), sptr)
+        torch.cuda.synchronize(dev)
+        tt = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s.calcv_device(dV.data_ptr(), dq.data_ptr(), sptr)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            tt += a.elapsed_time(b)
+        for _ in range(2):
+            s.calcv(qh, out=Vh)
+        e2e = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            s.calcv(qh, out=Vh)
+            e2e += time.perf_counter() - t0
+        V = np.array(Vh)
+        if Ve is None:
+            Ve = s.calcv_exact_subset(idx, q)
+        out[prec] = {"value": w.n * steps / (tt / 1e3), "unit": UNIT, "ms_per_step": tt / steps,
+                     "e2e": {"value": w.n * steps / e2e, "unit": UNIT,
+                             "h2d_bytes_per_step": int(q.nbytes),
+                             "d2h_bytes_per_step": int(Vh.nbytes)},
+                     "setup_seconds": setup_s,
+                     "accuracy_vs_exact_fp64_sampled": {
+                         "rel_rms_V": rel_rms(V[idx, 0], Ve[:, 0]),
+                         "rel_rms_gradV": rel_rms(V[idx, 1:], Ve[:, 1:]),
+                         "targets": int(idx.size)}}
+        s.close()
+    out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    if with_cpu:
+        try:
+            kind, cores, calc, qq, setup_s = cpu_baseline(w, None)
+            calc(qq)
+            t0 = time.perf_counter()
+            calc(qq)
+            cs = time.perf_counter() - t0
+            out["cpu_baseline"] = {
+                "value": w.n / cs, "unit": UNIT, "cores": cores, "kind": kind,
+                "sample": f"full workload: one CalcV after a warm-up call and one SetUp "
+                          f"({setup_s and round(setup_s, 2)} s)"
+                          + ("; reference AVX2 build with its OpenMP direct sums, FFTs by the "
+                             "project FFT shim (MKL absent)" if kind == "reference" else "")}
+        except Exception as e:  # the baseline must never break the GPU line
+            out["cpu_baseline"] = {"value": None, "kind": "unavailable", "sample": str(e)[:200]}
+    return out
+
+
+def bounded_serving(local, count=256):
+    """The first `count` requests of the serving stream (Poisson arrivals at
+    200/s, sizes log-uniform in [1e3, 2e5], 60 % 1/r, 25 % r^-0.5,
+    15 % Helmholtz), autotuned for 1e-5: served in real time (FP32 bulk,
+    continuous batching), the same requests all at t = 0 (offline capacity),
+    and the plain FP64 port on the same requests (one request per batch, one
+    set-up thread) at t = 0; rel-RMS errors of 16 served results against
+    the exact FP64 sum."""
+    import npme_b200
+    from npme_b200 import api, serving
+    reqs = serving.serving_stream(count=2048)[:count]
+    warm = serving.serving_stream(count=24, n_max=20_000, seed=99, rate=1e4)
+    srv = serving.Server(device=local)
+    n_plans = srv.warm_plans(reqs)
+    srv.run(warm, realtime=False)
+    live = srv.run(reqs, realtime=True)
+    V_live = {r.rid: r.V for r in reqs}
+    offline = srv.run(reqs, realtime=False)
+    srv.close()
+    plain = serving.Server(device=local, precision="fp64", max_batch=1, setup_workers=1)
+    plain.warm_plans(reqs)
+    plain_stats = plain.run(reqs, realtime=False)
+    plain.close()
+    errs = []
+    for r in reqs[:: max(1, count // 16)][:16]:
+        with npme_b200.Solver(serving.params_for(r, precision="fp64", device=local)) as s:
+            s.setup(r.coord)
+            t = np.sort(np.random.default_rng(r.rid).choice(r.n, min(r.n, 1024),
+                                                            replace=False)).astype(np.uint32)
+            Ve = s.calcv_exact_subset(t, r.q)
+        errs.append(rel_rms(V_live[r.rid][t, 0], Ve[:, 0]))
+    keep = ("requests", "points", "makespan_s", "throughput", "p50_latency_s",
+            "p99_latency_s", "mean_batch", "batches", "setup_ms_median", "setup_ms_p90")
+    return {"requests": count, "rate_per_s": 200,
+            "served_fp32": {k: live[k] for k in keep},
+            "offline_capacity_fp32": {k: offline[k] for k in keep},
+            "offline_capacity_plain_fp64": {k: plain_stats[k] for k in keep},
+            "capacity_ratio_fp32_batched_over_plain_fp64":
+                offline["throughput"] / plain_stats["throughput"],
+            "rel_rms_V_vs_exact_fp64": {"max": max(errs), "median": float(np.median(errs)),
+                                        "requests": len(errs), "targets_each": "<= 1024"},
+            "note": f"cuFFT plans of the {n_plans} FFT boxes built before the runs "
+                    "(server start-up); plain FP64 = the same server with one request per "
+                    "batch and one set-up thread"}
 
 
 def run_serving(args):
@@ -413,8 +554,23 @@ def main():
                 b.record(stream)
                 torch.cuda.synchronize(dev)
                 tt += a.elapsed_time(b)
+            # and end to end through the C ABI, as the headline's e2e
+            qh64 = torch.from_numpy(q).pin_memory().numpy()
+            Vh64 = torch.empty((w.n, 4), dtype=torch.complex128 if cplx else torch.float64)
+            Vh64 = Vh64.pin_memory().numpy()
+            s64.calcv(qh64, out=Vh64)
+            e64 = 0.0
+            for _ in range(k64):
+                flush.zero_()
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                s64.calcv(qh64, out=Vh64)
+                e64 += time.perf_counter() - t0
             extra["plain_fp64"] = {"value": w.n * k64 / (tt / 1e3), "unit": UNIT,
-                                   "ms_per_step": tt / k64, "steps": k64}
+                                   "ms_per_step": tt / k64, "steps": k64,
+                                   "e2e": {"value": w.n * k64 / e64, "unit": UNIT,
+                                           "h2d_bytes_per_step": int(q.nbytes),
+                                           "d2h_bytes_per_step": int(Vh64.nbytes)}}
             # accuracy of both forms against the exact O(N^2) FP64 sum
             Ve = s64.calcv_exact(q)
             V64 = s64.calcv(q)
@@ -441,6 +597,15 @@ def main():
                             "eps_gradV": float(errG / np.mean(np.abs(Ve[:, :3])))}}
             extra["accuracy_vs_exact_fp64"] = {"fp32_bulk": acc(V32), "plain_fp64": acc(V64)}
             s64.close()
+        if args.workload == "laplace_dm_1m" and not args.no_extra:
+            # the other configurations and a bounded serving run, after the
+            # headline's timed region
+            from npme_b200 import workloads as wl
+            extra["other_configs"] = {
+                ww.name: measure_config(ww, local, stream, flush, max(3, args.steps // 2),
+                                        with_cpu=not args.no_cpu)
+                for ww in (wl.RALPHA_500K, wl.HELMHOLTZ_250K)}
+            extra["serving_bounded"] = bounded_serving(local)
 
     if rank == 0:
         st = {k: v / args.steps for k, v in stage_sum.items()}  # timed steps

@@ -405,7 +405,8 @@ def test_full_size_matches_reference_and_exact(w):
     assert rel(V32[:, 1:], Vref[:, 1:]) < FP32_G_TOL
     assert rel(V32[idx, 0], Ve[:, 0]) < FULL_FP32_VS_EXACT
     assert rel(V64[idx, 0], Ve[:, 0]) < FULL_FP32_VS_EXACT  # method error of the config
-    # total charge-weighted potential (checksum of checksums) is stable
+    # total charge-weighted potential (checksum of checksums) is stable; the
+    # sum cancels (net-zero charges), so its relative error exceeds V's
     e64 = np.sum(np.conj(q) * V64[:, 0])
     e32 = np.sum(np.conj(q) * V32[:, 0])
-    assert abs(e32 - e64) <= 1e-6 * abs(e64)
+    assert abs(e32 - e64) <= 1e-5 * abs(e64)
