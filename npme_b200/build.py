@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libnpme_gpu.so")
-SOURCES = ["npme_gpu.cu", "recsum.cu", "direct.cu", "noalloc.cu", "batch.cu", "fft.cu",
+SOURCES = ["npme_gpu.cu", "setup.cu", "recsum.cu", "direct.cu", "noalloc.cu", "batch.cu", "fft.cu",
            "server.cu", "choose.cu"]
 APPS = os.path.join(HERE, "apps")
 BIN = os.path.join(HERE, "bin")

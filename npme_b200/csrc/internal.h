@@ -17,6 +17,8 @@ namespace npme {
 
 // Brick edge (grid points) of the spread tiles.
 constexpr int kBrick = 8;
+// Scratch buffers the device set-up keeps on a handle (setup.cu).
+constexpr int kSetupScratch = 48;
 
 // Geometry of the reciprocal-space grid and of the brick decomposition.
 struct GridGeom {
@@ -73,6 +75,7 @@ struct npme_handle {
   // set-up state
   size_t n = 0;
   double box[9];  // X Y Z R[3] L[3]
+  double bmin[3], bmax[3];  // bounding box of the points
   double fself_r = 0, fself_i = 0;
   double a_r[32], a_i[32], b_r[32], b_i[32];
   double beta = 0;
@@ -111,6 +114,8 @@ struct npme_handle {
   double *d_fax[3] = {nullptr, nullptr, nullptr};
   double *d_flam[3] = {nullptr, nullptr, nullptr};
   double *d_fcos[3] = {nullptr, nullptr, nullptr};
+  // device set-up scratch (sort keys, counts, group records), kept to reuse
+  void *d_su[npme::kSetupScratch] = {};
 
   // direct sum (both precisions): warp groups of <= 32 z-sorted points of
   // one xy column and, per group, the source segments (neighbour-column z
@@ -151,6 +156,13 @@ int handle_buffer(npme_handle *h, void **field, size_t bytes);
 // PME-corrected half extent X of a box of half extent X0 for an N-point FFT
 // axis (src/RecSumSupportFunctions.cpp:137-147)
 double compact_extent(double X0, double del, long order, long N);
+
+// setup.cu: the caller's coordinates to d_coord, their bounding box (and
+// the non-finite check) read back into mn / mx
+int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3]);
+// brick order, direct-sum orders, warp groups and segments, buffers (the box,
+// grid geometry and h->bmin / bmax set)
+int device_bin(npme_handle *h);
 
 // fft.cu
 int prepare_plans(npme_handle *h);

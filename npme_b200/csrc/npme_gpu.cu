@@ -5,7 +5,6 @@
 #include <cufft.h>
 
 #include <algorithm>
-#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdlib>
@@ -13,12 +12,10 @@
 #include <map>
 #include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "internal.h"
 
-using npme::BrickPoint;
 
 namespace {
 
@@ -109,8 +106,6 @@ double min_x_compact(double X0, double del, long order, long N) {
   return X0 > X ? X0 : X;
 }
 
-// src/RecSumSupportFunctions.h:123-127
-long start_index(double w) { return w < 0 ? (long)(-w) + 1 : (long)(-w); }
 
 // Device memory of all handles comes from one stream-ordered pool per device
 // (cudaMallocFromPoolAsync / cudaFreeAsync on the handle's stream).  Unlike
@@ -214,514 +209,6 @@ int npme::record_error(npme_handle *h, int code, const std::string &msg) {
 }
 
 namespace {
-
-// Host threads for the set-up of an n-point system: the machine's cores
-// shared among the set-ups running at the same time (a serving process runs
-// several on its own threads), one for small systems.
-std::atomic<int> g_active_setups{0};
-
-#ifndef NPME_SETUP_THREADS_MAX
-#define NPME_SETUP_THREADS_MAX 16
-#endif
-
-int setup_threads(size_t n) {
-  if (n < 50000) return 1;
-  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-  return std::max(1, std::min(NPME_SETUP_THREADS_MAX, hw / std::max(1, g_active_setups.load())));
-}
-
-// fn(begin, end) over [0, count) split into contiguous ranges, one host
-// thread each; the thread count follows `work` (points handled; default
-// count), the calling thread alone for small systems.
-template <class F>
-void parallel_ranges(size_t count, F fn, size_t work = 0) {
-  const int nt = (int)std::min<size_t>(setup_threads(work ? work : count),
-                                       std::max<size_t>(1, count));
-  if (nt <= 1) {
-    fn((size_t)0, count);
-    return;
-  }
-  std::vector<std::thread> pool;
-  for (int t = 0; t < nt; t++)
-    pool.emplace_back(fn, count * t / nt, count * (t + 1) / nt);
-  for (auto &th : pool) th.join();
-}
-
-// Sorts the points by xy column (`col`, ncol columns), then by (z, index)
-// inside each column.  Fills the permutation, the column starts and the
-// sorted z.
-void column_sort(const double *coord, size_t n, long ncol, const std::vector<int> &col,
-                 std::vector<uint32_t> &order, std::vector<long> &cstart,
-                 std::vector<double> &zs) {
-  // counting sort by column (stable), then each column by (z, index)
-  cstart.assign(ncol + 1, 0);
-  for (size_t i = 0; i < n; i++) cstart[col[i] + 1]++;
-  for (long c = 0; c < ncol; c++) cstart[c + 1] += cstart[c];
-  order.resize(n);
-  {
-    std::vector<long> fill(cstart.begin(), cstart.end() - 1);
-    for (size_t i = 0; i < n; i++) order[fill[col[i]]++] = (uint32_t)i;
-  }
-  zs.resize(n);
-  auto sort_columns = [&](long c0, long c1) {
-    std::vector<std::pair<double, uint32_t>> zc;
-    for (long c = c0; c < c1; c++) {
-      const long b = cstart[c], e1 = cstart[c + 1];
-      zc.resize(e1 - b);
-      for (long k = b; k < e1; k++) zc[k - b] = {coord[3 * (size_t)order[k] + 2], order[k]};
-      std::sort(zc.begin(), zc.end());
-      for (long k = b; k < e1; k++) zs[k] = zc[k - b].first, order[k] = zc[k - b].second;
-    }
-  };
-  const int nt = setup_threads(n);
-  if (nt == 1) {
-    sort_columns(0, ncol);
-  } else {
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nt; t++) pool.emplace_back(sort_columns, ncol * t / nt, ncol * (t + 1) / nt);
-    for (auto &th : pool) th.join();
-  }
-}
-
-// gpos[k] = coord[gorder[k]], spos[k] = coord[sorder[k]] (FP64, w unused)
-__global__ void gather_positions_kernel(const double *__restrict__ coord,
-                                        const uint32_t *__restrict__ gorder,
-                                        const uint32_t *__restrict__ sorder, long n,
-                                        double4 *__restrict__ gpos, double4 *__restrict__ spos) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const double *x = coord + 3 * (long)gorder[k];
-  gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
-  const double *y = coord + 3 * (long)sorder[k];
-  spos[k] = make_double4(y[0], y[1], y[2], 0.0);
-}
-
-#ifndef NPME_SOURCE_SPLIT
-#define NPME_SOURCE_SPLIT 2
-#endif
-
-// Warp groups for the FP32 direct sum.  Targets are binned into xy columns
-// of edge e ~ (32 / density)^(1/3) and sorted by z inside each column; each
-// run of 32 consecutive points of a column is one group (a compact, roughly
-// cubic cluster).  Sources are binned the same way into finer columns (edge
-// e / NPME_SOURCE_SPLIT) and sorted by z.  For every group the source
-// segments are the z ranges of the fine columns that can hold a point within
-// Rdir of the group's bounding box: |dz| <= sqrt(Rdir^2 - d_xy^2), d_xy the
-// distance from the bounding box to the column in the xy plane; finer source
-// columns bound that distance more tightly, so fewer sources are staged per
-// group.  Geometry is fixed between CalcV calls (the reference's contract),
-// so this is set-up work.  Returns the group-order permutation of the
-// targets in `order` and the source-order permutation in `sorder`.
-int build_groups(npme_handle *h, const double *coord, std::vector<uint32_t> &order,
-                 std::vector<uint32_t> &sorder) {
-  const size_t n = h->n;
-  const double R = h->p.Rdir, R2 = R * R;
-  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
-  for (size_t i = 0; i < n; i++)
-    for (int d = 0; d < 3; d++) {
-      mn[d] = std::min(mn[d], coord[3 * i + d]);
-      mx[d] = std::max(mx[d], coord[3 * i + d]);
-    }
-  // column edge from the mean density of the bounding box (degenerate axes
-  // are given a nominal thickness of Rdir / 4)
-  double vol = 1.0;
-  for (int d = 0; d < 3; d++) vol *= std::max(mx[d] - mn[d], 0.25 * R);
-  double e = std::cbrt(32.0 * vol / (double)n);
-  e = std::max(e, 1e-3 * R);
-  constexpr int S = NPME_SOURCE_SPLIT;
-  int nc[2], ns[2];
-  double edge[2], sedge[2];
-  for (int d = 0; d < 2; d++) {
-    const double ext = mx[d] - mn[d];
-    nc[d] = std::max(1, std::min((int)std::ceil(ext / e), 1 << 14));
-    edge[d] = std::max(ext / nc[d], 1e-12);
-    ns[d] = nc[d] * S;
-    sedge[d] = edge[d] / S;
-  }
-  // every fine column lies inside one coarse column: a point's fine column
-  // is its coarse column's sub-column
-  std::vector<int> ccol(n), scol(n);
-  for (size_t i = 0; i < n; i++) {
-    int cs[2], ss[2];
-    for (int d = 0; d < 2; d++) {
-      const double u = coord[3 * i + d] - mn[d];
-      cs[d] = std::min(nc[d] - 1, std::max(0, (int)(u / edge[d])));
-      ss[d] = cs[d] * S + std::min(S - 1, std::max(0, (int)((u - cs[d] * edge[d]) / sedge[d])));
-    }
-    ccol[i] = cs[0] * nc[1] + cs[1];
-    scol[i] = ss[0] * ns[1] + ss[1];
-  }
-  std::vector<long> cstart, sstart;
-  std::vector<double> zt, zs;
-  const long ncol = (long)nc[0] * nc[1];
-  column_sort(coord, n, ncol, ccol, order, cstart, zt);
-  column_sort(coord, n, (long)ns[0] * ns[1], scol, sorder, sstart, zs);
-  // position of each source in the coarse (group) order: increasing inside
-  // a fine column, since both orders sort a column by (z, index)
-  const bool half = true;
-  std::vector<uint32_t> fcpos;
-  if (half) {
-    std::vector<uint32_t> cpos(n);
-    for (size_t k = 0; k < n; k++) cpos[order[k]] = (uint32_t)k;
-    fcpos.resize(n);
-    for (size_t k = 0; k < n; k++) fcpos[k] = cpos[sorder[k]];
-  }
-
-  // Per coarse column: the fine columns that can hold a source within R of
-  // the column's points, each with a pair of cursors into its z-sorted
-  // sources.  The groups of a column come in increasing z, so the cursors
-  // only creep forward (a few steps per group, either direction as the
-  // window half-height varies) instead of a binary search per group and
-  // column, and the column's source z values stay in cache.  Coarse columns
-  // are independent: large systems split them over host threads, each
-  // filling its own lists, concatenated in column order afterwards.
-  struct Part {
-    std::vector<int4> groups, hgroups;
-    std::vector<double4> cen;
-    std::vector<int2> segs, hsegs;
-    std::vector<long> work, hwork;  // sources staged per group (launch order)
-    double cand = 0, hcand = 0;
-  };
-  auto build_part = [&](long c_begin, long c_end, Part &out) {
-    std::vector<long> nb_col, nb_cc, pa, pb;
-    std::vector<int> nb_s0, nb_s1;
-    std::vector<double> dxv, dyv;
-    for (long c = c_begin; c < c_end; c++) {
-      if (cstart[c] == cstart[c + 1]) continue;
-      double cl[2] = {1e300, 1e300}, ch[2] = {-1e300, -1e300};
-      for (long k = cstart[c]; k < cstart[c + 1]; k++)
-        for (int d = 0; d < 2; d++) {
-          const double x = coord[3 * (size_t)order[k] + d];
-          cl[d] = std::min(cl[d], x);
-          ch[d] = std::max(ch[d], x);
-        }
-      int lo[2], hi[2];
-      for (int d = 0; d < 2; d++) {
-        lo[d] = (int)std::max(0.0, std::floor((cl[d] - R - mn[d]) / sedge[d]));
-        hi[d] = (int)std::min((double)(ns[d] - 1), std::floor((ch[d] + R - mn[d]) / sedge[d]));
-      }
-      nb_col.clear(), nb_cc.clear(), nb_s0.clear(), nb_s1.clear();
-      for (int s0 = lo[0]; s0 <= hi[0]; s0++)
-        for (int s1 = lo[1]; s1 <= hi[1]; s1++) {
-          const long sc = (long)s0 * ns[1] + s1;
-          if (sstart[sc] == sstart[sc + 1]) continue;
-          nb_col.push_back(sc), nb_s0.push_back(s0 - lo[0]), nb_s1.push_back(s1 - lo[1]);
-          nb_cc.push_back((long)(s0 / S) * nc[1] + s1 / S);
-        }
-      pa.assign(nb_col.size(), 0), pb.assign(nb_col.size(), 0);
-      for (size_t t = 0; t < nb_col.size(); t++) pa[t] = pb[t] = sstart[nb_col[t]];
-      dxv.resize(hi[0] - lo[0] + 1), dyv.resize(hi[1] - lo[1] + 1);
-      for (long p0 = cstart[c]; p0 < cstart[c + 1]; p0 += 32) {
-        const long p1 = std::min(p0 + 32, cstart[c + 1]);
-        double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
-        for (long k = p0; k < p1; k++)
-          for (int d = 0; d < 3; d++) {
-            const double x = coord[3 * (size_t)order[k] + d];
-            bl[d] = std::min(bl[d], x);
-            bh[d] = std::max(bh[d], x);
-          }
-        // squared xy distances from the bounding box to each fine column
-        for (size_t u = 0; u < dxv.size(); u++) {
-          const double l0 = mn[0] + (lo[0] + (long)u) * sedge[0], h0 = l0 + sedge[0];
-          const double d = std::max(0.0, std::max(l0 - bh[0], bl[0] - h0));
-          dxv[u] = d * d;
-        }
-        for (size_t u = 0; u < dyv.size(); u++) {
-          const double l1 = mn[1] + (lo[1] + (long)u) * sedge[1], h1 = l1 + sedge[1];
-          const double d = std::max(0.0, std::max(l1 - bh[1], bl[1] - h1));
-          dyv[u] = d * d;
-        }
-        const int seg0 = (int)out.segs.size(), hseg0 = (int)out.hsegs.size();
-        long gwork = 0, hwork = 0;
-        for (size_t t = 0; t < nb_col.size(); t++) {
-          const double d2 = dxv[nb_s0[t]] + dyv[nb_s1[t]];
-          if (d2 > R2) continue;
-          const double hz = std::sqrt(R2 - d2), zlo = bl[2] - hz, zhi = bh[2] + hz;
-          const long zb = sstart[nb_col[t]], ze = sstart[nb_col[t] + 1];
-          long a = pa[t], b = pb[t];
-          // a: first source with z >= zlo; b: first source with z > zhi
-          while (a < ze && zs[a] < zlo) a++;
-          while (a > zb && zs[a - 1] >= zlo) a--;
-          while (b < ze && zs[b] <= zhi) b++;
-          while (b > zb && zs[b - 1] > zhi) b--;
-          pa[t] = a, pb[t] = b;
-          if (b > a) {
-            out.segs.push_back(make_int2((int)a, (int)(b - a)));
-            out.cand += (double)(b - a) * (double)(p1 - p0);
-            gwork += b - a;
-          }
-          // half shell: later coarse columns whole, the group's own column
-          // from the first point after the group
-          if (half && b > a && nb_cc[t] >= c) {
-            long a2 = a;
-            if (nb_cc[t] == c)
-              a2 = std::lower_bound(fcpos.begin() + a, fcpos.begin() + b, (uint32_t)p1) -
-                   fcpos.begin();
-            if (b > a2) {
-              out.hsegs.push_back(make_int2((int)a2, (int)(b - a2)));
-              out.hcand += (double)(b - a2) * (double)(p1 - p0);
-              hwork += b - a2;
-            }
-          }
-        }
-        out.groups.push_back(make_int4((int)p0, (int)(p1 - p0), seg0, (int)out.segs.size()));
-        out.work.push_back(gwork);
-        if (half) {
-          out.hgroups.push_back(
-              make_int4((int)p0, (int)(p1 - p0), hseg0, (int)out.hsegs.size()));
-          out.hwork.push_back(hwork);
-        }
-        // centre and half-diagonal of the bounding box
-        out.cen.push_back(make_double4(
-            0.5 * (bl[0] + bh[0]), 0.5 * (bl[1] + bh[1]), 0.5 * (bl[2] + bh[2]),
-            0.5 * std::sqrt((bh[0] - bl[0]) * (bh[0] - bl[0]) + (bh[1] - bl[1]) * (bh[1] - bl[1]) +
-                            (bh[2] - bl[2]) * (bh[2] - bl[2]))));
-      }
-    }
-  };
-  const int nthreads = setup_threads(n);
-  std::vector<Part> parts(nthreads);
-  if (nthreads == 1) {
-    build_part(0, ncol, parts[0]);
-  } else {
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nthreads; t++)
-      pool.emplace_back(build_part, ncol * t / nthreads, ncol * (t + 1) / nthreads,
-                        std::ref(parts[t]));
-    for (auto &th : pool) th.join();
-  }
-  // group records with segment indices made global; the segment lists stay
-  // in their parts and are uploaded part by part (no host concatenation)
-  std::vector<int4> groups, hgroups;
-  std::vector<double4> cen;
-  std::vector<long> work, hwork;
-  size_t nsegs = 0, nhsegs = 0;
-  double cand = 0, hcand = 0;
-  for (Part &pt : parts) {
-    const int base = (int)nsegs, hbase = (int)nhsegs;
-    for (int4 g : pt.groups) groups.push_back(make_int4(g.x, g.y, g.z + base, g.w + base));
-    for (int4 g : pt.hgroups) hgroups.push_back(make_int4(g.x, g.y, g.z + hbase, g.w + hbase));
-    cen.insert(cen.end(), pt.cen.begin(), pt.cen.end());
-    work.insert(work.end(), pt.work.begin(), pt.work.end());
-    hwork.insert(hwork.end(), pt.hwork.begin(), pt.hwork.end());
-    nsegs += pt.segs.size(), nhsegs += pt.hsegs.size();
-    cand += pt.cand, hcand += pt.hcand;
-  }
-  // group records hold segment indices as int
-  if (nsegs >= ((size_t)1 << 31) || nhsegs >= ((size_t)1 << 31))
-    return fail(h, NPME_EINVAL, "too many direct-sum source segments (2^31)");
-  // heaviest groups first, so the last wave of the launch holds the light
-  // ones (each list by its own work)
-  auto by_work = [](std::vector<int4> &gl, const std::vector<long> &wk,
-                    const std::vector<double4> &cin, std::vector<double4> &cout) {
-    std::vector<uint32_t> go(gl.size());
-    for (size_t g = 0; g < go.size(); g++) go[g] = (uint32_t)g;
-    std::stable_sort(go.begin(), go.end(), [&](uint32_t a, uint32_t b) { return wk[a] > wk[b]; });
-    std::vector<int4> g2(gl.size());
-    cout.resize(gl.size());
-    for (size_t g = 0; g < go.size(); g++) g2[g] = gl[go[g]], cout[g] = cin[go[g]];
-    gl.swap(g2);
-  };
-  std::vector<double4> gcen, hcen;
-  by_work(groups, work, cen, gcen);
-  if (half) by_work(hgroups, hwork, cen, hcen);
-  cen.swap(gcen);
-  h->n_groups = (long)groups.size();
-  h->n_segs = (long)nsegs;
-  h->cand_per_point = cand / (double)n;
-  h->n_hgroups = (long)hgroups.size();
-  h->n_hsegs = (long)nhsegs;
-  h->hcand_per_point = hcand / (double)n;
-  // heads of offsets up to ~the group half-diagonal carry ~6e-8 e absolute
-  // error; below r = e/4 the relative error would exceed ~1e-6, so refine
-  h->refine2 = (0.25 * e) * (0.25 * e);
-  int rc;
-  if ((rc = dalloc(h, &h->d_coord, sizeof(double) * 3 * n))) return rc;
-  if ((rc = dalloc(h, &h->d_gpos, sizeof(double4) * n))) return rc;
-  if ((rc = dalloc(h, &h->d_spos, sizeof(double4) * n))) return rc;
-  if ((rc = dalloc(h, &h->d_cperm, sizeof(uint32_t) * n))) return rc;
-  if ((rc = dalloc(h, &h->d_sperm, sizeof(uint32_t) * n))) return rc;
-  if ((rc = dalloc(h, &h->d_groups, sizeof(int4) * groups.size()))) return rc;
-  if ((rc = dalloc(h, &h->d_gcen, sizeof(double4) * cen.size()))) return rc;
-  if ((rc = dalloc(h, &h->d_segs, sizeof(int2) * std::max<size_t>(1, nsegs)))) return rc;
-  // target and source positions are gathered on the device from the
-  // caller's coordinates and the two orders
-  CK(cudaMemcpyAsync(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_cperm, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
-                     h->stream));
-  CK(cudaMemcpyAsync(h->d_sperm, sorder.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice,
-                     h->stream));
-  gather_positions_kernel<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
-      h->d_coord, h->d_cperm, h->d_sperm, (long)n, h->d_gpos, h->d_spos);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(h->d_groups, groups.data(), sizeof(int4) * groups.size(),
-                     cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_gcen, cen.data(), sizeof(double4) * cen.size(), cudaMemcpyHostToDevice,
-                     h->stream));
-  {
-    size_t off = 0;
-    for (const Part &pt : parts) {
-      if (!pt.segs.empty())
-        CK(cudaMemcpyAsync(h->d_segs + off, pt.segs.data(), sizeof(int2) * pt.segs.size(),
-                           cudaMemcpyHostToDevice, h->stream));
-      off += pt.segs.size();
-    }
-  }
-  if (half) {
-    if ((rc = dalloc(h, &h->d_hgroups, sizeof(int4) * hgroups.size()))) return rc;
-    if ((rc = dalloc(h, &h->d_hcen, sizeof(double4) * hcen.size()))) return rc;
-    if ((rc = dalloc(h, &h->d_hsegs, sizeof(int2) * std::max<size_t>(1, nhsegs)))) return rc;
-    if (h->fp32) {
-      const size_t nv = (h->complex_kernel ? 2 : 1) * n;  // float4 per source (two if complex)
-      if ((rc = dalloc(h, &h->d_vsrc, sizeof(float4) * nv))) return rc;
-      CK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * nv, h->stream));
-    } else {
-      if ((rc = dalloc(h, &h->d_vsrc64, sizeof(double) * 4 * n))) return rc;
-      CK(cudaMemsetAsync(h->d_vsrc64, 0, sizeof(double) * 4 * n, h->stream));
-    }
-    CK(cudaMemcpyAsync(h->d_hgroups, hgroups.data(), sizeof(int4) * hgroups.size(),
-                       cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d_hcen, hcen.data(), sizeof(double4) * hcen.size(),
-                       cudaMemcpyHostToDevice, h->stream));
-    size_t off = 0;
-    for (const Part &pt : parts) {
-      if (!pt.hsegs.empty())
-        CK(cudaMemcpyAsync(h->d_hsegs + off, pt.hsegs.data(), sizeof(int2) * pt.hsegs.size(),
-                           cudaMemcpyHostToDevice, h->stream));
-      off += pt.hsegs.size();
-    }
-  }
-  return NPME_OK;
-}
-
-template <typename T>
-int upload_points(npme_handle *h, const double *coord) {
-  const size_t n = h->n;
-  const npme::GridGeom &g = h->grid;
-  const double *R = h->box + 3, *L = h->box + 6;
-  const int P = g.order;
-  // --- brick order for spread / interpolation ---
-  std::vector<BrickPoint<T>> pts(n);
-  std::vector<int> bid(n);
-  // the first point (lowest index) whose stencil leaves the octant, and its axis
-  std::atomic<long> bad{(long)n};
-  std::atomic<int> bad_axis{0};
-  parallel_ranges(n, [&](size_t i0, size_t i1) {
-    for (size_t i = i0; i < i1; i++) {
-      uint32_t g0[3];
-      T u[3];
-      for (int d = 0; d < 3; d++) {
-        const double w = (double)g.N[d] / L[d] * (coord[3 * i + d] - R[d]);
-        const long ms = start_index(w);
-        const long o = ms + g.N[d] / 4;
-        if (o < 0 || o + P - 1 > g.H[d] - 1) {
-          long cur = bad.load();
-          while ((long)i < cur && !bad.compare_exchange_weak(cur, (long)i)) {
-          }
-          if (bad.load() == (long)i) bad_axis = d;
-          return;
-        }
-        g0[d] = (uint32_t)o;
-        u[d] = (T)(w + (double)ms);
-      }
-      BrickPoint<T> &bp = pts[i];
-      bp.u[0] = u[0], bp.u[1] = u[1], bp.u[2] = u[2];
-      bp.g0 = (g0[0] << 20) | (g0[1] << 10) | g0[2];
-      bp.orig = (uint32_t)i;
-      bid[i] = (int)(((g0[0] / npme::kBrick) * g.nb[1] + g0[1] / npme::kBrick) * g.nb[2] +
-                     g0[2] / npme::kBrick);
-    }
-  });
-  if (bad.load() < (long)n)
-    return fail(h, NPME_EINVAL,
-                "point " + std::to_string(bad.load()) + " has a B-spline stencil outside the "
-                "charge octant (axis " + std::to_string(bad_axis.load()) + ")");
-  const long nbt = g.nb[0] * g.nb[1] * g.nb[2];
-  std::vector<int> bstart(nbt + 1, 0);
-  for (size_t i = 0; i < n; i++) bstart[bid[i] + 1]++;
-  for (long b = 0; b < nbt; b++) bstart[b + 1] += bstart[b];
-  std::vector<int> fillp(bstart.begin(), bstart.end() - 1);
-  std::vector<BrickPoint<T>> sorted(n);
-  for (size_t i = 0; i < n; i++) sorted[fillp[bid[i]]++] = pts[i];
-  std::vector<int> blist;
-  for (long b = 0; b < nbt; b++)
-    if (bstart[b + 1] > bstart[b]) blist.push_back((int)b);
-  // inside a brick, points sorted by the shared-memory bank of their stencil
-  // origin in the brick's tile (the kernels give the lanes of a warp points
-  // of different banks; see brick_point in bodies.cuh)
-  {
-    const int TL = npme::kBrick + P - 1;
-    const int words = (int)(sizeof(T) / 4) * (h->complex_kernel ? 2 : 1);
-    const int nkeys = 32 / words;
-    parallel_ranges(blist.size(), [&](size_t k0, size_t k1) {
-    std::vector<BrickPoint<T>> tmp;
-    int cnt[32];
-    for (size_t kb = k0; kb < k1; kb++) {
-      const int b = blist[kb];
-      const int beg = bstart[b], end = bstart[b + 1];
-      const long b3 = b % g.nb[2], b2 = (b / g.nb[2]) % g.nb[1], b1 = b / (g.nb[2] * g.nb[1]);
-      auto key = [&](const BrickPoint<T> &pt) {
-        const long l1 = (long)(pt.g0 >> 20) - b1 * npme::kBrick;
-        const long l2 = (long)((pt.g0 >> 10) & 1023u) - b2 * npme::kBrick;
-        const long l3 = (long)(pt.g0 & 1023u) - b3 * npme::kBrick;
-        return (int)(((l1 * TL + l2) * TL + l3) % nkeys);
-      };
-      tmp.assign(sorted.begin() + beg, sorted.begin() + end);
-      std::fill(cnt, cnt + 32, 0);
-      for (const auto &pt : tmp) cnt[key(pt)]++;
-      int acc = beg;
-      for (int k = 0; k < nkeys; k++) {
-        const int c = cnt[k];
-        cnt[k] = acc;
-        acc += c;
-      }
-      for (const auto &pt : tmp) sorted[cnt[key(pt)]++] = pt;
-    }
-    }, n);
-  }
-  h->n_bricks = nbt;
-  h->n_nonempty = (long)blist.size();
-
-  std::vector<uint32_t> cperm;  // group order -> caller index (build_groups)
-  const int C = h->complex_kernel ? 2 : 1;
-  int rc;
-  // the direct sum walks warp groups: targets in group order, sources
-  // (and their gathered charges) in fine-column order
-  std::vector<uint32_t> sperm;
-  if ((rc = build_groups(h, coord, cperm, sperm))) return rc;
-  if ((rc = dalloc(h, (BrickPoint<T> **)&h->d_bpts, sizeof(BrickPoint<T>) * n))) return rc;
-  if ((rc = dalloc(h, &h->d_brick_start, sizeof(int) * (nbt + 1)))) return rc;
-  if ((rc = dalloc(h, &h->d_brick_list, sizeof(int) * std::max<size_t>(1, blist.size()))))
-    return rc;
-  if ((rc = dalloc(h, (T **)&h->d_qb, sizeof(T) * C * n))) return rc;
-  if ((rc = dalloc(h, (T **)&h->d_qc, sizeof(T) * C * n))) return rc;
-  if ((rc = dalloc(h, &h->d_q_in, sizeof(double) * C * n))) return rc;
-  if ((rc = dalloc(h, &h->d_V, sizeof(double) * 4 * C * n))) return rc;
-  CK(cudaMemcpyAsync(h->d_bpts, sorted.data(), sizeof(BrickPoint<T>) * n, cudaMemcpyHostToDevice,
-                     h->stream));
-  CK(cudaMemcpyAsync(h->d_brick_start, bstart.data(), sizeof(int) * (nbt + 1),
-                     cudaMemcpyHostToDevice, h->stream));
-  if (!blist.empty())
-    CK(cudaMemcpyAsync(h->d_brick_list, blist.data(), sizeof(int) * blist.size(),
-                       cudaMemcpyHostToDevice, h->stream));
-  // charges of the direct sum are gathered into its source order
-  h->d_dperm = h->d_sperm;
-
-  // --- grids ---
-  const long *N = g.N;
-  const size_t Ntot = (size_t)N[0] * N[1] * N[2];
-  const size_t Mtot = (size_t)(N[0] / 2 + 1) * (N[1] / 2 + 1) * (N[2] / 2 + 1);
-  if (h->complex_kernel) {
-    if ((rc = dalloc(h, (T **)&h->d_grid, sizeof(T) * 2 * Ntot))) return rc;
-    if ((rc = dalloc(h, (T **)&h->d_G, sizeof(T) * 2 * Mtot))) return rc;
-  } else {
-    if ((rc = dalloc(h, (T **)&h->d_grid, sizeof(T) * Ntot))) return rc;
-    if ((rc = dalloc(h, (T **)&h->d_kgrid, sizeof(T) * 2 * (size_t)N[0] * N[1] * (N[2] / 2 + 1))))
-      return rc;
-    if ((rc = dalloc(h, (T **)&h->d_G, sizeof(T) * Mtot))) return rc;
-  }
-  return NPME_OK;
-}
 
 int check_params(npme_handle *h, const npme_params &p) {
   if (!(p.Rdir > 0)) return fail(h, NPME_EINVAL, "Rdir must be > 0");
@@ -894,10 +381,7 @@ int npme_gpu_set_user_kernel(npme_handle *h, const npme_user_ops *ops) {
 static int setup_impl(npme_handle *h, size_t n, const double *coord);
 
 int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
-  g_active_setups++;
-  const int rc = setup_impl(h, n, coord);
-  g_active_setups--;
-  return rc;
+  return setup_impl(h, n, coord);
 }
 
 static int setup_impl(npme_handle *h, size_t n, const double *coord) {
@@ -923,15 +407,12 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
   h->ready = false;
   h->n = n;
   const npme_params &p = h->p;
-  // box (src/RecSumSupportFunctions.cpp:182-201, 276-296)
-  double mx[3] = {-1e300, -1e300, -1e300}, mn[3] = {1e300, 1e300, 1e300};
-  for (size_t i = 0; i < n; i++)
-    for (int d = 0; d < 3; d++) {
-      const double x = coord[3 * i + d];
-      if (!std::isfinite(x)) return fail(h, NPME_EINVAL, "non-finite coordinate");
-      mx[d] = std::max(mx[d], x);
-      mn[d] = std::min(mn[d], x);
-    }
+  // box (src/RecSumSupportFunctions.cpp:182-201, 276-296) from the points'
+  // bounding box, reduced on the device
+  double mx[3], mn[3];
+  int rc = npme::device_bbox(h, coord, mn, mx);
+  if (rc) return rc;
+  for (int d = 0; d < 3; d++) h->bmin[d] = mn[d], h->bmax[d] = mx[d];
   const long Ns[3] = {p.N1, p.N2, p.N3};
   const double dels[3] = {p.del1, p.del2, p.del3};
   for (int d = 0; d < 3; d++) {
@@ -962,7 +443,7 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
     const char *e = std::getenv("NPME_PAIRS_ONCE");
     h->use_sym = !(e && e[0] == '0');
   }
-  int rc = h->fp32 ? upload_points<float>(h, coord) : upload_points<double>(h, coord);
+  rc = npme::device_bin(h);
   if (rc) {
     release(h);
     return rc;

@@ -1,0 +1,758 @@
+// Per-geometry set-up on the device: everything CalcV needs that depends on
+// the point positions, built from the caller's coordinates in HBM.
+//
+//  * bounding box and coordinate check (one reduction, read back by the host,
+//    which derives the PME box, src/RecSumSupportFunctions.cpp:182-201,
+//    276-296);
+//  * brick order of the spreading and interpolation (src/RecSumQ.cpp:527-895,
+//    NPME_RecSumQ_CreateBlock): each point's stencil origin and fractional
+//    offset (src/RecSumSupportFunctions.h:123-151), points sorted by brick
+//    and, inside a brick, by the shared-memory bank of their stencil origin;
+//  * the direct sum's warp groups (the reference's cells and cluster pairs,
+//    src/PartitionEmbeddedBox.cpp:47-205, src/PartitionBox.cpp:789-923):
+//    targets sorted by (xy column, z, index) and cut into runs of 32,
+//    sources sorted by (fine xy column, z, index); for every group the z
+//    ranges of the fine columns that can hold a point within Rdir of the
+//    group's bounding box, and the half-shell part of them for the
+//    every-pair-once walk; groups ordered by their work, heaviest first.
+//
+// Sorting is done with stable radix sorts (values = point indices in
+// increasing order), so every order is (key, index) lexicographic and the
+// result does not depend on timing.  Work per point or per group is a
+// thread or a warp; the host reads back four small records (box, group
+// count, segment counts) and sizes the buffers from them.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "internal.h"
+
+namespace npme {
+namespace {
+
+constexpr int kSourceSplit = 2;  // fine source columns per coarse column edge
+
+// Order-preserving 64-bit key of a double (total order of the finite values).
+__device__ __forceinline__ unsigned long long dkey(double x) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+inline double dkey_inv(unsigned long long k) {
+  const unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  double x;
+  std::memcpy(&x, &u, sizeof(x));
+  return x;
+}
+
+// Results the host reads back.
+struct SetupStats {
+  unsigned long long mn[3], mx[3];  // dkey of the per-axis minimum / maximum
+  unsigned int nonfinite;
+  unsigned int pad;
+  long long bad;                    // lowest index whose stencil leaves the octant
+  unsigned long long cand, hcand;   // staged (target, source) candidates, both walks
+};
+
+__global__ void init_stats_kernel(SetupStats *st, long long n) {
+  for (int d = 0; d < 3; d++) st->mn[d] = ~0ull, st->mx[d] = 0ull;
+  st->nonfinite = 0;
+  st->bad = n;
+  st->cand = st->hcand = 0;
+}
+
+__global__ void bbox_kernel(const double *__restrict__ coord, long n, SetupStats *st) {
+  unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0ull, 0ull, 0ull};
+  unsigned bad = 0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const double x = coord[3 * i + d];
+      if (!isfinite(x)) {
+        bad = 1;
+        continue;
+      }
+      const unsigned long long k = dkey(x);
+      lo[d] = min(lo[d], k);
+      hi[d] = max(hi[d], k);
+    }
+  }
+  const unsigned FULL = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      lo[d] = min(lo[d], __shfl_xor_sync(FULL, lo[d], o));
+      hi[d] = max(hi[d], __shfl_xor_sync(FULL, hi[d], o));
+    }
+    bad |= __shfl_xor_sync(FULL, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int d = 0; d < 3; d++) {
+      atomicMin(&st->mn[d], lo[d]);
+      atomicMax(&st->mx[d], hi[d]);
+    }
+    if (bad) atomicOr(&st->nonfinite, 1u);
+  }
+}
+
+// Geometry the binning kernel needs (host-computed from the box).
+struct BinGeom {
+  double N[3], L[3], R[3];
+  long Nl[3], H[3], nb[3];
+  int P, TL, nkeys;
+  // direct-sum columns
+  double mn[2], edge[2], sedge[2];
+  int nc[2], ns[2];
+};
+
+// start index of the B-spline stencil (src/RecSumSupportFunctions.h:123-127)
+__device__ __forceinline__ long stencil_start(double w) {
+  return w < 0 ? (long)(-w) + 1 : (long)(-w);
+}
+
+// Per point: the spread/interpolation record, its brick-and-bank sort key,
+// its coarse and fine xy columns and its z sort key; per brick and column
+// the point counts.  Arithmetic as the host restatement of the reference
+// (explicit round-to-nearest operations, no contraction), so that every
+// point lands in the same brick, bank and column on any machine.
+template <typename T>
+__global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
+                           BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
+                           unsigned *__restrict__ ccol, unsigned *__restrict__ scol,
+                           unsigned long long *__restrict__ zkey, unsigned *__restrict__ iota,
+                           int *__restrict__ bcount, int *__restrict__ ccount,
+                           int *__restrict__ scount, SetupStats *st) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
+  long o[3];
+  T u[3];
+  bool out = false;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double w = __dmul_rn(__ddiv_rn(g.N[d], g.L[d]), __dsub_rn(x[d], g.R[d]));
+    const long ms = stencil_start(w);
+    o[d] = ms + g.Nl[d] / 4;
+    if (o[d] < 0 || o[d] + g.P - 1 > g.H[d] - 1) out = true;
+    u[d] = (T)__dadd_rn(w, (double)ms);
+  }
+  if (out) {
+    atomicMin(&st->bad, (long long)i);
+    o[0] = o[1] = o[2] = 0;  // any in-range brick: the set-up fails anyway
+  }
+  const long b1 = o[0] / kBrick, b2 = o[1] / kBrick, b3 = o[2] / kBrick;
+  const long bid = (b1 * g.nb[1] + b2) * g.nb[2] + b3;
+  const long l1 = o[0] - b1 * kBrick, l2 = o[1] - b2 * kBrick, l3 = o[2] - b3 * kBrick;
+  const unsigned key = (unsigned)(((l1 * g.TL + l2) * g.TL + l3) % g.nkeys);
+  BrickPoint<T> bp;
+  bp.u[0] = u[0], bp.u[1] = u[1], bp.u[2] = u[2];
+  bp.g0 = ((uint32_t)o[0] << 20) | ((uint32_t)o[1] << 10) | (uint32_t)o[2];
+  bp.orig = (uint32_t)i;
+  pts[i] = bp;
+  bkey[i] = ((unsigned)bid << 5) | key;
+  if (!out) atomicAdd(&bcount[bid], 1);
+  int cs[2], ss[2];
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    const double v = __dsub_rn(x[d], g.mn[d]);
+    cs[d] = min(g.nc[d] - 1, max(0, (int)__ddiv_rn(v, g.edge[d])));
+    const double r = __dsub_rn(v, __dmul_rn((double)cs[d], g.edge[d]));
+    ss[d] = cs[d] * kSourceSplit +
+            min(kSourceSplit - 1, max(0, (int)__ddiv_rn(r, g.sedge[d])));
+  }
+  const unsigned cc = (unsigned)(cs[0] * g.nc[1] + cs[1]);
+  const unsigned sc = (unsigned)(ss[0] * g.ns[1] + ss[1]);
+  ccol[i] = cc;
+  scol[i] = sc;
+  atomicAdd(&ccount[cc], 1);
+  atomicAdd(&scount[sc], 1);
+  zkey[i] = dkey(x[2]);
+  iota[i] = (unsigned)i;
+}
+
+template <typename T>
+__global__ void gather_bpts_kernel(const BrickPoint<T> *__restrict__ pts,
+                                   const unsigned *__restrict__ perm, long n,
+                                   BrickPoint<T> *__restrict__ out) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = pts[perm[k]];
+}
+
+__global__ void gather_u32_kernel(const unsigned *__restrict__ src,
+                                  const unsigned *__restrict__ perm, long n,
+                                  unsigned *__restrict__ out) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = src[perm[k]];
+}
+
+// flag[b] = 1 for non-empty bricks (flag[nb] = 0)
+__global__ void nonempty_flags_kernel(const int *__restrict__ count, long nb,
+                                      int *__restrict__ flag) {
+  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b <= nb) flag[b] = b < nb && count[b] > 0;
+}
+
+__global__ void brick_list_kernel(const int *__restrict__ count, const int *__restrict__ pos,
+                                  long nb, int *__restrict__ list) {
+  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nb && count[b] > 0) list[pos[b]] = (int)b;
+}
+
+// zs[k] = z of source k; cpos[cperm[k]] = k (position of a point in the group order)
+__global__ void source_z_kernel(const double *__restrict__ coord, const unsigned *__restrict__ sperm,
+                                const unsigned *__restrict__ cperm, long n, double *__restrict__ zs,
+                                unsigned *__restrict__ cpos) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  zs[k] = coord[3 * (long)sperm[k] + 2];
+  cpos[cperm[k]] = (unsigned)k;
+}
+
+__global__ void gather_positions_kernel(const double *__restrict__ coord,
+                                        const uint32_t *__restrict__ gorder,
+                                        const uint32_t *__restrict__ sorder, long n,
+                                        double4 *__restrict__ gpos, double4 *__restrict__ spos) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double *x = coord + 3 * (long)gorder[k];
+  gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
+  const double *y = coord + 3 * (long)sorder[k];
+  spos[k] = make_double4(y[0], y[1], y[2], 0.0);
+}
+
+// groups per coarse column: ceil(count / 32) (entry ncol = 0)
+__global__ void groups_per_column_kernel(const int *__restrict__ ccount, long ncol,
+                                         int *__restrict__ gcount) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c <= ncol) gcount[c] = c < ncol ? (ccount[c] + 31) / 32 : 0;
+}
+
+// group g of column c: points [p0, p1) of the group order
+__global__ void group_records_kernel(const int *__restrict__ cstart, const int *__restrict__ goff,
+                                     long ncol, int4 *__restrict__ grec) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const int p_end = cstart[c + 1];
+  int g = goff[c];
+  for (int p0 = cstart[c]; p0 < p_end; p0 += 32, g++)
+    grec[g] = make_int4(p0, min(p0 + 32, p_end), (int)c, 0);
+}
+
+struct GroupGeom {
+  double R, R2;
+  double mn[2], sedge[2];
+  int ns[2], nc1;
+};
+
+// Bounding box of every group (warp per group): lo/hi corners, and the
+// frame origin (centre) with the half diagonal in w.
+__global__ void group_box_kernel(const double4 *__restrict__ gpos, const int4 *__restrict__ grec,
+                                 long ngroups, double4 *__restrict__ blo,
+                                 double4 *__restrict__ bhi, double4 *__restrict__ cen) {
+  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= ngroups) return;  // warp-uniform
+  const int4 G = grec[g];
+  double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
+  if (G.x + lane < G.y) {
+    const double4 p = gpos[G.x + lane];
+    l[0] = h[0] = p.x, l[1] = h[1] = p.y, l[2] = h[2] = p.z;
+  }
+  const unsigned FULL = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      l[d] = fmin(l[d], __shfl_xor_sync(FULL, l[d], o));
+      h[d] = fmax(h[d], __shfl_xor_sync(FULL, h[d], o));
+    }
+  if (lane == 0) {
+    blo[g] = make_double4(l[0], l[1], l[2], 0.0);
+    bhi[g] = make_double4(h[0], h[1], h[2], 0.0);
+    const double dx = __dsub_rn(h[0], l[0]), dy = __dsub_rn(h[1], l[1]),
+                 dz = __dsub_rn(h[2], l[2]);
+    cen[g] = make_double4(
+        __dmul_rn(0.5, __dadd_rn(l[0], h[0])), __dmul_rn(0.5, __dadd_rn(l[1], h[1])),
+        __dmul_rn(0.5, __dadd_rn(l[2], h[2])),
+        __dmul_rn(0.5, __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                            __dmul_rn(dz, dz)))));
+  }
+}
+
+// first index in [a, b) with v[index] >= x (lower) or > x (upper)
+template <typename V>
+__device__ __forceinline__ int lower_idx(const V *__restrict__ v, int a, int b, V x) {
+  while (a < b) {
+    const int m = (a + b) >> 1;
+    if (v[m] < x) a = m + 1;
+    else b = m;
+  }
+  return a;
+}
+__device__ __forceinline__ int upper_idx(const double *__restrict__ v, int a, int b, double x) {
+  while (a < b) {
+    const int m = (a + b) >> 1;
+    if (v[m] <= x) a = m + 1;
+    else b = m;
+  }
+  return a;
+}
+
+// Source segments of every group (warp per group; lanes over the fine
+// columns of the group's window in (s0, s1) order, so that a group's
+// segments come in the same order as a sequential sweep).  A fine column
+// contributes the z range of its sources within Rdir of the group's box:
+// |dz| <= sqrt(Rdir^2 - d_xy^2), d_xy the xy distance from the box to the
+// column; the half shell keeps the fine columns of later coarse columns and,
+// in the group's own coarse column, the sources after the group in the
+// group order.  FILL = false counts (segments, work, candidates); FILL =
+// true writes the segments at the offsets of the count pass.
+template <bool FILL>
+__global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ grec, long ngroups,
+                                      const double4 *__restrict__ blo,
+                                      const double4 *__restrict__ bhi,
+                                      const int *__restrict__ sstart, const double *__restrict__ zs,
+                                      const unsigned *__restrict__ fcpos, int *__restrict__ nseg,
+                                      int *__restrict__ nhseg, unsigned *__restrict__ work,
+                                      unsigned *__restrict__ hwork,
+                                      const int *__restrict__ segoff,
+                                      const int *__restrict__ hsegoff, int2 *__restrict__ segs,
+                                      int2 *__restrict__ hsegs, int4 *__restrict__ groups,
+                                      int4 *__restrict__ hgroups, SetupStats *st) {
+  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= ngroups) return;  // warp-uniform
+  const unsigned FULL = 0xffffffffu;
+  const int4 G = grec[g];
+  const int p0 = G.x, p1 = G.y, c = G.z;
+  const double4 L = blo[g], Hh = bhi[g];
+  const double bl[2] = {L.x, L.y}, bh[2] = {Hh.x, Hh.y};
+  int lo[2], hi[2];
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    // one column of margin on each side: the distance test below decides
+    lo[d] = max(0, (int)floor((bl[d] - gg.R - gg.mn[d]) / gg.sedge[d]) - 1);
+    hi[d] = min(gg.ns[d] - 1, (int)floor((bh[d] + gg.R - gg.mn[d]) / gg.sedge[d]) + 1);
+  }
+  const int w1 = hi[1] - lo[1] + 1;
+  const int nwin = (hi[0] - lo[0] + 1) * w1;
+  int ns_ = 0, nh_ = 0;
+  unsigned long long wk = 0, hwk = 0, cand = 0, hcand = 0;
+  const int base = FILL ? segoff[g] : 0, hbase = FILL ? hsegoff[g] : 0;
+  for (int t0 = 0; t0 < nwin; t0 += 32) {
+    const int t = t0 + lane;
+    bool has = false, hhas = false;
+    int a = 0, b = 0, a2 = 0;
+    if (t < nwin) {
+      const int s0 = lo[0] + t / w1, s1 = lo[1] + t % w1;
+      const long sc = (long)s0 * gg.ns[1] + s1;
+      const int zb = sstart[sc], ze = sstart[sc + 1];
+      if (ze > zb) {
+        const double l0 = __dadd_rn(gg.mn[0], __dmul_rn((double)s0, gg.sedge[0]));
+        const double h0 = __dadd_rn(l0, gg.sedge[0]);
+        const double l1 = __dadd_rn(gg.mn[1], __dmul_rn((double)s1, gg.sedge[1]));
+        const double h1 = __dadd_rn(l1, gg.sedge[1]);
+        const double dx = fmax(0.0, fmax(__dsub_rn(l0, bh[0]), __dsub_rn(bl[0], h0)));
+        const double dy = fmax(0.0, fmax(__dsub_rn(l1, bh[1]), __dsub_rn(bl[1], h1)));
+        const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+        if (d2 <= gg.R2) {
+          const double hz = __dsqrt_rn(__dsub_rn(gg.R2, d2));
+          const double zlo = __dsub_rn(L.z, hz), zhi = __dadd_rn(Hh.z, hz);
+          a = lower_idx(zs, zb, ze, zlo);
+          b = upper_idx(zs, a, ze, zhi);
+          has = b > a;
+          const long cc = (long)(s0 / kSourceSplit) * gg.nc1 + s1 / kSourceSplit;
+          if (has && cc >= c) {
+            a2 = cc == c ? lower_idx(fcpos, a, b, (unsigned)p1) : a;
+            hhas = b > a2;
+          }
+        }
+      }
+    }
+    const unsigned m = __ballot_sync(FULL, has), hm = __ballot_sync(FULL, hhas);
+    const unsigned below = (1u << lane) - 1u;
+    if (FILL) {
+      if (has) segs[base + ns_ + __popc(m & below)] = make_int2(a, b - a);
+      if (hhas) hsegs[hbase + nh_ + __popc(hm & below)] = make_int2(a2, b - a2);
+    }
+    ns_ += __popc(m);
+    nh_ += __popc(hm);
+    if (has) wk += (unsigned long long)(b - a);
+    if (hhas) hwk += (unsigned long long)(b - a2);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    wk += __shfl_xor_sync(FULL, wk, o);
+    hwk += __shfl_xor_sync(FULL, hwk, o);
+  }
+  if (lane == 0) {
+    if (FILL) {
+      groups[g] = make_int4(p0, p1 - p0, base, base + ns_);
+      hgroups[g] = make_int4(p0, p1 - p0, hbase, hbase + nh_);
+    } else {
+      nseg[g] = ns_;
+      nhseg[g] = nh_;
+      // heaviest first: sort keys are the complements of the work
+      work[g] = ~(unsigned)min(wk, 0xffffffffull);
+      hwork[g] = ~(unsigned)min(hwk, 0xffffffffull);
+      cand = wk * (unsigned long long)(p1 - p0);
+      hcand = hwk * (unsigned long long)(p1 - p0);
+      atomicAdd(&st->cand, cand);
+      atomicAdd(&st->hcand, hcand);
+    }
+  }
+}
+
+// final group records and frame origins in work order
+__global__ void order_groups_kernel(const int4 *__restrict__ gin, const double4 *__restrict__ cin,
+                                    const unsigned *__restrict__ ord, long ngroups,
+                                    int4 *__restrict__ gout, double4 *__restrict__ cout) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ngroups) return;
+  gout[k] = gin[ord[k]];
+  cout[k] = cin[ord[k]];
+}
+
+__global__ void iota_kernel(unsigned *__restrict__ v, long n) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) v[k] = (unsigned)k;
+}
+
+int bits_for(unsigned long long v) {  // bits to hold values < v
+  int b = 1;
+  while (b < 64 && (1ull << b) < v) b++;
+  return b;
+}
+
+inline unsigned blocks_for(long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// Scratch buffers of the set-up (handle-owned, reused by the next set-up).
+enum Scratch {
+  kPts, kBKey, kBKeyOut, kIota, kBPerm, kCCol, kSCol, kZKey, kZKeyOut, kZPerm, kColZ, kColOut,
+  kBCount, kCCount, kSCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
+  kGRec, kBLo, kBHi, kCen, kNSeg, kNHSeg, kWork, kHWork, kSegOff, kHSegOff, kUGroups, kUHGroups,
+  kWorkOut, kOrd, kStats, kCub, kScratchCount
+};
+static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
+
+#define SCK(call)                                                                         \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return record_error(h, NPME_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename P>
+int scratch(npme_handle *h, Scratch i, size_t bytes, P **out) {
+  const int rc = handle_buffer(h, &h->d_su[i], bytes);
+  *out = (P *)h->d_su[i];
+  return rc;
+}
+
+// CUB temporary storage of at least `bytes`
+int cub_tmp(npme_handle *h, size_t bytes, void **out) {
+  return scratch(h, kCub, std::max<size_t>(bytes, 256), out);
+}
+
+template <typename K>
+int sort_pairs(npme_handle *h, const K *kin, K *kout, const unsigned *vin, unsigned *vout,
+               long n, int end_bit, cudaStream_t s) {
+  size_t tb = 0;
+  SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
+  void *tmp;
+  int rc;
+  if ((rc = cub_tmp(h, tb, &tmp))) return rc;
+  SCK(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
+  return NPME_OK;
+}
+
+int exclusive_sum(npme_handle *h, const int *in, int *out, long n, cudaStream_t s) {
+  size_t tb = 0;
+  SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, (int)n, s));
+  void *tmp;
+  int rc;
+  if ((rc = cub_tmp(h, tb, &tmp))) return rc;
+  SCK(cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, (int)n, s));
+  return NPME_OK;
+}
+
+template <typename T>
+int bin_points(npme_handle *h) {
+  const long n = (long)h->n;
+  cudaStream_t s = h->stream;
+  const GridGeom &gr = h->grid;
+  const double *R = h->box + 3, *L = h->box + 6;
+  int rc;
+  SetupStats *st = (SetupStats *)h->d_su[kStats];
+  BinGeom g;
+  for (int d = 0; d < 3; d++) {
+    g.N[d] = (double)gr.N[d], g.L[d] = L[d], g.R[d] = R[d];
+    g.Nl[d] = gr.N[d], g.H[d] = gr.H[d], g.nb[d] = gr.nb[d];
+  }
+  g.P = gr.order;
+  g.TL = kBrick + gr.order - 1;
+  g.nkeys = 32 / ((int)(sizeof(T) / 4) * (h->complex_kernel ? 2 : 1));
+  // direct-sum columns: edge e ~ (32 / density)^(1/3) over the bounding box
+  // (degenerate axes are given a nominal thickness of Rdir / 4)
+  const double Rd = h->p.Rdir;
+  double vol = 1.0;
+  for (int d = 0; d < 3; d++) vol *= std::max(h->bmax[d] - h->bmin[d], 0.25 * Rd);
+  double e = std::cbrt(32.0 * vol / (double)n);
+  e = std::max(e, 1e-3 * Rd);
+  for (int d = 0; d < 2; d++) {
+    const double ext = h->bmax[d] - h->bmin[d];
+    g.nc[d] = std::max(1, std::min((int)std::ceil(ext / e), 1 << 14));
+    g.edge[d] = std::max(ext / g.nc[d], 1e-12);
+    g.ns[d] = g.nc[d] * kSourceSplit;
+    g.sedge[d] = g.edge[d] / kSourceSplit;
+    g.mn[d] = h->bmin[d];
+  }
+  // heads of offsets up to ~the group half-diagonal carry ~6e-8 e absolute
+  // error; below r = e/4 the relative error would exceed ~1e-6, so refine
+  h->refine2 = (0.25 * e) * (0.25 * e);
+  const long nbt = gr.nb[0] * gr.nb[1] * gr.nb[2];
+  const long ncol = (long)g.nc[0] * g.nc[1], nscol = (long)g.ns[0] * g.ns[1];
+  h->n_bricks = nbt;
+
+  BrickPoint<T> *pts;
+  unsigned *bkey, *bkey_out, *iota, *bperm, *ccol, *scol, *colz, *colout, *zperm;
+  unsigned long long *zkey, *zkey_out;
+  int *bcount, *ccount, *scount, *cstart, *sstart, *flag, *pos;
+  if ((rc = scratch(h, kPts, sizeof(BrickPoint<T>) * n, &pts)) ||
+      (rc = scratch(h, kBKey, sizeof(unsigned) * n, &bkey)) ||
+      (rc = scratch(h, kBKeyOut, sizeof(unsigned) * n, &bkey_out)) ||
+      (rc = scratch(h, kIota, sizeof(unsigned) * n, &iota)) ||
+      (rc = scratch(h, kBPerm, sizeof(unsigned) * n, &bperm)) ||
+      (rc = scratch(h, kCCol, sizeof(unsigned) * n, &ccol)) ||
+      (rc = scratch(h, kSCol, sizeof(unsigned) * n, &scol)) ||
+      (rc = scratch(h, kColZ, sizeof(unsigned) * n, &colz)) ||
+      (rc = scratch(h, kColOut, sizeof(unsigned) * n, &colout)) ||
+      (rc = scratch(h, kZPerm, sizeof(unsigned) * n, &zperm)) ||
+      (rc = scratch(h, kZKey, sizeof(unsigned long long) * n, &zkey)) ||
+      (rc = scratch(h, kZKeyOut, sizeof(unsigned long long) * n, &zkey_out)) ||
+      (rc = scratch(h, kBCount, sizeof(int) * (nbt + 1), &bcount)) ||
+      (rc = scratch(h, kCCount, sizeof(int) * (ncol + 1), &ccount)) ||
+      (rc = scratch(h, kSCount, sizeof(int) * (nscol + 1), &scount)) ||
+      (rc = scratch(h, kCStart, sizeof(int) * (ncol + 1), &cstart)) ||
+      (rc = scratch(h, kSStart, sizeof(int) * (nscol + 1), &sstart)) ||
+      (rc = scratch(h, kFlag, sizeof(int) * (nbt + 1), &flag)) ||
+      (rc = scratch(h, kPos, sizeof(int) * (nbt + 1), &pos)))
+    return rc;
+  const int C = h->complex_kernel ? 2 : 1;
+  if ((rc = handle_buffer(h, &h->d_bpts, sizeof(BrickPoint<T>) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_brick_start, sizeof(int) * (nbt + 1))) ||
+      (rc = handle_buffer(h, (void **)&h->d_cperm, sizeof(uint32_t) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_sperm, sizeof(uint32_t) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_gpos, sizeof(double4) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_spos, sizeof(double4) * n)) ||
+      (rc = handle_buffer(h, &h->d_qb, sizeof(T) * C * n)) ||
+      (rc = handle_buffer(h, &h->d_qc, sizeof(T) * C * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_q_in, sizeof(double) * C * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_V, sizeof(double) * 4 * C * n)))
+    return rc;
+
+  SCK(cudaMemsetAsync(bcount, 0, sizeof(int) * (nbt + 1), s));
+  SCK(cudaMemsetAsync(ccount, 0, sizeof(int) * (ncol + 1), s));
+  SCK(cudaMemsetAsync(scount, 0, sizeof(int) * (nscol + 1), s));
+  bin_kernel<T><<<blocks_for(n), 256, 0, s>>>(h->d_coord, n, g, pts, bkey, ccol, scol, zkey, iota,
+                                              bcount, ccount, scount, st);
+  SCK(cudaGetLastError());
+
+  // --- brick order: (brick, bank key, index) ---
+  if ((rc = sort_pairs(h, bkey, bkey_out, iota, bperm, n, 5 + bits_for(nbt), s))) return rc;
+  gather_bpts_kernel<T><<<blocks_for(n), 256, 0, s>>>(pts, bperm, n, (BrickPoint<T> *)h->d_bpts);
+  if ((rc = exclusive_sum(h, bcount, h->d_brick_start, nbt + 1, s))) return rc;
+  nonempty_flags_kernel<<<blocks_for(nbt + 1), 256, 0, s>>>(bcount, nbt, flag);
+  if ((rc = exclusive_sum(h, flag, pos, nbt + 1, s))) return rc;
+
+  // --- direct-sum orders: (column, z, index) for targets and sources ---
+  if ((rc = sort_pairs(h, zkey, zkey_out, iota, zperm, n, 64, s))) return rc;
+  gather_u32_kernel<<<blocks_for(n), 256, 0, s>>>(ccol, zperm, n, colz);
+  if ((rc = sort_pairs(h, colz, colout, zperm, h->d_cperm, n, bits_for(ncol), s))) return rc;
+  gather_u32_kernel<<<blocks_for(n), 256, 0, s>>>(scol, zperm, n, colz);
+  if ((rc = sort_pairs(h, colz, colout, zperm, h->d_sperm, n, bits_for(nscol), s))) return rc;
+  if ((rc = exclusive_sum(h, ccount, cstart, ncol + 1, s))) return rc;
+  if ((rc = exclusive_sum(h, scount, sstart, nscol + 1, s))) return rc;
+  gather_positions_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_cperm, h->d_sperm, n,
+                                                        h->d_gpos, h->d_spos);
+  double *zs;
+  unsigned *cpos, *fcpos;
+  int *gcount, *goff;
+  if ((rc = scratch(h, kZs, sizeof(double) * n, &zs)) ||
+      (rc = scratch(h, kCPos, sizeof(unsigned) * n, &cpos)) ||
+      (rc = scratch(h, kFCPos, sizeof(unsigned) * n, &fcpos)) ||
+      (rc = scratch(h, kGCount, sizeof(int) * (ncol + 1), &gcount)) ||
+      (rc = scratch(h, kGOff, sizeof(int) * (ncol + 1), &goff)))
+    return rc;
+  source_z_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_sperm, h->d_cperm, n, zs, cpos);
+  gather_u32_kernel<<<blocks_for(n), 256, 0, s>>>(cpos, h->d_sperm, n, fcpos);
+  groups_per_column_kernel<<<blocks_for(ncol + 1), 256, 0, s>>>(ccount, ncol, gcount);
+  if ((rc = exclusive_sum(h, gcount, goff, ncol + 1, s))) return rc;
+  SCK(cudaGetLastError());
+
+  // read back: groups, non-empty bricks, the stencil check
+  struct {
+    int ngroups, nnonempty, lastflag;
+    long long bad;
+  } rb;
+  SCK(cudaMemcpyAsync(&rb.ngroups, goff + ncol, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SCK(cudaMemcpyAsync(&rb.nnonempty, pos + nbt, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SCK(cudaMemcpyAsync(&rb.bad, &st->bad, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  SCK(cudaStreamSynchronize(s));
+  if (rb.bad < n) {
+    // the axis of the first offending point, from its coordinates
+    double x[3];
+    SCK(cudaMemcpy(x, h->d_coord + 3 * rb.bad, sizeof(x), cudaMemcpyDeviceToHost));
+    int axis = 0;
+    for (int d = 0; d < 3; d++) {
+      const double w = (double)gr.N[d] / L[d] * (x[d] - R[d]);
+      const long ms = w < 0 ? (long)(-w) + 1 : (long)(-w);
+      const long o = ms + gr.N[d] / 4;
+      if (o < 0 || o + gr.order - 1 > gr.H[d] - 1) {
+        axis = d;
+        break;
+      }
+    }
+    return record_error(h, NPME_EINVAL,
+                        "point " + std::to_string(rb.bad) + " has a B-spline stencil outside "
+                        "the charge octant (axis " + std::to_string(axis) + ")");
+  }
+  h->n_nonempty = rb.nnonempty;
+  if ((rc = handle_buffer(h, (void **)&h->d_brick_list,
+                          sizeof(int) * std::max<long>(1, rb.nnonempty))))
+    return rc;
+  brick_list_kernel<<<blocks_for(nbt), 256, 0, s>>>(bcount, pos, nbt, h->d_brick_list);
+
+  // --- warp groups and their source segments ---
+  const long ng = rb.ngroups;
+  int4 *grec;
+  double4 *blo, *bhi, *cen;
+  int *nseg, *nhseg, *segoff, *hsegoff;
+  unsigned *work, *hwork, *work_out, *ord;
+  int4 *ug, *uh;
+  if ((rc = scratch(h, kGRec, sizeof(int4) * ng, &grec)) ||
+      (rc = scratch(h, kBLo, sizeof(double4) * ng, &blo)) ||
+      (rc = scratch(h, kBHi, sizeof(double4) * ng, &bhi)) ||
+      (rc = scratch(h, kCen, sizeof(double4) * ng, &cen)) ||
+      (rc = scratch(h, kNSeg, sizeof(int) * (ng + 1), &nseg)) ||
+      (rc = scratch(h, kNHSeg, sizeof(int) * (ng + 1), &nhseg)) ||
+      (rc = scratch(h, kSegOff, sizeof(int) * (ng + 1), &segoff)) ||
+      (rc = scratch(h, kHSegOff, sizeof(int) * (ng + 1), &hsegoff)) ||
+      (rc = scratch(h, kWork, sizeof(unsigned) * ng, &work)) ||
+      (rc = scratch(h, kHWork, sizeof(unsigned) * ng, &hwork)) ||
+      (rc = scratch(h, kWorkOut, sizeof(unsigned) * ng, &work_out)) ||
+      (rc = scratch(h, kOrd, sizeof(unsigned) * ng, &ord)) ||
+      (rc = scratch(h, kUGroups, sizeof(int4) * ng, &ug)) ||
+      (rc = scratch(h, kUHGroups, sizeof(int4) * ng, &uh)))
+    return rc;
+  group_records_kernel<<<blocks_for(ncol), 256, 0, s>>>(cstart, goff, ncol, grec);
+  group_box_kernel<<<blocks_for(32 * ng), 256, 0, s>>>(h->d_gpos, grec, ng, blo, bhi, cen);
+  GroupGeom gg;
+  gg.R = Rd, gg.R2 = Rd * Rd;
+  for (int d = 0; d < 2; d++) gg.mn[d] = g.mn[d], gg.sedge[d] = g.sedge[d], gg.ns[d] = g.ns[d];
+  gg.nc1 = g.nc[1];
+  SCK(cudaMemsetAsync(nseg + ng, 0, sizeof(int), s));
+  SCK(cudaMemsetAsync(nhseg + ng, 0, sizeof(int), s));
+  group_segments_kernel<false><<<blocks_for(32 * ng), 256, 0, s>>>(
+      gg, grec, ng, blo, bhi, sstart, zs, fcpos, nseg, nhseg, work, hwork, nullptr, nullptr,
+      nullptr, nullptr, nullptr, nullptr, st);
+  if ((rc = exclusive_sum(h, nseg, segoff, ng + 1, s))) return rc;
+  if ((rc = exclusive_sum(h, nhseg, hsegoff, ng + 1, s))) return rc;
+  SCK(cudaGetLastError());
+  struct {
+    int nsegs, nhsegs;
+    unsigned long long cand, hcand;
+  } sb;
+  SCK(cudaMemcpyAsync(&sb.nsegs, segoff + ng, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SCK(cudaMemcpyAsync(&sb.nhsegs, hsegoff + ng, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SCK(cudaMemcpyAsync(&sb.cand, &st->cand, 2 * sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost, s));
+  SCK(cudaStreamSynchronize(s));
+  if (sb.nsegs < 0 || sb.nhsegs < 0)  // int offsets of the group records
+    return record_error(h, NPME_EINVAL, "too many direct-sum source segments (2^31)");
+  if ((rc = handle_buffer(h, (void **)&h->d_segs, sizeof(int2) * std::max(1, sb.nsegs))) ||
+      (rc = handle_buffer(h, (void **)&h->d_hsegs, sizeof(int2) * std::max(1, sb.nhsegs))) ||
+      (rc = handle_buffer(h, (void **)&h->d_groups, sizeof(int4) * ng)) ||
+      (rc = handle_buffer(h, (void **)&h->d_gcen, sizeof(double4) * ng)) ||
+      (rc = handle_buffer(h, (void **)&h->d_hgroups, sizeof(int4) * ng)) ||
+      (rc = handle_buffer(h, (void **)&h->d_hcen, sizeof(double4) * ng)))
+    return rc;
+  group_segments_kernel<true><<<blocks_for(32 * ng), 256, 0, s>>>(
+      gg, grec, ng, blo, bhi, sstart, zs, fcpos, nullptr, nullptr, nullptr, nullptr, segoff,
+      hsegoff, h->d_segs, h->d_hsegs, ug, uh, st);
+  // heaviest groups first, so that the last wave of a launch holds the light
+  // ones (each list by its own work; ties keep the column order)
+  iota_kernel<<<blocks_for(ng), 256, 0, s>>>(iota, ng);
+  if ((rc = sort_pairs(h, work, work_out, iota, ord, ng, 32, s))) return rc;
+  order_groups_kernel<<<blocks_for(ng), 256, 0, s>>>(ug, cen, ord, ng, h->d_groups, h->d_gcen);
+  if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ng, 32, s))) return rc;
+  order_groups_kernel<<<blocks_for(ng), 256, 0, s>>>(uh, cen, ord, ng, h->d_hgroups, h->d_hcen);
+  SCK(cudaGetLastError());
+  h->n_groups = h->n_hgroups = ng;
+  h->n_segs = sb.nsegs;
+  h->n_hsegs = sb.nhsegs;
+  h->cand_per_point = (double)sb.cand / (double)n;
+  h->hcand_per_point = (double)sb.hcand / (double)n;
+  h->d_dperm = h->d_sperm;  // direct-sum charges are gathered into the source order
+
+  // source-side sums of the pair-once walk start (and are kept) at zero
+  if (h->fp32) {
+    const size_t nv = (size_t)C * n;  // float4 per source (two if complex)
+    if ((rc = handle_buffer(h, (void **)&h->d_vsrc, sizeof(float4) * nv))) return rc;
+    SCK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * nv, s));
+  } else {
+    if ((rc = handle_buffer(h, (void **)&h->d_vsrc64, sizeof(double) * 4 * n))) return rc;
+    SCK(cudaMemsetAsync(h->d_vsrc64, 0, sizeof(double) * 4 * n, s));
+  }
+
+  // --- grids ---
+  const long *N = gr.N;
+  const size_t Ntot = (size_t)N[0] * N[1] * N[2];
+  const size_t Mtot = (size_t)(N[0] / 2 + 1) * (N[1] / 2 + 1) * (N[2] / 2 + 1);
+  if (h->complex_kernel) {
+    if ((rc = handle_buffer(h, &h->d_grid, sizeof(T) * 2 * Ntot)) ||
+        (rc = handle_buffer(h, &h->d_G, sizeof(T) * 2 * Mtot)))
+      return rc;
+  } else {
+    if ((rc = handle_buffer(h, &h->d_grid, sizeof(T) * Ntot)) ||
+        (rc = handle_buffer(h, &h->d_kgrid, sizeof(T) * 2 * (size_t)N[0] * N[1] * (N[2] / 2 + 1))) ||
+        (rc = handle_buffer(h, &h->d_G, sizeof(T) * Mtot)))
+      return rc;
+  }
+  return NPME_OK;
+}
+
+}  // namespace
+
+int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3]) {
+  const long n = (long)h->n;
+  cudaStream_t s = h->stream;
+  int rc;
+  if ((rc = handle_buffer(h, (void **)&h->d_coord, sizeof(double) * 3 * n))) return rc;
+  SetupStats *st;
+  if ((rc = scratch(h, kStats, sizeof(SetupStats), &st))) return rc;
+  SCK(cudaMemcpyAsync(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  init_stats_kernel<<<1, 1, 0, s>>>(st, n);
+  const unsigned blocks = (unsigned)std::min<long>(blocks_for(n), 148 * 8);
+  bbox_kernel<<<blocks, 256, 0, s>>>(h->d_coord, n, st);
+  SCK(cudaGetLastError());
+  SetupStats hs;
+  SCK(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  SCK(cudaStreamSynchronize(s));
+  if (hs.nonfinite) return record_error(h, NPME_EINVAL, "non-finite coordinate");
+  for (int d = 0; d < 3; d++) mn[d] = dkey_inv(hs.mn[d]), mx[d] = dkey_inv(hs.mx[d]);
+  return NPME_OK;
+}
+
+int device_bin(npme_handle *h) {
+  return h->fp32 ? bin_points<float>(h) : bin_points<double>(h);
+}
+
+}  // namespace npme
