@@ -154,6 +154,23 @@ def profile_traffic(kernel):
         return None
 
 
+def fp32_peak(device):
+    """FP32 FMA-pipe throughput of this GPU (TFLOP/s) from the probe library
+    npme_b200/libnpme_peak.so (best of scalar and two-wide FMA chains on
+    every SM), or None when it is not built."""
+    import ctypes
+    path = os.path.join(ROOT, "npme_b200", "libnpme_peak.so")
+    if not os.path.exists(path):
+        return None, None
+    L = ctypes.CDLL(path)
+    L.npme_peak_fp32.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    tf, ms = ctypes.c_double(), ctypes.c_double()
+    if L.npme_peak_fp32(device, 2048, 5, ctypes.byref(tf), ctypes.byref(ms)) != 0:
+        return None, None
+    return tf.value, ms.value
+
+
 def cpu_baseline(w, args):
     """The reference's own CPU implementation (oracle/_ref, built from the
     reference sources) timed on this host: setup once, then CalcV calls."""
@@ -527,6 +544,8 @@ def main():
         t0 = time.perf_counter()
         s.calcv(qh, out=Vh)
         e2e_ts.append(time.perf_counter() - t0)
+    # the FP32 pipe's measured throughput, at the clocks of this same sample
+    peak_tf, peak_ms = fp32_peak(local)
     clocks = sampler.stop()
     e2e_s = sum(e2e_ts)
 
@@ -616,9 +635,11 @@ def main():
         nd = w.nDeriv
         pairs = info0.get("pairs")
         flops_pair = DIRECT_FLOPS_PER_PAIR[w.func](nd)
-        fp_peak = 148 * 128 * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
+        fp_nominal = 148 * 128 * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
         if args.precision == "fp64":
-            fp_peak /= 2
+            fp_nominal /= 2
+        measured = args.precision == "fp32" and peak_tf is not None
+        fp_peak = peak_tf if measured else fp_nominal
         achieved = (pairs * flops_pair / (st["direct"] / 1e3) / 1e12
                     if pairs and st["direct"] > 0 else None)
         if info0.get("pairsOnce"):
@@ -630,8 +651,13 @@ def main():
                     "achieved": achieved, "peak": fp_peak, "unit": "TFLOP/s",
                     "frac": (achieved / fp_peak) if achieved else None,
                     "traffic": profile_traffic(dk),
-                    "peak_source": "nominal 148 SM x 128 lanes x 2 flop at the sampled median "
-                                   "SM clock (MEASURED_PEAKS.json has no FP32 figure)",
+                    "peak_source": (
+                        "measured: FP32 FMA chains on every SM (npme_peak_fp32, best of scalar "
+                        "and two-wide FMA, %.2f ms launch) run inside the clock sample; "
+                        "MEASURED_PEAKS.json has no FP32 figure" % peak_ms) if measured else
+                    "nominal 148 SM x 128 lanes x 2 flop at the sampled median SM clock",
+                    "nominal_peak": fp_nominal,
+                    "frac_of_nominal": (achieved / fp_nominal) if achieved else None,
                     "work": f"{pairs} unordered pairs within Rdir x {flops_pair} flop"}
         hbm = peaks.get("hbm_gbs", 6535.7)
         G = (w.grid[0] // 2) * (w.grid[1] // 2) * (w.grid[2] // 2)

@@ -77,8 +77,24 @@ def build(force=False, verbose=False):
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + p.stderr[-4000:])
+    build_peak(force)
     build_apps(force)
     return LIB
+
+
+PEAK = os.path.join(HERE, "libnpme_peak.so")
+
+
+def build_peak(force=False):
+    """The FP32 FMA throughput probe bench.py reports as the direct sum's
+    roofline peak (npme_b200/libnpme_peak.so, C entry npme_peak_fp32)."""
+    src = os.path.join(CSRC, "peak.cu")
+    if not force and not _stale(PEAK, [src]):
+        return
+    cmd = [nvcc()] + FLAGS + ["-shared", "-o", PEAK, src]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + p.stderr[-4000:])
 
 
 def build_apps(force=False):

@@ -92,22 +92,25 @@ __global__ void __launch_bounds__(256) batch_spread_kernel(const BatchSys *__res
                               S.nb2, S.nb3, S.N1, S.N2, S.N3, reinterpret_cast<int *>(smem_raw));
 }
 
+// one warp per spectrum row of one system (units: rows)
 template <bool CPLX>
 __global__ void batch_multiply_kernel(const BatchSys *__restrict__ sys,
                                       const long long *__restrict__ off, int count) {
   const long long total = off[count];
-  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total;
-       u += (long long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (long long u = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; u < total;
+       u += (gridDim.x * (long long)blockDim.x) >> 5) {
     const int s = find_sys(off, count, u);
     const BatchSys &S = sys[s];
     const int M2 = (int)(S.N2 / 2 + 1), M3 = (int)(S.N3 / 2 + 1);
+    const int r = (int)(u - off[s]);
     if (CPLX)
-      multiply_cplx_body<float>(reinterpret_cast<float2 *>(S.grid),
-                                reinterpret_cast<const float2 *>(S.G), (long)(u - off[s]), S.N1,
-                                S.N2, S.N3, M2, M3);
+      multiply_cplx_row<float>(reinterpret_cast<float2 *>(S.grid),
+                               reinterpret_cast<const float2 *>(S.G), r, (int)S.N1, (int)S.N2,
+                               (int)S.N3, M2, M3, lane);
     else
-      multiply_real_body<float>(S.kgrid, S.G, (long)(u - off[s]), S.N1, S.N2, S.N3 / 2 + 1, M2,
-                                M3);
+      multiply_real_row<float>(S.kgrid, S.G, r, (int)S.N1, (int)S.N2, (int)(S.N3 / 2 + 1), M2,
+                               M3, lane);
   }
 }
 
@@ -381,10 +384,9 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   }
   auto units_gather = [&](int k) { return (long long)hs[f32[k]]->n; };
   auto units_spread = [&](int k) { return (long long)hs[f32[k]]->n_nonempty; };
-  auto units_mult = [&](int k) {
-    const npme_handle *h = hs[f32[k]];
-    const long *N = h->grid.N;
-    return (long long)N[0] * N[1] * (h->complex_kernel ? N[2] : N[2] / 2 + 1);
+  auto units_mult = [&](int k) {  // spectrum rows
+    const long *N = hs[f32[k]]->grid.N;
+    return (long long)N[0] * N[1];
   };
   auto units_dir = [&](int k) {
     const npme_handle *h = hs[f32[k]];
@@ -554,7 +556,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   // 5. kernel multiply
   for (auto &kv : mult) {
     Class &c = kv.second;
-    const unsigned g = grid_of(c.off.back(), 256, 148 * 16);
+    const unsigned g = grid_of(c.off.back(), 8, 148 * 16);  // 8 rows (warps) per CTA
     if (kv.first) batch_multiply_kernel<true><<<g, 256, 0, s>>>(D(c), O(c), (int)c.members.size());
     else batch_multiply_kernel<false><<<g, 256, 0, s>>>(D(c), O(c), (int)c.members.size());
     b->launches++;

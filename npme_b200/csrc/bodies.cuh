@@ -38,16 +38,20 @@ __device__ __forceinline__ void gather_body(const double *__restrict__ q,
   }
 }
 
-// Points of a brick are stored sorted by the shared-memory bank of their
-// stencil origin in the brick's tile (set-up, npme_gpu.cu).  Virtual warp vw
-// of a brick with nb points takes the points at positions lane * W + vw of
-// that order (W = ceil(nb / 32) virtual warps), so the 32 lanes of a warp
-// hold points of 32 different banks as long as no bank holds more than W
-// points: the shared-memory accesses of a stencil step are then free of bank
-// conflicts and of colliding atomics.
+// Points of a brick are stored in rounds over the shared-memory banks of
+// their stencil origins in the brick's tile (set-up, setup.cu): round r holds
+// the r-th point of every bank that has more than r points, in bank order.
+// Virtual warp vw of a brick with nb points takes the 32 consecutive points
+// at positions 32 vw + lane (contiguous record loads).  Two lanes share a
+// bank only where a warp's run of 32 spans rounds; but the bank counts of a
+// brick are Poisson-like (uniform points over 512 stencil origins, 16 per
+// bank), so a brick's fullest bank usually holds more points than the brick
+// has warps, and no assignment of one point per lane avoids conflicts: at
+// 1M points (244 per brick) a stencil step costs 2.08 shared wavefronts per
+// warp on average, against 1.71 for the best possible assignment and 1 for
+// none.
 __device__ __forceinline__ int brick_point(int nb, int vw, int lane) {
-  const int W = (nb + 31) >> 5;
-  const int p = lane * W + vw;
+  const int p = vw * 32 + lane;
   return p < nb ? p : -1;
 }
 
@@ -211,36 +215,48 @@ __device__ __forceinline__ void spread_brick_fixed(int brick, const int *__restr
   }
 }
 
-// X(k) *= G(|k1|, |k2|, k3) on the R2C half spectrum (src/RecSumV.cpp:639-707).
+// X(k) *= G(|k1|, |k2|, k3) on the R2C half spectrum (src/RecSumV.cpp:639-707),
+// one spectrum row (k1, k2) = (r / N2, r % N2) per warp: one division per
+// row, and the lanes stride the row's contiguous k3 run (coalesced X and G
+// rows; the compact G octant stays in L2).
 template <typename T>
-__device__ __forceinline__ void multiply_real_body(typename Vec2<T>::type *__restrict__ X,
-                                                   const T *__restrict__ G, long idx, long N1,
-                                                   long N2, long N3h, int M2, int M3) {
-  const long k3 = idx % N3h, k2 = (idx / N3h) % N2, k1 = idx / (N3h * N2);
-  const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
-  const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
-  const T g = __ldg(G + (f1 * M2 + f2) * M3 + k3);
-  typename Vec2<T>::type v = X[idx];
-  v.x *= g;
-  v.y *= g;
-  X[idx] = v;
+__device__ __forceinline__ void multiply_real_row(typename Vec2<T>::type *__restrict__ X,
+                                                  const T *__restrict__ G, int r, int N1, int N2,
+                                                  int N3h, int M2, int M3, int lane) {
+  const int k1 = r / N2, k2 = r - k1 * N2;
+  const int f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
+  const int f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
+  const T *__restrict__ g = G + ((long)f1 * M2 + f2) * M3;
+  typename Vec2<T>::type *__restrict__ x = X + (long)r * N3h;
+  for (int k3 = lane; k3 < N3h; k3 += 32) {
+    const T gv = __ldg(g + k3);
+    typename Vec2<T>::type v = x[k3];
+    v.x *= gv;
+    v.y *= gv;
+    x[k3] = v;
+  }
 }
 
-// X(k) *= G(|k1|, |k2|, |k3|) on the full complex spectrum.
+// X(k) *= G(|k1|, |k2|, |k3|) on the full complex spectrum, one row per warp.
 template <typename T>
-__device__ __forceinline__ void multiply_cplx_body(typename Vec2<T>::type *__restrict__ X,
-                                                   const typename Vec2<T>::type *__restrict__ G,
-                                                   long idx, long N1, long N2, long N3, int M2,
-                                                   int M3) {
-  const long k3 = idx % N3, k2 = (idx / N3) % N2, k1 = idx / (N3 * N2);
-  const long f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
-  const long f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
-  const long f3 = k3 <= N3 / 2 ? k3 : N3 - k3;
-  const typename Vec2<T>::type g = G[(f1 * M2 + f2) * M3 + f3];
-  typename Vec2<T>::type v = X[idx], o;
-  o.x = v.x * g.x - v.y * g.y;
-  o.y = v.x * g.y + v.y * g.x;
-  X[idx] = o;
+__device__ __forceinline__ void multiply_cplx_row(typename Vec2<T>::type *__restrict__ X,
+                                                  const typename Vec2<T>::type *__restrict__ G,
+                                                  int r, int N1, int N2, int N3, int M2, int M3,
+                                                  int lane) {
+  const int k1 = r / N2, k2 = r - k1 * N2;
+  const int f1 = k1 <= N1 / 2 ? k1 : N1 - k1;
+  const int f2 = k2 <= N2 / 2 ? k2 : N2 - k2;
+  const typename Vec2<T>::type *__restrict__ g = G + ((long)f1 * M2 + f2) * M3;
+  typename Vec2<T>::type *__restrict__ x = X + (long)r * N3;
+  for (int k3 = lane; k3 < N3; k3 += 32) {
+    const int f3 = k3 <= N3 / 2 ? k3 : N3 - k3;
+    const typename Vec2<T>::type gv = g[f3];
+    const typename Vec2<T>::type v = x[k3];
+    typename Vec2<T>::type o;
+    o.x = v.x * gv.x - v.y * gv.y;
+    o.y = v.x * gv.y + v.y * gv.x;
+    x[k3] = o;
+  }
 }
 
 // One element of the windowed eight-image sum that samples f_LR on the

@@ -434,42 +434,48 @@ void launch_spread(npme_handle *h, cudaStream_t s) {
 
 template <typename T>
 __global__ void multiply_real_kernel(typename Vec2<T>::type *__restrict__ X,
-                                     const T *__restrict__ G, long N1, long N2, long N3h,
-                                     int M2, int M3) {
-  const long total = N1 * N2 * N3h;
-  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x)
-    multiply_real_body<T>(X, G, idx, N1, N2, N3h, M2, M3);
+                                     const T *__restrict__ G, int N1, int N2, int N3h, int M2,
+                                     int M3) {
+  const int rows = N1 * N2, lane = threadIdx.x & 31;
+  for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < rows;
+       r += (int)((gridDim.x * blockDim.x) >> 5))
+    multiply_real_row<T>(X, G, r, N1, N2, N3h, M2, M3, lane);
 }
 
 template <typename T>
 __global__ void multiply_cplx_kernel(typename Vec2<T>::type *__restrict__ X,
-                                     const typename Vec2<T>::type *__restrict__ G, long N1,
-                                     long N2, long N3, int M2, int M3) {
-  const long total = N1 * N2 * N3;
-  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x)
-    multiply_cplx_body<T>(X, G, idx, N1, N2, N3, M2, M3);
+                                     const typename Vec2<T>::type *__restrict__ G, int N1, int N2,
+                                     int N3, int M2, int M3) {
+  const int rows = N1 * N2, lane = threadIdx.x & 31;
+  for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < rows;
+       r += (int)((gridDim.x * blockDim.x) >> 5))
+    multiply_cplx_row<T>(X, G, r, N1, N2, N3, M2, M3, lane);
 }
 
 void launch_multiply(npme_handle *h, cudaStream_t s) {
   const long *N = h->grid.N;
   const int M2 = N[1] / 2 + 1, M3 = N[2] / 2 + 1;
-  const int threads = 256, blocks = 148 * 16;
+  // one warp per spectrum row, 8 rows per CTA, as many CTAs as rows need
+  // (at most 148 x 16, each then looping)
+  const int threads = 256;
+  const int blocks = (int)std::min<long>(148 * 16, (N[0] * N[1] + 7) / 8);
   if (h->complex_kernel) {
     if (h->fp32)
       multiply_cplx_kernel<float><<<blocks, threads, 0, s>>>(
-          (float2 *)h->d_grid, (const float2 *)h->d_G, N[0], N[1], N[2], M2, M3);
+          (float2 *)h->d_grid, (const float2 *)h->d_G, (int)N[0], (int)N[1], (int)N[2], M2, M3);
     else
       multiply_cplx_kernel<double><<<blocks, threads, 0, s>>>(
-          (double2 *)h->d_grid, (const double2 *)h->d_G, N[0], N[1], N[2], M2, M3);
+          (double2 *)h->d_grid, (const double2 *)h->d_G, (int)N[0], (int)N[1], (int)N[2], M2,
+          M3);
   } else {
     if (h->fp32)
       multiply_real_kernel<float><<<blocks, threads, 0, s>>>(
-          (float2 *)h->d_kgrid, (const float *)h->d_G, N[0], N[1], N[2] / 2 + 1, M2, M3);
+          (float2 *)h->d_kgrid, (const float *)h->d_G, (int)N[0], (int)N[1],
+          (int)(N[2] / 2 + 1), M2, M3);
     else
       multiply_real_kernel<double><<<blocks, threads, 0, s>>>(
-          (double2 *)h->d_kgrid, (const double *)h->d_G, N[0], N[1], N[2] / 2 + 1, M2, M3);
+          (double2 *)h->d_kgrid, (const double *)h->d_G, (int)N[0], (int)N[1],
+          (int)(N[2] / 2 + 1), M2, M3);
   }
   h->launches++;
 }

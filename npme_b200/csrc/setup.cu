@@ -185,6 +185,29 @@ __global__ void gather_bpts_kernel(const BrickPoint<T> *__restrict__ pts,
   if (k < n) out[k] = pts[perm[k]];
 }
 
+// Start of the run of equal (brick, bank) keys at each position k of the
+// brick-sorted order (k itself where a run starts, else 0; a max-scan then
+// gives every position its run's start).
+__global__ void run_head_kernel(const unsigned *__restrict__ key, long n, int *__restrict__ head) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) head[k] = (k == 0 || key[k] != key[k - 1]) ? (int)k : 0;
+}
+
+// Round-robin key (brick, rank inside its bank, bank): sorting by it puts
+// the r-th point of every bank of a brick into round r.
+__global__ void round_key_kernel(const unsigned *__restrict__ key, const int *__restrict__ start,
+                                 long n, unsigned long long *__restrict__ rkey) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const unsigned kk = key[k];
+  rkey[k] = ((unsigned long long)(kk >> 5) << 37) | ((unsigned long long)(k - start[k]) << 5) |
+            (unsigned long long)(kk & 31u);
+}
+
+struct MaxOp {
+  __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
+};
+
 __global__ void gather_u32_kernel(const unsigned *__restrict__ src,
                                   const unsigned *__restrict__ perm, long n,
                                   unsigned *__restrict__ out) {
@@ -438,7 +461,7 @@ enum Scratch {
   kPts, kBKey, kBKeyOut, kIota, kBPerm, kCCol, kSCol, kZKey, kZKeyOut, kZPerm, kColZ, kColOut,
   kBCount, kCCount, kSCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
   kGRec, kBLo, kBHi, kCen, kNSeg, kNHSeg, kWork, kHWork, kSegOff, kHSegOff, kUGroups, kUHGroups,
-  kWorkOut, kOrd, kStats, kCub, kScratchCount
+  kWorkOut, kOrd, kStats, kCub, kHead, kRunStart, kRKey, kRKeyOut, kBPerm2, kScratchCount
 };
 static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
 
@@ -470,6 +493,16 @@ int sort_pairs(npme_handle *h, const K *kin, K *kout, const unsigned *vin, unsig
   int rc;
   if ((rc = cub_tmp(h, tb, &tmp))) return rc;
   SCK(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
+  return NPME_OK;
+}
+
+int inclusive_max(npme_handle *h, const int *in, int *out, long n, cudaStream_t s) {
+  size_t tb = 0;
+  SCK(cub::DeviceScan::InclusiveScan(nullptr, tb, in, out, MaxOp(), (int)n, s));
+  void *tmp;
+  int rc;
+  if ((rc = cub_tmp(h, tb, &tmp))) return rc;
+  SCK(cub::DeviceScan::InclusiveScan(tmp, tb, in, out, MaxOp(), (int)n, s));
   return NPME_OK;
 }
 
@@ -565,9 +598,26 @@ int bin_points(npme_handle *h) {
                                               bcount, ccount, scount, st);
   SCK(cudaGetLastError());
 
-  // --- brick order: (brick, bank key, index) ---
+  // --- brick order: by brick, inside a brick in rounds over the banks ---
+  // (brick, bank, index) first, then (brick, rank inside the bank, bank)
   if ((rc = sort_pairs(h, bkey, bkey_out, iota, bperm, n, 5 + bits_for(nbt), s))) return rc;
-  gather_bpts_kernel<T><<<blocks_for(n), 256, 0, s>>>(pts, bperm, n, (BrickPoint<T> *)h->d_bpts);
+  {
+    int *head, *rstart;
+    unsigned long long *rkey, *rkey_out;
+    unsigned *bperm2;
+    if ((rc = scratch(h, kHead, sizeof(int) * n, &head)) ||
+        (rc = scratch(h, kRunStart, sizeof(int) * n, &rstart)) ||
+        (rc = scratch(h, kRKey, sizeof(unsigned long long) * n, &rkey)) ||
+        (rc = scratch(h, kRKeyOut, sizeof(unsigned long long) * n, &rkey_out)) ||
+        (rc = scratch(h, kBPerm2, sizeof(unsigned) * n, &bperm2)))
+      return rc;
+    run_head_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, n, head);
+    if ((rc = inclusive_max(h, head, rstart, n, s))) return rc;
+    round_key_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, rstart, n, rkey);
+    if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, 37 + bits_for(nbt), s))) return rc;
+    gather_bpts_kernel<T><<<blocks_for(n), 256, 0, s>>>(pts, bperm2, n,
+                                                        (BrickPoint<T> *)h->d_bpts);
+  }
   if ((rc = exclusive_sum(h, bcount, h->d_brick_start, nbt + 1, s))) return rc;
   nonempty_flags_kernel<<<blocks_for(nbt + 1), 256, 0, s>>>(bcount, nbt, flag);
   if ((rc = exclusive_sum(h, flag, pos, nbt + 1, s))) return rc;
