@@ -52,7 +52,8 @@ struct BatchSys {
   const int4 *hgroups;
   const double4 *hcen;
   const int2 *hsegs;
-  float4 *vsrc;
+  float4 *vsrc;            // source-side sums, slot = brick-order position
+  const uint32_t *bperm;   // brick-order position -> caller index
   float refine2;
   double fself_r, fself_i;
 };
@@ -173,8 +174,9 @@ __global__ void __launch_bounds__(32 * kGroupWarps) batch_sym_kernel(
                                      ta[wid], tb[wid], lane);
 }
 
-// V[caller(j)] += the source-side sums of source j (scaled by vs for the
-// potential, gs for the gradient; complex: re, im pairs), then zero them.
+// V[caller(j)] += the source-side sums of brick-order slot j (scaled by vs
+// for the potential, gs for the gradient; complex: re, im pairs), then zero
+// them.
 template <bool CPLX>
 __global__ void batch_merge_kernel(const BatchSys *__restrict__ sys,
                                    const long long *__restrict__ off, int count, double vs,
@@ -187,7 +189,7 @@ __global__ void batch_merge_kernel(const BatchSys *__restrict__ sys,
     const long j = (long)(u - off[s]);
     double4 *o = reinterpret_cast<double4 *>(S.V);
     if (CPLX) {
-      o += 2 * (long)S.dperm[j];
+      o += 2 * (long)S.bperm[j];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const float4 a = S.vsrc[2 * j + h];
@@ -197,7 +199,7 @@ __global__ void batch_merge_kernel(const BatchSys *__restrict__ sys,
         o[h] = v;
       }
     } else {
-      o += S.dperm[j];
+      o += S.bperm[j];
       const float4 a = S.vsrc[j];
       S.vsrc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
       double4 v = *o;
@@ -361,6 +363,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     S.hcen = h->d_hcen;
     S.hsegs = h->d_hsegs;
     S.vsrc = h->d_vsrc;
+    S.bperm = h->d_bperm;
     S.refine2 = (float)h->refine2;
     S.fself_r = h->fself_r;
     S.fself_i = h->fself_i;

@@ -288,14 +288,18 @@ __device__ __forceinline__ double2 fhat_sample_body(const LR &lr, long idx, int 
 // the brick's theta tile of (kBrick + P - 1)^3 grid points is read into
 // shared memory once, then every point gathers its p^3 stencil from the
 // tile: V += sum theta B1 B2 B3, grad += (N/L) sum theta dB ..., added into
-// the caller-order output.
+// the caller-order output.  With vsrc (CalcV after a pair-once direct sum)
+// the point's source-side direct-sum slot (same brick-order position) is
+// added in the same read-modify-write of V (potential scaled by vs,
+// gradient by gs) and cleared for the next call.
 template <typename T, int P, bool CPLX>
 __device__ __forceinline__ void interp_brick_body(int brick, const int *__restrict__ brick_start,
                                                   const BrickPoint<T> *__restrict__ bp,
                                                   const T *__restrict__ theta,
                                                   double *__restrict__ V, int nb2, int nb3,
                                                   long N1, long N2, long N3, T c1, T c2, T c3,
-                                                  T *tile) {
+                                                  T *tile, void *vsrc = nullptr, double vs = 1.0,
+                                                  double gs = 1.0) {
   constexpr int TL = kBrick + P - 1;
   constexpr int TV = TL * TL * TL;
   constexpr int C = CPLX ? 2 : 1;
@@ -358,23 +362,47 @@ __device__ __forceinline__ void interp_brick_body(int brick, const int *__restri
       }
     }
     const T sc[4] = {T(1), c1, c2, c3};
-    const long o = pt.orig;
+    const long o = pt.orig, slot = beg + pi;
     if (CPLX) {
+      // source-side slot (FP32 complex): (V re, V im, x re, x im), (y .., z ..)
+      double d[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (vsrc) {
+        float4 *vp = reinterpret_cast<float4 *>(vsrc) + 2 * slot;
+        const float4 a = vp[0], b = vp[1];
+        vp[0] = vp[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        d[0] = a.x, d[1] = a.y, d[2] = a.z, d[3] = a.w;
+        d[4] = b.x, d[5] = b.y, d[6] = b.z, d[7] = b.w;
+      }
       double2 *Vo = reinterpret_cast<double2 *>(V) + 4 * o;
 #pragma unroll
       for (int m = 0; m < 4; m++) {
         double2 a = Vo[m];
-        a.x += (double)(v[m] * sc[m]);
-        a.y += (double)(vi[m] * sc[m]);
+        a.x += (double)(v[m] * sc[m]) + d[2 * m];
+        a.y += (double)(vi[m] * sc[m]) + d[2 * m + 1];
         Vo[m] = a;
       }
     } else {
+      double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+      if (vsrc) {
+        if (sizeof(T) == 4) {  // FP32: float4 per slot, scaled frame
+          float4 *vp = reinterpret_cast<float4 *>(vsrc) + slot;
+          const float4 a = *vp;
+          *vp = make_float4(0.f, 0.f, 0.f, 0.f);
+          s0 = vs * (double)a.x, s1 = gs * (double)a.y, s2 = gs * (double)a.z,
+          s3 = gs * (double)a.w;
+        } else {  // FP64: [4] doubles per slot
+          double4 *vp = reinterpret_cast<double4 *>(vsrc) + slot;
+          const double4 a = *vp;
+          *vp = make_double4(0, 0, 0, 0);
+          s0 = vs * a.x, s1 = gs * a.y, s2 = gs * a.z, s3 = gs * a.w;
+        }
+      }
       double4 *Vo = reinterpret_cast<double4 *>(V) + o;
       double4 a = *Vo;
-      a.x += (double)v[0];
-      a.y += (double)(v[1] * c1);
-      a.z += (double)(v[2] * c2);
-      a.w += (double)(v[3] * c3);
+      a.x += (double)v[0] + s0;
+      a.y += (double)(v[1] * c1) + s1;
+      a.z += (double)(v[2] * c2) + s2;
+      a.w += (double)(v[3] * c3) + s3;
       *Vo = a;
     }
   }
@@ -720,12 +748,13 @@ __device__ __forceinline__ void sym_block(
 // reference's own cell-pair loops do: src/PotentialLaplace.cpp:145-197,
 // :3447-3610).  The group walks its half-shell source segments: sources
 // whose point lies in a later coarse column, or later in the group's own
-// column, than the group's targets (build_groups); the pairs inside the
+// column, than the group's targets (set-up, setup.cu); the pairs inside the
 // group are the first phase, from both sides with target-side sums only.
 // Target-side sums accumulate per chunk in FP32 and across chunks in FP64,
 // as in the one-sided body; the source-side sums of a chunk are added to
-// vsrc (source order, FP32, scaled frame) with one vector atomic per source
-// and folded into V by merge_source_kernel.
+// vsrc (FP32, scaled frame; slot = the source's brick-order position, from
+// spos[j].w) with one vector atomic per source, and folded into V by the
+// interpolation (CalcV) or by merge_source_kernel.
 template <int FUNC, int ND>
 __device__ __forceinline__ void direct_group_sym(
     const PairCoef<float> &k, const double4 *__restrict__ gpos, const double4 *__restrict__ spos,
@@ -799,7 +828,8 @@ __device__ __forceinline__ void direct_group_sym(
     float hxa = -1e18f, hya = -1e18f, hza = -1e18f, lxa = 0.f, lya = 0.f, lza = 0.f;
     float hxb = -1e18f, hyb = -1e18f, hzb = -1e18f, lxb = 0.f, lyb = 0.f, lzb = 0.f;
     bool near = false;
-    const long ka = va ? ja : -1, kb = vb ? jb : -1;
+    // source-side slots: the sources' brick-order positions
+    const long ka = va ? (long)pa.w : -1, kb = vb ? (long)pb.w : -1;
     float q0 = 0.f, q1 = 0.f;
     if (va) {
       const double dx = (pa.x - c.x) * ir, dy = (pa.y - c.y) * ir, dz = (pa.z - c.z) * ir;
@@ -1025,7 +1055,7 @@ __device__ __forceinline__ void direct_group_sym_helm(
     float sx[2] = {-1e18f, -1e18f}, sy[2] = {-1e18f, -1e18f}, sz[2] = {-1e18f, -1e18f};
     float lx[2] = {0.f, 0.f}, ly[2] = {0.f, 0.f}, lz[2] = {0.f, 0.f};
     float2 sq[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    const long kidx[2] = {va ? ja : -1, vb ? jb : -1};
+    const long kidx[2] = {va ? (long)pa.w : -1, vb ? (long)pb.w : -1};  // brick positions
     if (va) {
       const double dx = pa.x - c.x, dy = pa.y - c.y, dz = pa.z - c.z;
       sx[0] = (float)dx, sy[0] = (float)dy, sz[0] = (float)dz;
@@ -1406,7 +1436,7 @@ __device__ __forceinline__ void direct_group_sym_scalar(
     // idle targets, with charge 0
     float sx[2] = {-1e18f, -1e18f}, sy[2] = {-1e18f, -1e18f}, sz[2] = {-1e18f, -1e18f};
     float lx[2] = {0.f, 0.f}, ly[2] = {0.f, 0.f}, lz[2] = {0.f, 0.f}, sq[2] = {0.f, 0.f};
-    const long kidx[2] = {va ? ja : -1, vb ? jb : -1};
+    const long kidx[2] = {va ? (long)pa.w : -1, vb ? (long)pb.w : -1};  // brick positions
     if (va) {
       const double dx = pa.x - c.x, dy = pa.y - c.y, dz = pa.z - c.z;
       sx[0] = (float)dx, sy[0] = (float)dy, sz[0] = (float)dz;
@@ -1481,8 +1511,8 @@ __device__ __forceinline__ void direct_group_sym_scalar(
 // group's targets (x, y, z, q) sit in shared memory, each lane holds two
 // sources of a 64-source chunk of the half-shell segments, target (l + k)
 // mod 32 meets lane l at step k and its sums rotate one lane down per step;
-// the source-side sums of a chunk go to vsrc ([n][4] doubles, source order)
-// with one FP64 atomic per component.  Pairs inside the group are a first,
+// the source-side sums of a chunk go to vsrc ([n][4] doubles, slot = the
+// source's brick-order position) with one FP64 atomic per component.  Pairs inside the group are a first,
 // one-sided pass.  Same pair arithmetic as direct_group_fp64.
 template <int FUNC, int SPLIT, int ND, class PK = BuiltinPair>
 __device__ __forceinline__ void direct_group_sym64(
@@ -1527,23 +1557,23 @@ __device__ __forceinline__ void direct_group_sym64(
   SrcCursor cb{ca.seg, ca.off + 32};
   cb.normalize(segs, G.w);
   bool va = ca.seg < G.w, vb = cb.seg < G.w;
-  long ja = -1, jb = -1;
+  long ja = -1, jb = -1, sla = -1, slb = -1;  // sla, slb: source-side slots (brick positions)
   double4 pa = make_double4(0, 0, 0, 0), pb = pa;
-  if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], pa.w = qs[ja];
-  if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], pb.w = qs[jb];
+  if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], sla = (long)pa.w, pa.w = qs[ja];
+  if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], slb = (long)pb.w, pb.w = qs[jb];
   while (__any_sync(FULL, va)) {
     // empty slots far away on the other side from idle targets, no charge
     double4 A = make_double4(-1e150, -1e150, -1e150, 0.0), B = A;
     if (va) A = make_double4(pa.x - c.x, pa.y - c.y, pa.z - c.z, pa.w);
     if (vb) B = make_double4(pb.x - c.x, pb.y - c.y, pb.z - c.z, pb.w);
-    const long ka = va ? ja : -1, kb = vb ? jb : -1;
+    const long ka = va ? sla : -1, kb = vb ? slb : -1;
     ca.off += 64;
     ca.normalize(segs, G.w);
     cb.off += 64;
     cb.normalize(segs, G.w);
     va = ca.seg < G.w, vb = cb.seg < G.w;
-    if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], pa.w = qs[ja];
-    if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], pb.w = qs[jb];
+    if (va) ja = (long)segs[ca.seg].x + ca.off, pa = spos[ja], sla = (long)pa.w, pa.w = qs[ja];
+    if (vb) jb = (long)segs[cb.seg].x + cb.off, pb = spos[jb], slb = (long)pb.w, pb.w = qs[jb];
 
     double aV = 0, aX = 0, aY = 0, aZ = 0;           // target side, rotating
     double sa[4] = {0, 0, 0, 0}, sb[4] = {0, 0, 0, 0};  // source side

@@ -108,6 +108,20 @@ static void groups_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s
       a.V);
 }
 
+// After a pair-once launch: the source-side sums are merged into V now, or,
+// when CalcV asked for it, left for the interpolation (which visits every
+// point in brick order and folds its slot in, saving a pass over V).
+static void merge_or_defer(npme_handle *h, const DirectArgs &a, cudaStream_t s, double vs,
+                           double gs) {
+  if (a.defer_merge) {
+    h->merge_pending = true;
+    h->merge_vs = vs, h->merge_gs = gs;
+  } else {
+    launch_merge_source(h, a.V, s, vs, gs);
+    h->launches++;
+  }
+}
+
 // FP32 real-DM direct sum with every pair evaluated once (direct_group_sym),
 // then the source-side sums folded into V.
 template <int FUNC, int ND>
@@ -126,14 +140,15 @@ __global__ void __launch_bounds__(32 * kGroupWarps, kGroupMinBlocks) direct_sym_
                              refine2, fself_r, V, vsrc, tsm[wid], tlo[wid], lane);
 }
 
-// V[caller(s)] += scale * vsrc[s], then vsrc[s] = 0 for the next call.
-__global__ void merge_source_kernel(float4 *__restrict__ vsrc, const uint32_t *__restrict__ sperm,
+// V[caller(i)] += scale * vsrc[i] for every brick-order slot i, then
+// vsrc[i] = 0 for the next call.
+__global__ void merge_source_kernel(float4 *__restrict__ vsrc, const uint32_t *__restrict__ bperm,
                                     long n, double vs, double gs, double *__restrict__ V) {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const float4 a = vsrc[s];
   vsrc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-  double4 *o = reinterpret_cast<double4 *>(V) + sperm[s];
+  double4 *o = reinterpret_cast<double4 *>(V) + bperm[s];
   double4 v = *o;
   v.x += vs * (double)a.x;
   v.y += gs * (double)a.y;
@@ -160,15 +175,15 @@ __global__ void __launch_bounds__(32 * kGroupWarps) direct_sym_helm_kernel(
                             fself_r, fself_i, V, vsrc, th[wid], tl[wid], lane);
 }
 
-// Complex V[caller(s)][0..3] += vsrc[2s], vsrc[2s + 1] (re, im pairs), then zero.
+// Complex V[caller(i)][0..3] += vsrc[2i], vsrc[2i + 1] (re, im pairs), then zero.
 __global__ void merge_source_cplx_kernel(float4 *__restrict__ vsrc,
-                                         const uint32_t *__restrict__ sperm, long n,
+                                         const uint32_t *__restrict__ bperm, long n,
                                          double *__restrict__ V) {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const float4 a = vsrc[2 * s], b = vsrc[2 * s + 1];
   vsrc[2 * s] = vsrc[2 * s + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-  double4 *o = reinterpret_cast<double4 *>(V) + 2 * (long)sperm[s];
+  double4 *o = reinterpret_cast<double4 *>(V) + 2 * (long)bperm[s];
   double4 u = o[0], w = o[1];
   u.x += a.x, u.y += a.y, u.z += a.z, u.w += a.w;
   w.x += b.x, w.y += b.y, w.z += b.z, w.w += b.w;
@@ -183,8 +198,7 @@ static void sym_helm_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t
       make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
       h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2,
       a.fself_r, a.fself_i, a.V, h->d_vsrc);
-  launch_merge_source(h, a.V, s, 1.0, 1.0);
-  h->launches++;
+  merge_or_defer(h, a, s, 1.0, 1.0);
 }
 
 template <int FUNC, int ND>
@@ -195,8 +209,7 @@ static void sym_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   direct_sym_kernel<FUNC, ND><<<(unsigned)blocks, 32 * kGroupWarps, 0, s>>>(
       k, h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller, h->d_hgroups, h->d_hcen,
       h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2, a.fself_r, a.V, h->d_vsrc);
-  launch_merge_source(h, a.V, s, k.vscale, k.gscale);
-  h->launches++;
+  merge_or_defer(h, a, s, k.vscale, k.gscale);
 }
 
 // FP32 form with the scalar pair kernel (original Ewald split).
@@ -233,15 +246,15 @@ __global__ void __launch_bounds__(32 * kGroupWarps) direct_sym64_kernel(
                                       fself_r, V, vsrc, tsm[wid], lane);
 }
 
-// V[caller(s)][m] += vsrc[s][m], then vsrc[s] = 0 for the next call.
+// V[caller(i)][m] += vsrc[i][m], then vsrc[i] = 0 for the next call.
 __global__ void merge_source64_kernel(double4 *__restrict__ vsrc,
-                                      const uint32_t *__restrict__ sperm, long n,
+                                      const uint32_t *__restrict__ bperm, long n,
                                       double *__restrict__ V) {
   const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const double4 a = vsrc[s];
   vsrc[s] = make_double4(0, 0, 0, 0);
-  double4 *o = reinterpret_cast<double4 *>(V) + sperm[s];
+  double4 *o = reinterpret_cast<double4 *>(V) + bperm[s];
   double4 v = *o;
   v.x += a.x, v.y += a.y, v.z += a.z, v.w += a.w;
   *o = v;
@@ -255,8 +268,7 @@ static void sym64_launch_nd(npme_handle *h, const DirectArgs &a, cudaStream_t s)
       make_pair_coef<double>(h), h->d_gpos, h->d_spos, (const double *)a.q, a.qcaller,
       h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, a.fself_r, a.V,
       h->d_vsrc64);
-  launch_merge_source(h, a.V, s, 1.0, 1.0);
-  h->launches++;
+  merge_or_defer(h, a, s, 1.0, 1.0);
 }
 
 template <int FUNC, int SPLIT>
@@ -274,11 +286,11 @@ void launch_merge_source(npme_handle *h, double *V, cudaStream_t s, double vs, d
   const unsigned blocks = (unsigned)((n + 255) / 256);
   if (!h->fp32)
     merge_source64_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<double4 *>(h->d_vsrc64),
-                                                 h->d_sperm, n, V);
+                                                 h->d_bperm, n, V);
   else if (h->complex_kernel)
-    merge_source_cplx_kernel<<<blocks, 256, 0, s>>>(h->d_vsrc, h->d_sperm, n, V);
+    merge_source_cplx_kernel<<<blocks, 256, 0, s>>>(h->d_vsrc, h->d_bperm, n, V);
   else
-    merge_source_kernel<<<blocks, 256, 0, s>>>(h->d_vsrc, h->d_sperm, n, vs, gs, V);
+    merge_source_kernel<<<blocks, 256, 0, s>>>(h->d_vsrc, h->d_bperm, n, vs, gs, V);
 }
 
 // The pair-once form applies to the built-in kernels: in FP32 the DM kernels
@@ -312,8 +324,7 @@ static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
           make_pair_coef<float>(h), h->d_gpos, h->d_spos, (const float *)a.q, a.qcaller,
           h->d_hgroups, h->d_hcen, h->d_hsegs, h->d_cperm, h->n_hgroups, (float)h->refine2,
           a.fself_r, a.V, h->d_vsrc);
-      launch_merge_source(h, a.V, s, 1.0, 1.0);
-      h->launches++;
+      merge_or_defer(h, a, s, 1.0, 1.0);
     }
     return true;
   }
@@ -396,6 +407,7 @@ int launch_direct_args(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
 
 int launch_direct(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s) {
   DirectArgs a{h->d_qc, d_q, h->fself_r, h->fself_i, d_V};
+  a.defer_merge = true;  // CalcV: the interpolation folds the source-side sums in
   return launch_direct_args(h, a, s);
 }
 

@@ -127,6 +127,7 @@ struct npme_handle {
   double4 *d_gpos = nullptr;     // targets in group order, FP64 positions
   double4 *d_spos = nullptr;     // sources in fine-column order, FP64 positions
   uint32_t *d_sperm = nullptr;   // source order -> caller index
+  uint32_t *d_bperm = nullptr;   // brick order position -> caller index
   const uint32_t *d_dperm = nullptr;  // gather order of the direct-sum charges (d_sperm or d_cperm)
   int4 *d_groups = nullptr;      // (first point, count, first segment, end segment)
   double4 *d_gcen = nullptr;     // group frame origin (bbox centre)
@@ -140,8 +141,15 @@ struct npme_handle {
   int4 *d_hgroups = nullptr;
   double4 *d_hcen = nullptr;
   int2 *d_hsegs = nullptr;
-  float4 *d_vsrc = nullptr;      // FP32: source-side sums (source order; two float4 if complex), kept zero
-  double *d_vsrc64 = nullptr;    // FP64: source-side sums [n][4] (source order), kept zero
+  // the source-side sums are indexed by the source point's position in the
+  // brick order (spos[k].w holds it), so that the interpolation, which visits
+  // the points in that order, can fold them into V
+  float4 *d_vsrc = nullptr;      // FP32: source-side sums (two float4 if complex), kept zero
+  double *d_vsrc64 = nullptr;    // FP64: source-side sums [n][4], kept zero
+  // CalcV leaves the source-side sums of its pair-once walk to the
+  // interpolation (scale vs for the potential, gs for the gradient)
+  bool merge_pending = false;
+  double merge_vs = 1.0, merge_gs = 1.0;
 
   npme::Timing timing;
   bool timing_pending = false;
@@ -186,6 +194,9 @@ struct DirectArgs {
   const double *qcaller;  // caller-order charges (the self term)
   double fself_r, fself_i;
   double *V;
+  // built-in pair-once walks: leave the source-side sums for the
+  // interpolation instead of merging them (sets h->merge_pending)
+  bool defer_merge = false;
 };
 // status `code` with `msg` recorded on the handle (or, for a null handle, as
 // the library's last error), as every entry point reports failures

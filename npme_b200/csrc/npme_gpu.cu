@@ -481,6 +481,7 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   // timing mode it starts after the reciprocal chain, so that each stage's
   // events time that stage alone
   const bool serial = h->timing.enabled && h->timing.serial;
+  h->merge_pending = false;
   auto fork_direct = [&]() -> int {
     CK(cudaEventRecord(h->ev_fork, s));
     CK(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));

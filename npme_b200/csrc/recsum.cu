@@ -491,10 +491,12 @@ template <typename T, int P, bool CPLX>
 __global__ void __launch_bounds__(256) interp_kernel(
     const int *__restrict__ brick_list, const int *__restrict__ brick_start,
     const BrickPoint<T> *__restrict__ bp, const T *__restrict__ theta, double *__restrict__ V,
-    int nb2, int nb3, long N1, long N2, long N3, T c1, T c2, T c3) {
+    int nb2, int nb3, long N1, long N2, long N3, T c1, T c2, T c3, void *vsrc, double vs,
+    double gs) {
   extern __shared__ unsigned char smem_raw[];
   interp_brick_body<T, P, CPLX>(brick_list[blockIdx.x], brick_start, bp, theta, V, nb2, nb3, N1,
-                                N2, N3, c1, c2, c3, reinterpret_cast<T *>(smem_raw));
+                                N2, N3, c1, c2, c3, reinterpret_cast<T *>(smem_raw), vsrc, vs,
+                                gs);
 }
 
 template <typename T, bool CPLX, int P>
@@ -507,7 +509,9 @@ static void interp_dispatch(npme_handle *h, double *d_V, cudaStream_t s) {
   kern<<<(unsigned)h->n_nonempty, 256, smem, s>>>(
       h->d_brick_list, h->d_brick_start, (const BrickPoint<T> *)h->d_bpts, (const T *)h->d_grid,
       d_V, (int)h->grid.nb[1], (int)h->grid.nb[2], h->grid.N[0], h->grid.N[1], h->grid.N[2],
-      (T)(h->grid.N[0] / L[0]), (T)(h->grid.N[1] / L[1]), (T)(h->grid.N[2] / L[2]));
+      (T)(h->grid.N[0] / L[0]), (T)(h->grid.N[1] / L[1]), (T)(h->grid.N[2] / L[2]),
+      h->merge_pending ? (h->fp32 ? (void *)h->d_vsrc : (void *)h->d_vsrc64) : nullptr,
+      h->merge_vs, h->merge_gs);
 }
 
 template <typename T, bool CPLX>
@@ -530,6 +534,7 @@ void launch_interp(npme_handle *h, double *d_V, cudaStream_t s) {
     if (h->complex_kernel) interp_order<double, true>(h, d_V, s);
     else interp_order<double, false>(h, d_V, s);
   }
+  h->merge_pending = false;  // folded in (and cleared) by this launch
   h->launches++;
 }
 

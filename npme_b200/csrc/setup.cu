@@ -238,16 +238,27 @@ __global__ void source_z_kernel(const double *__restrict__ coord, const unsigned
   cpos[cperm[k]] = (unsigned)k;
 }
 
+// inverse of the brick order: bpos[caller index] = brick-order position
+__global__ void brick_position_kernel(const uint32_t *__restrict__ bperm, long n,
+                                      unsigned *__restrict__ bpos) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) bpos[bperm[k]] = (unsigned)k;
+}
+
+// FP64 positions in the target (group) and source orders; a source's w holds
+// its brick-order position, the slot of its source-side sums
 __global__ void gather_positions_kernel(const double *__restrict__ coord,
                                         const uint32_t *__restrict__ gorder,
-                                        const uint32_t *__restrict__ sorder, long n,
+                                        const uint32_t *__restrict__ sorder,
+                                        const unsigned *__restrict__ bpos, long n,
                                         double4 *__restrict__ gpos, double4 *__restrict__ spos) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const double *x = coord + 3 * (long)gorder[k];
   gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
-  const double *y = coord + 3 * (long)sorder[k];
-  spos[k] = make_double4(y[0], y[1], y[2], 0.0);
+  const unsigned j = sorder[k];
+  const double *y = coord + 3 * (long)j;
+  spos[k] = make_double4(y[0], y[1], y[2], (double)bpos[j]);
 }
 
 // groups per coarse column: ceil(count / 32) (entry ncol = 0)
@@ -461,7 +472,7 @@ enum Scratch {
   kPts, kBKey, kBKeyOut, kIota, kBPerm, kCCol, kSCol, kZKey, kZKeyOut, kZPerm, kColZ, kColOut,
   kBCount, kCCount, kSCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
   kGRec, kBLo, kBHi, kCen, kNSeg, kNHSeg, kWork, kHWork, kSegOff, kHSegOff, kUGroups, kUHGroups,
-  kWorkOut, kOrd, kStats, kCub, kHead, kRunStart, kRKey, kRKeyOut, kBPerm2, kScratchCount
+  kWorkOut, kOrd, kStats, kCub, kHead, kRunStart, kRKey, kRKeyOut, kBPos, kScratchCount
 };
 static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
 
@@ -604,13 +615,13 @@ int bin_points(npme_handle *h) {
   {
     int *head, *rstart;
     unsigned long long *rkey, *rkey_out;
-    unsigned *bperm2;
     if ((rc = scratch(h, kHead, sizeof(int) * n, &head)) ||
         (rc = scratch(h, kRunStart, sizeof(int) * n, &rstart)) ||
         (rc = scratch(h, kRKey, sizeof(unsigned long long) * n, &rkey)) ||
         (rc = scratch(h, kRKeyOut, sizeof(unsigned long long) * n, &rkey_out)) ||
-        (rc = scratch(h, kBPerm2, sizeof(unsigned) * n, &bperm2)))
+        (rc = handle_buffer(h, (void **)&h->d_bperm, sizeof(uint32_t) * n)))
       return rc;
+    unsigned *bperm2 = h->d_bperm;
     run_head_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, n, head);
     if ((rc = inclusive_max(h, head, rstart, n, s))) return rc;
     round_key_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, rstart, n, rkey);
@@ -630,8 +641,11 @@ int bin_points(npme_handle *h) {
   if ((rc = sort_pairs(h, colz, colout, zperm, h->d_sperm, n, bits_for(nscol), s))) return rc;
   if ((rc = exclusive_sum(h, ccount, cstart, ncol + 1, s))) return rc;
   if ((rc = exclusive_sum(h, scount, sstart, nscol + 1, s))) return rc;
-  gather_positions_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_cperm, h->d_sperm, n,
-                                                        h->d_gpos, h->d_spos);
+  unsigned *bpos;
+  if ((rc = scratch(h, kBPos, sizeof(unsigned) * n, &bpos))) return rc;
+  brick_position_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_bperm, n, bpos);
+  gather_positions_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_cperm, h->d_sperm, bpos,
+                                                        n, h->d_gpos, h->d_spos);
   double *zs;
   unsigned *cpos, *fcpos;
   int *gcount, *goff;
