@@ -114,6 +114,8 @@ struct npme_handle {
   double *d_fax[3] = {nullptr, nullptr, nullptr};
   double *d_flam[3] = {nullptr, nullptr, nullptr};
   double *d_fcos[3] = {nullptr, nullptr, nullptr};
+  double *d_fdct[3] = {nullptr, nullptr, nullptr};  // DCT-I matrices per axis
+  long fdct_N[3] = {0, 0, 0};                        // the FFT lengths they were built for
   // device set-up scratch (sort keys, counts, group records), kept to reuse
   void *d_su[npme::kSetupScratch] = {};
 

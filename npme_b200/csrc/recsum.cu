@@ -76,32 +76,74 @@ __global__ void sample_fhat_kernel(LRKernel k, int M1, int M2, int M3,
     out[idx] = fhat_sample_body(lr, idx, M1, M2, M3, ax, ay, az);
 }
 
-// out[k] = f[0] + (-1)^k f[M-1] + 2 sum_{j=1}^{M-2} f[j] cos(2 pi j k / N)
-// along axis `ax` of an M1 x M2 x M3 array.
-__global__ void dct1_axis_kernel(const double2 *__restrict__ in, double2 *__restrict__ out,
-                                 int M1, int M2, int M3, int ax, int N,
-                                 const double *__restrict__ cosN) {
-  const long total = (long)M1 * M2 * M3;
-  const int M = ax == 0 ? M1 : (ax == 1 ? M2 : M3);
-  const long stride = ax == 0 ? (long)M2 * M3 : (ax == 1 ? M3 : 1);
-  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x) {
-    const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
-    const int k = ax == 0 ? i1 : (ax == 1 ? i2 : i3);
-    const long base = idx - (long)k * stride;
-    const double2 f0 = in[base], fl = in[base + (long)(M - 1) * stride];
-    const double sg = (k & 1) ? -1.0 : 1.0;
-    double sr = f0.x + sg * fl.x, si = f0.y + sg * fl.y;
-    int m = k;  // (j * k) mod N, advanced incrementally
-    for (int j = 1; j < M - 1; j++) {
-      const double c = 2.0 * cosN[m];
-      const double2 f = in[base + (long)j * stride];
-      sr = fma(c, f.x, sr);
-      si = fma(c, f.y, si);
-      m += k;
-      if (m >= N) m -= N;
+// The DCT-I along one axis of the M1 x M2 x M3 compact octant,
+//   out[k] = f[0] + (-1)^k f[M-1] + 2 sum_{j=1}^{M-2} f[j] cos(2 pi j k / N),
+// is the matrix product out[k, line] = sum_j C[k, j] f[j, line] over all
+// lines of that axis, with C[k, j] = c_j cos(2 pi (j k mod N) / N), c_0 =
+// c_{M-1} = 1, else 2 (cos(pi k) = (-1)^k for j = M - 1 = N/2).
+
+// C (M x M, row k) from the cosine table cosN[m] = cos(2 pi m / N)
+__global__ void dct1_matrix_kernel(const double *__restrict__ cosN, int M, int N,
+                                   double *__restrict__ C) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)M * M) return;
+  const int k = (int)(t / M), j = (int)(t - (long)k * M);
+  const double c = (j == 0 || j == M - 1) ? 1.0 : 2.0;
+  C[t] = c * cosN[(int)(((long)j * k) % N)];
+}
+
+// Offset of element j of line `line` along axis `ax`.
+__device__ __forceinline__ long dct_addr(int ax, long line, int j, int M2, int M3) {
+  if (ax == 0) return line + (long)j * M2 * M3;        // lines (i2, i3)
+  if (ax == 1) return (line / M3) * (long)M2 * M3 + line % M3 + (long)j * M3;  // (i1, i3)
+  return line * M3 + j;                                 // lines (i1, i2)
+}
+
+// Tiled FP64 GEMM: a CTA computes 64 outputs k for 32 lines; tiles of C
+// (64 x 16) and of the complex input (16 x 32) pass through shared memory.
+constexpr int kDctK = 64, kDctL = 32, kDctJ = 16;
+__global__ void __launch_bounds__(256) dct1_gemm_kernel(const double2 *__restrict__ in,
+                                                        double2 *__restrict__ out,
+                                                        const double *__restrict__ C, int ax,
+                                                        int M, long nlines, int M2, int M3) {
+  __shared__ double Cs[kDctK][kDctJ + 1];
+  __shared__ double2 Fs[kDctJ][kDctL];
+  const int tl = threadIdx.x & 31, tk = threadIdx.x >> 5;  // line in tile, k group
+  const long l0 = (long)blockIdx.x * kDctL;
+  const int k0 = blockIdx.y * kDctK;
+  double ar[8], ai[8];
+#pragma unroll
+  for (int r = 0; r < 8; r++) ar[r] = ai[r] = 0.0;
+  for (int j0 = 0; j0 < M; j0 += kDctJ) {
+    for (int t = threadIdx.x; t < kDctK * kDctJ; t += 256) {
+      const int kk = t / kDctJ, jj = t % kDctJ;
+      Cs[kk][jj] = (k0 + kk < M && j0 + jj < M) ? C[(long)(k0 + kk) * M + j0 + jj] : 0.0;
     }
-    out[idx] = make_double2(sr, si);
+    for (int t = threadIdx.x; t < kDctJ * kDctL; t += 256) {
+      const int jj = t / kDctL, ll = t % kDctL;
+      const long line = l0 + ll;
+      Fs[jj][ll] = (line < nlines && j0 + jj < M) ? in[dct_addr(ax, line, j0 + jj, M2, M3)]
+                                                  : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < kDctJ; jj++) {
+      const double2 f = Fs[jj][tl];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const double c = Cs[tk + 8 * r][jj];
+        ar[r] = fma(c, f.x, ar[r]);
+        ai[r] = fma(c, f.y, ai[r]);
+      }
+    }
+    __syncthreads();
+  }
+  const long line = l0 + tl;
+  if (line >= nlines) return;
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const int k = k0 + tk + 8 * r;
+    if (k < M) out[dct_addr(ax, line, k, M2, M3)] = make_double2(ar[r], ai[r]);
   }
 }
 
@@ -259,9 +301,19 @@ int build_kernel_transform(npme_handle *h) {
                                                           h->d_fax[1], h->d_fax[2], h->d_ft0);
   }
   double2 *src = h->d_ft0, *dst = h->d_ft1;
+  const int Ms[3] = {M1, M2, M3};
   for (int d = 0; d < 3; d++) {
-    dct1_axis_kernel<<<blocks, threads, 0, h->stream>>>(src, dst, M1, M2, M3, d, (int)N[d],
-                                                        h->d_fcos[d]);
+    // the DCT matrix of this axis, rebuilt only when the axis length changed
+    const int M = Ms[d];
+    if ((rc = handle_buffer(h, (void **)&h->d_fdct[d], sizeof(double) * M * M))) return rc;
+    if (h->fdct_N[d] != N[d]) {
+      dct1_matrix_kernel<<<(unsigned)(((long)M * M + 255) / 256), 256, 0, h->stream>>>(
+          h->d_fcos[d], M, (int)N[d], h->d_fdct[d]);
+      h->fdct_N[d] = N[d];
+    }
+    const long nlines = MT / M;
+    const dim3 grid((unsigned)((nlines + kDctL - 1) / kDctL), (unsigned)((M + kDctK - 1) / kDctK));
+    dct1_gemm_kernel<<<grid, 256, 0, h->stream>>>(src, dst, h->d_fdct[d], d, M, nlines, M2, M3);
     std::swap(src, dst);
   }
   const double inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);

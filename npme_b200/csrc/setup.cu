@@ -56,6 +56,8 @@ struct SetupStats {
   unsigned int nonfinite;
   unsigned int pad;
   long long bad;                    // lowest index whose stencil leaves the octant
+  unsigned int maxb;                // points in the fullest brick
+  unsigned int pad2;
   unsigned long long cand, hcand;   // staged (target, source) candidates, both walks
 };
 
@@ -63,6 +65,7 @@ __global__ void init_stats_kernel(SetupStats *st, long long n) {
   for (int d = 0; d < 3; d++) st->mn[d] = ~0ull, st->mx[d] = 0ull;
   st->nonfinite = 0;
   st->bad = n;
+  st->maxb = 0;
   st->cand = st->hcand = 0;
 }
 
@@ -121,16 +124,15 @@ __device__ __forceinline__ long stencil_start(double w) {
 // its coarse and fine xy columns and its z sort key; per brick and column
 // the point counts.  Arithmetic as the host restatement of the reference
 // (explicit round-to-nearest operations, no contraction), so that every
-// point lands in the same brick, bank and column on any machine.
+// point lands in the same brick, bank and column on any machine.  Returns
+// the brick's count after this point's insertion (0 outside the octant).
 template <typename T>
-__global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
+__device__ __forceinline__ unsigned bin_point(const double *__restrict__ coord, long i, BinGeom g,
                            BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
                            unsigned *__restrict__ ccol, unsigned *__restrict__ scol,
                            unsigned long long *__restrict__ zkey, unsigned *__restrict__ iota,
                            int *__restrict__ bcount, int *__restrict__ ccount,
                            int *__restrict__ scount, SetupStats *st) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
   const double x[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
   long o[3];
   T u[3];
@@ -157,7 +159,7 @@ __global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
   bp.orig = (uint32_t)i;
   pts[i] = bp;
   bkey[i] = ((unsigned)bid << 5) | key;
-  if (!out) atomicAdd(&bcount[bid], 1);
+  const unsigned cnt = out ? 0u : (unsigned)atomicAdd(&bcount[bid], 1) + 1u;
   int cs[2], ss[2];
 #pragma unroll
   for (int d = 0; d < 2; d++) {
@@ -175,6 +177,23 @@ __global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
   atomicAdd(&scount[sc], 1);
   zkey[i] = dkey(x[2]);
   iota[i] = (unsigned)i;
+  return cnt;
+}
+
+template <typename T>
+__global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
+                           BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
+                           unsigned *__restrict__ ccol, unsigned *__restrict__ scol,
+                           unsigned long long *__restrict__ zkey, unsigned *__restrict__ iota,
+                           int *__restrict__ bcount, int *__restrict__ ccount,
+                           int *__restrict__ scount, SetupStats *st) {
+  const long i0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  // the fullest brick's count, reduced per warp before the atomic
+  unsigned cnt = 0;
+  if (i0 < n) cnt = bin_point<T>(coord, i0, g, pts, bkey, ccol, scol, zkey, iota, bcount, ccount,
+                                 scount, st);
+  cnt = __reduce_max_sync(0xffffffffu, cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicMax(&st->maxb, cnt);
 }
 
 template <typename T>
@@ -193,15 +212,16 @@ __global__ void run_head_kernel(const unsigned *__restrict__ key, long n, int *_
   if (k < n) head[k] = (k == 0 || key[k] != key[k - 1]) ? (int)k : 0;
 }
 
-// Round-robin key (brick, rank inside its bank, bank): sorting by it puts
-// the r-th point of every bank of a brick into round r.
+// Round-robin key (brick, rank inside its bank, bank), the rank in rbits
+// bits: sorting by it puts the r-th point of every bank of a brick into
+// round r.
+template <typename K>
 __global__ void round_key_kernel(const unsigned *__restrict__ key, const int *__restrict__ start,
-                                 long n, unsigned long long *__restrict__ rkey) {
+                                 long n, int rbits, K *__restrict__ rkey) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const unsigned kk = key[k];
-  rkey[k] = ((unsigned long long)(kk >> 5) << 37) | ((unsigned long long)(k - start[k]) << 5) |
-            (unsigned long long)(kk & 31u);
+  rkey[k] = ((K)(kk >> 5) << (rbits + 5)) | ((K)(k - start[k]) << 5) | (K)(kk & 31u);
 }
 
 struct MaxOp {
@@ -610,25 +630,16 @@ int bin_points(npme_handle *h) {
   SCK(cudaGetLastError());
 
   // --- brick order: by brick, inside a brick in rounds over the banks ---
-  // (brick, bank, index) first, then (brick, rank inside the bank, bank)
-  if ((rc = sort_pairs(h, bkey, bkey_out, iota, bperm, n, 5 + bits_for(nbt), s))) return rc;
-  {
-    int *head, *rstart;
-    unsigned long long *rkey, *rkey_out;
-    if ((rc = scratch(h, kHead, sizeof(int) * n, &head)) ||
-        (rc = scratch(h, kRunStart, sizeof(int) * n, &rstart)) ||
-        (rc = scratch(h, kRKey, sizeof(unsigned long long) * n, &rkey)) ||
-        (rc = scratch(h, kRKeyOut, sizeof(unsigned long long) * n, &rkey_out)) ||
-        (rc = handle_buffer(h, (void **)&h->d_bperm, sizeof(uint32_t) * n)))
-      return rc;
-    unsigned *bperm2 = h->d_bperm;
-    run_head_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, n, head);
-    if ((rc = inclusive_max(h, head, rstart, n, s))) return rc;
-    round_key_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, rstart, n, rkey);
-    if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, 37 + bits_for(nbt), s))) return rc;
-    gather_bpts_kernel<T><<<blocks_for(n), 256, 0, s>>>(pts, bperm2, n,
-                                                        (BrickPoint<T> *)h->d_bpts);
-  }
+  // (brick, bank, index) first here; (brick, rank inside the bank, bank)
+  // after the read-back below, which gives the rank's bit count
+  int *head, *rstart;
+  if ((rc = sort_pairs(h, bkey, bkey_out, iota, bperm, n, 5 + bits_for(nbt), s)) ||
+      (rc = scratch(h, kHead, sizeof(int) * n, &head)) ||
+      (rc = scratch(h, kRunStart, sizeof(int) * n, &rstart)) ||
+      (rc = handle_buffer(h, (void **)&h->d_bperm, sizeof(uint32_t) * n)))
+    return rc;
+  run_head_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, n, head);
+  if ((rc = inclusive_max(h, head, rstart, n, s))) return rc;
   if ((rc = exclusive_sum(h, bcount, h->d_brick_start, nbt + 1, s))) return rc;
   nonempty_flags_kernel<<<blocks_for(nbt + 1), 256, 0, s>>>(bcount, nbt, flag);
   if ((rc = exclusive_sum(h, flag, pos, nbt + 1, s))) return rc;
@@ -641,11 +652,6 @@ int bin_points(npme_handle *h) {
   if ((rc = sort_pairs(h, colz, colout, zperm, h->d_sperm, n, bits_for(nscol), s))) return rc;
   if ((rc = exclusive_sum(h, ccount, cstart, ncol + 1, s))) return rc;
   if ((rc = exclusive_sum(h, scount, sstart, nscol + 1, s))) return rc;
-  unsigned *bpos;
-  if ((rc = scratch(h, kBPos, sizeof(unsigned) * n, &bpos))) return rc;
-  brick_position_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_bperm, n, bpos);
-  gather_positions_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_cperm, h->d_sperm, bpos,
-                                                        n, h->d_gpos, h->d_spos);
   double *zs;
   unsigned *cpos, *fcpos;
   int *gcount, *goff;
@@ -663,12 +669,14 @@ int bin_points(npme_handle *h) {
 
   // read back: groups, non-empty bricks, the stencil check
   struct {
-    int ngroups, nnonempty, lastflag;
+    int ngroups, nnonempty;
     long long bad;
+    unsigned maxb;
   } rb;
   SCK(cudaMemcpyAsync(&rb.ngroups, goff + ncol, sizeof(int), cudaMemcpyDeviceToHost, s));
   SCK(cudaMemcpyAsync(&rb.nnonempty, pos + nbt, sizeof(int), cudaMemcpyDeviceToHost, s));
   SCK(cudaMemcpyAsync(&rb.bad, &st->bad, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  SCK(cudaMemcpyAsync(&rb.maxb, &st->maxb, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   SCK(cudaStreamSynchronize(s));
   if (rb.bad < n) {
     // the axis of the first offending point, from its coordinates
@@ -693,6 +701,37 @@ int bin_points(npme_handle *h) {
                           sizeof(int) * std::max<long>(1, rb.nnonempty))))
     return rc;
   brick_list_kernel<<<blocks_for(nbt), 256, 0, s>>>(bcount, pos, nbt, h->d_brick_list);
+
+  // brick order in rounds over the banks: ranks inside a bank are below the
+  // fullest brick's count, so the key takes bits(nbt) + bits(maxb) + 5 bits
+  {
+    const int rbits = bits_for(std::max(1u, rb.maxb));
+    const int kbits = bits_for(nbt) + rbits + 5;
+    unsigned *bperm2 = h->d_bperm;
+    if (kbits <= 32) {
+      unsigned *rkey, *rkey_out;
+      if ((rc = scratch(h, kRKey, sizeof(unsigned) * n, &rkey)) ||
+          (rc = scratch(h, kRKeyOut, sizeof(unsigned) * n, &rkey_out)))
+        return rc;
+      round_key_kernel<unsigned><<<blocks_for(n), 256, 0, s>>>(bkey_out, rstart, n, rbits, rkey);
+      if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, kbits, s))) return rc;
+    } else {
+      unsigned long long *rkey, *rkey_out;
+      if ((rc = scratch(h, kRKey, sizeof(unsigned long long) * n, &rkey)) ||
+          (rc = scratch(h, kRKeyOut, sizeof(unsigned long long) * n, &rkey_out)))
+        return rc;
+      round_key_kernel<unsigned long long>
+          <<<blocks_for(n), 256, 0, s>>>(bkey_out, rstart, n, rbits, rkey);
+      if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, kbits, s))) return rc;
+    }
+    gather_bpts_kernel<T><<<blocks_for(n), 256, 0, s>>>(pts, bperm2, n,
+                                                        (BrickPoint<T> *)h->d_bpts);
+  }
+  unsigned *bpos;
+  if ((rc = scratch(h, kBPos, sizeof(unsigned) * n, &bpos))) return rc;
+  brick_position_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_bperm, n, bpos);
+  gather_positions_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_cperm, h->d_sperm, bpos,
+                                                        n, h->d_gpos, h->d_spos);
 
   // --- warp groups and their source segments ---
   const long ng = rb.ngroups;
