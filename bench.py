@@ -328,11 +328,14 @@ def bounded_serving(local, count=256):
     srv.run(warm, realtime=False)
     live = srv.run(reqs, realtime=True)
     V_live = {r.rid: r.V for r in reqs}
-    offline = srv.run(reqs, realtime=False)
+    # offline capacity: best of two passes (a pass lasts a fraction of a second)
+    offline = max((srv.run(reqs, realtime=False) for _ in range(2)),
+                  key=lambda st: st["throughput"])
     srv.close()
     plain = serving.Server(device=local, precision="fp64", max_batch=1, setup_workers=1)
     plain.warm_plans(reqs)
-    plain_stats = plain.run(reqs, realtime=False)
+    plain_stats = max((plain.run(reqs, realtime=False) for _ in range(2)),
+                      key=lambda st: st["throughput"])
     plain.close()
     errs = []
     for r in reqs[:: max(1, count // 16)][:16]:
@@ -353,8 +356,9 @@ def bounded_serving(local, count=256):
             "rel_rms_V_vs_exact_fp64": {"max": max(errs), "median": float(np.median(errs)),
                                         "requests": len(errs), "targets_each": "<= 1024"},
             "note": f"cuFFT plans of the {n_plans} FFT boxes built before the runs "
-                    "(server start-up); plain FP64 = the same server with one request per "
-                    "batch and one set-up thread"}
+                    "(server start-up); FP32 server: 4 set-up threads, batches up to 64; plain "
+                    "FP64 = the same server with one request per batch and one set-up thread; "
+                    "offline figures are the better of two passes"}
 
 
 def run_serving(args):
