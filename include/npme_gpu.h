@@ -75,7 +75,7 @@ typedef struct {
   double Rdir;      /* direct-space cutoff (required, > 0) */
   double tol;       /* original-Ewald tolerance (default 1e-6) */
   int nDeriv;       /* derivative-match order (default from BnOrder) */
-  int BnOrder;      /* B-spline order, even, 4..12 (default 8) */
+  int BnOrder;      /* B-spline order, even, 4..16 (default 8) */
   long N1, N2, N3;  /* full FFT box, multiples of 4 (required) */
   long n1, n2, n3;  /* reference block size keywords; accepted, not used */
   double a1, a2, a3;       /* Fourier-extension window (default 4.0) */

@@ -541,6 +541,8 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     case 8: NPME_BS(8, CX); break;       \
     case 10: NPME_BS(10, CX); break;     \
     case 12: NPME_BS(12, CX); break;     \
+    case 14: NPME_BS(14, CX); break;     \
+    case 16: NPME_BS(16, CX); break;     \
   }
     if (cx) { NPME_BS_P(true); } else { NPME_BS_P(false); }
 #undef NPME_BS_P
@@ -597,6 +599,8 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     case 8: NPME_BI(8, CX); break;      \
     case 10: NPME_BI(10, CX); break;    \
     case 12: NPME_BI(12, CX); break;    \
+    case 14: NPME_BI(14, CX); break;    \
+    case 16: NPME_BI(16, CX); break;    \
   }
     if (cx) { NPME_BI_P(true); } else { NPME_BI_P(false); }
 #undef NPME_BI_P

@@ -38,6 +38,12 @@ __device__ __forceinline__ void gather_body(const double *__restrict__ q,
   }
 }
 
+// Unroll of the outer stencil axis: complete up to order 12; orders 14 and
+// 16 (up to 16^3 = 4,096 stencil points) keep it as a loop, so the unrolled
+// inner P^2 block stays a size the instruction cache holds.
+template <int P>
+constexpr int kStencilUnroll = P <= 12 ? P : 1;
+
 // Points of a brick are stored in rounds over the shared-memory banks of
 // their stencil origins in the brick's tile (set-up, setup.cu): round r holds
 // the r-th point of every bank that has more than r points, in bank order.
@@ -85,7 +91,7 @@ __device__ __forceinline__ void spread_brick_body(int brick, const int *__restri
     const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
     const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
     const T qr = q[C * (long)i], qi = CPLX ? q[2 * (long)i + 1] : T(0);
-#pragma unroll
+#pragma unroll(kStencilUnroll<P>)
     for (int t1 = 0; t1 < P; t1++) {
 #pragma unroll
       for (int t2 = 0; t2 < P; t2++) {
@@ -171,7 +177,7 @@ __device__ __forceinline__ void spread_brick_fixed(int brick, const int *__restr
     const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
     const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
     const float qr = q[C * (long)i] * S, qi = CPLX ? q[2 * (long)i + 1] * S : 0.f;
-#pragma unroll
+#pragma unroll(kStencilUnroll<P>)
     for (int t1 = 0; t1 < P; t1++) {
 #pragma unroll
       for (int t2 = 0; t2 < P; t2++) {
@@ -331,7 +337,7 @@ __device__ __forceinline__ void interp_brick_body(int brick, const int *__restri
     const int l2 = (int)((pt.g0 >> 10) & 1023u) - b2 * kBrick;
     const int l3 = (int)(pt.g0 & 1023u) - b3 * kBrick;
     T v[4] = {0, 0, 0, 0}, vi[4] = {0, 0, 0, 0};
-#pragma unroll
+#pragma unroll(kStencilUnroll<P>)
     for (int t1 = 0; t1 < P; t1++) {
 #pragma unroll
       for (int t2 = 0; t2 < P; t2++) {

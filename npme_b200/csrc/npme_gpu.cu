@@ -223,8 +223,8 @@ int check_params(npme_handle *h, const npme_params &p) {
     return fail(h, NPME_EINVAL, "tol must be in (0, 1)");
   if (p.EwaldSplit == NPME_SPLIT_DERIVMATCH && (p.nDeriv < 2 || p.nDeriv > npme::kMaxDeriv))
     return fail(h, NPME_EINVAL, "nDeriv must be in [2, 15]");
-  if (p.BnOrder < 4 || p.BnOrder > 12 || (p.BnOrder & 1))
-    return fail(h, NPME_EINVAL, "BnOrder must be even and in [4, 12]");
+  if (p.BnOrder < 4 || p.BnOrder > 16 || (p.BnOrder & 1))
+    return fail(h, NPME_EINVAL, "BnOrder must be even and in [4, 16]");
   const long Ns[3] = {p.N1, p.N2, p.N3};
   for (int d = 0; d < 3; d++) {
     if (Ns[d] % 4 != 0 || Ns[d] < 4)  // src/RecSumSupportFunctions.cpp:42-58

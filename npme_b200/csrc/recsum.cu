@@ -463,6 +463,8 @@ static void spread_order(npme_handle *h, cudaStream_t s) {
     case 8: spread_dispatch<T, CPLX, 8>(h, s); break;
     case 10: spread_dispatch<T, CPLX, 10>(h, s); break;
     case 12: spread_dispatch<T, CPLX, 12>(h, s); break;
+    case 14: spread_dispatch<T, CPLX, 14>(h, s); break;
+    case 16: spread_dispatch<T, CPLX, 16>(h, s); break;
   }
 }
 
@@ -574,6 +576,8 @@ static void interp_order(npme_handle *h, double *d_V, cudaStream_t s) {
     case 8: interp_dispatch<T, CPLX, 8>(h, d_V, s); break;
     case 10: interp_dispatch<T, CPLX, 10>(h, d_V, s); break;
     case 12: interp_dispatch<T, CPLX, 12>(h, d_V, s); break;
+    case 14: interp_dispatch<T, CPLX, 14>(h, d_V, s); break;
+    case 16: interp_dispatch<T, CPLX, 16>(h, d_V, s); break;
   }
 }
 

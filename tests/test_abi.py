@@ -41,7 +41,7 @@ def test_default_params_are_reference_defaults():
 
 
 @pytest.mark.parametrize("field,value", [
-    ("Rdir", 0.0), ("BnOrder", 7), ("BnOrder", 14), ("N1", 66), ("nDeriv", 1),
+    ("Rdir", 0.0), ("BnOrder", 7), ("BnOrder", 18), ("N1", 66), ("nDeriv", 1),
     ("nDeriv", 16), ("funcType", 5), ("precision", 9), ("nNeigh", 0)])
 def test_invalid_params_rejected_before_touching_the_device(field, value):
     p = api.make_params("laplace", "dm", 8.0, 6, grid=(64, 64, 64))

@@ -335,6 +335,32 @@ def test_clustered_points(prec):
     assert rel(V[:, 1:], Vo[:, 1:]) < tol[1]
 
 
+@pytest.mark.parametrize("order", [14, 16])
+@pytest.mark.parametrize("kernel", ["laplace", "helmholtz"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_high_bspline_orders_match_reference(order, kernel, prec):
+    """B-spline orders 14 and 16 (the reference's RSEM tables include order
+    16) against the reference's own CalcV (oracle/_ref) on a small system;
+    order 16 in FP64 complex uses the largest shared-memory tile (23^3
+    complex doubles)."""
+    from oracle import refbind as rb
+    if not rb.available():
+        pytest.skip("reference build (oracle/_ref) absent")
+    w = wl.Workload(f"{kernel}_dm_o{order}", 2000, (14.0, 14.0, 14.0), kernel, "dm", order,
+                    (96, 96, 96), 5.0, k0=0.5 if kernel == "helmholtz" else 0.0,
+                    complex_charge=kernel == "helmholtz", seed=1016)
+    c, q = w.generate()
+    ref = rb.RefSolver(rb.make_params(w.func, w.split, w.Rdir, w.order, nDeriv=w.nDeriv,
+                                      N=w.grid, k0=w.k0), c)
+    Vr = ref.calcv(q)
+    ref.close()
+    with solver(w, prec) as s:
+        V = s.calcv(q)
+    tol = (FP64_TOL, FP64_TOL) if prec == "fp64" else (FP32_V_TOL, FP32_G_TOL)
+    assert rel(V[:, 0], Vr[:, 0]) < tol[0]
+    assert rel(V[:, 1:], Vr[:, 1:]) < tol[1]
+
+
 # ---------------------------------------------------------------------------
 # full benchmark sizes: the reference's own CalcV on identical inputs, the
 # exact O(N^2) FP64 sum on sampled targets, size-independent properties
