@@ -231,7 +231,7 @@ int npme_gpu_batch_destroy(npme_batch *b);
 typedef struct npme_server npme_server;
 typedef struct {
   int device;
-  int setup_threads;   /* host threads running set-up (default 8) */
+  int setup_threads;   /* host threads issuing requests' set-ups (default 8) */
   int max_batch;       /* systems per batched CalcV (default 64) */
   size_t hbm_budget;   /* device bytes in flight; 0: half the free memory */
   int pool_capacity;   /* idle handles kept for reuse (default 64) */

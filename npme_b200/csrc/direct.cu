@@ -6,7 +6,7 @@
 // common.cuh): V_i = sum_{j != i, r_ij <= Rdir} q_j f_SR(r_ij),
 // dV_i/dx = sum q_j f1_SR(r_ij) (x_i - x_j).  Targets are grouped by 32 in
 // z-sorted coarse columns and every group owns a list of source segments
-// (build_groups in npme_gpu.cu); one warp walks one group in both
+// (built on the device at set-up, setup.cu); one warp walks one group in both
 // precisions.  In the pair-once walk the target-side sums stay in registers
 // and each output row is written once, while the source-side sums are added
 // with float (FP32) or double (FP64) atomics into a per-source buffer that a

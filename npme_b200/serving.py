@@ -6,8 +6,9 @@ the library's native queue (npme_gpu_submit, csrc/server.cu):
 
   * admits requests while the estimated device footprint of the requests in
     flight stays under the budget (HBM admission);
-  * sets requests up on native threads (host binning and the device-side
-    kernel transform run while the previous batch computes on the GPU),
+  * sets requests up on native threads (each runs its request's device
+    set-up, binning, warp groups and kernel transform, on its handle's
+    stream while the previous batch computes on the GPU),
     reusing pooled handles (buffers and transform scratch stay on the device,
     FFT plans come from a process-wide cache);
   * every time the GPU is free, runs all set-up requests as one batch
