@@ -111,9 +111,12 @@ struct npme_handle {
   std::map<void *, size_t> caps;  // pointer field -> capacity of its buffer
   // kernel-transform construction scratch (kept to reuse across set-ups)
   double2 *d_ft0 = nullptr, *d_ft1 = nullptr;
-  double *d_fax[3] = {nullptr, nullptr, nullptr};
-  double *d_flam[3] = {nullptr, nullptr, nullptr};
-  double *d_fcos[3] = {nullptr, nullptr, nullptr};
+  double *d_ftab = nullptr;    // per-axis tables of the transform, one block:
+  double *d_fax[3] = {nullptr, nullptr, nullptr};   //   windows (views into d_ftab)
+  double *d_flam[3] = {nullptr, nullptr, nullptr};  //   lambda^2
+  double *d_fcos[3] = {nullptr, nullptr, nullptr};  //   cos(2 pi m / N)
+  double *h_fstage = nullptr;  // pinned staging of those tables (freed at destroy)
+  size_t fstage_cap = 0;
   double *d_fdct[3] = {nullptr, nullptr, nullptr};  // DCT-I matrices per axis
   long fdct_N[3] = {0, 0, 0};                        // the FFT lengths they were built for
   // device set-up scratch (sort keys, counts, group records), kept to reuse

@@ -457,6 +457,15 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
     release(h);
     return rc;
   }
+  // all set-up work is on the handle's stream; CalcV may be enqueued on any
+  // stream, so the set-up completes here
+  {
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      release(h);
+      return fail(h, NPME_ECUDA, std::string("set-up: ") + cudaGetErrorString(e));
+    }
+  }
   h->ready = true;
   return NPME_OK;
 }
@@ -714,6 +723,7 @@ int npme_gpu_destroy(npme_handle *h) {
   if (h->stream2) cudaStreamSynchronize(h->stream2);
   release(h);
   pool_release(h);
+  if (h->h_fstage) cudaFreeHost(h->h_fstage);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);

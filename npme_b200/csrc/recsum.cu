@@ -10,6 +10,7 @@
 // theta (src/RecSumV.cpp:766-840) without its 8 even/odd half transforms.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -274,22 +275,35 @@ int build_kernel_transform(npme_handle *h) {
   if ((rc = handle_buffer(h, (void **)&h->d_ft0, sizeof(double2) * MT)) ||
       (rc = handle_buffer(h, (void **)&h->d_ft1, sizeof(double2) * MT)))
     return rc;
+  // the per-axis tables (window x1, x2, T1, T2; lambda^2; cosines of the
+  // DCT) go through one pinned staging block kept by the handle, in one
+  // asynchronous copy; the next set-up on the handle waits for the handle's
+  // stream before it refills the block
+  size_t off[3][3], total = 0;
   for (int d = 0; d < 3; d++) {
-    if ((rc = handle_buffer(h, (void **)&h->d_fax[d], sizeof(double) * ax[d].size())) ||
-        (rc = handle_buffer(h, (void **)&h->d_flam[d], sizeof(double) * lam[d].size())) ||
-        (rc = handle_buffer(h, (void **)&h->d_fcos[d], sizeof(double) * N[d])))
-      return rc;
+    off[d][0] = total, total += ax[d].size();
+    off[d][1] = total, total += lam[d].size();
+    off[d][2] = total, total += (size_t)N[d];
   }
-  std::vector<double> cs[3];
+  if (h->fstage_cap < total) {
+    if (h->h_fstage) cudaFreeHost(h->h_fstage);
+    h->h_fstage = nullptr, h->fstage_cap = 0;
+    NPME_CK(cudaHostAlloc((void **)&h->h_fstage, sizeof(double) * total, cudaHostAllocDefault));
+    h->fstage_cap = total;
+  }
   for (int d = 0; d < 3; d++) {
-    cs[d].resize(N[d]);
-    for (long m = 0; m < N[d]; m++) cs[d][m] = std::cos(2.0 * M_PI * (double)m / (double)N[d]);
-    cudaMemcpyAsync(h->d_fax[d], ax[d].data(), sizeof(double) * ax[d].size(),
-                    cudaMemcpyHostToDevice, h->stream);
-    cudaMemcpyAsync(h->d_flam[d], lam[d].data(), sizeof(double) * lam[d].size(),
-                    cudaMemcpyHostToDevice, h->stream);
-    cudaMemcpyAsync(h->d_fcos[d], cs[d].data(), sizeof(double) * N[d], cudaMemcpyHostToDevice,
-                    h->stream);
+    std::copy(ax[d].begin(), ax[d].end(), h->h_fstage + off[d][0]);
+    std::copy(lam[d].begin(), lam[d].end(), h->h_fstage + off[d][1]);
+    double *cs = h->h_fstage + off[d][2];
+    for (long m = 0; m < N[d]; m++) cs[m] = std::cos(2.0 * M_PI * (double)m / (double)N[d]);
+  }
+  if ((rc = handle_buffer(h, (void **)&h->d_ftab, sizeof(double) * total))) return rc;
+  NPME_CK(cudaMemcpyAsync(h->d_ftab, h->h_fstage, sizeof(double) * total, cudaMemcpyHostToDevice,
+                          h->stream));
+  for (int d = 0; d < 3; d++) {
+    h->d_fax[d] = h->d_ftab + off[d][0];
+    h->d_flam[d] = h->d_ftab + off[d][1];
+    h->d_fcos[d] = h->d_ftab + off[d][2];
   }
   const int threads = 256, blocks = 148 * 8;
   if (h->user_kernel) {
@@ -333,9 +347,8 @@ int build_kernel_transform(npme_handle *h) {
       scale_fhat_kernel<double, false><<<blocks, threads, 0, h->stream>>>(
           src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (double *)h->d_G);
   }
-  // the host vectors above are read by the asynchronous copies: wait here
-  cudaError_t e = cudaStreamSynchronize(h->stream);
-  if (e == cudaSuccess) e = cudaGetLastError();
+  // launch errors now; npme_gpu_setup waits for the stream before it returns
+  const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     h->err = std::string("kernel transform: ") + cudaGetErrorString(e);
     rc = NPME_ECUDA;

@@ -10,8 +10,8 @@
 //    and, inside a brick, by the shared-memory bank of their stencil origin;
 //  * the direct sum's warp groups (the reference's cells and cluster pairs,
 //    src/PartitionEmbeddedBox.cpp:47-205, src/PartitionBox.cpp:789-923):
-//    targets sorted by (xy column, z, index) and cut into runs of 32,
-//    sources sorted by (fine xy column, z, index); for every group the z
+//    targets sorted by (xy column, quantised z, index) and cut into runs of
+//    32, sources sorted by (fine xy column, quantised z, index); for every group the z
 //    ranges of the fine columns that can hold a point within Rdir of the
 //    group's bounding box, and the half-shell part of them for the
 //    every-pair-once walk; groups ordered by their work, heaviest first.
@@ -113,7 +113,23 @@ struct BinGeom {
   // direct-sum columns
   double mn[2], edge[2], sedge[2];
   int nc[2], ns[2];
+  // quantised z: floor((z - zmin) * zscale) in [0, 2^zbits)
+  double zmin, zscale;
+  int zbits;
 };
+
+// z quantised to zbits bits (a quantum of at most 1/1024 of the column edge),
+// non-decreasing in z.  The direct sum's two point orders sort by (column,
+// quantised z, index); the source segments are searched with the same
+// quantisation, widened to whole quanta, so a segment is a superset of the
+// sources within reach (the pair test rejects the few extra) and no pair is
+// lost.
+__device__ __forceinline__ unsigned zquant(double z, double zmin, double zscale, int zbits) {
+  const double t = __dmul_rn(__dsub_rn(z, zmin), zscale);
+  if (!(t > 0.0)) return 0u;
+  const double mx = (double)((1u << zbits) - 1u);
+  return (unsigned)floor(fmin(t, mx));
+}
 
 // start index of the B-spline stencil (src/RecSumSupportFunctions.h:123-127)
 __device__ __forceinline__ long stencil_start(double w) {
@@ -121,16 +137,16 @@ __device__ __forceinline__ long stencil_start(double w) {
 }
 
 // Per point: the spread/interpolation record, its brick-and-bank sort key,
-// its coarse and fine xy columns and its z sort key; per brick and column
-// the point counts.  Arithmetic as the host restatement of the reference
+// its (coarse column, quantised z) and (fine column, quantised z) sort keys;
+// per brick and column the point counts.  Arithmetic as the host restatement of the reference
 // (explicit round-to-nearest operations, no contraction), so that every
 // point lands in the same brick, bank and column on any machine.  Returns
 // the brick's count after this point's insertion (0 outside the octant).
 template <typename T>
 __device__ __forceinline__ unsigned bin_point(const double *__restrict__ coord, long i, BinGeom g,
                            BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
-                           unsigned *__restrict__ ccol, unsigned *__restrict__ scol,
-                           unsigned long long *__restrict__ zkey, unsigned *__restrict__ iota,
+                           unsigned long long *__restrict__ ckey,
+                           unsigned long long *__restrict__ skey, unsigned *__restrict__ iota,
                            int *__restrict__ bcount, int *__restrict__ ccount,
                            int *__restrict__ scount, SetupStats *st) {
   const double x[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
@@ -171,11 +187,11 @@ __device__ __forceinline__ unsigned bin_point(const double *__restrict__ coord, 
   }
   const unsigned cc = (unsigned)(cs[0] * g.nc[1] + cs[1]);
   const unsigned sc = (unsigned)(ss[0] * g.ns[1] + ss[1]);
-  ccol[i] = cc;
-  scol[i] = sc;
+  const unsigned long long zq = zquant(x[2], g.zmin, g.zscale, g.zbits);
+  ckey[i] = ((unsigned long long)cc << g.zbits) | zq;
+  skey[i] = ((unsigned long long)sc << g.zbits) | zq;
   atomicAdd(&ccount[cc], 1);
   atomicAdd(&scount[sc], 1);
-  zkey[i] = dkey(x[2]);
   iota[i] = (unsigned)i;
   return cnt;
 }
@@ -183,14 +199,14 @@ __device__ __forceinline__ unsigned bin_point(const double *__restrict__ coord, 
 template <typename T>
 __global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
                            BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
-                           unsigned *__restrict__ ccol, unsigned *__restrict__ scol,
-                           unsigned long long *__restrict__ zkey, unsigned *__restrict__ iota,
+                           unsigned long long *__restrict__ ckey,
+                           unsigned long long *__restrict__ skey, unsigned *__restrict__ iota,
                            int *__restrict__ bcount, int *__restrict__ ccount,
                            int *__restrict__ scount, SetupStats *st) {
   const long i0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
   // the fullest brick's count, reduced per warp before the atomic
   unsigned cnt = 0;
-  if (i0 < n) cnt = bin_point<T>(coord, i0, g, pts, bkey, ccol, scol, zkey, iota, bcount, ccount,
+  if (i0 < n) cnt = bin_point<T>(coord, i0, g, pts, bkey, ckey, skey, iota, bcount, ccount,
                                  scount, st);
   cnt = __reduce_max_sync(0xffffffffu, cnt);
   if ((threadIdx.x & 31) == 0 && cnt) atomicMax(&st->maxb, cnt);
@@ -248,13 +264,14 @@ __global__ void brick_list_kernel(const int *__restrict__ count, const int *__re
   if (b < nb && count[b] > 0) list[pos[b]] = (int)b;
 }
 
-// zs[k] = z of source k; cpos[cperm[k]] = k (position of a point in the group order)
-__global__ void source_z_kernel(const double *__restrict__ coord, const unsigned *__restrict__ sperm,
-                                const unsigned *__restrict__ cperm, long n, double *__restrict__ zs,
-                                unsigned *__restrict__ cpos) {
+// zq[k] = quantised z of source k (from its sorted key); cpos[cperm[k]] = k
+// (position of a point in the group order)
+__global__ void source_z_kernel(const unsigned long long *__restrict__ skey,
+                                const unsigned *__restrict__ cperm, long n, int zbits,
+                                unsigned *__restrict__ zq, unsigned *__restrict__ cpos) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  zs[k] = coord[3 * (long)sperm[k] + 2];
+  zq[k] = (unsigned)(skey[k] & ((1ull << zbits) - 1ull));
   cpos[cperm[k]] = (unsigned)k;
 }
 
@@ -303,6 +320,8 @@ struct GroupGeom {
   double R, R2;
   double mn[2], sedge[2];
   int ns[2], nc1;
+  double zmin, zscale;  // the z quantisation of the sort keys
+  int zbits;
 };
 
 // Bounding box of every group (warp per group): lo/hi corners, and the
@@ -350,7 +369,7 @@ __device__ __forceinline__ int lower_idx(const V *__restrict__ v, int a, int b, 
   }
   return a;
 }
-__device__ __forceinline__ int upper_idx(const double *__restrict__ v, int a, int b, double x) {
+__device__ __forceinline__ int upper_idx(const unsigned *__restrict__ v, int a, int b, unsigned x) {
   while (a < b) {
     const int m = (a + b) >> 1;
     if (v[m] <= x) a = m + 1;
@@ -372,7 +391,7 @@ template <bool FILL>
 __global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ grec, long ngroups,
                                       const double4 *__restrict__ blo,
                                       const double4 *__restrict__ bhi,
-                                      const int *__restrict__ sstart, const double *__restrict__ zs,
+                                      const int *__restrict__ sstart, const unsigned *__restrict__ zq,
                                       const unsigned *__restrict__ fcpos, int *__restrict__ nseg,
                                       int *__restrict__ nhseg, unsigned *__restrict__ work,
                                       unsigned *__restrict__ hwork,
@@ -419,8 +438,9 @@ __global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ gre
         if (d2 <= gg.R2) {
           const double hz = __dsqrt_rn(__dsub_rn(gg.R2, d2));
           const double zlo = __dsub_rn(L.z, hz), zhi = __dadd_rn(Hh.z, hz);
-          a = lower_idx(zs, zb, ze, zlo);
-          b = upper_idx(zs, a, ze, zhi);
+          // whole quanta: every source with zlo <= z <= zhi is inside [a, b)
+          a = lower_idx(zq, zb, ze, zquant(zlo, gg.zmin, gg.zscale, gg.zbits));
+          b = upper_idx(zq, a, ze, zquant(zhi, gg.zmin, gg.zscale, gg.zbits));
           has = b > a;
           const long cc = (long)(s0 / kSourceSplit) * gg.nc1 + s1 / kSourceSplit;
           if (has && cc >= c) {
@@ -453,9 +473,9 @@ __global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ gre
     } else {
       nseg[g] = ns_;
       nhseg[g] = nh_;
-      // heaviest first: sort keys are the complements of the work
-      work[g] = ~(unsigned)min(wk, 0xffffffffull);
-      hwork[g] = ~(unsigned)min(hwk, 0xffffffffull);
+      // sources staged by the group (at most n: its segments are disjoint)
+      work[g] = (unsigned)min(wk, 0xffffffffull);
+      hwork[g] = (unsigned)min(hwk, 0xffffffffull);
       cand = wk * (unsigned long long)(p1 - p0);
       hcand = hwk * (unsigned long long)(p1 - p0);
       atomicAdd(&st->cand, cand);
@@ -489,7 +509,7 @@ inline unsigned blocks_for(long n, int t = 256) { return (unsigned)((n + t - 1) 
 
 // Scratch buffers of the set-up (handle-owned, reused by the next set-up).
 enum Scratch {
-  kPts, kBKey, kBKeyOut, kIota, kBPerm, kCCol, kSCol, kZKey, kZKeyOut, kZPerm, kColZ, kColOut,
+  kPts, kBKey, kBKeyOut, kIota, kBPerm, kCKey, kSKey, kKeyOut,
   kBCount, kCCount, kSCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
   kGRec, kBLo, kBHi, kCen, kNSeg, kNHSeg, kWork, kHWork, kSegOff, kHSegOff, kUGroups, kUHGroups,
   kWorkOut, kOrd, kStats, kCub, kHead, kRunStart, kRKey, kRKeyOut, kBPos, kScratchCount
@@ -515,15 +535,26 @@ int cub_tmp(npme_handle *h, size_t bytes, void **out) {
   return scratch(h, kCub, std::max<size_t>(bytes, 256), out);
 }
 
+// stable radix sort of (key, value) pairs on bits [0, end_bit), ascending
+// or descending
 template <typename K>
 int sort_pairs(npme_handle *h, const K *kin, K *kout, const unsigned *vin, unsigned *vout,
-               long n, int end_bit, cudaStream_t s) {
+               long n, int end_bit, cudaStream_t s, bool descending = false) {
   size_t tb = 0;
-  SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
+  if (descending)
+    SCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kin, kout, vin, vout, (int)n, 0,
+                                                   end_bit, s));
+  else
+    SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit,
+                                        s));
   void *tmp;
   int rc;
   if ((rc = cub_tmp(h, tb, &tmp))) return rc;
-  SCK(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
+  if (descending)
+    SCK(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, kin, kout, vin, vout, (int)n, 0,
+                                                   end_bit, s));
+  else
+    SCK(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
   return NPME_OK;
 }
 
@@ -578,6 +609,12 @@ int bin_points(npme_handle *h) {
     g.sedge[d] = g.edge[d] / kSourceSplit;
     g.mn[d] = h->bmin[d];
   }
+  {
+    const double H = h->bmax[2] - h->bmin[2];
+    g.zbits = std::max(8, std::min(20, (int)std::ceil(std::log2(std::max(1.0, 1024.0 * H / e)))));
+    g.zmin = h->bmin[2];
+    g.zscale = (double)((1u << g.zbits) - 1u) / std::max(H, 1e-300);
+  }
   // heads of offsets up to ~the group half-diagonal carry ~6e-8 e absolute
   // error; below r = e/4 the relative error would exceed ~1e-6, so refine
   h->refine2 = (0.25 * e) * (0.25 * e);
@@ -586,21 +623,17 @@ int bin_points(npme_handle *h) {
   h->n_bricks = nbt;
 
   BrickPoint<T> *pts;
-  unsigned *bkey, *bkey_out, *iota, *bperm, *ccol, *scol, *colz, *colout, *zperm;
-  unsigned long long *zkey, *zkey_out;
+  unsigned *bkey, *bkey_out, *iota, *bperm;
+  unsigned long long *ckey, *skey, *key_out;
   int *bcount, *ccount, *scount, *cstart, *sstart, *flag, *pos;
   if ((rc = scratch(h, kPts, sizeof(BrickPoint<T>) * n, &pts)) ||
       (rc = scratch(h, kBKey, sizeof(unsigned) * n, &bkey)) ||
       (rc = scratch(h, kBKeyOut, sizeof(unsigned) * n, &bkey_out)) ||
       (rc = scratch(h, kIota, sizeof(unsigned) * n, &iota)) ||
       (rc = scratch(h, kBPerm, sizeof(unsigned) * n, &bperm)) ||
-      (rc = scratch(h, kCCol, sizeof(unsigned) * n, &ccol)) ||
-      (rc = scratch(h, kSCol, sizeof(unsigned) * n, &scol)) ||
-      (rc = scratch(h, kColZ, sizeof(unsigned) * n, &colz)) ||
-      (rc = scratch(h, kColOut, sizeof(unsigned) * n, &colout)) ||
-      (rc = scratch(h, kZPerm, sizeof(unsigned) * n, &zperm)) ||
-      (rc = scratch(h, kZKey, sizeof(unsigned long long) * n, &zkey)) ||
-      (rc = scratch(h, kZKeyOut, sizeof(unsigned long long) * n, &zkey_out)) ||
+      (rc = scratch(h, kCKey, sizeof(unsigned long long) * n, &ckey)) ||
+      (rc = scratch(h, kSKey, sizeof(unsigned long long) * n, &skey)) ||
+      (rc = scratch(h, kKeyOut, sizeof(unsigned long long) * n, &key_out)) ||
       (rc = scratch(h, kBCount, sizeof(int) * (nbt + 1), &bcount)) ||
       (rc = scratch(h, kCCount, sizeof(int) * (ncol + 1), &ccount)) ||
       (rc = scratch(h, kSCount, sizeof(int) * (nscol + 1), &scount)) ||
@@ -625,7 +658,7 @@ int bin_points(npme_handle *h) {
   SCK(cudaMemsetAsync(bcount, 0, sizeof(int) * (nbt + 1), s));
   SCK(cudaMemsetAsync(ccount, 0, sizeof(int) * (ncol + 1), s));
   SCK(cudaMemsetAsync(scount, 0, sizeof(int) * (nscol + 1), s));
-  bin_kernel<T><<<blocks_for(n), 256, 0, s>>>(h->d_coord, n, g, pts, bkey, ccol, scol, zkey, iota,
+  bin_kernel<T><<<blocks_for(n), 256, 0, s>>>(h->d_coord, n, g, pts, bkey, ckey, skey, iota,
                                               bcount, ccount, scount, st);
   SCK(cudaGetLastError());
 
@@ -644,24 +677,23 @@ int bin_points(npme_handle *h) {
   nonempty_flags_kernel<<<blocks_for(nbt + 1), 256, 0, s>>>(bcount, nbt, flag);
   if ((rc = exclusive_sum(h, flag, pos, nbt + 1, s))) return rc;
 
-  // --- direct-sum orders: (column, z, index) for targets and sources ---
-  if ((rc = sort_pairs(h, zkey, zkey_out, iota, zperm, n, 64, s))) return rc;
-  gather_u32_kernel<<<blocks_for(n), 256, 0, s>>>(ccol, zperm, n, colz);
-  if ((rc = sort_pairs(h, colz, colout, zperm, h->d_cperm, n, bits_for(ncol), s))) return rc;
-  gather_u32_kernel<<<blocks_for(n), 256, 0, s>>>(scol, zperm, n, colz);
-  if ((rc = sort_pairs(h, colz, colout, zperm, h->d_sperm, n, bits_for(nscol), s))) return rc;
+  // --- direct-sum orders: (column, quantised z, index) for targets and
+  // sources, one radix sort each ---
+  if ((rc = sort_pairs(h, ckey, key_out, iota, h->d_cperm, n, bits_for(ncol) + g.zbits, s)) ||
+      (rc = sort_pairs(h, skey, key_out, iota, h->d_sperm, n, bits_for(nscol) + g.zbits, s)))
+    return rc;
   if ((rc = exclusive_sum(h, ccount, cstart, ncol + 1, s))) return rc;
   if ((rc = exclusive_sum(h, scount, sstart, nscol + 1, s))) return rc;
-  double *zs;
+  unsigned *zs;  // quantised z of the sources, in source order
   unsigned *cpos, *fcpos;
   int *gcount, *goff;
-  if ((rc = scratch(h, kZs, sizeof(double) * n, &zs)) ||
+  if ((rc = scratch(h, kZs, sizeof(unsigned) * n, &zs)) ||
       (rc = scratch(h, kCPos, sizeof(unsigned) * n, &cpos)) ||
       (rc = scratch(h, kFCPos, sizeof(unsigned) * n, &fcpos)) ||
       (rc = scratch(h, kGCount, sizeof(int) * (ncol + 1), &gcount)) ||
       (rc = scratch(h, kGOff, sizeof(int) * (ncol + 1), &goff)))
     return rc;
-  source_z_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_sperm, h->d_cperm, n, zs, cpos);
+  source_z_kernel<<<blocks_for(n), 256, 0, s>>>(key_out, h->d_cperm, n, g.zbits, zs, cpos);
   gather_u32_kernel<<<blocks_for(n), 256, 0, s>>>(cpos, h->d_sperm, n, fcpos);
   groups_per_column_kernel<<<blocks_for(ncol + 1), 256, 0, s>>>(ccount, ncol, gcount);
   if ((rc = exclusive_sum(h, gcount, goff, ncol + 1, s))) return rc;
@@ -761,6 +793,7 @@ int bin_points(npme_handle *h) {
   gg.R = Rd, gg.R2 = Rd * Rd;
   for (int d = 0; d < 2; d++) gg.mn[d] = g.mn[d], gg.sedge[d] = g.sedge[d], gg.ns[d] = g.ns[d];
   gg.nc1 = g.nc[1];
+  gg.zmin = g.zmin, gg.zscale = g.zscale, gg.zbits = g.zbits;
   SCK(cudaMemsetAsync(nseg + ng, 0, sizeof(int), s));
   SCK(cudaMemsetAsync(nhseg + ng, 0, sizeof(int), s));
   group_segments_kernel<false><<<blocks_for(32 * ng), 256, 0, s>>>(
@@ -793,9 +826,10 @@ int bin_points(npme_handle *h) {
   // heaviest groups first, so that the last wave of a launch holds the light
   // ones (each list by its own work; ties keep the column order)
   iota_kernel<<<blocks_for(ng), 256, 0, s>>>(iota, ng);
-  if ((rc = sort_pairs(h, work, work_out, iota, ord, ng, 32, s))) return rc;
+  const int wbits = bits_for((unsigned long long)n + 1);
+  if ((rc = sort_pairs(h, work, work_out, iota, ord, ng, wbits, s, true))) return rc;
   order_groups_kernel<<<blocks_for(ng), 256, 0, s>>>(ug, cen, ord, ng, h->d_groups, h->d_gcen);
-  if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ng, 32, s))) return rc;
+  if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ng, wbits, s, true))) return rc;
   order_groups_kernel<<<blocks_for(ng), 256, 0, s>>>(uh, cen, ord, ng, h->d_hgroups, h->d_hcen);
   SCK(cudaGetLastError());
   h->n_groups = h->n_hgroups = ng;
