@@ -514,10 +514,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   cudaEventRecord(b->ev_join, b->stream2);
   // 3. spread (grids zeroed first)
   for (int k = 0; k < m; k++) {
-    const npme_handle *h = hs[f32[k]];
-    const size_t gbytes = sizeof(float) * (h->complex_kernel ? 2 : 1) *
-                          (size_t)h->grid.N[0] * h->grid.N[1] * h->grid.N[2];
-    cudaMemsetAsync(h->d_grid, 0, gbytes, s);
+    grid_clear(hs[f32[k]], s);
   }
   for (auto &kv : spr) {
     Class &c = kv.second;

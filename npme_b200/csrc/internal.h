@@ -86,7 +86,9 @@ struct npme_handle {
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;  // direct sum runs here, overlapped with the FFTs
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  npme::FFTPlan *pf = nullptr, *pi = nullptr;  // shared plans (not owned)
+  // shared plans (not owned): (y, z) slab transforms forward and inverse,
+  // and the transforms along x (fft.cu)
+  npme::FFTPlan *pf = nullptr, *pi = nullptr, *px = nullptr;
   void *d_work = nullptr;                        // this handle's cuFFT work area
   cudaMemPool_t pool = nullptr;                  // device memory pool (shared, not owned)
 
@@ -179,6 +181,8 @@ int device_bin(npme_handle *h);
 
 // fft.cu
 int prepare_plans(npme_handle *h);
+// zeroes what the spread adds into and the forward transform reads
+int grid_clear(npme_handle *h, cudaStream_t s);
 int fft_forward(npme_handle *h, cudaStream_t s);
 int fft_inverse(npme_handle *h, cudaStream_t s);
 

@@ -150,7 +150,7 @@ void pool_release(npme_handle *h) {
 // Frees every device buffer of the handle (stream-ordered; the caller has
 // synchronised the handle's streams).
 void release(npme_handle *h) {
-  h->pf = h->pi = nullptr;  // shared plans stay in the process-wide cache
+  h->pf = h->pi = h->px = nullptr;  // shared plans stay in the process-wide cache
   h->d_dperm = nullptr;
   // every device buffer was obtained through dalloc, which records the
   // address of the pointer field it fills
@@ -481,8 +481,6 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   CK(cudaSetDevice(h->device));
   cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
   h->launches = 0;
-  const size_t gbytes = (h->fp32 ? 4 : 8) * (h->complex_kernel ? 2 : 1) *
-                        (size_t)h->grid.N[0] * h->grid.N[1] * h->grid.N[2];
   tmark(h, 0, s);
   npme::launch_gather_charges(h, d_charge, s);
   CK(cudaGetLastError());  // launch errors are checked before cuFFT runs
@@ -505,7 +503,7 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   };
   int frc;
   if (!serial && (frc = fork_direct())) return frc;
-  CK(cudaMemsetAsync(h->d_grid, 0, gbytes, s));
+  if (npme::grid_clear(h, s)) return fail(h, NPME_ECUDA, "clearing the spread grid failed");
   npme::launch_spread(h, s);
   CK(cudaGetLastError());
   tmark(h, 2, s);
