@@ -118,6 +118,7 @@ struct npme_handle {
   double *d_flam[3] = {nullptr, nullptr, nullptr};  //   lambda^2
   double *d_fcos[3] = {nullptr, nullptr, nullptr};  //   cos(2 pi m / N)
   double *h_fstage = nullptr;  // pinned staging of those tables (freed at destroy)
+  void *h_counts = nullptr;    // pinned: the set-up's counts (setup.cu, freed at destroy)
   size_t fstage_cap = 0;
   double *d_fdct[3] = {nullptr, nullptr, nullptr};  // DCT-I matrices per axis
   long fdct_N[3] = {0, 0, 0};                        // the FFT lengths they were built for
@@ -176,8 +177,11 @@ double compact_extent(double X0, double del, long order, long N);
 // the non-finite check) read back into mn / mx
 int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3]);
 // brick order, direct-sum orders, warp groups and segments, buffers (the box,
-// grid geometry and h->bmin / bmax set)
+// grid geometry and h->bmin / bmax set); enqueued without waiting: the counts
+// reach the host with the set-up's final synchronisation
 int device_bin(npme_handle *h);
+// after that synchronisation: the counts into the handle, the stencil check
+int finish_setup(npme_handle *h);
 
 // fft.cu
 int prepare_plans(npme_handle *h);

@@ -458,13 +458,17 @@ static int setup_impl(npme_handle *h, size_t n, const double *coord) {
     return rc;
   }
   // all set-up work is on the handle's stream; CalcV may be enqueued on any
-  // stream, so the set-up completes here
+  // stream, so the set-up completes here (and its counts arrive)
   {
     const cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
       release(h);
       return fail(h, NPME_ECUDA, std::string("set-up: ") + cudaGetErrorString(e));
     }
+  }
+  if ((rc = npme::finish_setup(h))) {
+    release(h);
+    return rc;
   }
   h->ready = true;
   return NPME_OK;
@@ -722,6 +726,7 @@ int npme_gpu_destroy(npme_handle *h) {
   release(h);
   pool_release(h);
   if (h->h_fstage) cudaFreeHost(h->h_fstage);
+  if (h->h_counts) cudaFreeHost(h->h_counts);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);

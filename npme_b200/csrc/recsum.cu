@@ -12,6 +12,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 #include "bodies.cuh"
@@ -185,17 +188,40 @@ static double bspline_host(int n, double w) {
 
 // |1/sum_p B_n(p) exp(-2 pi i k p / N)|^2 for k = 0..N/2 (src/RecSumV.cpp:565-581)
 static void lambda2_host(long N, int order, std::vector<double> &out) {
+  std::vector<double> b(order + 1);
+  for (int p = 0; p <= order; p++) b[p] = bspline_host(order, p);
   out.resize(N / 2 + 1);
   for (long k = 0; k <= N / 2; k++) {
     const double z = (double)k / (double)N;
     double dr = 0, di = 0;
     for (int p = 0; p <= order; p++) {
-      const double b = bspline_host(order, p);
-      dr += b * std::cos(2.0 * M_PI * z * p);
-      di -= b * std::sin(2.0 * M_PI * z * p);
+      dr += b[p] * std::cos(2.0 * M_PI * z * p);
+      di -= b[p] * std::sin(2.0 * M_PI * z * p);
     }
     out[k] = 1.0 / (dr * dr + di * di);
   }
+}
+
+// lambda^2 (per N and order) and cos(2 pi m / N) (per N) of every axis a
+// process has seen: a serving process meets the same few FFT lengths again
+// and again, and the kernel transform of each request needs them.
+struct AxisTables {
+  std::vector<double> lam, cosines;
+};
+static std::mutex g_axis_mu;
+static std::map<std::pair<long, int>, std::shared_ptr<const AxisTables>> g_axis_tables;
+
+static std::shared_ptr<const AxisTables> axis_tables(long N, int order) {
+  std::lock_guard<std::mutex> lk(g_axis_mu);
+  auto &slot = g_axis_tables[std::make_pair(N, order)];
+  if (!slot) {
+    auto t = std::make_shared<AxisTables>();
+    lambda2_host(N, order, t->lam);
+    t->cosines.resize(N);
+    for (long m = 0; m < N; m++) t->cosines[m] = std::cos(2.0 * M_PI * (double)m / (double)N);
+    slot = t;
+  }
+  return slot;
 }
 
 static double hramp(double x, double a) {
@@ -254,10 +280,11 @@ int build_kernel_transform(npme_handle *h) {
   const long MT = (long)M1 * M2 * M3;
   const double dels[3] = {h->p.del1, h->p.del2, h->p.del3};
   const double as[3] = {h->p.a1, h->p.a2, h->p.a3};
-  std::vector<double> ax[3], lam[3];
+  std::vector<double> ax[3];
+  std::shared_ptr<const AxisTables> tab[3];
   for (int d = 0; d < 3; d++) {
     window_axis(N[d], h->box[d], dels[d], as[d], ax[d]);
-    lambda2_host(N[d], h->grid.order, lam[d]);
+    tab[d] = axis_tables(N[d], h->grid.order);
   }
   LRKernel k{};
   k.func = h->p.funcType;
@@ -282,7 +309,7 @@ int build_kernel_transform(npme_handle *h) {
   size_t off[3][3], total = 0;
   for (int d = 0; d < 3; d++) {
     off[d][0] = total, total += ax[d].size();
-    off[d][1] = total, total += lam[d].size();
+    off[d][1] = total, total += tab[d]->lam.size();
     off[d][2] = total, total += (size_t)N[d];
   }
   if (h->fstage_cap < total) {
@@ -293,9 +320,8 @@ int build_kernel_transform(npme_handle *h) {
   }
   for (int d = 0; d < 3; d++) {
     std::copy(ax[d].begin(), ax[d].end(), h->h_fstage + off[d][0]);
-    std::copy(lam[d].begin(), lam[d].end(), h->h_fstage + off[d][1]);
-    double *cs = h->h_fstage + off[d][2];
-    for (long m = 0; m < N[d]; m++) cs[m] = std::cos(2.0 * M_PI * (double)m / (double)N[d]);
+    std::copy(tab[d]->lam.begin(), tab[d]->lam.end(), h->h_fstage + off[d][1]);
+    std::copy(tab[d]->cosines.begin(), tab[d]->cosines.end(), h->h_fstage + off[d][2]);
   }
   if ((rc = handle_buffer(h, (void **)&h->d_ftab, sizeof(double) * total))) return rc;
   NPME_CK(cudaMemcpyAsync(h->d_ftab, h->h_fstage, sizeof(double) * total, cudaMemcpyHostToDevice,

@@ -37,6 +37,7 @@ namespace npme {
 namespace {
 
 constexpr int kSourceSplit = 2;  // fine source columns per coarse column edge
+constexpr long kHostBoxPoints = 1L << 15;  // below: bounding box on the host
 
 // Order-preserving 64-bit key of a double (total order of the finite values).
 __device__ __forceinline__ unsigned long long dkey(double x) {
@@ -56,8 +57,6 @@ struct SetupStats {
   unsigned int nonfinite;
   unsigned int pad;
   long long bad;                    // lowest index whose stencil leaves the octant
-  unsigned int maxb;                // points in the fullest brick
-  unsigned int pad2;
   unsigned long long cand, hcand;   // staged (target, source) candidates, both walks
 };
 
@@ -65,7 +64,6 @@ __global__ void init_stats_kernel(SetupStats *st, long long n) {
   for (int d = 0; d < 3; d++) st->mn[d] = ~0ull, st->mx[d] = 0ull;
   st->nonfinite = 0;
   st->bad = n;
-  st->maxb = 0;
   st->cand = st->hcand = 0;
 }
 
@@ -140,10 +138,9 @@ __device__ __forceinline__ long stencil_start(double w) {
 // its (coarse column, quantised z) and (fine column, quantised z) sort keys;
 // per brick and column the point counts.  Arithmetic as the host restatement of the reference
 // (explicit round-to-nearest operations, no contraction), so that every
-// point lands in the same brick, bank and column on any machine.  Returns
-// the brick's count after this point's insertion (0 outside the octant).
+// point lands in the same brick, bank and column on any machine.
 template <typename T>
-__device__ __forceinline__ unsigned bin_point(const double *__restrict__ coord, long i, BinGeom g,
+__device__ __forceinline__ void bin_point(const double *__restrict__ coord, long i, BinGeom g,
                            BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
                            unsigned long long *__restrict__ ckey,
                            unsigned long long *__restrict__ skey, unsigned *__restrict__ iota,
@@ -175,7 +172,7 @@ __device__ __forceinline__ unsigned bin_point(const double *__restrict__ coord, 
   bp.orig = (uint32_t)i;
   pts[i] = bp;
   bkey[i] = ((unsigned)bid << 5) | key;
-  const unsigned cnt = out ? 0u : (unsigned)atomicAdd(&bcount[bid], 1) + 1u;
+  if (!out) atomicAdd(&bcount[bid], 1);
   int cs[2], ss[2];
 #pragma unroll
   for (int d = 0; d < 2; d++) {
@@ -193,7 +190,6 @@ __device__ __forceinline__ unsigned bin_point(const double *__restrict__ coord, 
   atomicAdd(&ccount[cc], 1);
   atomicAdd(&scount[sc], 1);
   iota[i] = (unsigned)i;
-  return cnt;
 }
 
 template <typename T>
@@ -203,13 +199,8 @@ __global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
                            unsigned long long *__restrict__ skey, unsigned *__restrict__ iota,
                            int *__restrict__ bcount, int *__restrict__ ccount,
                            int *__restrict__ scount, SetupStats *st) {
-  const long i0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  // the fullest brick's count, reduced per warp before the atomic
-  unsigned cnt = 0;
-  if (i0 < n) cnt = bin_point<T>(coord, i0, g, pts, bkey, ckey, skey, iota, bcount, ccount,
-                                 scount, st);
-  cnt = __reduce_max_sync(0xffffffffu, cnt);
-  if ((threadIdx.x & 31) == 0 && cnt) atomicMax(&st->maxb, cnt);
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bin_point<T>(coord, i, g, pts, bkey, ckey, skey, iota, bcount, ccount, scount, st);
 }
 
 template <typename T>
@@ -327,11 +318,11 @@ struct GroupGeom {
 // Bounding box of every group (warp per group): lo/hi corners, and the
 // frame origin (centre) with the half diagonal in w.
 __global__ void group_box_kernel(const double4 *__restrict__ gpos, const int4 *__restrict__ grec,
-                                 long ngroups, double4 *__restrict__ blo,
+                                 const int *__restrict__ ngroups, double4 *__restrict__ blo,
                                  double4 *__restrict__ bhi, double4 *__restrict__ cen) {
   const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (g >= ngroups) return;  // warp-uniform
+  if (g >= *ngroups) return;  // warp-uniform (launched for an upper bound)
   const int4 G = grec[g];
   double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
   if (G.x + lane < G.y) {
@@ -388,7 +379,8 @@ __device__ __forceinline__ int upper_idx(const unsigned *__restrict__ v, int a, 
 // group order.  FILL = false counts (segments, work, candidates); FILL =
 // true writes the segments at the offsets of the count pass.
 template <bool FILL>
-__global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ grec, long ngroups,
+__global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ grec,
+                                      const int *__restrict__ ngroups,
                                       const double4 *__restrict__ blo,
                                       const double4 *__restrict__ bhi,
                                       const int *__restrict__ sstart, const unsigned *__restrict__ zq,
@@ -401,7 +393,7 @@ __global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ gre
                                       int4 *__restrict__ hgroups, SetupStats *st) {
   const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (g >= ngroups) return;  // warp-uniform
+  if (g >= *ngroups) return;  // warp-uniform (launched for an upper bound)
   const unsigned FULL = 0xffffffffu;
   const int4 G = grec[g];
   const int p0 = G.x, p1 = G.y, c = G.z;
@@ -484,14 +476,37 @@ __global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ gre
   }
 }
 
-// final group records and frame origins in work order
+// final group records and frame origins in work order (the first ngroups
+// entries of the order; the slots past ngroups have no work and sort last)
 __global__ void order_groups_kernel(const int4 *__restrict__ gin, const double4 *__restrict__ cin,
-                                    const unsigned *__restrict__ ord, long ngroups,
+                                    const unsigned *__restrict__ ord,
+                                    const int *__restrict__ ngroups, long bound,
                                     int4 *__restrict__ gout, double4 *__restrict__ cout) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ngroups) return;
+  if (k >= bound || k >= *ngroups) return;
   gout[k] = gin[ord[k]];
   cout[k] = cin[ord[k]];
+}
+
+// The counts the host needs after set-up, gathered for one copy.
+struct SetupCounts {
+  long long bad;
+  unsigned long long cand, hcand;
+  int ngroups, nnonempty, nsegs, nhsegs;
+};
+__global__ void collect_counts_kernel(const SetupStats *__restrict__ st,
+                                      const int *__restrict__ ngroups,
+                                      const int *__restrict__ nnonempty,
+                                      const int *__restrict__ nsegs,
+                                      const int *__restrict__ nhsegs,
+                                      SetupCounts *__restrict__ out) {
+  out->bad = st->bad;
+  out->cand = st->cand;
+  out->hcand = st->hcand;
+  out->ngroups = *ngroups;
+  out->nnonempty = *nnonempty;
+  out->nsegs = *nsegs;
+  out->nhsegs = *nhsegs;
 }
 
 __global__ void iota_kernel(unsigned *__restrict__ v, long n) {
@@ -512,7 +527,7 @@ enum Scratch {
   kPts, kBKey, kBKeyOut, kIota, kBPerm, kCKey, kSKey, kKeyOut,
   kBCount, kCCount, kSCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
   kGRec, kBLo, kBHi, kCen, kNSeg, kNHSeg, kWork, kHWork, kSegOff, kHSegOff, kUGroups, kUHGroups,
-  kWorkOut, kOrd, kStats, kCub, kHead, kRunStart, kRKey, kRKeyOut, kBPos, kScratchCount
+  kWorkOut, kOrd, kStats, kCub, kHead, kRunStart, kRKey, kRKeyOut, kBPos, kCounts, kScratchCount
 };
 static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
 
@@ -663,8 +678,7 @@ int bin_points(npme_handle *h) {
   SCK(cudaGetLastError());
 
   // --- brick order: by brick, inside a brick in rounds over the banks ---
-  // (brick, bank, index) first here; (brick, rank inside the bank, bank)
-  // after the read-back below, which gives the rank's bit count
+  // (brick, bank, index) first; (brick, rank inside the bank, bank) below
   int *head, *rstart;
   if ((rc = sort_pairs(h, bkey, bkey_out, iota, bperm, n, 5 + bits_for(nbt), s)) ||
       (rc = scratch(h, kHead, sizeof(int) * n, &head)) ||
@@ -699,45 +713,29 @@ int bin_points(npme_handle *h) {
   if ((rc = exclusive_sum(h, gcount, goff, ncol + 1, s))) return rc;
   SCK(cudaGetLastError());
 
-  // read back: groups, non-empty bricks, the stencil check
-  struct {
-    int ngroups, nnonempty;
-    long long bad;
-    unsigned maxb;
-  } rb;
-  SCK(cudaMemcpyAsync(&rb.ngroups, goff + ncol, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SCK(cudaMemcpyAsync(&rb.nnonempty, pos + nbt, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SCK(cudaMemcpyAsync(&rb.bad, &st->bad, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  SCK(cudaMemcpyAsync(&rb.maxb, &st->maxb, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-  SCK(cudaStreamSynchronize(s));
-  if (rb.bad < n) {
-    // the axis of the first offending point, from its coordinates
-    double x[3];
-    SCK(cudaMemcpy(x, h->d_coord + 3 * rb.bad, sizeof(x), cudaMemcpyDeviceToHost));
-    int axis = 0;
-    for (int d = 0; d < 3; d++) {
-      const double w = (double)gr.N[d] / L[d] * (x[d] - R[d]);
-      const long ms = w < 0 ? (long)(-w) + 1 : (long)(-w);
-      const long o = ms + gr.N[d] / 4;
-      if (o < 0 || o + gr.order - 1 > gr.H[d] - 1) {
-        axis = d;
-        break;
-      }
-    }
-    return record_error(h, NPME_EINVAL,
-                        "point " + std::to_string(rb.bad) + " has a B-spline stencil outside "
-                        "the charge octant (axis " + std::to_string(axis) + ")");
-  }
-  h->n_nonempty = rb.nnonempty;
+  // No read-back here: the group and segment arrays are sized from upper
+  // bounds and the kernels read the actual counts on the device; the host
+  // reads every count once, when the set-up has completed (finish_setup).
+  //   groups   <= n / 32 + non-empty columns <= n / 32 + min(n, ncol)
+  //   segments <= groups x the fine columns of a group's window (a group lies
+  //               in one coarse column, so its window spans at most
+  //               (edge + 2 Rdir) / sedge + 4 fine columns per axis)
+  //   non-empty bricks <= min(n, nbt)
+  const long ngb = n / 32 + std::min(n, ncol) + 1;
+  long wmax = 1;
+  for (int d = 0; d < 2; d++)
+    wmax *= std::min<long>(g.ns[d], (long)std::floor((g.edge[d] + 2.0 * Rd) / g.sedge[d]) + 4);
+  const long nsb = ngb * wmax;
+  if (nsb >= (1L << 31))  // int offsets in the group records
+    return record_error(h, NPME_EINVAL, "too many direct-sum source segments (2^31)");
   if ((rc = handle_buffer(h, (void **)&h->d_brick_list,
-                          sizeof(int) * std::max<long>(1, rb.nnonempty))))
+                          sizeof(int) * std::max<long>(1, std::min(n, nbt)))))
     return rc;
   brick_list_kernel<<<blocks_for(nbt), 256, 0, s>>>(bcount, pos, nbt, h->d_brick_list);
 
-  // brick order in rounds over the banks: ranks inside a bank are below the
-  // fullest brick's count, so the key takes bits(nbt) + bits(maxb) + 5 bits
+  // brick order in rounds over the banks: the rank inside a bank is below n
   {
-    const int rbits = bits_for(std::max(1u, rb.maxb));
+    const int rbits = bits_for((unsigned long long)n);
     const int kbits = bits_for(nbt) + rbits + 5;
     unsigned *bperm2 = h->d_bperm;
     if (kbits <= 32) {
@@ -766,77 +764,69 @@ int bin_points(npme_handle *h) {
                                                         n, h->d_gpos, h->d_spos);
 
   // --- warp groups and their source segments ---
-  const long ng = rb.ngroups;
+  const int *ngp = goff + ncol;  // the actual group count, on the device
   int4 *grec;
   double4 *blo, *bhi, *cen;
   int *nseg, *nhseg, *segoff, *hsegoff;
   unsigned *work, *hwork, *work_out, *ord;
   int4 *ug, *uh;
-  if ((rc = scratch(h, kGRec, sizeof(int4) * ng, &grec)) ||
-      (rc = scratch(h, kBLo, sizeof(double4) * ng, &blo)) ||
-      (rc = scratch(h, kBHi, sizeof(double4) * ng, &bhi)) ||
-      (rc = scratch(h, kCen, sizeof(double4) * ng, &cen)) ||
-      (rc = scratch(h, kNSeg, sizeof(int) * (ng + 1), &nseg)) ||
-      (rc = scratch(h, kNHSeg, sizeof(int) * (ng + 1), &nhseg)) ||
-      (rc = scratch(h, kSegOff, sizeof(int) * (ng + 1), &segoff)) ||
-      (rc = scratch(h, kHSegOff, sizeof(int) * (ng + 1), &hsegoff)) ||
-      (rc = scratch(h, kWork, sizeof(unsigned) * ng, &work)) ||
-      (rc = scratch(h, kHWork, sizeof(unsigned) * ng, &hwork)) ||
-      (rc = scratch(h, kWorkOut, sizeof(unsigned) * ng, &work_out)) ||
-      (rc = scratch(h, kOrd, sizeof(unsigned) * ng, &ord)) ||
-      (rc = scratch(h, kUGroups, sizeof(int4) * ng, &ug)) ||
-      (rc = scratch(h, kUHGroups, sizeof(int4) * ng, &uh)))
+  if ((rc = scratch(h, kGRec, sizeof(int4) * ngb, &grec)) ||
+      (rc = scratch(h, kBLo, sizeof(double4) * ngb, &blo)) ||
+      (rc = scratch(h, kBHi, sizeof(double4) * ngb, &bhi)) ||
+      (rc = scratch(h, kCen, sizeof(double4) * ngb, &cen)) ||
+      (rc = scratch(h, kNSeg, sizeof(int) * (ngb + 1), &nseg)) ||
+      (rc = scratch(h, kNHSeg, sizeof(int) * (ngb + 1), &nhseg)) ||
+      (rc = scratch(h, kSegOff, sizeof(int) * (ngb + 1), &segoff)) ||
+      (rc = scratch(h, kHSegOff, sizeof(int) * (ngb + 1), &hsegoff)) ||
+      (rc = scratch(h, kWork, sizeof(unsigned) * ngb, &work)) ||
+      (rc = scratch(h, kHWork, sizeof(unsigned) * ngb, &hwork)) ||
+      (rc = scratch(h, kWorkOut, sizeof(unsigned) * ngb, &work_out)) ||
+      (rc = scratch(h, kOrd, sizeof(unsigned) * ngb, &ord)) ||
+      (rc = scratch(h, kUGroups, sizeof(int4) * ngb, &ug)) ||
+      (rc = scratch(h, kUHGroups, sizeof(int4) * ngb, &uh)) ||
+      (rc = handle_buffer(h, (void **)&h->d_segs, sizeof(int2) * nsb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_hsegs, sizeof(int2) * nsb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_groups, sizeof(int4) * ngb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_gcen, sizeof(double4) * ngb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_hgroups, sizeof(int4) * ngb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_hcen, sizeof(double4) * ngb)))
     return rc;
   group_records_kernel<<<blocks_for(ncol), 256, 0, s>>>(cstart, goff, ncol, grec);
-  group_box_kernel<<<blocks_for(32 * ng), 256, 0, s>>>(h->d_gpos, grec, ng, blo, bhi, cen);
+  group_box_kernel<<<blocks_for(32 * ngb), 256, 0, s>>>(h->d_gpos, grec, ngp, blo, bhi, cen);
   GroupGeom gg;
   gg.R = Rd, gg.R2 = Rd * Rd;
   for (int d = 0; d < 2; d++) gg.mn[d] = g.mn[d], gg.sedge[d] = g.sedge[d], gg.ns[d] = g.ns[d];
   gg.nc1 = g.nc[1];
   gg.zmin = g.zmin, gg.zscale = g.zscale, gg.zbits = g.zbits;
-  SCK(cudaMemsetAsync(nseg + ng, 0, sizeof(int), s));
-  SCK(cudaMemsetAsync(nhseg + ng, 0, sizeof(int), s));
-  group_segments_kernel<false><<<blocks_for(32 * ng), 256, 0, s>>>(
-      gg, grec, ng, blo, bhi, sstart, zs, fcpos, nseg, nhseg, work, hwork, nullptr, nullptr,
+  // slots past the actual groups: no segments, no work (they sort last)
+  SCK(cudaMemsetAsync(nseg, 0, sizeof(int) * (ngb + 1), s));
+  SCK(cudaMemsetAsync(nhseg, 0, sizeof(int) * (ngb + 1), s));
+  SCK(cudaMemsetAsync(work, 0, sizeof(unsigned) * ngb, s));
+  SCK(cudaMemsetAsync(hwork, 0, sizeof(unsigned) * ngb, s));
+  group_segments_kernel<false><<<blocks_for(32 * ngb), 256, 0, s>>>(
+      gg, grec, ngp, blo, bhi, sstart, zs, fcpos, nseg, nhseg, work, hwork, nullptr, nullptr,
       nullptr, nullptr, nullptr, nullptr, st);
-  if ((rc = exclusive_sum(h, nseg, segoff, ng + 1, s))) return rc;
-  if ((rc = exclusive_sum(h, nhseg, hsegoff, ng + 1, s))) return rc;
-  SCK(cudaGetLastError());
-  struct {
-    int nsegs, nhsegs;
-    unsigned long long cand, hcand;
-  } sb;
-  SCK(cudaMemcpyAsync(&sb.nsegs, segoff + ng, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SCK(cudaMemcpyAsync(&sb.nhsegs, hsegoff + ng, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SCK(cudaMemcpyAsync(&sb.cand, &st->cand, 2 * sizeof(unsigned long long),
-                      cudaMemcpyDeviceToHost, s));
-  SCK(cudaStreamSynchronize(s));
-  if (sb.nsegs < 0 || sb.nhsegs < 0)  // int offsets of the group records
-    return record_error(h, NPME_EINVAL, "too many direct-sum source segments (2^31)");
-  if ((rc = handle_buffer(h, (void **)&h->d_segs, sizeof(int2) * std::max(1, sb.nsegs))) ||
-      (rc = handle_buffer(h, (void **)&h->d_hsegs, sizeof(int2) * std::max(1, sb.nhsegs))) ||
-      (rc = handle_buffer(h, (void **)&h->d_groups, sizeof(int4) * ng)) ||
-      (rc = handle_buffer(h, (void **)&h->d_gcen, sizeof(double4) * ng)) ||
-      (rc = handle_buffer(h, (void **)&h->d_hgroups, sizeof(int4) * ng)) ||
-      (rc = handle_buffer(h, (void **)&h->d_hcen, sizeof(double4) * ng)))
-    return rc;
-  group_segments_kernel<true><<<blocks_for(32 * ng), 256, 0, s>>>(
-      gg, grec, ng, blo, bhi, sstart, zs, fcpos, nullptr, nullptr, nullptr, nullptr, segoff,
+  if ((rc = exclusive_sum(h, nseg, segoff, ngb + 1, s))) return rc;
+  if ((rc = exclusive_sum(h, nhseg, hsegoff, ngb + 1, s))) return rc;
+  group_segments_kernel<true><<<blocks_for(32 * ngb), 256, 0, s>>>(
+      gg, grec, ngp, blo, bhi, sstart, zs, fcpos, nullptr, nullptr, nullptr, nullptr, segoff,
       hsegoff, h->d_segs, h->d_hsegs, ug, uh, st);
   // heaviest groups first, so that the last wave of a launch holds the light
   // ones (each list by its own work; ties keep the column order)
-  iota_kernel<<<blocks_for(ng), 256, 0, s>>>(iota, ng);
+  iota_kernel<<<blocks_for(ngb), 256, 0, s>>>(iota, ngb);
   const int wbits = bits_for((unsigned long long)n + 1);
-  if ((rc = sort_pairs(h, work, work_out, iota, ord, ng, wbits, s, true))) return rc;
-  order_groups_kernel<<<blocks_for(ng), 256, 0, s>>>(ug, cen, ord, ng, h->d_groups, h->d_gcen);
-  if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ng, wbits, s, true))) return rc;
-  order_groups_kernel<<<blocks_for(ng), 256, 0, s>>>(uh, cen, ord, ng, h->d_hgroups, h->d_hcen);
+  if ((rc = sort_pairs(h, work, work_out, iota, ord, ngb, wbits, s, true))) return rc;
+  order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(ug, cen, ord, ngp, ngb, h->d_groups,
+                                                      h->d_gcen);
+  if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ngb, wbits, s, true))) return rc;
+  order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(uh, cen, ord, ngp, ngb, h->d_hgroups,
+                                                      h->d_hcen);
+  // the counts, for the host to read when the set-up has completed
+  SetupCounts *dc;
+  if ((rc = scratch(h, kCounts, sizeof(SetupCounts), &dc))) return rc;
+  collect_counts_kernel<<<1, 1, 0, s>>>(st, ngp, pos + nbt, segoff + ngb, hsegoff + ngb, dc);
+  SCK(cudaMemcpyAsync(h->h_counts, dc, sizeof(SetupCounts), cudaMemcpyDeviceToHost, s));
   SCK(cudaGetLastError());
-  h->n_groups = h->n_hgroups = ng;
-  h->n_segs = sb.nsegs;
-  h->n_hsegs = sb.nhsegs;
-  h->cand_per_point = (double)sb.cand / (double)n;
-  h->hcand_per_point = (double)sb.hcand / (double)n;
   h->d_dperm = h->d_sperm;  // direct-sum charges are gathered into the source order
 
   // source-side sums of the pair-once walk start (and are kept) at zero
@@ -875,8 +865,23 @@ int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3])
   if ((rc = handle_buffer(h, (void **)&h->d_coord, sizeof(double) * 3 * n))) return rc;
   SetupStats *st;
   if ((rc = scratch(h, kStats, sizeof(SetupStats), &st))) return rc;
+  if (!h->h_counts) SCK(cudaHostAlloc(&h->h_counts, sizeof(SetupCounts), cudaHostAllocDefault));
   SCK(cudaMemcpyAsync(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
   init_stats_kernel<<<1, 1, 0, s>>>(st, n);
+  if (n < kHostBoxPoints) {
+    // small systems: one host pass costs less than a device reduction and
+    // the wait for it
+    for (int d = 0; d < 3; d++) mn[d] = 1e300, mx[d] = -1e300;
+    for (long i = 0; i < n; i++)
+      for (int d = 0; d < 3; d++) {
+        const double x = coord[3 * i + d];
+        if (!std::isfinite(x)) return record_error(h, NPME_EINVAL, "non-finite coordinate");
+        mn[d] = std::min(mn[d], x);
+        mx[d] = std::max(mx[d], x);
+      }
+    SCK(cudaGetLastError());
+    return NPME_OK;
+  }
   const unsigned blocks = (unsigned)std::min<long>(blocks_for(n), 148 * 8);
   bbox_kernel<<<blocks, 256, 0, s>>>(h->d_coord, n, st);
   SCK(cudaGetLastError());
@@ -885,6 +890,38 @@ int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3])
   SCK(cudaStreamSynchronize(s));
   if (hs.nonfinite) return record_error(h, NPME_EINVAL, "non-finite coordinate");
   for (int d = 0; d < 3; d++) mn[d] = dkey_inv(hs.mn[d]), mx[d] = dkey_inv(hs.mx[d]);
+  return NPME_OK;
+}
+
+int finish_setup(npme_handle *h) {
+  const SetupCounts &c = *static_cast<const SetupCounts *>(h->h_counts);
+  const long n = (long)h->n;
+  if (c.bad < n) {
+    // the axis of the first offending point, from its coordinates
+    double x[3];
+    SCK(cudaMemcpy(x, h->d_coord + 3 * c.bad, sizeof(x), cudaMemcpyDeviceToHost));
+    const GridGeom &gr = h->grid;
+    const double *R = h->box + 3, *L = h->box + 6;
+    int axis = 0;
+    for (int d = 0; d < 3; d++) {
+      const double w = (double)gr.N[d] / L[d] * (x[d] - R[d]);
+      const long ms = w < 0 ? (long)(-w) + 1 : (long)(-w);
+      const long o = ms + gr.N[d] / 4;
+      if (o < 0 || o + gr.order - 1 > gr.H[d] - 1) {
+        axis = d;
+        break;
+      }
+    }
+    return record_error(h, NPME_EINVAL,
+                        "point " + std::to_string(c.bad) + " has a B-spline stencil outside "
+                        "the charge octant (axis " + std::to_string(axis) + ")");
+  }
+  h->n_nonempty = c.nnonempty;
+  h->n_groups = h->n_hgroups = c.ngroups;
+  h->n_segs = c.nsegs;
+  h->n_hsegs = c.nhsegs;
+  h->cand_per_point = (double)c.cand / (double)n;
+  h->hcand_per_point = (double)c.hcand / (double)n;
   return NPME_OK;
 }
 
