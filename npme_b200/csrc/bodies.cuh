@@ -9,7 +9,6 @@
 
 namespace npme {
 
-constexpr int kGroupWarps = 4;  // warps per CTA of the FP32 direct sum
 #ifndef NPME_GROUP_MIN_BLOCKS
 #define NPME_GROUP_MIN_BLOCKS 1
 #endif

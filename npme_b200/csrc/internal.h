@@ -17,6 +17,8 @@ namespace npme {
 
 // Brick edge (grid points) of the spread tiles.
 constexpr int kBrick = 8;
+// Warps (one group of 32 targets each) per CTA of the direct sums.
+constexpr int kGroupWarps = 4;
 // Scratch buffers the device set-up keeps on a handle (setup.cu).
 constexpr int kSetupScratch = 48;
 

@@ -38,6 +38,8 @@ namespace {
 
 constexpr int kSourceSplit = 2;  // fine source columns per coarse column edge
 constexpr long kHostBoxPoints = 1L << 15;  // below: bounding box on the host
+// direct-sum groups of about one wave (148 SMs, about 4 resident CTAs each)
+constexpr long kOneWaveGroups = 148 * 4 * kGroupWarps;
 
 // Order-preserving 64-bit key of a double (total order of the finite values).
 __device__ __forceinline__ unsigned long long dkey(double x) {
@@ -211,29 +213,24 @@ __global__ void gather_bpts_kernel(const BrickPoint<T> *__restrict__ pts,
   if (k < n) out[k] = pts[perm[k]];
 }
 
-// Start of the run of equal (brick, bank) keys at each position k of the
-// brick-sorted order (k itself where a run starts, else 0; a max-scan then
-// gives every position its run's start).
-__global__ void run_head_kernel(const unsigned *__restrict__ key, long n, int *__restrict__ head) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) head[k] = (k == 0 || key[k] != key[k - 1]) ? (int)k : 0;
-}
-
 // Round-robin key (brick, rank inside its bank, bank), the rank in rbits
 // bits: sorting by it puts the r-th point of every bank of a brick into
-// round r.
+// round r.  The rank is the distance to the first equal key of the sorted
+// (brick, bank) keys, found by binary search.
 template <typename K>
-__global__ void round_key_kernel(const unsigned *__restrict__ key, const int *__restrict__ start,
-                                 long n, int rbits, K *__restrict__ rkey) {
+__global__ void round_key_kernel(const unsigned *__restrict__ key, long n, int rbits,
+                                 K *__restrict__ rkey) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const unsigned kk = key[k];
-  rkey[k] = ((K)(kk >> 5) << (rbits + 5)) | ((K)(k - start[k]) << 5) | (K)(kk & 31u);
+  long lo = 0, hi = k;  // first position with key == kk in [0, k]
+  while (lo < hi) {
+    const long m = (lo + hi) >> 1;
+    if (key[m] < kk) lo = m + 1;
+    else hi = m;
+  }
+  rkey[k] = ((K)(kk >> 5) << (rbits + 5)) | ((K)(k - lo) << 5) | (K)(kk & 31u);
 }
-
-struct MaxOp {
-  __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
-};
 
 __global__ void gather_u32_kernel(const unsigned *__restrict__ src,
                                   const unsigned *__restrict__ perm, long n,
@@ -525,9 +522,9 @@ inline unsigned blocks_for(long n, int t = 256) { return (unsigned)((n + t - 1) 
 // Scratch buffers of the set-up (handle-owned, reused by the next set-up).
 enum Scratch {
   kPts, kBKey, kBKeyOut, kIota, kBPerm, kCKey, kSKey, kKeyOut,
-  kBCount, kCCount, kSCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
-  kGRec, kBLo, kBHi, kCen, kNSeg, kNHSeg, kWork, kHWork, kSegOff, kHSegOff, kUGroups, kUHGroups,
-  kWorkOut, kOrd, kStats, kCub, kHead, kRunStart, kRKey, kRKeyOut, kBPos, kCounts, kScratchCount
+  kBCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
+  kGRec, kBLo, kBHi, kCen, kNSeg, kSegOff, kHSegOff, kUGroups, kUHGroups,
+  kWorkOut, kOrd, kStats, kCub, kRKey, kRKeyOut, kBPos, kCounts, kScratchCount
 };
 static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
 
@@ -570,16 +567,6 @@ int sort_pairs(npme_handle *h, const K *kin, K *kout, const unsigned *vin, unsig
                                                    end_bit, s));
   else
     SCK(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
-  return NPME_OK;
-}
-
-int inclusive_max(npme_handle *h, const int *in, int *out, long n, cudaStream_t s) {
-  size_t tb = 0;
-  SCK(cub::DeviceScan::InclusiveScan(nullptr, tb, in, out, MaxOp(), (int)n, s));
-  void *tmp;
-  int rc;
-  if ((rc = cub_tmp(h, tb, &tmp))) return rc;
-  SCK(cub::DeviceScan::InclusiveScan(tmp, tb, in, out, MaxOp(), (int)n, s));
   return NPME_OK;
 }
 
@@ -649,9 +636,7 @@ int bin_points(npme_handle *h) {
       (rc = scratch(h, kCKey, sizeof(unsigned long long) * n, &ckey)) ||
       (rc = scratch(h, kSKey, sizeof(unsigned long long) * n, &skey)) ||
       (rc = scratch(h, kKeyOut, sizeof(unsigned long long) * n, &key_out)) ||
-      (rc = scratch(h, kBCount, sizeof(int) * (nbt + 1), &bcount)) ||
-      (rc = scratch(h, kCCount, sizeof(int) * (ncol + 1), &ccount)) ||
-      (rc = scratch(h, kSCount, sizeof(int) * (nscol + 1), &scount)) ||
+      (rc = scratch(h, kBCount, sizeof(int) * (nbt + ncol + nscol + 3), &bcount)) ||
       (rc = scratch(h, kCStart, sizeof(int) * (ncol + 1), &cstart)) ||
       (rc = scratch(h, kSStart, sizeof(int) * (nscol + 1), &sstart)) ||
       (rc = scratch(h, kFlag, sizeof(int) * (nbt + 1), &flag)) ||
@@ -670,23 +655,19 @@ int bin_points(npme_handle *h) {
       (rc = handle_buffer(h, (void **)&h->d_V, sizeof(double) * 4 * C * n)))
     return rc;
 
-  SCK(cudaMemsetAsync(bcount, 0, sizeof(int) * (nbt + 1), s));
-  SCK(cudaMemsetAsync(ccount, 0, sizeof(int) * (ncol + 1), s));
-  SCK(cudaMemsetAsync(scount, 0, sizeof(int) * (nscol + 1), s));
+  // brick, coarse-column and fine-column counts in one block, one clear
+  ccount = bcount + nbt + 1;
+  scount = ccount + ncol + 1;
+  SCK(cudaMemsetAsync(bcount, 0, sizeof(int) * (nbt + ncol + nscol + 3), s));
   bin_kernel<T><<<blocks_for(n), 256, 0, s>>>(h->d_coord, n, g, pts, bkey, ckey, skey, iota,
                                               bcount, ccount, scount, st);
   SCK(cudaGetLastError());
 
   // --- brick order: by brick, inside a brick in rounds over the banks ---
   // (brick, bank, index) first; (brick, rank inside the bank, bank) below
-  int *head, *rstart;
   if ((rc = sort_pairs(h, bkey, bkey_out, iota, bperm, n, 5 + bits_for(nbt), s)) ||
-      (rc = scratch(h, kHead, sizeof(int) * n, &head)) ||
-      (rc = scratch(h, kRunStart, sizeof(int) * n, &rstart)) ||
       (rc = handle_buffer(h, (void **)&h->d_bperm, sizeof(uint32_t) * n)))
     return rc;
-  run_head_kernel<<<blocks_for(n), 256, 0, s>>>(bkey_out, n, head);
-  if ((rc = inclusive_max(h, head, rstart, n, s))) return rc;
   if ((rc = exclusive_sum(h, bcount, h->d_brick_start, nbt + 1, s))) return rc;
   nonempty_flags_kernel<<<blocks_for(nbt + 1), 256, 0, s>>>(bcount, nbt, flag);
   if ((rc = exclusive_sum(h, flag, pos, nbt + 1, s))) return rc;
@@ -743,7 +724,7 @@ int bin_points(npme_handle *h) {
       if ((rc = scratch(h, kRKey, sizeof(unsigned) * n, &rkey)) ||
           (rc = scratch(h, kRKeyOut, sizeof(unsigned) * n, &rkey_out)))
         return rc;
-      round_key_kernel<unsigned><<<blocks_for(n), 256, 0, s>>>(bkey_out, rstart, n, rbits, rkey);
+      round_key_kernel<unsigned><<<blocks_for(n), 256, 0, s>>>(bkey_out, n, rbits, rkey);
       if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, kbits, s))) return rc;
     } else {
       unsigned long long *rkey, *rkey_out;
@@ -751,7 +732,7 @@ int bin_points(npme_handle *h) {
           (rc = scratch(h, kRKeyOut, sizeof(unsigned long long) * n, &rkey_out)))
         return rc;
       round_key_kernel<unsigned long long>
-          <<<blocks_for(n), 256, 0, s>>>(bkey_out, rstart, n, rbits, rkey);
+          <<<blocks_for(n), 256, 0, s>>>(bkey_out, n, rbits, rkey);
       if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, kbits, s))) return rc;
     }
     gather_bpts_kernel<T><<<blocks_for(n), 256, 0, s>>>(pts, bperm2, n,
@@ -774,12 +755,10 @@ int bin_points(npme_handle *h) {
       (rc = scratch(h, kBLo, sizeof(double4) * ngb, &blo)) ||
       (rc = scratch(h, kBHi, sizeof(double4) * ngb, &bhi)) ||
       (rc = scratch(h, kCen, sizeof(double4) * ngb, &cen)) ||
-      (rc = scratch(h, kNSeg, sizeof(int) * (ngb + 1), &nseg)) ||
-      (rc = scratch(h, kNHSeg, sizeof(int) * (ngb + 1), &nhseg)) ||
+      (rc = scratch(h, kNSeg, sizeof(int) * 4 * (ngb + 1), &nseg)) ||
       (rc = scratch(h, kSegOff, sizeof(int) * (ngb + 1), &segoff)) ||
       (rc = scratch(h, kHSegOff, sizeof(int) * (ngb + 1), &hsegoff)) ||
-      (rc = scratch(h, kWork, sizeof(unsigned) * ngb, &work)) ||
-      (rc = scratch(h, kHWork, sizeof(unsigned) * ngb, &hwork)) ||
+
       (rc = scratch(h, kWorkOut, sizeof(unsigned) * ngb, &work_out)) ||
       (rc = scratch(h, kOrd, sizeof(unsigned) * ngb, &ord)) ||
       (rc = scratch(h, kUGroups, sizeof(int4) * ngb, &ug)) ||
@@ -791,6 +770,12 @@ int bin_points(npme_handle *h) {
       (rc = handle_buffer(h, (void **)&h->d_hgroups, sizeof(int4) * ngb)) ||
       (rc = handle_buffer(h, (void **)&h->d_hcen, sizeof(double4) * ngb)))
     return rc;
+  // Heaviest groups first, so that the last wave of a direct-sum launch holds
+  // the light ones; when every group fits in one wave (4 groups per CTA,
+  // about 4 CTAs per SM) the order does not matter and the lists are
+  // written in column order directly.
+  const bool order_by_work = ngb > kOneWaveGroups;
+  if (!order_by_work) cen = h->d_gcen, ug = h->d_groups, uh = h->d_hgroups;
   group_records_kernel<<<blocks_for(ncol), 256, 0, s>>>(cstart, goff, ncol, grec);
   group_box_kernel<<<blocks_for(32 * ngb), 256, 0, s>>>(h->d_gpos, grec, ngp, blo, bhi, cen);
   GroupGeom gg;
@@ -798,11 +783,12 @@ int bin_points(npme_handle *h) {
   for (int d = 0; d < 2; d++) gg.mn[d] = g.mn[d], gg.sedge[d] = g.sedge[d], gg.ns[d] = g.ns[d];
   gg.nc1 = g.nc[1];
   gg.zmin = g.zmin, gg.zscale = g.zscale, gg.zbits = g.zbits;
-  // slots past the actual groups: no segments, no work (they sort last)
-  SCK(cudaMemsetAsync(nseg, 0, sizeof(int) * (ngb + 1), s));
-  SCK(cudaMemsetAsync(nhseg, 0, sizeof(int) * (ngb + 1), s));
-  SCK(cudaMemsetAsync(work, 0, sizeof(unsigned) * ngb, s));
-  SCK(cudaMemsetAsync(hwork, 0, sizeof(unsigned) * ngb, s));
+  // segment counts and work of both lists in one block, one clear (slots
+  // past the actual groups: no segments, no work, so they sort last)
+  nhseg = nseg + (ngb + 1);
+  work = (unsigned *)(nhseg + (ngb + 1));
+  hwork = work + (ngb + 1);
+  SCK(cudaMemsetAsync(nseg, 0, sizeof(int) * 4 * (ngb + 1), s));
   group_segments_kernel<false><<<blocks_for(32 * ngb), 256, 0, s>>>(
       gg, grec, ngp, blo, bhi, sstart, zs, fcpos, nseg, nhseg, work, hwork, nullptr, nullptr,
       nullptr, nullptr, nullptr, nullptr, st);
@@ -811,16 +797,18 @@ int bin_points(npme_handle *h) {
   group_segments_kernel<true><<<blocks_for(32 * ngb), 256, 0, s>>>(
       gg, grec, ngp, blo, bhi, sstart, zs, fcpos, nullptr, nullptr, nullptr, nullptr, segoff,
       hsegoff, h->d_segs, h->d_hsegs, ug, uh, st);
-  // heaviest groups first, so that the last wave of a launch holds the light
-  // ones (each list by its own work; ties keep the column order)
-  iota_kernel<<<blocks_for(ngb), 256, 0, s>>>(iota, ngb);
-  const int wbits = bits_for((unsigned long long)n + 1);
-  if ((rc = sort_pairs(h, work, work_out, iota, ord, ngb, wbits, s, true))) return rc;
-  order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(ug, cen, ord, ngp, ngb, h->d_groups,
-                                                      h->d_gcen);
-  if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ngb, wbits, s, true))) return rc;
-  order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(uh, cen, ord, ngp, ngb, h->d_hgroups,
-                                                      h->d_hcen);
+  if (order_by_work) {  // each list by its own work; ties keep the column order
+    iota_kernel<<<blocks_for(ngb), 256, 0, s>>>(iota, ngb);
+    const int wbits = bits_for((unsigned long long)n + 1);
+    if ((rc = sort_pairs(h, work, work_out, iota, ord, ngb, wbits, s, true))) return rc;
+    order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(ug, cen, ord, ngp, ngb, h->d_groups,
+                                                        h->d_gcen);
+    if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ngb, wbits, s, true))) return rc;
+    order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(uh, cen, ord, ngp, ngb, h->d_hgroups,
+                                                        h->d_hcen);
+  } else {
+    SCK(cudaMemcpyAsync(h->d_hcen, h->d_gcen, sizeof(double4) * ngb, cudaMemcpyDeviceToDevice, s));
+  }
   // the counts, for the host to read when the set-up has completed
   SetupCounts *dc;
   if ((rc = scratch(h, kCounts, sizeof(SetupCounts), &dc))) return rc;
