@@ -120,7 +120,8 @@ struct npme_handle {
   double *d_flam[3] = {nullptr, nullptr, nullptr};  //   lambda^2
   double *d_fcos[3] = {nullptr, nullptr, nullptr};  //   cos(2 pi m / N)
   double *h_fstage = nullptr;  // pinned staging of those tables (freed at destroy)
-  void *h_counts = nullptr;    // pinned: the set-up's counts (setup.cu, freed at destroy)
+  void *h_counts = nullptr;    // pinned: set-up counts of the batches this handle owned
+  int counts_cap = 0;          //   (setup.cu, freed at destroy)
   size_t fstage_cap = 0;
   double *d_fdct[3] = {nullptr, nullptr, nullptr};  // DCT-I matrices per axis
   long fdct_N[3] = {0, 0, 0};                        // the FFT lengths they were built for
@@ -178,12 +179,20 @@ double compact_extent(double X0, double del, long order, long N);
 // setup.cu: the caller's coordinates to d_coord, their bounding box (and
 // the non-finite check) read back into mn / mx
 int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3]);
-// brick order, direct-sum orders, warp groups and segments, buffers (the box,
-// grid geometry and h->bmin / bmax set); enqueued without waiting: the counts
-// reach the host with the set-up's final synchronisation
-int device_bin(npme_handle *h);
-// after that synchronisation: the counts into the handle, the stencil check
-int finish_setup(npme_handle *h);
+// brick order, direct-sum orders, warp groups and segments, buffers of R
+// handles of one precision in one pass on stream s (each with its box, grid
+// geometry and bmin / bmax set, its coordinates on its own stream); hs[0]
+// owns the scratch.  Enqueued without waiting: the counts reach
+// hs[0]->h_counts with the caller's synchronisation.
+int setup_geometry(npme_handle **hs, int R, cudaStream_t s);
+// after that synchronisation: system r's counts (from owner) into handle h,
+// and its stencil check
+int finish_setup(npme_handle *h, const npme_handle *owner, int r);
+// Sets up R handles (npme_gpu_setup's work for each, geometry in shared
+// passes); status[r] is each handle's result (its message in h->err).
+// Returns NPME_OK when every handle was set up.
+int setup_many(npme_handle **hs, int R, const size_t *n, const double *const *coord,
+               int *status);
 
 // fft.cu
 int prepare_plans(npme_handle *h);

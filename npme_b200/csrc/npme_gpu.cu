@@ -281,6 +281,122 @@ void fill_default_del(npme_params &p) {
 
 }  // namespace
 
+// Set-up in three stages: per handle, the checks, coordinates and box
+// (setup_prepare); for all handles at once, the geometry on the device
+// (npme::setup_geometry); per handle, FFT plans and the kernel transform
+// (setup_transform); then one wait and the counts (npme::finish_setup).
+static int setup_prepare(npme_handle *h, size_t n, const double *coord) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (h->user_kernel && !h->uops.direct)
+    return fail(h, NPME_ESTATE, "user kernel: npme_gpu_set_user_kernel before setup");
+  if (!coord && n) return fail(h, NPME_EINVAL, "null coord");
+  if (n == 0) return fail(h, NPME_EINVAL, "nCharge must be > 0");
+  if (n >= (size_t)1 << 31) return fail(h, NPME_EINVAL, "nCharge must be < 2^31");
+  CK(cudaSetDevice(h->device));
+  {
+    // load the no-allocation entry point's static scratch now, while the
+    // caller allows allocation (a failure shows up in that entry point)
+    std::string ignored;
+    npme::noalloc_preload(ignored);
+  }
+  // A handle that was set up before keeps its buffers (grown when needed),
+  // its FFT plans (the FFT box is a handle parameter) and its kernel-transform
+  // scratch: only the geometry-dependent state is rebuilt (ResetCoord,
+  // src/Interface.cpp:1958-1987).
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->stream2) cudaStreamSynchronize(h->stream2);
+  h->ready = false;
+  h->n = n;
+  const npme_params &p = h->p;
+  // box (src/RecSumSupportFunctions.cpp:182-201, 276-296) from the points'
+  // bounding box
+  double mx[3], mn[3];
+  int rc = npme::device_bbox(h, coord, mn, mx);
+  if (rc) return rc;
+  for (int d = 0; d < 3; d++) h->bmin[d] = mn[d], h->bmax[d] = mx[d];
+  const long Ns[3] = {p.N1, p.N2, p.N3};
+  const double dels[3] = {p.del1, p.del2, p.del3};
+  for (int d = 0; d < 3; d++) {
+    const double X0 = mx[d] - mn[d], R0 = 0.5 * (mx[d] + mn[d]);
+    const double X = min_x_compact(X0, dels[d], p.BnOrder, Ns[d]);
+    h->box[d] = X;
+    h->box[3 + d] = R0 + 0.5 * (X0 - X);
+    h->box[6 + d] = 2 * (X + dels[d]);
+    h->grid.N[d] = Ns[d];
+    h->grid.H[d] = Ns[d] / 2;
+    h->grid.nb[d] = (Ns[d] / 2 + npme::kBrick - 1) / npme::kBrick;
+  }
+  h->grid.order = p.BnOrder;
+  // the reference's cells of edge >= Rdir / nNeigh (reported by
+  // npme_gpu_get_info; the direct sum walks warp groups instead)
+  const double target = p.Rdir / p.nNeigh;
+  for (int d = 0; d < 3; d++) {
+    const double ext = mx[d] - mn[d];
+    int nc = (int)std::floor(ext / target);
+    nc = std::max(1, std::min(nc, 1 << 16));
+    h->cells.nc[d] = nc;
+    h->cells.edge[d] = (nc == 1) ? std::max(ext, target) : ext / nc;
+    h->cells.origin[d] = mn[d];
+  }
+  h->cells.reach = p.nNeigh;
+  // the built-in kernels evaluate every pair once unless NPME_PAIRS_ONCE=0
+  {
+    const char *e = std::getenv("NPME_PAIRS_ONCE");
+    h->use_sym = !(e && e[0] == '0');
+  }
+  return NPME_OK;
+}
+
+static int setup_transform(npme_handle *h) {
+  int rc;
+  if ((rc = npme::prepare_plans(h))) return rc;
+  return npme::build_kernel_transform(h);
+}
+
+int npme::setup_many(npme_handle **hs, int R, const size_t *n, const double *const *coord,
+                     int *status) {
+  std::vector<int> st(R, NPME_OK);
+  // per handle: checks, coordinates, box
+  for (int r = 0; r < R; r++) st[r] = setup_prepare(hs[r], n[r], coord[r]);
+  // the geometry of the prepared handles, one pass per precision
+  for (int prec = 0; prec < 2; prec++) {
+    std::vector<npme_handle *> group;
+    std::vector<int> idx;
+    for (int r = 0; r < R; r++)
+      if (!st[r] && hs[r]->fp32 == (prec == 0)) group.push_back(hs[r]), idx.push_back(r);
+    if (group.empty()) continue;
+    npme_handle *owner = group[0];
+    int rc = npme::setup_geometry(group.data(), (int)group.size(), owner->stream);
+    if (rc) {
+      for (size_t k = 0; k < group.size(); k++) {
+        if (group[k] != owner) group[k]->err = owner->err;
+        st[idx[k]] = rc;
+      }
+      continue;
+    }
+    for (size_t k = 0; k < group.size(); k++) st[idx[k]] = setup_transform(group[k]);
+    // the owner's stream carries the shared passes; every handle's stream
+    // its own transform: CalcV may be enqueued on any stream, so the set-up
+    // completes here (and the counts arrive)
+    for (size_t k = 0; k < group.size(); k++) {
+      npme_handle *h = group[k];
+      const cudaError_t e = cudaStreamSynchronize(h->stream);
+      if (e != cudaSuccess && !st[idx[k]])
+        st[idx[k]] = fail(h, NPME_ECUDA, std::string("set-up: ") + cudaGetErrorString(e));
+    }
+    for (size_t k = 0; k < group.size(); k++)
+      if (!st[idx[k]]) st[idx[k]] = npme::finish_setup(group[k], owner, (int)k);
+  }
+  int all = NPME_OK;
+  for (int r = 0; r < R; r++) {
+    if (st[r] && hs[r]) release(hs[r]);
+    if (!st[r]) hs[r]->ready = true;
+    if (status) status[r] = st[r];
+    if (st[r] && !all) all = st[r];
+  }
+  return all;
+}
+
 extern "C" {
 
 void npme_gpu_default_params(npme_params *p) {
@@ -379,100 +495,11 @@ int npme_gpu_set_user_kernel(npme_handle *h, const npme_user_ops *ops) {
   return NPME_OK;
 }
 
-static int setup_impl(npme_handle *h, size_t n, const double *coord);
-
 int npme_gpu_setup(npme_handle *h, size_t n, const double *coord) {
-  return setup_impl(h, n, coord);
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  return npme::setup_many(&h, 1, &n, &coord, nullptr);
 }
 
-static int setup_impl(npme_handle *h, size_t n, const double *coord) {
-  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
-  if (h->user_kernel && !h->uops.direct)
-    return fail(h, NPME_ESTATE, "user kernel: npme_gpu_set_user_kernel before setup");
-  if (!coord && n) return fail(h, NPME_EINVAL, "null coord");
-  if (n == 0) return fail(h, NPME_EINVAL, "nCharge must be > 0");
-  if (n >= (size_t)1 << 31) return fail(h, NPME_EINVAL, "nCharge must be < 2^31");
-  CK(cudaSetDevice(h->device));
-  {
-    // load the no-allocation entry point's static scratch now, while the
-    // caller allows allocation (a failure shows up in that entry point)
-    std::string ignored;
-    npme::noalloc_preload(ignored);
-  }
-  // A handle that was set up before keeps its buffers (grown when needed),
-  // its FFT plans (the FFT box is a handle parameter) and its kernel-transform
-  // scratch: only the geometry-dependent state is rebuilt (ResetCoord,
-  // src/Interface.cpp:1958-1987).
-  if (h->stream) cudaStreamSynchronize(h->stream);
-  if (h->stream2) cudaStreamSynchronize(h->stream2);
-  h->ready = false;
-  h->n = n;
-  const npme_params &p = h->p;
-  // box (src/RecSumSupportFunctions.cpp:182-201, 276-296) from the points'
-  // bounding box, reduced on the device
-  double mx[3], mn[3];
-  int rc = npme::device_bbox(h, coord, mn, mx);
-  if (rc) return rc;
-  for (int d = 0; d < 3; d++) h->bmin[d] = mn[d], h->bmax[d] = mx[d];
-  const long Ns[3] = {p.N1, p.N2, p.N3};
-  const double dels[3] = {p.del1, p.del2, p.del3};
-  for (int d = 0; d < 3; d++) {
-    const double X0 = mx[d] - mn[d], R0 = 0.5 * (mx[d] + mn[d]);
-    const double X = min_x_compact(X0, dels[d], p.BnOrder, Ns[d]);
-    h->box[d] = X;
-    h->box[3 + d] = R0 + 0.5 * (X0 - X);
-    h->box[6 + d] = 2 * (X + dels[d]);
-    h->grid.N[d] = Ns[d];
-    h->grid.H[d] = Ns[d] / 2;
-    h->grid.nb[d] = (Ns[d] / 2 + npme::kBrick - 1) / npme::kBrick;
-  }
-  h->grid.order = p.BnOrder;
-  // the reference's cells of edge >= Rdir / nNeigh (reported by
-  // npme_gpu_get_info; the direct sum walks warp groups instead)
-  const double target = p.Rdir / p.nNeigh;
-  for (int d = 0; d < 3; d++) {
-    const double ext = mx[d] - mn[d];
-    int nc = (int)std::floor(ext / target);
-    nc = std::max(1, std::min(nc, 1 << 16));
-    h->cells.nc[d] = nc;
-    h->cells.edge[d] = (nc == 1) ? std::max(ext, target) : ext / nc;
-    h->cells.origin[d] = mn[d];
-  }
-  h->cells.reach = p.nNeigh;
-  // the built-in kernels evaluate every pair once unless NPME_PAIRS_ONCE=0
-  {
-    const char *e = std::getenv("NPME_PAIRS_ONCE");
-    h->use_sym = !(e && e[0] == '0');
-  }
-  rc = npme::device_bin(h);
-  if (rc) {
-    release(h);
-    return rc;
-  }
-  if ((rc = npme::prepare_plans(h))) {
-    release(h);
-    return rc;
-  }
-  if ((rc = npme::build_kernel_transform(h))) {
-    release(h);
-    return rc;
-  }
-  // all set-up work is on the handle's stream; CalcV may be enqueued on any
-  // stream, so the set-up completes here (and its counts arrive)
-  {
-    const cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) {
-      release(h);
-      return fail(h, NPME_ECUDA, std::string("set-up: ") + cudaGetErrorString(e));
-    }
-  }
-  if ((rc = npme::finish_setup(h))) {
-    release(h);
-    return rc;
-  }
-  h->ready = true;
-  return NPME_OK;
-}
 
 static void tmark(npme_handle *h, int i, cudaStream_t s) {
   if (h->timing.enabled) cudaEventRecord(h->timing.ev[i], s);

@@ -16,11 +16,15 @@
 //    group's bounding box, and the half-shell part of them for the
 //    every-pair-once walk; groups ordered by their work, heaviest first.
 //
+// Any number of systems are set up in one pass (a batch: the serving queue
+// sets up the requests it admits together; npme_gpu_setup is a batch of
+// one), so the kernel launches of a set-up are shared by all its systems.
 // Sorting is done with stable radix sorts (values = point indices in
-// increasing order), so every order is (key, index) lexicographic and the
-// result does not depend on timing.  Work per point or per group is a
-// thread or a warp; the host reads back four small records (box, group
-// count, segment counts) and sizes the buffers from them.
+// increasing order) on keys that start with the system's index, so every
+// order is (system, key, index) lexicographic and the result does not
+// depend on timing or on the other systems of the batch.  Work per point or
+// per group is a thread or a warp.  Buffers are sized from upper bounds and
+// the host reads the counts once, when the set-up has completed.
 #include <cuda_runtime.h>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -30,6 +34,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "internal.h"
 
@@ -38,8 +43,6 @@ namespace {
 
 constexpr int kSourceSplit = 2;  // fine source columns per coarse column edge
 constexpr long kHostBoxPoints = 1L << 15;  // below: bounding box on the host
-// direct-sum groups of about one wave (148 SMs, about 4 resident CTAs each)
-constexpr long kOneWaveGroups = 148 * 4 * kGroupWarps;
 
 // Order-preserving 64-bit key of a double (total order of the finite values).
 __device__ __forceinline__ unsigned long long dkey(double x) {
@@ -53,20 +56,15 @@ inline double dkey_inv(unsigned long long k) {
   return x;
 }
 
-// Results the host reads back.
+// The bounding box of one system's coordinates, read back by the host.
 struct SetupStats {
   unsigned long long mn[3], mx[3];  // dkey of the per-axis minimum / maximum
   unsigned int nonfinite;
-  unsigned int pad;
-  long long bad;                    // lowest index whose stencil leaves the octant
-  unsigned long long cand, hcand;   // staged (target, source) candidates, both walks
 };
 
-__global__ void init_stats_kernel(SetupStats *st, long long n) {
+__global__ void init_stats_kernel(SetupStats *st) {
   for (int d = 0; d < 3; d++) st->mn[d] = ~0ull, st->mx[d] = 0ull;
   st->nonfinite = 0;
-  st->bad = n;
-  st->cand = st->hcand = 0;
 }
 
 __global__ void bbox_kernel(const double *__restrict__ coord, long n, SetupStats *st) {
@@ -136,32 +134,105 @@ __device__ __forceinline__ long stencil_start(double w) {
   return w < 0 ? (long)(-w) + 1 : (long)(-w);
 }
 
+struct GroupGeom {
+  double R, R2;
+  double mn[2], sedge[2];
+  int ns[2], nc1;
+  double zmin, zscale;  // the z quantisation of the sort keys
+  int zbits;
+};
+
+// One system of a set-up batch: its geometry and sizes, where its elements
+// start in the batch's concatenated scratch arrays, and its handle's output
+// buffers.  Index spaces of the batch: points (p_off), brick slots (b_off,
+// nbt + 1 per system: the bricks and an empty end slot), coarse and fine
+// column slots (c_off, s_off: columns and an end slot), group slots (g_off,
+// ngb per system: an upper bound of its groups).  Every sort key of the
+// batch starts with the system's index, so a system's elements stay
+// contiguous and in their own order through every sort.
+struct SysDesc {
+  BinGeom g;
+  GroupGeom gg;
+  long n, nbt, ncol, nscol, ngb;
+  long p_off, b_off, c_off, s_off, g_off;
+  const double *coord;
+  void *bpts;        // BrickPoint<T>[n]
+  int *brick_start;  // [nbt + 1]
+  int *brick_list;   // [min(n, nbt)]
+  uint32_t *cperm, *sperm, *bperm;
+  double4 *gpos, *spos;
+  int2 *segs, *hsegs;
+  int4 *groups, *hgroups;
+  double4 *gcen, *hcen;
+};
+
+// Per system, accumulated on the device.
+struct SysStats {
+  long long bad;                   // lowest index whose stencil leaves the octant
+  unsigned long long cand, hcand;  // staged (target, source) candidates, both walks
+};
+
+// The counts the host reads once the set-up has completed.
+struct SetupCounts {
+  long long bad;
+  unsigned long long cand, hcand;
+  int ngroups, nnonempty, nsegs, nhsegs;
+};
+
+constexpr int kZField = 20;  // bits of the quantised-z field of the column keys
+
+// The system owning element x of an index space with starts off[0..R).
+__device__ __forceinline__ int owner(const long *__restrict__ off, int R, long x) {
+  int lo = 0, hi = R - 1;
+  while (lo < hi) {
+    const int m = (lo + hi + 1) >> 1;
+    if (off[m] <= x) lo = m;
+    else hi = m - 1;
+  }
+  return lo;
+}
+
+__global__ void init_sys_stats_kernel(const SysDesc *__restrict__ d, int R, SysStats *st) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  st[r].bad = d[r].n;
+  st[r].cand = st[r].hcand = 0;
+}
+
 // Per point: the spread/interpolation record, its brick-and-bank sort key,
 // its (coarse column, quantised z) and (fine column, quantised z) sort keys;
-// per brick and column the point counts.  Arithmetic as the host restatement of the reference
-// (explicit round-to-nearest operations, no contraction), so that every
-// point lands in the same brick, bank and column on any machine.
+// per brick and column the point counts.  Arithmetic as the host restatement
+// of the reference (explicit round-to-nearest operations, no contraction),
+// so that every point lands in the same brick, bank and column on any
+// machine.
 template <typename T>
-__device__ __forceinline__ void bin_point(const double *__restrict__ coord, long i, BinGeom g,
-                           BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
+__global__ void bin_kernel(const SysDesc *__restrict__ d, const long *__restrict__ poff, int R,
+                           long P, int bbits, int cbits, int sbits,
+                           BrickPoint<T> *__restrict__ pts, unsigned long long *__restrict__ bkey,
                            unsigned long long *__restrict__ ckey,
                            unsigned long long *__restrict__ skey, unsigned *__restrict__ iota,
                            int *__restrict__ bcount, int *__restrict__ ccount,
-                           int *__restrict__ scount, SetupStats *st) {
-  const double x[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
+                           int *__restrict__ scount, SysStats *st) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int r = owner(poff, R, p);
+  const SysDesc &D = d[r];
+  const BinGeom &g = D.g;
+  const long i = p - D.p_off;
+  const double x[3] = {D.coord[3 * i], D.coord[3 * i + 1], D.coord[3 * i + 2]};
   long o[3];
   T u[3];
   bool out = false;
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const double w = __dmul_rn(__ddiv_rn(g.N[d], g.L[d]), __dsub_rn(x[d], g.R[d]));
+  for (int a = 0; a < 3; a++) {
+    const double w = __dmul_rn(__ddiv_rn(g.N[a], g.L[a]), __dsub_rn(x[a], g.R[a]));
     const long ms = stencil_start(w);
-    o[d] = ms + g.Nl[d] / 4;
-    if (o[d] < 0 || o[d] + g.P - 1 > g.H[d] - 1) out = true;
-    u[d] = (T)__dadd_rn(w, (double)ms);
+    o[a] = ms + g.Nl[a] / 4;
+    if (o[a] < 0 || o[a] + g.P - 1 > g.H[a] - 1) out = true;
+    u[a] = (T)__dadd_rn(w, (double)ms);
   }
   if (out) {
-    atomicMin(&st->bad, (long long)i);
+    atomicMin(&st[r].bad, (long long)i);
     o[0] = o[1] = o[2] = 0;  // any in-range brick: the set-up fails anyway
   }
   const long b1 = o[0] / kBrick, b2 = o[1] / kBrick, b3 = o[2] / kBrick;
@@ -172,64 +243,107 @@ __device__ __forceinline__ void bin_point(const double *__restrict__ coord, long
   bp.u[0] = u[0], bp.u[1] = u[1], bp.u[2] = u[2];
   bp.g0 = ((uint32_t)o[0] << 20) | ((uint32_t)o[1] << 10) | (uint32_t)o[2];
   bp.orig = (uint32_t)i;
-  pts[i] = bp;
-  bkey[i] = ((unsigned)bid << 5) | key;
-  if (!out) atomicAdd(&bcount[bid], 1);
+  pts[p] = bp;
+  bkey[p] = ((unsigned long long)r << (bbits + 5)) | ((unsigned long long)bid << 5) | key;
+  if (!out) atomicAdd(&bcount[D.b_off + bid], 1);
   int cs[2], ss[2];
 #pragma unroll
-  for (int d = 0; d < 2; d++) {
-    const double v = __dsub_rn(x[d], g.mn[d]);
-    cs[d] = min(g.nc[d] - 1, max(0, (int)__ddiv_rn(v, g.edge[d])));
-    const double r = __dsub_rn(v, __dmul_rn((double)cs[d], g.edge[d]));
-    ss[d] = cs[d] * kSourceSplit +
-            min(kSourceSplit - 1, max(0, (int)__ddiv_rn(r, g.sedge[d])));
+  for (int a = 0; a < 2; a++) {
+    const double v = __dsub_rn(x[a], g.mn[a]);
+    cs[a] = min(g.nc[a] - 1, max(0, (int)__ddiv_rn(v, g.edge[a])));
+    const double rr = __dsub_rn(v, __dmul_rn((double)cs[a], g.edge[a]));
+    ss[a] = cs[a] * kSourceSplit + min(kSourceSplit - 1, max(0, (int)__ddiv_rn(rr, g.sedge[a])));
   }
-  const unsigned cc = (unsigned)(cs[0] * g.nc[1] + cs[1]);
-  const unsigned sc = (unsigned)(ss[0] * g.ns[1] + ss[1]);
+  const unsigned long long cc = (unsigned long long)(cs[0] * g.nc[1] + cs[1]);
+  const unsigned long long sc = (unsigned long long)(ss[0] * g.ns[1] + ss[1]);
   const unsigned long long zq = zquant(x[2], g.zmin, g.zscale, g.zbits);
-  ckey[i] = ((unsigned long long)cc << g.zbits) | zq;
-  skey[i] = ((unsigned long long)sc << g.zbits) | zq;
-  atomicAdd(&ccount[cc], 1);
-  atomicAdd(&scount[sc], 1);
-  iota[i] = (unsigned)i;
+  ckey[p] = ((unsigned long long)r << (cbits + kZField)) | (cc << kZField) | zq;
+  skey[p] = ((unsigned long long)r << (sbits + kZField)) | (sc << kZField) | zq;
+  atomicAdd(&ccount[D.c_off + (long)cc], 1);
+  atomicAdd(&scount[D.s_off + (long)sc], 1);
+  iota[p] = (unsigned)p;
 }
 
-template <typename T>
-__global__ void bin_kernel(const double *__restrict__ coord, long n, BinGeom g,
-                           BrickPoint<T> *__restrict__ pts, unsigned *__restrict__ bkey,
-                           unsigned long long *__restrict__ ckey,
-                           unsigned long long *__restrict__ skey, unsigned *__restrict__ iota,
-                           int *__restrict__ bcount, int *__restrict__ ccount,
-                           int *__restrict__ scount, SetupStats *st) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) bin_point<T>(coord, i, g, pts, bkey, ckey, skey, iota, bcount, ccount, scount, st);
-}
-
-template <typename T>
-__global__ void gather_bpts_kernel(const BrickPoint<T> *__restrict__ pts,
-                                   const unsigned *__restrict__ perm, long n,
-                                   BrickPoint<T> *__restrict__ out) {
+// Round-robin key (system and brick, rank inside its bank, bank): sorting by
+// it puts the r-th point of every bank of a brick into round r.  The rank is
+// the distance to the first equal key of the sorted (system, brick, bank)
+// keys, found by binary search.
+__global__ void round_key_kernel(const unsigned long long *__restrict__ key, long P, int rankbits,
+                                 unsigned long long *__restrict__ rkey) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) out[k] = pts[perm[k]];
-}
-
-// Round-robin key (brick, rank inside its bank, bank), the rank in rbits
-// bits: sorting by it puts the r-th point of every bank of a brick into
-// round r.  The rank is the distance to the first equal key of the sorted
-// (brick, bank) keys, found by binary search.
-template <typename K>
-__global__ void round_key_kernel(const unsigned *__restrict__ key, long n, int rbits,
-                                 K *__restrict__ rkey) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const unsigned kk = key[k];
+  if (k >= P) return;
+  const unsigned long long kk = key[k];
   long lo = 0, hi = k;  // first position with key == kk in [0, k]
   while (lo < hi) {
     const long m = (lo + hi) >> 1;
     if (key[m] < kk) lo = m + 1;
     else hi = m;
   }
-  rkey[k] = ((K)(kk >> 5) << (rbits + 5)) | ((K)(k - lo) << 5) | (K)(kk & 31u);
+  rkey[k] = ((kk >> 5) << (rankbits + 5)) | ((unsigned long long)(k - lo) << 5) | (kk & 31ull);
+}
+
+// Final brick order of every system: its records, the brick-order
+// permutation, and each point's brick-order position (the slot of its
+// source-side direct-sum sums).
+template <typename T>
+__global__ void place_bricks_kernel(const SysDesc *__restrict__ d, const long *__restrict__ poff,
+                                    int R, long P, const unsigned *__restrict__ order,
+                                    const BrickPoint<T> *__restrict__ pts,
+                                    unsigned *__restrict__ bpos) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= P) return;
+  const int r = owner(poff, R, k);
+  const SysDesc &D = d[r];
+  const long p = order[k], kl = k - D.p_off;
+  reinterpret_cast<BrickPoint<T> *>(D.bpts)[kl] = pts[p];
+  D.bperm[kl] = (uint32_t)(p - D.p_off);
+  bpos[p] = (unsigned)kl;
+}
+
+// flag[b] = 1 for non-empty brick slots (end slots are empty)
+__global__ void nonempty_flags_kernel(const int *__restrict__ count, long nb,
+                                      int *__restrict__ flag) {
+  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nb) flag[b] = count[b] > 0;
+}
+
+// Every system's brick starts (local positions) and non-empty brick list.
+__global__ void bricks_kernel(const SysDesc *__restrict__ d, const long *__restrict__ boff, int R,
+                              long B, const int *__restrict__ count, const int *__restrict__ start,
+                              const int *__restrict__ pos) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= B) return;
+  const int r = owner(boff, R, slot);
+  const SysDesc &D = d[r];
+  const long b = slot - D.b_off;  // 0 .. nbt (end slot)
+  D.brick_start[b] = start[slot] - start[D.b_off];
+  if (b < D.nbt && count[slot] > 0) D.brick_list[pos[slot] - pos[D.b_off]] = (int)b;
+}
+
+// The direct sum's two orders of every system: local permutations, FP64
+// positions (a source's w holds its brick-order position), the sources'
+// quantised z, and each point's position in the target (group) order.
+__global__ void place_orders_kernel(const SysDesc *__restrict__ d, const long *__restrict__ poff,
+                                    int R, long P, const unsigned *__restrict__ corder,
+                                    const unsigned *__restrict__ sorder,
+                                    const unsigned long long *__restrict__ skey,
+                                    const unsigned *__restrict__ bpos, unsigned *__restrict__ zq,
+                                    unsigned *__restrict__ cpos) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= P) return;
+  const int r = owner(poff, R, k);
+  const SysDesc &D = d[r];
+  const long kl = k - D.p_off;
+  const long pc = corder[k], ic = pc - D.p_off;
+  D.cperm[kl] = (uint32_t)ic;
+  cpos[pc] = (unsigned)k;
+  const double *x = D.coord + 3 * ic;
+  D.gpos[kl] = make_double4(x[0], x[1], x[2], 0.0);
+  const long ps = sorder[k], is = ps - D.p_off;
+  D.sperm[kl] = (uint32_t)is;
+  zq[k] = (unsigned)(skey[k] & ((1ull << kZField) - 1ull));
+  const double *y = D.coord + 3 * is;
+  D.spos[kl] = make_double4(y[0], y[1], y[2], (double)bpos[ps]);
 }
 
 __global__ void gather_u32_kernel(const unsigned *__restrict__ src,
@@ -239,107 +353,67 @@ __global__ void gather_u32_kernel(const unsigned *__restrict__ src,
   if (k < n) out[k] = src[perm[k]];
 }
 
-// flag[b] = 1 for non-empty bricks (flag[nb] = 0)
-__global__ void nonempty_flags_kernel(const int *__restrict__ count, long nb,
-                                      int *__restrict__ flag) {
-  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b <= nb) flag[b] = b < nb && count[b] > 0;
-}
-
-__global__ void brick_list_kernel(const int *__restrict__ count, const int *__restrict__ pos,
-                                  long nb, int *__restrict__ list) {
-  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < nb && count[b] > 0) list[pos[b]] = (int)b;
-}
-
-// zq[k] = quantised z of source k (from its sorted key); cpos[cperm[k]] = k
-// (position of a point in the group order)
-__global__ void source_z_kernel(const unsigned long long *__restrict__ skey,
-                                const unsigned *__restrict__ cperm, long n, int zbits,
-                                unsigned *__restrict__ zq, unsigned *__restrict__ cpos) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  zq[k] = (unsigned)(skey[k] & ((1ull << zbits) - 1ull));
-  cpos[cperm[k]] = (unsigned)k;
-}
-
-// inverse of the brick order: bpos[caller index] = brick-order position
-__global__ void brick_position_kernel(const uint32_t *__restrict__ bperm, long n,
-                                      unsigned *__restrict__ bpos) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) bpos[bperm[k]] = (unsigned)k;
-}
-
-// FP64 positions in the target (group) and source orders; a source's w holds
-// its brick-order position, the slot of its source-side sums
-__global__ void gather_positions_kernel(const double *__restrict__ coord,
-                                        const uint32_t *__restrict__ gorder,
-                                        const uint32_t *__restrict__ sorder,
-                                        const unsigned *__restrict__ bpos, long n,
-                                        double4 *__restrict__ gpos, double4 *__restrict__ spos) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const double *x = coord + 3 * (long)gorder[k];
-  gpos[k] = make_double4(x[0], x[1], x[2], 0.0);
-  const unsigned j = sorder[k];
-  const double *y = coord + 3 * (long)j;
-  spos[k] = make_double4(y[0], y[1], y[2], (double)bpos[j]);
-}
-
-// groups per coarse column: ceil(count / 32) (entry ncol = 0)
+// groups per coarse column slot: ceil(count / 32) (end slots: 0)
 __global__ void groups_per_column_kernel(const int *__restrict__ ccount, long ncol,
                                          int *__restrict__ gcount) {
   const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c <= ncol) gcount[c] = c < ncol ? (ccount[c] + 31) / 32 : 0;
+  if (c < ncol) gcount[c] = (ccount[c] + 31) / 32;
 }
 
-// group g of column c: points [p0, p1) of the group order
-__global__ void group_records_kernel(const int *__restrict__ cstart, const int *__restrict__ goff,
-                                     long ncol, int4 *__restrict__ grec) {
-  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncol) return;
-  const int p_end = cstart[c + 1];
-  int g = goff[c];
-  for (int p0 = cstart[c]; p0 < p_end; p0 += 32, g++)
-    grec[g] = make_int4(p0, min(p0 + 32, p_end), (int)c, 0);
+// The groups of every column: points [p0, p1) of the batch's target order
+// (runs of 32 in the column), the column and the system.
+__global__ void group_records_kernel(const SysDesc *__restrict__ d, const long *__restrict__ coff,
+                                     int R, long C, const int *__restrict__ cstart,
+                                     const int *__restrict__ goff, int4 *__restrict__ grec) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= C) return;
+  const int r = owner(coff, R, slot);
+  const SysDesc &D = d[r];
+  const long c = slot - D.c_off;
+  if (c >= D.ncol) return;  // end slot
+  const int p_end = cstart[slot + 1];
+  long gs = D.g_off + (goff[slot] - goff[D.c_off]);
+  for (int p0 = cstart[slot]; p0 < p_end; p0 += 32, gs++)
+    grec[gs] = make_int4(p0, min(p0 + 32, p_end), (int)c, r);
 }
 
-struct GroupGeom {
-  double R, R2;
-  double mn[2], sedge[2];
-  int ns[2], nc1;
-  double zmin, zscale;  // the z quantisation of the sort keys
-  int zbits;
-};
+// the number of groups of system D (on the device)
+__device__ __forceinline__ long sys_groups(const SysDesc &D, const int *__restrict__ goff) {
+  return goff[D.c_off + D.ncol] - goff[D.c_off];
+}
 
-// Bounding box of every group (warp per group): lo/hi corners, and the
+// Bounding box of every group (warp per group slot): lo/hi corners, and the
 // frame origin (centre) with the half diagonal in w.
-__global__ void group_box_kernel(const double4 *__restrict__ gpos, const int4 *__restrict__ grec,
-                                 const int *__restrict__ ngroups, double4 *__restrict__ blo,
+__global__ void group_box_kernel(const SysDesc *__restrict__ d, const long *__restrict__ goffs,
+                                 int R, long G, const int *__restrict__ goff,
+                                 const int4 *__restrict__ grec, double4 *__restrict__ blo,
                                  double4 *__restrict__ bhi, double4 *__restrict__ cen) {
-  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long slot = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (g >= *ngroups) return;  // warp-uniform (launched for an upper bound)
-  const int4 G = grec[g];
+  if (slot >= G) return;  // warp-uniform
+  const int r = owner(goffs, R, slot);
+  const SysDesc &D = d[r];
+  if (slot - D.g_off >= sys_groups(D, goff)) return;  // a spare slot of the bound
+  const int4 Gr = grec[slot];
   double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
-  if (G.x + lane < G.y) {
-    const double4 p = gpos[G.x + lane];
+  if (Gr.x + lane < Gr.y) {
+    const double4 p = D.gpos[Gr.x + lane - D.p_off];
     l[0] = h[0] = p.x, l[1] = h[1] = p.y, l[2] = h[2] = p.z;
   }
   const unsigned FULL = 0xffffffffu;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      l[d] = fmin(l[d], __shfl_xor_sync(FULL, l[d], o));
-      h[d] = fmax(h[d], __shfl_xor_sync(FULL, h[d], o));
+    for (int a = 0; a < 3; a++) {
+      l[a] = fmin(l[a], __shfl_xor_sync(FULL, l[a], o));
+      h[a] = fmax(h[a], __shfl_xor_sync(FULL, h[a], o));
     }
   if (lane == 0) {
-    blo[g] = make_double4(l[0], l[1], l[2], 0.0);
-    bhi[g] = make_double4(h[0], h[1], h[2], 0.0);
+    blo[slot] = make_double4(l[0], l[1], l[2], 0.0);
+    bhi[slot] = make_double4(h[0], h[1], h[2], 0.0);
     const double dx = __dsub_rn(h[0], l[0]), dy = __dsub_rn(h[1], l[1]),
                  dz = __dsub_rn(h[2], l[2]);
-    cen[g] = make_double4(
+    cen[slot] = make_double4(
         __dmul_rn(0.5, __dadd_rn(l[0], h[0])), __dmul_rn(0.5, __dadd_rn(l[1], h[1])),
         __dmul_rn(0.5, __dadd_rn(l[2], h[2])),
         __dmul_rn(0.5, __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
@@ -348,8 +422,7 @@ __global__ void group_box_kernel(const double4 *__restrict__ gpos, const int4 *_
 }
 
 // first index in [a, b) with v[index] >= x (lower) or > x (upper)
-template <typename V>
-__device__ __forceinline__ int lower_idx(const V *__restrict__ v, int a, int b, V x) {
+__device__ __forceinline__ int lower_idx(const unsigned *__restrict__ v, int a, int b, unsigned x) {
   while (a < b) {
     const int m = (a + b) >> 1;
     if (v[m] < x) a = m + 1;
@@ -366,55 +439,64 @@ __device__ __forceinline__ int upper_idx(const unsigned *__restrict__ v, int a, 
   return a;
 }
 
-// Source segments of every group (warp per group; lanes over the fine
+// Source segments of every group (warp per group slot; lanes over the fine
 // columns of the group's window in (s0, s1) order, so that a group's
 // segments come in the same order as a sequential sweep).  A fine column
 // contributes the z range of its sources within Rdir of the group's box:
 // |dz| <= sqrt(Rdir^2 - d_xy^2), d_xy the xy distance from the box to the
 // column; the half shell keeps the fine columns of later coarse columns and,
 // in the group's own coarse column, the sources after the group in the
-// group order.  FILL = false counts (segments, work, candidates); FILL =
-// true writes the segments at the offsets of the count pass.
+// group order.  Positions are the batch's (cstart, sstart, fcpos); the
+// written segments and group records are the system's own (local).  FILL =
+// false counts (segments, work, candidates); FILL = true writes the
+// segments at the offsets of the count pass.
 template <bool FILL>
-__global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ grec,
-                                      const int *__restrict__ ngroups,
+__global__ void group_segments_kernel(const SysDesc *__restrict__ d, const long *__restrict__ goffs,
+                                      int R, long G, const int *__restrict__ goff,
+                                      const int4 *__restrict__ grec,
                                       const double4 *__restrict__ blo,
                                       const double4 *__restrict__ bhi,
-                                      const int *__restrict__ sstart, const unsigned *__restrict__ zq,
+                                      const int *__restrict__ sstart,
+                                      const unsigned *__restrict__ zq,
                                       const unsigned *__restrict__ fcpos, int *__restrict__ nseg,
                                       int *__restrict__ nhseg, unsigned *__restrict__ work,
                                       unsigned *__restrict__ hwork,
                                       const int *__restrict__ segoff,
-                                      const int *__restrict__ hsegoff, int2 *__restrict__ segs,
-                                      int2 *__restrict__ hsegs, int4 *__restrict__ groups,
-                                      int4 *__restrict__ hgroups, SetupStats *st) {
-  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                                      const int *__restrict__ hsegoff, int4 *__restrict__ ug,
+                                      int4 *__restrict__ uh, SysStats *st) {
+  const long slot = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (g >= *ngroups) return;  // warp-uniform (launched for an upper bound)
+  if (slot >= G) return;  // warp-uniform
+  const int r = owner(goffs, R, slot);
+  const SysDesc &D = d[r];
+  if (slot - D.g_off >= sys_groups(D, goff)) return;  // a spare slot of the bound
+  const GroupGeom &gg = D.gg;
   const unsigned FULL = 0xffffffffu;
-  const int4 G = grec[g];
-  const int p0 = G.x, p1 = G.y, c = G.z;
-  const double4 L = blo[g], Hh = bhi[g];
+  const int4 Gr = grec[slot];
+  const int p0 = Gr.x, p1 = Gr.y, c = Gr.z;
+  const double4 L = blo[slot], Hh = bhi[slot];
   const double bl[2] = {L.x, L.y}, bh[2] = {Hh.x, Hh.y};
   int lo[2], hi[2];
 #pragma unroll
-  for (int d = 0; d < 2; d++) {
+  for (int a = 0; a < 2; a++) {
     // one column of margin on each side: the distance test below decides
-    lo[d] = max(0, (int)floor((bl[d] - gg.R - gg.mn[d]) / gg.sedge[d]) - 1);
-    hi[d] = min(gg.ns[d] - 1, (int)floor((bh[d] + gg.R - gg.mn[d]) / gg.sedge[d]) + 1);
+    lo[a] = max(0, (int)floor((bl[a] - gg.R - gg.mn[a]) / gg.sedge[a]) - 1);
+    hi[a] = min(gg.ns[a] - 1, (int)floor((bh[a] + gg.R - gg.mn[a]) / gg.sedge[a]) + 1);
   }
   const int w1 = hi[1] - lo[1] + 1;
   const int nwin = (hi[0] - lo[0] + 1) * w1;
   int ns_ = 0, nh_ = 0;
-  unsigned long long wk = 0, hwk = 0, cand = 0, hcand = 0;
-  const int base = FILL ? segoff[g] : 0, hbase = FILL ? hsegoff[g] : 0;
+  unsigned long long wk = 0, hwk = 0;
+  const int base = FILL ? segoff[slot] - segoff[D.g_off] : 0;
+  const int hbase = FILL ? hsegoff[slot] - hsegoff[D.g_off] : 0;
+  const int pl = (int)D.p_off;  // batch position -> system position
   for (int t0 = 0; t0 < nwin; t0 += 32) {
     const int t = t0 + lane;
     bool has = false, hhas = false;
     int a = 0, b = 0, a2 = 0;
     if (t < nwin) {
       const int s0 = lo[0] + t / w1, s1 = lo[1] + t % w1;
-      const long sc = (long)s0 * gg.ns[1] + s1;
+      const long sc = D.s_off + (long)s0 * gg.ns[1] + s1;
       const int zb = sstart[sc], ze = sstart[sc + 1];
       if (ze > zb) {
         const double l0 = __dadd_rn(gg.mn[0], __dmul_rn((double)s0, gg.sedge[0]));
@@ -442,8 +524,8 @@ __global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ gre
     const unsigned m = __ballot_sync(FULL, has), hm = __ballot_sync(FULL, hhas);
     const unsigned below = (1u << lane) - 1u;
     if (FILL) {
-      if (has) segs[base + ns_ + __popc(m & below)] = make_int2(a, b - a);
-      if (hhas) hsegs[hbase + nh_ + __popc(hm & below)] = make_int2(a2, b - a2);
+      if (has) D.segs[base + ns_ + __popc(m & below)] = make_int2(a - pl, b - a);
+      if (hhas) D.hsegs[hbase + nh_ + __popc(hm & below)] = make_int2(a2 - pl, b - a2);
     }
     ns_ += __popc(m);
     nh_ += __popc(hm);
@@ -457,58 +539,70 @@ __global__ void group_segments_kernel(GroupGeom gg, const int4 *__restrict__ gre
   }
   if (lane == 0) {
     if (FILL) {
-      groups[g] = make_int4(p0, p1 - p0, base, base + ns_);
-      hgroups[g] = make_int4(p0, p1 - p0, hbase, hbase + nh_);
+      ug[slot] = make_int4(p0 - pl, p1 - p0, base, base + ns_);
+      uh[slot] = make_int4(p0 - pl, p1 - p0, hbase, hbase + nh_);
     } else {
-      nseg[g] = ns_;
-      nhseg[g] = nh_;
+      nseg[slot] = ns_;
+      nhseg[slot] = nh_;
       // sources staged by the group (at most n: its segments are disjoint)
-      work[g] = (unsigned)min(wk, 0xffffffffull);
-      hwork[g] = (unsigned)min(hwk, 0xffffffffull);
-      cand = wk * (unsigned long long)(p1 - p0);
-      hcand = hwk * (unsigned long long)(p1 - p0);
-      atomicAdd(&st->cand, cand);
-      atomicAdd(&st->hcand, hcand);
+      work[slot] = (unsigned)min(wk, 0xffffffffull);
+      hwork[slot] = (unsigned)min(hwk, 0xffffffffull);
+      atomicAdd(&st[r].cand, wk * (unsigned long long)(p1 - p0));
+      atomicAdd(&st[r].hcand, hwk * (unsigned long long)(p1 - p0));
     }
   }
 }
 
-// final group records and frame origins in work order (the first ngroups
-// entries of the order; the slots past ngroups have no work and sort last)
-__global__ void order_groups_kernel(const int4 *__restrict__ gin, const double4 *__restrict__ cin,
+// Sort key of a group slot: the system, then the work, heaviest first; spare
+// slots of a system's bound last.
+__global__ void work_key_kernel(const SysDesc *__restrict__ d, const long *__restrict__ goffs,
+                                int R, long G, const int *__restrict__ goff,
+                                const unsigned *__restrict__ work, int wbits,
+                                unsigned long long *__restrict__ key, unsigned *__restrict__ iota) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= G) return;
+  const int r = owner(goffs, R, slot);
+  const SysDesc &D = d[r];
+  const unsigned long long mask = (1ull << wbits) - 1ull;
+  const bool real = slot - D.g_off < sys_groups(D, goff);
+  const unsigned long long w = real ? mask - min((unsigned long long)work[slot], mask) : mask;
+  key[slot] = ((unsigned long long)r << wbits) | w;
+  iota[slot] = (unsigned)slot;
+}
+
+// A system's final group records and frame origins, in work order.
+__global__ void order_groups_kernel(const SysDesc *__restrict__ d, const long *__restrict__ goffs,
+                                    int R, long G, const int *__restrict__ goff,
                                     const unsigned *__restrict__ ord,
-                                    const int *__restrict__ ngroups, long bound,
-                                    int4 *__restrict__ gout, double4 *__restrict__ cout) {
+                                    const int4 *__restrict__ gin, const double4 *__restrict__ cin,
+                                    bool half) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= bound || k >= *ngroups) return;
-  gout[k] = gin[ord[k]];
-  cout[k] = cin[ord[k]];
+  if (k >= G) return;
+  const int r = owner(goffs, R, k);
+  const SysDesc &D = d[r];
+  const long dest = k - D.g_off;
+  if (dest >= sys_groups(D, goff)) return;
+  const long s = ord[k];
+  (half ? D.hgroups : D.groups)[dest] = gin[s];
+  (half ? D.hcen : D.gcen)[dest] = cin[s];
 }
 
-// The counts the host needs after set-up, gathered for one copy.
-struct SetupCounts {
-  long long bad;
-  unsigned long long cand, hcand;
-  int ngroups, nnonempty, nsegs, nhsegs;
-};
-__global__ void collect_counts_kernel(const SetupStats *__restrict__ st,
-                                      const int *__restrict__ ngroups,
-                                      const int *__restrict__ nnonempty,
-                                      const int *__restrict__ nsegs,
-                                      const int *__restrict__ nhsegs,
+__global__ void collect_counts_kernel(const SysDesc *__restrict__ d, int R,
+                                      const SysStats *__restrict__ st,
+                                      const int *__restrict__ goff, const int *__restrict__ pos,
+                                      const int *__restrict__ segoff,
+                                      const int *__restrict__ hsegoff,
                                       SetupCounts *__restrict__ out) {
-  out->bad = st->bad;
-  out->cand = st->cand;
-  out->hcand = st->hcand;
-  out->ngroups = *ngroups;
-  out->nnonempty = *nnonempty;
-  out->nsegs = *nsegs;
-  out->nhsegs = *nhsegs;
-}
-
-__global__ void iota_kernel(unsigned *__restrict__ v, long n) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) v[k] = (unsigned)k;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  const SysDesc &D = d[r];
+  out[r].bad = st[r].bad;
+  out[r].cand = st[r].cand;
+  out[r].hcand = st[r].hcand;
+  out[r].ngroups = (int)sys_groups(D, goff);
+  out[r].nnonempty = pos[D.b_off + D.nbt] - pos[D.b_off];
+  out[r].nsegs = segoff[D.g_off + D.ngb] - segoff[D.g_off];
+  out[r].nhsegs = hsegoff[D.g_off + D.ngb] - hsegoff[D.g_off];
 }
 
 int bits_for(unsigned long long v) {  // bits to hold values < v
@@ -519,12 +613,14 @@ int bits_for(unsigned long long v) {  // bits to hold values < v
 
 inline unsigned blocks_for(long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
-// Scratch buffers of the set-up (handle-owned, reused by the next set-up).
+// Scratch buffers of the set-up, kept by the handle that owns a batch (the
+// first) and reused by its next set-up.
 enum Scratch {
-  kPts, kBKey, kBKeyOut, kIota, kBPerm, kCKey, kSKey, kKeyOut,
-  kBCount, kCStart, kSStart, kFlag, kPos, kZs, kCPos, kFCPos, kGCount, kGOff,
-  kGRec, kBLo, kBHi, kCen, kNSeg, kSegOff, kHSegOff, kUGroups, kUHGroups,
-  kWorkOut, kOrd, kStats, kCub, kRKey, kRKeyOut, kBPos, kCounts, kScratchCount
+  kPts, kBKey, kBKeyOut, kIota, kBPerm, kCKey, kSKey, kKeyOut, kCOrder, kSOrder, kBOrder,
+  kCounts3, kBStart, kFlag, kPos, kCStart, kSStart, kZs, kCPos, kFCPos, kGCount, kGOff,
+  kGRec, kBLo, kBHi, kCen, kGroupCounters, kSegOff, kHSegOff, kUGroups, kUHGroups,
+  kWKey, kWKeyOut, kOrd, kGIota, kStats, kSysStats, kDesc, kOffs, kCub, kRKey, kBPos, kCountsDev,
+  kScratchCount
 };
 static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
 
@@ -537,7 +633,7 @@ static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
 
 template <typename P>
 int scratch(npme_handle *h, Scratch i, size_t bytes, P **out) {
-  const int rc = handle_buffer(h, &h->d_su[i], bytes);
+  const int rc = handle_buffer(h, &h->d_su[i], std::max<size_t>(bytes, 16));
   *out = (P *)h->d_su[i];
   return rc;
 }
@@ -548,25 +644,15 @@ int cub_tmp(npme_handle *h, size_t bytes, void **out) {
 }
 
 // stable radix sort of (key, value) pairs on bits [0, end_bit), ascending
-// or descending
 template <typename K>
 int sort_pairs(npme_handle *h, const K *kin, K *kout, const unsigned *vin, unsigned *vout,
-               long n, int end_bit, cudaStream_t s, bool descending = false) {
+               long n, int end_bit, cudaStream_t s) {
   size_t tb = 0;
-  if (descending)
-    SCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kin, kout, vin, vout, (int)n, 0,
-                                                   end_bit, s));
-  else
-    SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit,
-                                        s));
+  SCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
   void *tmp;
   int rc;
   if ((rc = cub_tmp(h, tb, &tmp))) return rc;
-  if (descending)
-    SCK(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, kin, kout, vin, vout, (int)n, 0,
-                                                   end_bit, s));
-  else
-    SCK(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
+  SCK(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, s));
   return NPME_OK;
 }
 
@@ -580,18 +666,18 @@ int exclusive_sum(npme_handle *h, const int *in, int *out, long n, cudaStream_t 
   return NPME_OK;
 }
 
+// Host side of one system: its binning geometry (and the handle's refine2),
+// its sizes and its output buffers.
 template <typename T>
-int bin_points(npme_handle *h) {
+int describe(npme_handle *h, SysDesc &D) {
   const long n = (long)h->n;
-  cudaStream_t s = h->stream;
   const GridGeom &gr = h->grid;
   const double *R = h->box + 3, *L = h->box + 6;
   int rc;
-  SetupStats *st = (SetupStats *)h->d_su[kStats];
-  BinGeom g;
-  for (int d = 0; d < 3; d++) {
-    g.N[d] = (double)gr.N[d], g.L[d] = L[d], g.R[d] = R[d];
-    g.Nl[d] = gr.N[d], g.H[d] = gr.H[d], g.nb[d] = gr.nb[d];
+  BinGeom &g = D.g;
+  for (int a = 0; a < 3; a++) {
+    g.N[a] = (double)gr.N[a], g.L[a] = L[a], g.R[a] = R[a];
+    g.Nl[a] = gr.N[a], g.H[a] = gr.H[a], g.nb[a] = gr.nb[a];
   }
   g.P = gr.order;
   g.TL = kBrick + gr.order - 1;
@@ -600,234 +686,81 @@ int bin_points(npme_handle *h) {
   // (degenerate axes are given a nominal thickness of Rdir / 4)
   const double Rd = h->p.Rdir;
   double vol = 1.0;
-  for (int d = 0; d < 3; d++) vol *= std::max(h->bmax[d] - h->bmin[d], 0.25 * Rd);
+  for (int a = 0; a < 3; a++) vol *= std::max(h->bmax[a] - h->bmin[a], 0.25 * Rd);
   double e = std::cbrt(32.0 * vol / (double)n);
   e = std::max(e, 1e-3 * Rd);
-  for (int d = 0; d < 2; d++) {
-    const double ext = h->bmax[d] - h->bmin[d];
-    g.nc[d] = std::max(1, std::min((int)std::ceil(ext / e), 1 << 14));
-    g.edge[d] = std::max(ext / g.nc[d], 1e-12);
-    g.ns[d] = g.nc[d] * kSourceSplit;
-    g.sedge[d] = g.edge[d] / kSourceSplit;
-    g.mn[d] = h->bmin[d];
+  for (int a = 0; a < 2; a++) {
+    const double ext = h->bmax[a] - h->bmin[a];
+    g.nc[a] = std::max(1, std::min((int)std::ceil(ext / e), 1 << 14));
+    g.edge[a] = std::max(ext / g.nc[a], 1e-12);
+    g.ns[a] = g.nc[a] * kSourceSplit;
+    g.sedge[a] = g.edge[a] / kSourceSplit;
+    g.mn[a] = h->bmin[a];
   }
   {
     const double H = h->bmax[2] - h->bmin[2];
-    g.zbits = std::max(8, std::min(20, (int)std::ceil(std::log2(std::max(1.0, 1024.0 * H / e)))));
+    g.zbits = std::max(8, std::min(kZField,
+                                   (int)std::ceil(std::log2(std::max(1.0, 1024.0 * H / e)))));
     g.zmin = h->bmin[2];
     g.zscale = (double)((1u << g.zbits) - 1u) / std::max(H, 1e-300);
   }
+  GroupGeom &gg = D.gg;
+  gg.R = Rd, gg.R2 = Rd * Rd;
+  for (int a = 0; a < 2; a++) gg.mn[a] = g.mn[a], gg.sedge[a] = g.sedge[a], gg.ns[a] = g.ns[a];
+  gg.nc1 = g.nc[1];
+  gg.zmin = g.zmin, gg.zscale = g.zscale, gg.zbits = g.zbits;
   // heads of offsets up to ~the group half-diagonal carry ~6e-8 e absolute
   // error; below r = e/4 the relative error would exceed ~1e-6, so refine
   h->refine2 = (0.25 * e) * (0.25 * e);
-  const long nbt = gr.nb[0] * gr.nb[1] * gr.nb[2];
-  const long ncol = (long)g.nc[0] * g.nc[1], nscol = (long)g.ns[0] * g.ns[1];
-  h->n_bricks = nbt;
-
-  BrickPoint<T> *pts;
-  unsigned *bkey, *bkey_out, *iota, *bperm;
-  unsigned long long *ckey, *skey, *key_out;
-  int *bcount, *ccount, *scount, *cstart, *sstart, *flag, *pos;
-  if ((rc = scratch(h, kPts, sizeof(BrickPoint<T>) * n, &pts)) ||
-      (rc = scratch(h, kBKey, sizeof(unsigned) * n, &bkey)) ||
-      (rc = scratch(h, kBKeyOut, sizeof(unsigned) * n, &bkey_out)) ||
-      (rc = scratch(h, kIota, sizeof(unsigned) * n, &iota)) ||
-      (rc = scratch(h, kBPerm, sizeof(unsigned) * n, &bperm)) ||
-      (rc = scratch(h, kCKey, sizeof(unsigned long long) * n, &ckey)) ||
-      (rc = scratch(h, kSKey, sizeof(unsigned long long) * n, &skey)) ||
-      (rc = scratch(h, kKeyOut, sizeof(unsigned long long) * n, &key_out)) ||
-      (rc = scratch(h, kBCount, sizeof(int) * (nbt + ncol + nscol + 3), &bcount)) ||
-      (rc = scratch(h, kCStart, sizeof(int) * (ncol + 1), &cstart)) ||
-      (rc = scratch(h, kSStart, sizeof(int) * (nscol + 1), &sstart)) ||
-      (rc = scratch(h, kFlag, sizeof(int) * (nbt + 1), &flag)) ||
-      (rc = scratch(h, kPos, sizeof(int) * (nbt + 1), &pos)))
-    return rc;
-  const int C = h->complex_kernel ? 2 : 1;
-  if ((rc = handle_buffer(h, &h->d_bpts, sizeof(BrickPoint<T>) * n)) ||
-      (rc = handle_buffer(h, (void **)&h->d_brick_start, sizeof(int) * (nbt + 1))) ||
-      (rc = handle_buffer(h, (void **)&h->d_cperm, sizeof(uint32_t) * n)) ||
-      (rc = handle_buffer(h, (void **)&h->d_sperm, sizeof(uint32_t) * n)) ||
-      (rc = handle_buffer(h, (void **)&h->d_gpos, sizeof(double4) * n)) ||
-      (rc = handle_buffer(h, (void **)&h->d_spos, sizeof(double4) * n)) ||
-      (rc = handle_buffer(h, &h->d_qb, sizeof(T) * C * n)) ||
-      (rc = handle_buffer(h, &h->d_qc, sizeof(T) * C * n)) ||
-      (rc = handle_buffer(h, (void **)&h->d_q_in, sizeof(double) * C * n)) ||
-      (rc = handle_buffer(h, (void **)&h->d_V, sizeof(double) * 4 * C * n)))
-    return rc;
-
-  // brick, coarse-column and fine-column counts in one block, one clear
-  ccount = bcount + nbt + 1;
-  scount = ccount + ncol + 1;
-  SCK(cudaMemsetAsync(bcount, 0, sizeof(int) * (nbt + ncol + nscol + 3), s));
-  bin_kernel<T><<<blocks_for(n), 256, 0, s>>>(h->d_coord, n, g, pts, bkey, ckey, skey, iota,
-                                              bcount, ccount, scount, st);
-  SCK(cudaGetLastError());
-
-  // --- brick order: by brick, inside a brick in rounds over the banks ---
-  // (brick, bank, index) first; (brick, rank inside the bank, bank) below
-  if ((rc = sort_pairs(h, bkey, bkey_out, iota, bperm, n, 5 + bits_for(nbt), s)) ||
-      (rc = handle_buffer(h, (void **)&h->d_bperm, sizeof(uint32_t) * n)))
-    return rc;
-  if ((rc = exclusive_sum(h, bcount, h->d_brick_start, nbt + 1, s))) return rc;
-  nonempty_flags_kernel<<<blocks_for(nbt + 1), 256, 0, s>>>(bcount, nbt, flag);
-  if ((rc = exclusive_sum(h, flag, pos, nbt + 1, s))) return rc;
-
-  // --- direct-sum orders: (column, quantised z, index) for targets and
-  // sources, one radix sort each ---
-  if ((rc = sort_pairs(h, ckey, key_out, iota, h->d_cperm, n, bits_for(ncol) + g.zbits, s)) ||
-      (rc = sort_pairs(h, skey, key_out, iota, h->d_sperm, n, bits_for(nscol) + g.zbits, s)))
-    return rc;
-  if ((rc = exclusive_sum(h, ccount, cstart, ncol + 1, s))) return rc;
-  if ((rc = exclusive_sum(h, scount, sstart, nscol + 1, s))) return rc;
-  unsigned *zs;  // quantised z of the sources, in source order
-  unsigned *cpos, *fcpos;
-  int *gcount, *goff;
-  if ((rc = scratch(h, kZs, sizeof(unsigned) * n, &zs)) ||
-      (rc = scratch(h, kCPos, sizeof(unsigned) * n, &cpos)) ||
-      (rc = scratch(h, kFCPos, sizeof(unsigned) * n, &fcpos)) ||
-      (rc = scratch(h, kGCount, sizeof(int) * (ncol + 1), &gcount)) ||
-      (rc = scratch(h, kGOff, sizeof(int) * (ncol + 1), &goff)))
-    return rc;
-  source_z_kernel<<<blocks_for(n), 256, 0, s>>>(key_out, h->d_cperm, n, g.zbits, zs, cpos);
-  gather_u32_kernel<<<blocks_for(n), 256, 0, s>>>(cpos, h->d_sperm, n, fcpos);
-  groups_per_column_kernel<<<blocks_for(ncol + 1), 256, 0, s>>>(ccount, ncol, gcount);
-  if ((rc = exclusive_sum(h, gcount, goff, ncol + 1, s))) return rc;
-  SCK(cudaGetLastError());
-
-  // No read-back here: the group and segment arrays are sized from upper
-  // bounds and the kernels read the actual counts on the device; the host
-  // reads every count once, when the set-up has completed (finish_setup).
+  D.n = n;
+  D.nbt = gr.nb[0] * gr.nb[1] * gr.nb[2];
+  D.ncol = (long)g.nc[0] * g.nc[1];
+  D.nscol = (long)g.ns[0] * g.ns[1];
+  h->n_bricks = D.nbt;
+  // Upper bounds (the kernels read the actual counts on the device; the
+  // host reads them once the set-up has completed):
   //   groups   <= n / 32 + non-empty columns <= n / 32 + min(n, ncol)
   //   segments <= groups x the fine columns of a group's window (a group lies
   //               in one coarse column, so its window spans at most
   //               (edge + 2 Rdir) / sedge + 4 fine columns per axis)
   //   non-empty bricks <= min(n, nbt)
-  const long ngb = n / 32 + std::min(n, ncol) + 1;
+  D.ngb = n / 32 + std::min(n, D.ncol) + 1;
   long wmax = 1;
-  for (int d = 0; d < 2; d++)
-    wmax *= std::min<long>(g.ns[d], (long)std::floor((g.edge[d] + 2.0 * Rd) / g.sedge[d]) + 4);
-  const long nsb = ngb * wmax;
+  for (int a = 0; a < 2; a++)
+    wmax *= std::min<long>(g.ns[a], (long)std::floor((g.edge[a] + 2.0 * Rd) / g.sedge[a]) + 4);
+  const long nsb = D.ngb * wmax;
   if (nsb >= (1L << 31))  // int offsets in the group records
     return record_error(h, NPME_EINVAL, "too many direct-sum source segments (2^31)");
-  if ((rc = handle_buffer(h, (void **)&h->d_brick_list,
-                          sizeof(int) * std::max<long>(1, std::min(n, nbt)))))
-    return rc;
-  brick_list_kernel<<<blocks_for(nbt), 256, 0, s>>>(bcount, pos, nbt, h->d_brick_list);
-
-  // brick order in rounds over the banks: the rank inside a bank is below n
-  {
-    const int rbits = bits_for((unsigned long long)n);
-    const int kbits = bits_for(nbt) + rbits + 5;
-    unsigned *bperm2 = h->d_bperm;
-    if (kbits <= 32) {
-      unsigned *rkey, *rkey_out;
-      if ((rc = scratch(h, kRKey, sizeof(unsigned) * n, &rkey)) ||
-          (rc = scratch(h, kRKeyOut, sizeof(unsigned) * n, &rkey_out)))
-        return rc;
-      round_key_kernel<unsigned><<<blocks_for(n), 256, 0, s>>>(bkey_out, n, rbits, rkey);
-      if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, kbits, s))) return rc;
-    } else {
-      unsigned long long *rkey, *rkey_out;
-      if ((rc = scratch(h, kRKey, sizeof(unsigned long long) * n, &rkey)) ||
-          (rc = scratch(h, kRKeyOut, sizeof(unsigned long long) * n, &rkey_out)))
-        return rc;
-      round_key_kernel<unsigned long long>
-          <<<blocks_for(n), 256, 0, s>>>(bkey_out, n, rbits, rkey);
-      if ((rc = sort_pairs(h, rkey, rkey_out, bperm, bperm2, n, kbits, s))) return rc;
-    }
-    gather_bpts_kernel<T><<<blocks_for(n), 256, 0, s>>>(pts, bperm2, n,
-                                                        (BrickPoint<T> *)h->d_bpts);
-  }
-  unsigned *bpos;
-  if ((rc = scratch(h, kBPos, sizeof(unsigned) * n, &bpos))) return rc;
-  brick_position_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_bperm, n, bpos);
-  gather_positions_kernel<<<blocks_for(n), 256, 0, s>>>(h->d_coord, h->d_cperm, h->d_sperm, bpos,
-                                                        n, h->d_gpos, h->d_spos);
-
-  // --- warp groups and their source segments ---
-  const int *ngp = goff + ncol;  // the actual group count, on the device
-  int4 *grec;
-  double4 *blo, *bhi, *cen;
-  int *nseg, *nhseg, *segoff, *hsegoff;
-  unsigned *work, *hwork, *work_out, *ord;
-  int4 *ug, *uh;
-  if ((rc = scratch(h, kGRec, sizeof(int4) * ngb, &grec)) ||
-      (rc = scratch(h, kBLo, sizeof(double4) * ngb, &blo)) ||
-      (rc = scratch(h, kBHi, sizeof(double4) * ngb, &bhi)) ||
-      (rc = scratch(h, kCen, sizeof(double4) * ngb, &cen)) ||
-      (rc = scratch(h, kNSeg, sizeof(int) * 4 * (ngb + 1), &nseg)) ||
-      (rc = scratch(h, kSegOff, sizeof(int) * (ngb + 1), &segoff)) ||
-      (rc = scratch(h, kHSegOff, sizeof(int) * (ngb + 1), &hsegoff)) ||
-
-      (rc = scratch(h, kWorkOut, sizeof(unsigned) * ngb, &work_out)) ||
-      (rc = scratch(h, kOrd, sizeof(unsigned) * ngb, &ord)) ||
-      (rc = scratch(h, kUGroups, sizeof(int4) * ngb, &ug)) ||
-      (rc = scratch(h, kUHGroups, sizeof(int4) * ngb, &uh)) ||
+  const int C = h->complex_kernel ? 2 : 1;
+  if ((rc = handle_buffer(h, &h->d_bpts, sizeof(BrickPoint<T>) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_brick_start, sizeof(int) * (D.nbt + 1))) ||
+      (rc = handle_buffer(h, (void **)&h->d_brick_list,
+                          sizeof(int) * std::max<long>(1, std::min(n, D.nbt)))) ||
+      (rc = handle_buffer(h, (void **)&h->d_cperm, sizeof(uint32_t) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_sperm, sizeof(uint32_t) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_bperm, sizeof(uint32_t) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_gpos, sizeof(double4) * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_spos, sizeof(double4) * n)) ||
       (rc = handle_buffer(h, (void **)&h->d_segs, sizeof(int2) * nsb)) ||
       (rc = handle_buffer(h, (void **)&h->d_hsegs, sizeof(int2) * nsb)) ||
-      (rc = handle_buffer(h, (void **)&h->d_groups, sizeof(int4) * ngb)) ||
-      (rc = handle_buffer(h, (void **)&h->d_gcen, sizeof(double4) * ngb)) ||
-      (rc = handle_buffer(h, (void **)&h->d_hgroups, sizeof(int4) * ngb)) ||
-      (rc = handle_buffer(h, (void **)&h->d_hcen, sizeof(double4) * ngb)))
+      (rc = handle_buffer(h, (void **)&h->d_groups, sizeof(int4) * D.ngb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_gcen, sizeof(double4) * D.ngb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_hgroups, sizeof(int4) * D.ngb)) ||
+      (rc = handle_buffer(h, (void **)&h->d_hcen, sizeof(double4) * D.ngb)) ||
+      (rc = handle_buffer(h, &h->d_qb, sizeof(T) * C * n)) ||
+      (rc = handle_buffer(h, &h->d_qc, sizeof(T) * C * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_q_in, sizeof(double) * C * n)) ||
+      (rc = handle_buffer(h, (void **)&h->d_V, sizeof(double) * 4 * C * n)))
     return rc;
-  // Heaviest groups first, so that the last wave of a direct-sum launch holds
-  // the light ones; when every group fits in one wave (4 groups per CTA,
-  // about 4 CTAs per SM) the order does not matter and the lists are
-  // written in column order directly.
-  const bool order_by_work = ngb > kOneWaveGroups;
-  if (!order_by_work) cen = h->d_gcen, ug = h->d_groups, uh = h->d_hgroups;
-  group_records_kernel<<<blocks_for(ncol), 256, 0, s>>>(cstart, goff, ncol, grec);
-  group_box_kernel<<<blocks_for(32 * ngb), 256, 0, s>>>(h->d_gpos, grec, ngp, blo, bhi, cen);
-  GroupGeom gg;
-  gg.R = Rd, gg.R2 = Rd * Rd;
-  for (int d = 0; d < 2; d++) gg.mn[d] = g.mn[d], gg.sedge[d] = g.sedge[d], gg.ns[d] = g.ns[d];
-  gg.nc1 = g.nc[1];
-  gg.zmin = g.zmin, gg.zscale = g.zscale, gg.zbits = g.zbits;
-  // segment counts and work of both lists in one block, one clear (slots
-  // past the actual groups: no segments, no work, so they sort last)
-  nhseg = nseg + (ngb + 1);
-  work = (unsigned *)(nhseg + (ngb + 1));
-  hwork = work + (ngb + 1);
-  SCK(cudaMemsetAsync(nseg, 0, sizeof(int) * 4 * (ngb + 1), s));
-  group_segments_kernel<false><<<blocks_for(32 * ngb), 256, 0, s>>>(
-      gg, grec, ngp, blo, bhi, sstart, zs, fcpos, nseg, nhseg, work, hwork, nullptr, nullptr,
-      nullptr, nullptr, nullptr, nullptr, st);
-  if ((rc = exclusive_sum(h, nseg, segoff, ngb + 1, s))) return rc;
-  if ((rc = exclusive_sum(h, nhseg, hsegoff, ngb + 1, s))) return rc;
-  group_segments_kernel<true><<<blocks_for(32 * ngb), 256, 0, s>>>(
-      gg, grec, ngp, blo, bhi, sstart, zs, fcpos, nullptr, nullptr, nullptr, nullptr, segoff,
-      hsegoff, h->d_segs, h->d_hsegs, ug, uh, st);
-  if (order_by_work) {  // each list by its own work; ties keep the column order
-    iota_kernel<<<blocks_for(ngb), 256, 0, s>>>(iota, ngb);
-    const int wbits = bits_for((unsigned long long)n + 1);
-    if ((rc = sort_pairs(h, work, work_out, iota, ord, ngb, wbits, s, true))) return rc;
-    order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(ug, cen, ord, ngp, ngb, h->d_groups,
-                                                        h->d_gcen);
-    if ((rc = sort_pairs(h, hwork, work_out, iota, ord, ngb, wbits, s, true))) return rc;
-    order_groups_kernel<<<blocks_for(ngb), 256, 0, s>>>(uh, cen, ord, ngp, ngb, h->d_hgroups,
-                                                        h->d_hcen);
-  } else {
-    SCK(cudaMemcpyAsync(h->d_hcen, h->d_gcen, sizeof(double4) * ngb, cudaMemcpyDeviceToDevice, s));
-  }
-  // the counts, for the host to read when the set-up has completed
-  SetupCounts *dc;
-  if ((rc = scratch(h, kCounts, sizeof(SetupCounts), &dc))) return rc;
-  collect_counts_kernel<<<1, 1, 0, s>>>(st, ngp, pos + nbt, segoff + ngb, hsegoff + ngb, dc);
-  SCK(cudaMemcpyAsync(h->h_counts, dc, sizeof(SetupCounts), cudaMemcpyDeviceToHost, s));
-  SCK(cudaGetLastError());
-  h->d_dperm = h->d_sperm;  // direct-sum charges are gathered into the source order
-
   // source-side sums of the pair-once walk start (and are kept) at zero
   if (h->fp32) {
-    const size_t nv = (size_t)C * n;  // float4 per source (two if complex)
-    if ((rc = handle_buffer(h, (void **)&h->d_vsrc, sizeof(float4) * nv))) return rc;
-    SCK(cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * nv, s));
+    if ((rc = handle_buffer(h, (void **)&h->d_vsrc, sizeof(float4) * C * n))) return rc;
+    cudaMemsetAsync(h->d_vsrc, 0, sizeof(float4) * C * n, h->stream);
   } else {
     if ((rc = handle_buffer(h, (void **)&h->d_vsrc64, sizeof(double) * 4 * n))) return rc;
-    SCK(cudaMemsetAsync(h->d_vsrc64, 0, sizeof(double) * 4 * n, s));
+    cudaMemsetAsync(h->d_vsrc64, 0, sizeof(double) * 4 * n, h->stream);
   }
-
-  // --- grids ---
+  // grids
   const long *N = gr.N;
   const size_t Ntot = (size_t)N[0] * N[1] * N[2];
   const size_t Mtot = (size_t)(N[0] / 2 + 1) * (N[1] / 2 + 1) * (N[2] / 2 + 1);
@@ -841,6 +774,195 @@ int bin_points(npme_handle *h) {
         (rc = handle_buffer(h, &h->d_G, sizeof(T) * Mtot)))
       return rc;
   }
+  D.coord = h->d_coord;
+  D.bpts = h->d_bpts;
+  D.brick_start = h->d_brick_start;
+  D.brick_list = h->d_brick_list;
+  D.cperm = h->d_cperm, D.sperm = h->d_sperm, D.bperm = h->d_bperm;
+  D.gpos = h->d_gpos, D.spos = h->d_spos;
+  D.segs = h->d_segs, D.hsegs = h->d_hsegs;
+  D.groups = h->d_groups, D.hgroups = h->d_hgroups;
+  D.gcen = h->d_gcen, D.hcen = h->d_hcen;
+  h->d_dperm = h->d_sperm;  // direct-sum charges are gathered into the source order
+  return NPME_OK;
+}
+
+// Brick order, direct-sum orders, warp groups and segment lists of R systems
+// of one precision in one pass on stream s (h0 = hs[0] owns the scratch).
+// Enqueued without waiting; the counts arrive in h0->h_counts with the
+// caller's synchronisation.
+template <typename T>
+int geometry_batch(npme_handle **hs, int R, cudaStream_t s) {
+  npme_handle *h = hs[0];
+  int rc;
+  std::vector<SysDesc> ds(R);
+  long P = 0, B = 0, C = 0, S = 0, G = 0, nmax = 1, nbtmax = 1, ncolmax = 1, nscolmax = 1;
+  for (int r = 0; r < R; r++) {
+    if ((rc = describe<T>(hs[r], ds[r]))) {
+      if (hs[r] != h) h->err = hs[r]->err;
+      return rc;
+    }
+    SysDesc &D = ds[r];
+    D.p_off = P, D.b_off = B, D.c_off = C, D.s_off = S, D.g_off = G;
+    P += D.n, B += D.nbt + 1, C += D.ncol + 1, S += D.nscol + 1, G += D.ngb;
+    nmax = std::max(nmax, D.n), nbtmax = std::max(nbtmax, D.nbt);
+    ncolmax = std::max(ncolmax, D.ncol), nscolmax = std::max(nscolmax, D.nscol);
+    // the system's coordinates and buffers (on its own stream) come first
+    if (hs[r]->stream != s) {
+      SCK(cudaEventRecord(hs[r]->ev_fork, hs[r]->stream));
+      SCK(cudaStreamWaitEvent(s, hs[r]->ev_fork, 0));
+    }
+  }
+  if (P >= (1L << 31) || B >= (1L << 31) || G >= (1L << 31))
+    return record_error(h, NPME_EINVAL, "set-up batch too large for 32-bit indices");
+  const int rbits = bits_for((unsigned long long)R);
+  const int bbits = bits_for(nbtmax), cbits = bits_for(ncolmax), sbits = bits_for(nscolmax);
+  const int rankbits = bits_for((unsigned long long)nmax);
+  const int wbits = bits_for((unsigned long long)nmax + 1) + 1;
+  if (rbits + bbits + rankbits + 5 > 64 || rbits + sbits + kZField > 64)
+    return record_error(h, NPME_EINVAL, "set-up batch keys exceed 64 bits");
+
+  // descriptors and the index-space starts (points, bricks, columns, fine
+  // columns, groups), R each
+  SysDesc *dd;
+  long *offs;
+  if ((rc = scratch(h, kDesc, sizeof(SysDesc) * R, &dd)) ||
+      (rc = scratch(h, kOffs, sizeof(long) * 5 * R, &offs)))
+    return rc;
+  std::vector<long> ho(5 * R);
+  for (int r = 0; r < R; r++) {
+    ho[r] = ds[r].p_off, ho[R + r] = ds[r].b_off, ho[2 * R + r] = ds[r].c_off;
+    ho[3 * R + r] = ds[r].s_off, ho[4 * R + r] = ds[r].g_off;
+  }
+  SCK(cudaMemcpyAsync(dd, ds.data(), sizeof(SysDesc) * R, cudaMemcpyHostToDevice, s));
+  SCK(cudaMemcpyAsync(offs, ho.data(), sizeof(long) * 5 * R, cudaMemcpyHostToDevice, s));
+  const long *poff = offs, *boff = offs + R, *coff = offs + 2 * R, *goffs = offs + 4 * R;
+
+  BrickPoint<T> *pts;
+  unsigned long long *bkey, *bkey_out, *ckey, *skey, *key_out, *rkey;
+  unsigned *iota, *border, *corder, *sorder, *border2, *bpos, *zs, *cpos, *fcpos;
+  int *counts, *bstart, *flag, *pos, *cstart, *sstart, *gcount, *goff;
+  SysStats *st;
+  if ((rc = scratch(h, kPts, sizeof(BrickPoint<T>) * P, &pts)) ||
+      (rc = scratch(h, kBKey, sizeof(unsigned long long) * P, &bkey)) ||
+      (rc = scratch(h, kBKeyOut, sizeof(unsigned long long) * P, &bkey_out)) ||
+      (rc = scratch(h, kCKey, sizeof(unsigned long long) * P, &ckey)) ||
+      (rc = scratch(h, kSKey, sizeof(unsigned long long) * P, &skey)) ||
+      (rc = scratch(h, kKeyOut, sizeof(unsigned long long) * P, &key_out)) ||
+      (rc = scratch(h, kRKey, sizeof(unsigned long long) * P, &rkey)) ||
+      (rc = scratch(h, kIota, sizeof(unsigned) * P, &iota)) ||
+      (rc = scratch(h, kBPerm, sizeof(unsigned) * P, &border)) ||
+      (rc = scratch(h, kBOrder, sizeof(unsigned) * P, &border2)) ||
+      (rc = scratch(h, kCOrder, sizeof(unsigned) * P, &corder)) ||
+      (rc = scratch(h, kSOrder, sizeof(unsigned) * P, &sorder)) ||
+      (rc = scratch(h, kBPos, sizeof(unsigned) * P, &bpos)) ||
+      (rc = scratch(h, kZs, sizeof(unsigned) * P, &zs)) ||
+      (rc = scratch(h, kCPos, sizeof(unsigned) * P, &cpos)) ||
+      (rc = scratch(h, kFCPos, sizeof(unsigned) * P, &fcpos)) ||
+      (rc = scratch(h, kCounts3, sizeof(int) * (B + C + S), &counts)) ||
+      (rc = scratch(h, kBStart, sizeof(int) * B, &bstart)) ||
+      (rc = scratch(h, kFlag, sizeof(int) * B, &flag)) ||
+      (rc = scratch(h, kPos, sizeof(int) * B, &pos)) ||
+      (rc = scratch(h, kCStart, sizeof(int) * C, &cstart)) ||
+      (rc = scratch(h, kSStart, sizeof(int) * S, &sstart)) ||
+      (rc = scratch(h, kGCount, sizeof(int) * C, &gcount)) ||
+      (rc = scratch(h, kGOff, sizeof(int) * C, &goff)) ||
+      (rc = scratch(h, kSysStats, sizeof(SysStats) * R, &st)))
+    return rc;
+  int *bcount = counts, *ccount = counts + B, *scount = counts + B + C;
+
+  // --- binning: records, keys and counts of every point ---
+  SCK(cudaMemsetAsync(counts, 0, sizeof(int) * (B + C + S), s));
+  init_sys_stats_kernel<<<blocks_for(R, 64), 64, 0, s>>>(dd, R, st);
+  bin_kernel<T><<<blocks_for(P), 256, 0, s>>>(dd, poff, R, P, bbits, cbits, sbits, pts, bkey,
+                                              ckey, skey, iota, bcount, ccount, scount, st);
+  SCK(cudaGetLastError());
+
+  // --- brick order: by (system, brick), inside a brick in rounds over the
+  // banks: (system, brick, bank, index) first, then (system, brick, rank
+  // inside the bank, bank) ---
+  if ((rc = sort_pairs(h, bkey, bkey_out, iota, border, P, rbits + bbits + 5, s))) return rc;
+  round_key_kernel<<<blocks_for(P), 256, 0, s>>>(bkey_out, P, rankbits, rkey);
+  if ((rc = sort_pairs(h, rkey, key_out, border, border2, P, rbits + bbits + rankbits + 5, s)))
+    return rc;
+  place_bricks_kernel<T><<<blocks_for(P), 256, 0, s>>>(dd, poff, R, P, border2, pts, bpos);
+  if ((rc = exclusive_sum(h, bcount, bstart, B, s))) return rc;
+  nonempty_flags_kernel<<<blocks_for(B), 256, 0, s>>>(bcount, B, flag);
+  if ((rc = exclusive_sum(h, flag, pos, B, s))) return rc;
+  bricks_kernel<<<blocks_for(B), 256, 0, s>>>(dd, boff, R, B, bcount, bstart, pos);
+
+  // --- direct-sum orders: (system, column, quantised z, index) for targets
+  // and sources, one radix sort each ---
+  if ((rc = sort_pairs(h, ckey, key_out, iota, corder, P, rbits + cbits + kZField, s)) ||
+      (rc = sort_pairs(h, skey, key_out, iota, sorder, P, rbits + sbits + kZField, s)))
+    return rc;
+  place_orders_kernel<<<blocks_for(P), 256, 0, s>>>(dd, poff, R, P, corder, sorder, key_out, bpos,
+                                                    zs, cpos);
+  gather_u32_kernel<<<blocks_for(P), 256, 0, s>>>(cpos, sorder, P, fcpos);
+  if ((rc = exclusive_sum(h, ccount, cstart, C, s))) return rc;
+  if ((rc = exclusive_sum(h, scount, sstart, S, s))) return rc;
+  groups_per_column_kernel<<<blocks_for(C), 256, 0, s>>>(ccount, C, gcount);
+  if ((rc = exclusive_sum(h, gcount, goff, C, s))) return rc;
+  SCK(cudaGetLastError());
+
+  // --- warp groups and their source segments ---
+  int4 *grec, *ug, *uh;
+  double4 *blo, *bhi, *cen;
+  int *nseg, *segoff, *hsegoff;
+  unsigned long long *wkey, *wkey_out;
+  unsigned *ord, *giota;
+  if ((rc = scratch(h, kGRec, sizeof(int4) * G, &grec)) ||
+      (rc = scratch(h, kBLo, sizeof(double4) * G, &blo)) ||
+      (rc = scratch(h, kBHi, sizeof(double4) * G, &bhi)) ||
+      (rc = scratch(h, kCen, sizeof(double4) * G, &cen)) ||
+      (rc = scratch(h, kGroupCounters, sizeof(int) * 4 * (G + 1), &nseg)) ||
+      (rc = scratch(h, kSegOff, sizeof(int) * (G + 1), &segoff)) ||
+      (rc = scratch(h, kHSegOff, sizeof(int) * (G + 1), &hsegoff)) ||
+      (rc = scratch(h, kUGroups, sizeof(int4) * G, &ug)) ||
+      (rc = scratch(h, kUHGroups, sizeof(int4) * G, &uh)) ||
+      (rc = scratch(h, kWKey, sizeof(unsigned long long) * G, &wkey)) ||
+      (rc = scratch(h, kWKeyOut, sizeof(unsigned long long) * G, &wkey_out)) ||
+      (rc = scratch(h, kOrd, sizeof(unsigned) * G, &ord)) ||
+      (rc = scratch(h, kGIota, sizeof(unsigned) * G, &giota)))
+    return rc;
+  // segment counts and work of both lists in one block, one clear (spare
+  // slots of the bounds: no segments, no work)
+  int *nhseg = nseg + (G + 1);
+  unsigned *work = (unsigned *)(nhseg + (G + 1)), *hwork = work + (G + 1);
+  SCK(cudaMemsetAsync(nseg, 0, sizeof(int) * 4 * (G + 1), s));
+  group_records_kernel<<<blocks_for(C), 256, 0, s>>>(dd, coff, R, C, cstart, goff, grec);
+  group_box_kernel<<<blocks_for(32 * G), 256, 0, s>>>(dd, goffs, R, G, goff, grec, blo, bhi, cen);
+  group_segments_kernel<false><<<blocks_for(32 * G), 256, 0, s>>>(
+      dd, goffs, R, G, goff, grec, blo, bhi, sstart, zs, fcpos, nseg, nhseg, work, hwork, nullptr,
+      nullptr, nullptr, nullptr, st);
+  if ((rc = exclusive_sum(h, nseg, segoff, G + 1, s))) return rc;
+  if ((rc = exclusive_sum(h, nhseg, hsegoff, G + 1, s))) return rc;
+  group_segments_kernel<true><<<blocks_for(32 * G), 256, 0, s>>>(
+      dd, goffs, R, G, goff, grec, blo, bhi, sstart, zs, fcpos, nullptr, nullptr, nullptr,
+      nullptr, segoff, hsegoff, ug, uh, st);
+  // heaviest groups first, so that the last wave of a direct-sum launch
+  // holds the light ones (each list by its own work; ties keep the column
+  // order)
+  for (int half = 0; half < 2; half++) {
+    work_key_kernel<<<blocks_for(G), 256, 0, s>>>(dd, goffs, R, G, goff, half ? hwork : work,
+                                                  wbits, wkey, giota);
+    if ((rc = sort_pairs(h, wkey, wkey_out, giota, ord, G, rbits + wbits, s))) return rc;
+    order_groups_kernel<<<blocks_for(G), 256, 0, s>>>(dd, goffs, R, G, goff, ord,
+                                                      half ? uh : ug, cen, half != 0);
+  }
+  // the counts, for the host to read when the set-up has completed
+  SetupCounts *dc;
+  if ((rc = scratch(h, kCountsDev, sizeof(SetupCounts) * R, &dc))) return rc;
+  if (h->counts_cap < R) {
+    if (h->h_counts) cudaFreeHost(h->h_counts);
+    h->h_counts = nullptr, h->counts_cap = 0;
+    SCK(cudaHostAlloc(&h->h_counts, sizeof(SetupCounts) * R, cudaHostAllocDefault));
+    h->counts_cap = R;
+  }
+  collect_counts_kernel<<<blocks_for(R, 64), 64, 0, s>>>(dd, R, st, goff, pos, segoff, hsegoff,
+                                                         dc);
+  SCK(cudaMemcpyAsync(h->h_counts, dc, sizeof(SetupCounts) * R, cudaMemcpyDeviceToHost, s));
+  SCK(cudaGetLastError());
   return NPME_OK;
 }
 
@@ -851,25 +973,24 @@ int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3])
   cudaStream_t s = h->stream;
   int rc;
   if ((rc = handle_buffer(h, (void **)&h->d_coord, sizeof(double) * 3 * n))) return rc;
-  SetupStats *st;
-  if ((rc = scratch(h, kStats, sizeof(SetupStats), &st))) return rc;
-  if (!h->h_counts) SCK(cudaHostAlloc(&h->h_counts, sizeof(SetupCounts), cudaHostAllocDefault));
   SCK(cudaMemcpyAsync(h->d_coord, coord, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-  init_stats_kernel<<<1, 1, 0, s>>>(st, n);
   if (n < kHostBoxPoints) {
     // small systems: one host pass costs less than a device reduction and
     // the wait for it
-    for (int d = 0; d < 3; d++) mn[d] = 1e300, mx[d] = -1e300;
+    for (int a = 0; a < 3; a++) mn[a] = 1e300, mx[a] = -1e300;
     for (long i = 0; i < n; i++)
-      for (int d = 0; d < 3; d++) {
-        const double x = coord[3 * i + d];
+      for (int a = 0; a < 3; a++) {
+        const double x = coord[3 * i + a];
         if (!std::isfinite(x)) return record_error(h, NPME_EINVAL, "non-finite coordinate");
-        mn[d] = std::min(mn[d], x);
-        mx[d] = std::max(mx[d], x);
+        mn[a] = std::min(mn[a], x);
+        mx[a] = std::max(mx[a], x);
       }
     SCK(cudaGetLastError());
     return NPME_OK;
   }
+  SetupStats *st;
+  if ((rc = scratch(h, kStats, sizeof(SetupStats), &st))) return rc;
+  init_stats_kernel<<<1, 1, 0, s>>>(st);
   const unsigned blocks = (unsigned)std::min<long>(blocks_for(n), 148 * 8);
   bbox_kernel<<<blocks, 256, 0, s>>>(h->d_coord, n, st);
   SCK(cudaGetLastError());
@@ -877,12 +998,16 @@ int device_bbox(npme_handle *h, const double *coord, double mn[3], double mx[3])
   SCK(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
   SCK(cudaStreamSynchronize(s));
   if (hs.nonfinite) return record_error(h, NPME_EINVAL, "non-finite coordinate");
-  for (int d = 0; d < 3; d++) mn[d] = dkey_inv(hs.mn[d]), mx[d] = dkey_inv(hs.mx[d]);
+  for (int a = 0; a < 3; a++) mn[a] = dkey_inv(hs.mn[a]), mx[a] = dkey_inv(hs.mx[a]);
   return NPME_OK;
 }
 
-int finish_setup(npme_handle *h) {
-  const SetupCounts &c = *static_cast<const SetupCounts *>(h->h_counts);
+int setup_geometry(npme_handle **hs, int R, cudaStream_t s) {
+  return hs[0]->fp32 ? geometry_batch<float>(hs, R, s) : geometry_batch<double>(hs, R, s);
+}
+
+int finish_setup(npme_handle *h, const npme_handle *owner, int r) {
+  const SetupCounts &c = static_cast<const SetupCounts *>(owner->h_counts)[r];
   const long n = (long)h->n;
   if (c.bad < n) {
     // the axis of the first offending point, from its coordinates
@@ -891,12 +1016,12 @@ int finish_setup(npme_handle *h) {
     const GridGeom &gr = h->grid;
     const double *R = h->box + 3, *L = h->box + 6;
     int axis = 0;
-    for (int d = 0; d < 3; d++) {
-      const double w = (double)gr.N[d] / L[d] * (x[d] - R[d]);
+    for (int a = 0; a < 3; a++) {
+      const double w = (double)gr.N[a] / L[a] * (x[a] - R[a]);
       const long ms = w < 0 ? (long)(-w) + 1 : (long)(-w);
-      const long o = ms + gr.N[d] / 4;
-      if (o < 0 || o + gr.order - 1 > gr.H[d] - 1) {
-        axis = d;
+      const long o = ms + gr.N[a] / 4;
+      if (o < 0 || o + gr.order - 1 > gr.H[a] - 1) {
+        axis = a;
         break;
       }
     }
@@ -911,10 +1036,6 @@ int finish_setup(npme_handle *h) {
   h->cand_per_point = (double)c.cand / (double)n;
   h->hcand_per_point = (double)c.hcand / (double)n;
   return NPME_OK;
-}
-
-int device_bin(npme_handle *h) {
-  return h->fp32 ? bin_points<float>(h) : bin_points<double>(h);
 }
 
 }  // namespace npme
