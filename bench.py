@@ -332,7 +332,8 @@ def bounded_serving(local, count=256):
     offline = max((srv.run(reqs, realtime=False) for _ in range(2)),
                   key=lambda st: st["throughput"])
     srv.close()
-    plain = serving.Server(device=local, precision="fp64", max_batch=1, setup_workers=1)
+    plain = serving.Server(device=local, precision="fp64", max_batch=1, setup_workers=1,
+                           setup_batch=1)
     plain.warm_plans(reqs)
     plain_stats = max((plain.run(reqs, realtime=False) for _ in range(2)),
                       key=lambda st: st["throughput"])

@@ -235,6 +235,8 @@ typedef struct {
   int max_batch;       /* systems per batched CalcV (default 64) */
   size_t hbm_budget;   /* device bytes in flight; 0: half the free memory */
   int pool_capacity;   /* idle handles kept for reuse (default 64) */
+  int setup_batch;     /* admitted requests one set-up thread prepares in one
+                          pass of the set-up kernels (default 16) */
 } npme_server_config;
 enum {
   NPME_TICKET_QUEUED = 0,  /* waiting for admission */

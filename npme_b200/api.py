@@ -71,7 +71,7 @@ class UserOps(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("setup_threads", ctypes.c_int),
                 ("max_batch", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
-                ("pool_capacity", ctypes.c_int)]
+                ("pool_capacity", ctypes.c_int), ("setup_batch", ctypes.c_int)]
 
 
 class TicketInfo(ctypes.Structure):
@@ -406,12 +406,13 @@ class NativeServer:
     releases the ticket, so the buffers outlive the work."""
 
     def __init__(self, device=0, setup_threads=8, max_batch=64, hbm_budget=0,
-                 pool_capacity=64):
+                 pool_capacity=64, setup_batch=16):
         self.L = load_library()
         c = ServerConfig()
         self.L.npme_gpu_server_default_config(ctypes.byref(c))
         c.device, c.setup_threads, c.max_batch = device, setup_threads, max_batch
         c.hbm_budget, c.pool_capacity = int(hbm_budget), pool_capacity
+        c.setup_batch = setup_batch
         s = ctypes.c_void_p()
         rc = self.L.npme_gpu_server_create(ctypes.byref(c), ctypes.byref(s))
         if rc:

@@ -3,12 +3,13 @@
 // A server owns one device.  Requests (parameters, geometry, charges and the
 // caller's output buffer) are admitted in arrival order while the estimated
 // device bytes of the requests in flight stay under the budget; set-up
-// threads bin and upload each admitted request on a pooled handle (exact
-// parameter match first, else an idle handle given the new parameters with
-// npme_gpu_set_params, else a new one) and upload its charges; one dispatch
-// thread runs every set-up request it finds as one batched CalcV
-// (npme_gpu_calcv_batch), copies each result into the caller's buffer and
-// completes the tickets.  Set-up of the next requests overlaps the batch on
+// threads take the admitted requests (up to setup_batch at a time), give
+// each a pooled handle (exact parameter match first, else an idle handle
+// given the new parameters with npme_gpu_set_params, else a new one), set
+// them all up in one pass of the set-up kernels and upload their charges;
+// one dispatch thread runs every set-up request it finds as one batched
+// CalcV (npme_gpu_calcv_batch), copies each result into the caller's buffer
+// and completes the tickets.  Set-up of the next requests overlaps the batch on
 // the GPU.  All state is guarded by one mutex; the GPU work itself runs
 // outside it.
 #include <cuda_runtime.h>
@@ -162,65 +163,95 @@ struct npme_server {
 
 void npme_server::setup_loop() {
   cudaSetDevice(cfg.device);
+  std::vector<Request *> rs;
+  std::vector<npme_handle *> hs, sh;
+  std::vector<char> exact;
+  std::vector<int> rcs, st;
+  std::vector<std::string> msgs;
+  std::vector<size_t> sn, si;
+  std::vector<const double *> sc;
   for (;;) {
-    Request *r;
-    npme_handle *h = nullptr;
-    bool exact = false;
+    rs.clear(), hs.clear(), exact.clear();
     {
       std::unique_lock<std::mutex> lk(mu);
       // on shutdown, stay until every request has been admitted and set up
       cv_setup.wait(lk, [&] { return !admitted.empty() || (stopping && waiting.empty()); });
       if (admitted.empty()) return;
-      r = admitted.front();
-      admitted.pop_front();
-      r->state = NPME_TICKET_SETUP;
-      h = take_idle(r->p, &exact);
-      if (!h) stats.handles_created++;
-      else if (!exact) stats.handles_retuned++;
-    }
-    int rc = NPME_OK;
-    std::string msg;
-    if (!h) {
-      rc = npme_gpu_create(&r->p, &h);
-      if (rc) {
-        char buf[512];
-        npme_gpu_last_error(nullptr, buf, sizeof buf);
-        msg = buf;
-        h = nullptr;
-      }
-    } else if (!exact) {
-      rc = npme_gpu_set_params(h, &r->p);
-      if (rc) msg = h->err;
-    }
-    if (!rc) {
-      rc = npme_gpu_setup(h, r->n, r->coord);
-      if (rc) msg = h->err;
-    }
-    if (!rc) {
-      const size_t words = (complex_kernel(r->p) ? 2 : 1) * r->n;
-      cudaError_t e = cudaMemcpyAsync(h->d_q_in, r->charge, sizeof(double) * words,
-                                      cudaMemcpyHostToDevice, h->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-      if (e != cudaSuccess) {
-        rc = NPME_ECUDA;
-        msg = std::string("charge upload: ") + cudaGetErrorString(e);
+      // every admitted request up to setup_batch: one pass of the set-up
+      // kernels serves them all
+      while (!admitted.empty() && (int)rs.size() < cfg.setup_batch) {
+        Request *r = admitted.front();
+        admitted.pop_front();
+        r->state = NPME_TICKET_SETUP;
+        bool ex = false;
+        npme_handle *h = take_idle(r->p, &ex);
+        if (!h) stats.handles_created++;
+        else if (!ex) stats.handles_retuned++;
+        rs.push_back(r), hs.push_back(h), exact.push_back(ex);
       }
     }
-    npme_handle *drop = nullptr;
+    const size_t m = rs.size();
+    rcs.assign(m, NPME_OK);
+    msgs.assign(m, std::string());
+    for (size_t k = 0; k < m; k++) {
+      if (!hs[k]) {
+        rcs[k] = npme_gpu_create(&rs[k]->p, &hs[k]);
+        if (rcs[k]) {
+          char buf[512];
+          npme_gpu_last_error(nullptr, buf, sizeof buf);
+          msgs[k] = buf;
+          hs[k] = nullptr;
+        }
+      } else if (!exact[k]) {
+        rcs[k] = npme_gpu_set_params(hs[k], &rs[k]->p);
+        if (rcs[k]) msgs[k] = hs[k]->err;
+      }
+    }
+    sh.clear(), sn.clear(), sc.clear(), si.clear();
+    for (size_t k = 0; k < m; k++)
+      if (!rcs[k]) sh.push_back(hs[k]), sn.push_back(rs[k]->n), sc.push_back(rs[k]->coord),
+            si.push_back(k);
+    if (!sh.empty()) {
+      st.assign(sh.size(), NPME_OK);
+      npme::setup_many(sh.data(), (int)sh.size(), sn.data(), sc.data(), st.data());
+      for (size_t j = 0; j < sh.size(); j++)
+        if (st[j]) rcs[si[j]] = st[j], msgs[si[j]] = sh[j]->err;
+    }
+    // charges: every upload enqueued, then one wait per stream
+    for (size_t k = 0; k < m; k++) {
+      if (rcs[k]) continue;
+      const size_t words = (complex_kernel(rs[k]->p) ? 2 : 1) * rs[k]->n;
+      const cudaError_t e = cudaMemcpyAsync(hs[k]->d_q_in, rs[k]->charge, sizeof(double) * words,
+                                            cudaMemcpyHostToDevice, hs[k]->stream);
+      if (e != cudaSuccess)
+        rcs[k] = NPME_ECUDA, msgs[k] = std::string("charge upload: ") + cudaGetErrorString(e);
+    }
+    for (size_t k = 0; k < m; k++) {
+      if (rcs[k]) continue;
+      const cudaError_t e = cudaStreamSynchronize(hs[k]->stream);
+      if (e != cudaSuccess)
+        rcs[k] = NPME_ECUDA, msgs[k] = std::string("charge upload: ") + cudaGetErrorString(e);
+    }
+    std::vector<npme_handle *> drop;
     {
       std::lock_guard<std::mutex> lk(mu);
-      if (rc) {
-        drop = give_back(h);
-        finish(r, rc, msg);
-      } else {
-        r->h = h;
-        r->t_ready = now();
-        r->state = NPME_TICKET_READY;
-        ready.push_back(r);
-        cv_ready.notify_one();
+      bool any = false;
+      for (size_t k = 0; k < m; k++) {
+        Request *r = rs[k];
+        if (rcs[k]) {
+          if (npme_handle *d = give_back(hs[k])) drop.push_back(d);
+          finish(r, rcs[k], msgs[k]);
+        } else {
+          r->h = hs[k];
+          r->t_ready = now();
+          r->state = NPME_TICKET_READY;
+          ready.push_back(r);
+          any = true;
+        }
       }
+      if (any) cv_ready.notify_one();
     }
-    if (drop) npme_gpu_destroy(drop);
+    for (npme_handle *d : drop) npme_gpu_destroy(d);
   }
 }
 
@@ -301,13 +332,14 @@ void npme_gpu_server_default_config(npme_server_config *c) {
   c->max_batch = 64;
   c->hbm_budget = 0;
   c->pool_capacity = 64;
+  c->setup_batch = 16;
 }
 
 int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
   if (!cfg || !out) return NPME_EINVAL;
   *out = nullptr;
   if (cfg->setup_threads < 1 || cfg->setup_threads > 256 || cfg->max_batch < 1 ||
-      cfg->pool_capacity < 0)
+      cfg->pool_capacity < 0 || cfg->setup_batch < 1 || cfg->setup_batch > 1024)
     return NPME_EINVAL;
   npme_server *s = new (std::nothrow) npme_server;
   if (!s) return NPME_ENOMEM;

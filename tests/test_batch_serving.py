@@ -243,3 +243,31 @@ def test_native_queue_errors_budget_and_tickets():
     st = srv.stats()
     assert st["completed"] == 6 and st["failed"] == 1 and st["idle_handles"] <= 2
     srv.close()
+
+
+@pytest.mark.gpu
+def test_batched_setup_of_mixed_requests_equals_alone():
+    """One set-up thread taking every queued request in one set-up pass:
+    kernels, orders, FFT boxes and both precisions mixed in one batch, with
+    a request whose coordinates are not finite failing alone inside it."""
+    reqs = _mixed_systems()
+    precisions = ["fp64" if i % 3 == 1 else "fp32" for i in range(len(reqs))]
+    srv = api.NativeServer(0, setup_threads=1, max_batch=64, pool_capacity=4, setup_batch=64)
+    bad_c = reqs[2].coord.copy()
+    bad_c[7, 1] = np.nan
+    ts = [srv.submit(serving.params_for(r, precision=p), r.coord, r.q)
+          for r, p in zip(reqs[:6], precisions)]
+    tb = srv.submit(serving.params_for(reqs[2]), bad_c, reqs[2].q)
+    ts += [srv.submit(serving.params_for(r, precision=p), r.coord, r.q)
+           for r, p in zip(reqs[6:], precisions[6:])]
+    with pytest.raises(api.NPMEError) as e:
+        srv.result(tb)
+    assert e.value.code == api.EINVAL
+    for r, p, t in zip(reqs, precisions, ts):
+        V, info = srv.result(t)
+        with npme_b200.Solver(serving.params_for(r, precision=p)) as s:
+            alone = s.setup(r.coord).calcv(r.q)
+        assert rel(V, alone) < (1e-6 if p == "fp32" else 1e-12), (r.rid, p)
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 1
+    srv.close()
