@@ -220,9 +220,10 @@ int npme_gpu_batch_destroy(npme_batch *b);
  * server owns one device; requests are independent systems, each with its
  * own parameters, geometry and charges.  Requests are admitted in arrival
  * order while the estimated device bytes of the requests in flight stay
- * under hbm_budget; set-up threads prepare them on pooled handles (exact
- * parameter match, else an idle handle given the new parameters, else a new
- * one); a dispatch thread runs all prepared requests as one batched CalcV
+ * under hbm_budget; set-up threads prepare them, up to setup_batch in one
+ * pass of the set-up kernels, on pooled handles (an idle handle whose device
+ * buffers fit, given the request's parameters, else a new one); a dispatch
+ * thread runs all prepared requests as one batched CalcV
  * (npme_gpu_calcv_batch), writes each result into the caller's V and
  * completes its ticket.  Thread-safe: any thread may submit, poll or wait.
  * coord, charge and V are host buffers laid out as for npme_gpu_calcv_real /
@@ -234,9 +235,10 @@ typedef struct {
   int setup_threads;   /* host threads issuing requests' set-ups (default 8) */
   int max_batch;       /* systems per batched CalcV (default 64) */
   size_t hbm_budget;   /* device bytes in flight; 0: half the free memory */
-  int pool_capacity;   /* idle handles kept for reuse (default 64) */
+  int pool_capacity;   /* idle handles kept for reuse (default 256; their
+                          device bytes also stay under hbm_budget) */
   int setup_batch;     /* admitted requests one set-up thread prepares in one
-                          pass of the set-up kernels (default 16) */
+                          pass of the set-up kernels (default 4) */
 } npme_server_config;
 enum {
   NPME_TICKET_QUEUED = 0,  /* waiting for admission */

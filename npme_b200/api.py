@@ -406,7 +406,7 @@ class NativeServer:
     releases the ticket, so the buffers outlive the work."""
 
     def __init__(self, device=0, setup_threads=8, max_batch=64, hbm_budget=0,
-                 pool_capacity=64, setup_batch=16):
+                 pool_capacity=256, setup_batch=4):
         self.L = load_library()
         c = ServerConfig()
         self.L.npme_gpu_server_default_config(ctypes.byref(c))

@@ -119,10 +119,12 @@ struct npme_handle {
   double *d_fax[3] = {nullptr, nullptr, nullptr};   //   windows (views into d_ftab)
   double *d_flam[3] = {nullptr, nullptr, nullptr};  //   lambda^2
   double *d_fcos[3] = {nullptr, nullptr, nullptr};  //   cos(2 pi m / N)
-  double *h_fstage = nullptr;  // pinned staging of those tables (freed at destroy)
-  void *h_counts = nullptr;    // pinned: set-up counts of the batches this handle owned
-  int counts_cap = 0;          //   (setup.cu, freed at destroy)
-  size_t fstage_cap = 0;
+  // pinned host staging (pinned_block; back to the process-wide cache at
+  // destroy), capacities in bytes
+  double *h_fstage = nullptr;  // the kernel transform's per-axis tables
+  void *h_counts = nullptr;    // set-up counts of the batches this handle owned
+  void *h_desc = nullptr;      // set-up descriptors of those batches
+  size_t fstage_cap = 0, counts_cap = 0, desc_cap = 0;
   double *d_fdct[3] = {nullptr, nullptr, nullptr};  // DCT-I matrices per axis
   long fdct_N[3] = {0, 0, 0};                        // the FFT lengths they were built for
   // device set-up scratch (sort keys, counts, group records), kept to reuse
@@ -172,6 +174,15 @@ namespace npme {
 
 // npme_gpu.cu: capacity-tracked device buffer owned by the handle
 int handle_buffer(npme_handle *h, void **field, size_t bytes);
+// npme_gpu.cu: pinned host block of at least `bytes` in *block (capacity in
+// *cap); the block held before, if any, goes back to the process-wide cache,
+// so the caller makes sure no copy from or to it is still in flight.  Blocks
+// come from and return to that cache: cudaFreeHost synchronises the whole
+// device and cudaHostAlloc pins pages, both too slow for a server that
+// creates and retires handles while other requests run.
+int pinned_block(npme_handle *h, void **block, size_t *cap, size_t bytes);
+// returns a handle's pinned block to the cache (destroy)
+void pinned_return(void **block, size_t *cap);
 // PME-corrected half extent X of a box of half extent X0 for an N-point FFT
 // axis (src/RecSumSupportFunctions.cpp:137-147)
 double compact_extent(double X0, double del, long order, long N);

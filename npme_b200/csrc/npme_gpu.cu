@@ -197,6 +197,51 @@ int dalloc(npme_handle *h, P **ptr, size_t bytes) {
 
 }  // namespace
 
+namespace {
+std::mutex g_pinned_mu;
+std::multimap<size_t, void *> g_pinned;  // capacity -> idle pinned block
+size_t g_pinned_bytes = 0;               // bytes held by idle blocks
+constexpr size_t kPinnedKeep = 256ull << 20;  // above: idle blocks are freed
+}  // namespace
+
+int npme::pinned_block(npme_handle *h, void **block, size_t *cap, size_t bytes) {
+  if (*block && *cap >= bytes) return NPME_OK;
+  pinned_return(block, cap);
+  // power-of-two capacities (at least 4 KiB), so blocks are reused across sizes
+  size_t want = 4096;
+  while (want < bytes) want <<= 1;
+  {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    auto it = g_pinned.lower_bound(want);
+    if (it != g_pinned.end() && it->first <= 4 * want) {
+      *block = it->second, *cap = it->first;
+      g_pinned_bytes -= it->first;
+      g_pinned.erase(it);
+      return NPME_OK;
+    }
+  }
+  cudaError_t e = cudaHostAlloc(block, want, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    *block = nullptr, *cap = 0;
+    cudaGetLastError();
+    return fail(h, NPME_ENOMEM, std::string("pinned host allocation: ") + cudaGetErrorString(e));
+  }
+  *cap = want;
+  return NPME_OK;
+}
+
+void npme::pinned_return(void **block, size_t *cap) {
+  if (!*block) return;
+  bool keep;
+  {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    keep = g_pinned_bytes + *cap <= kPinnedKeep;
+    if (keep) g_pinned.emplace(*cap, *block), g_pinned_bytes += *cap;
+  }
+  if (!keep) cudaFreeHost(*block);
+  *block = nullptr, *cap = 0;
+}
+
 double npme::compact_extent(double X0, double del, long order, long N) {
   return min_x_compact(X0, del, order, N);
 }
@@ -752,8 +797,9 @@ int npme_gpu_destroy(npme_handle *h) {
   if (h->stream2) cudaStreamSynchronize(h->stream2);
   release(h);
   pool_release(h);
-  if (h->h_fstage) cudaFreeHost(h->h_fstage);
-  if (h->h_counts) cudaFreeHost(h->h_counts);
+  npme::pinned_return((void **)&h->h_fstage, &h->fstage_cap);
+  npme::pinned_return(&h->h_counts, &h->counts_cap);
+  npme::pinned_return(&h->h_desc, &h->desc_cap);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);

@@ -312,12 +312,8 @@ int build_kernel_transform(npme_handle *h) {
     off[d][1] = total, total += tab[d]->lam.size();
     off[d][2] = total, total += (size_t)N[d];
   }
-  if (h->fstage_cap < total) {
-    if (h->h_fstage) cudaFreeHost(h->h_fstage);
-    h->h_fstage = nullptr, h->fstage_cap = 0;
-    NPME_CK(cudaHostAlloc((void **)&h->h_fstage, sizeof(double) * total, cudaHostAllocDefault));
-    h->fstage_cap = total;
-  }
+  if ((rc = pinned_block(h, (void **)&h->h_fstage, &h->fstage_cap, sizeof(double) * total)))
+    return rc;
   for (int d = 0; d < 3; d++) {
     std::copy(ax[d].begin(), ax[d].end(), h->h_fstage + off[d][0]);
     std::copy(tab[d]->lam.begin(), tab[d]->lam.end(), h->h_fstage + off[d][1]);

@@ -4,13 +4,13 @@
 // caller's output buffer) are admitted in arrival order while the estimated
 // device bytes of the requests in flight stay under the budget; set-up
 // threads take the admitted requests (up to setup_batch at a time), give
-// each a pooled handle (exact parameter match first, else an idle handle
-// given the new parameters with npme_gpu_set_params, else a new one), set
-// them all up in one pass of the set-up kernels and upload their charges;
-// one dispatch thread runs every set-up request it finds as one batched
-// CalcV (npme_gpu_calcv_batch), copies each result into the caller's buffer
-// and completes the tickets.  Set-up of the next requests overlaps the batch on
-// the GPU.  All state is guarded by one mutex; the GPU work itself runs
+// each a pooled handle (an idle handle whose buffers fit, given the new
+// parameters with npme_gpu_set_params where they differ, else a new one),
+// set them all up in one pass of the set-up kernels and upload their
+// charges; one dispatch thread runs every set-up request it finds as one
+// batched CalcV (npme_gpu_calcv_batch), copies each result into the caller's
+// buffer and completes the tickets.  Set-up of the next requests overlaps the
+// batch on the GPU.  All state is guarded by one mutex; the GPU work itself runs
 // outside it.
 #include <cuda_runtime.h>
 
@@ -86,8 +86,8 @@ struct npme_server {
   std::unordered_map<unsigned long long, Request *> tickets;
   std::deque<Request *> waiting, admitted, ready;
   size_t in_flight = 0;
-  std::map<Key, std::vector<npme_handle *>> idle;
-  int idle_count = 0;
+  std::vector<npme_handle *> idle;  // idle handles, any parameters
+  size_t idle_bytes = 0;             // device bytes they hold
   npme_server_stats stats;
   std::vector<std::thread> workers;
   std::thread dispatcher;
@@ -110,37 +110,55 @@ struct npme_server {
     if (any) cv_setup.notify_all();
   }
 
-  // An idle handle for parameters p: one with the same parameters if there
-  // is one (*exact), else any of the same precision.  Caller holds mu.
-  npme_handle *take_idle(const npme_params &p, bool *exact) {
-    auto it = idle.find(key_of(p));
-    if (it != idle.end() && !it->second.empty()) {
-      npme_handle *h = it->second.back();
-      it->second.pop_back();
-      idle_count--;
-      *exact = true;
-      return h;
+  // An idle handle for a request with parameters p and estimated device
+  // bytes `bytes`, among the idle handles of p's precision: one with the same
+  // parameters that already holds enough device memory, else the smallest
+  // that holds enough (its buffers need not grow), else one with the same
+  // parameters, else the largest.  Parameters rarely repeat exactly (the FFT
+  // box follows each system's extent), so the fit of the buffers decides.
+  // *exact: same parameters.  Caller holds mu.
+  npme_handle *take_idle(const npme_params &p, size_t bytes, bool *exact) {
+    const Key k = key_of(p);
+    long best = -1;
+    int best_rank = 4;
+    size_t best_bytes = 0;
+    for (size_t i = 0; i < idle.size(); i++) {
+      const npme_handle *h = idle[i];
+      if (h->p.precision != p.precision) continue;
+      const bool fits = h->dev_bytes >= bytes, same = key_of(h->p) == k;
+      const int rank = same && fits ? 0 : fits ? 1 : same ? 2 : 3;
+      const bool better = rank < best_rank ||
+                          (rank == best_rank &&
+                           (fits ? h->dev_bytes < best_bytes : h->dev_bytes > best_bytes));
+      if (better) best = (long)i, best_rank = rank, best_bytes = h->dev_bytes;
     }
-    for (auto &kv : idle) {
-      if (!kv.second.empty() && std::get<11>(kv.first) == p.precision) {
-        npme_handle *h = kv.second.back();
-        kv.second.pop_back();
-        idle_count--;
-        *exact = false;
-        return h;
-      }
-    }
-    return nullptr;
+    if (best < 0) return nullptr;
+    npme_handle *h = idle[best];
+    idle[best] = idle.back();
+    idle.pop_back();
+    idle_bytes -= h->dev_bytes;
+    *exact = key_of(h->p) == k;
+    return h;
   }
 
-  // Caller holds mu; returns the handle to destroy outside the lock, if any.
+  // Keeps h for reuse; with the pool full (pool_capacity handles, or idle
+  // device bytes up to the budget), the smallest of the pool and h is let go.  Caller holds mu; returns the handle to destroy outside the lock,
+  // if any.
   npme_handle *give_back(npme_handle *h) {
     if (!h) return nullptr;
-    if (idle_count < cfg.pool_capacity) {
-      idle[key_of(h->p)].push_back(h);
-      idle_count++;
+    if ((int)idle.size() < cfg.pool_capacity && idle_bytes + h->dev_bytes <= cfg.hbm_budget) {
+      idle.push_back(h);
+      idle_bytes += h->dev_bytes;
       return nullptr;
     }
+    if (idle.empty()) return h;
+    size_t small = 0;
+    for (size_t i = 1; i < idle.size(); i++)
+      if (idle[i]->dev_bytes < idle[small]->dev_bytes) small = i;
+    const size_t swapped = idle_bytes - idle[small]->dev_bytes + h->dev_bytes;
+    if (idle[small]->dev_bytes >= h->dev_bytes || swapped > cfg.hbm_budget) return h;
+    idle_bytes = swapped;
+    std::swap(idle[small], h);
     return h;
   }
 
@@ -175,7 +193,13 @@ void npme_server::setup_loop() {
     {
       std::unique_lock<std::mutex> lk(mu);
       // on shutdown, stay until every request has been admitted and set up
-      cv_setup.wait(lk, [&] { return !admitted.empty() || (stopping && waiting.empty()); });
+      // a set-up thread runs at most one full batch ahead of the dispatch
+      // thread, so handles return to the pool instead of piling up in the
+      // ready queue
+      cv_setup.wait(lk, [&] {
+        return (!admitted.empty() && (int)ready.size() < cfg.max_batch) ||
+               (stopping && waiting.empty());
+      });
       if (admitted.empty()) return;
       // every admitted request up to setup_batch: one pass of the set-up
       // kernels serves them all
@@ -184,7 +208,7 @@ void npme_server::setup_loop() {
         admitted.pop_front();
         r->state = NPME_TICKET_SETUP;
         bool ex = false;
-        npme_handle *h = take_idle(r->p, &ex);
+        npme_handle *h = take_idle(r->p, r->footprint, &ex);
         if (!h) stats.handles_created++;
         else if (!ex) stats.handles_retuned++;
         rs.push_back(r), hs.push_back(h), exact.push_back(ex);
@@ -275,6 +299,7 @@ void npme_server::dispatch_loop() {
         ready.pop_front();
       }
       for (Request *r : rs) r->state = NPME_TICKET_RUNNING;
+      if (!admitted.empty()) cv_setup.notify_all();
     }
     hs.clear(), dV.clear(), dq.clear();
     for (Request *r : rs) {
@@ -331,8 +356,8 @@ void npme_gpu_server_default_config(npme_server_config *c) {
   c->setup_threads = 8;
   c->max_batch = 64;
   c->hbm_budget = 0;
-  c->pool_capacity = 64;
-  c->setup_batch = 16;
+  c->pool_capacity = 256;
+  c->setup_batch = 4;
 }
 
 int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
@@ -451,7 +476,7 @@ int npme_gpu_server_stats(npme_server *s, npme_server_stats *st) {
   if (!s || !st) return NPME_EINVAL;
   std::lock_guard<std::mutex> lk(s->mu);
   *st = s->stats;
-  st->idle_handles = s->idle_count;
+  st->idle_handles = (int)s->idle.size();
   st->in_flight_bytes = s->in_flight;
   st->hbm_budget = s->cfg.hbm_budget;
   st->clock_s = s->now();
@@ -477,8 +502,7 @@ int npme_gpu_server_destroy(npme_server *s) {
   s->cv_ready.notify_all();
   for (auto &t : s->workers) t.join();
   s->dispatcher.join();
-  for (auto &kv : s->idle)
-    for (npme_handle *h : kv.second) npme_gpu_destroy(h);
+  for (npme_handle *h : s->idle) npme_gpu_destroy(h);
   for (auto &kv : s->tickets) delete kv.second;
   npme_gpu_batch_destroy(s->batch);
   cudaStreamDestroy(s->stream);

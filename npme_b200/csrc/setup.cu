@@ -829,13 +829,20 @@ int geometry_batch(npme_handle **hs, int R, cudaStream_t s) {
   if ((rc = scratch(h, kDesc, sizeof(SysDesc) * R, &dd)) ||
       (rc = scratch(h, kOffs, sizeof(long) * 5 * R, &offs)))
     return rc;
-  std::vector<long> ho(5 * R);
+  // staged in pinned memory: a copy from pageable memory would first wait
+  // for everything enqueued on s
+  static_assert(sizeof(SysDesc) % sizeof(long) == 0, "descriptor alignment");
+  if ((rc = pinned_block(h, &h->h_desc, &h->desc_cap, (sizeof(SysDesc) + sizeof(long) * 5) * R)))
+    return rc;
+  SysDesc *hd = static_cast<SysDesc *>(h->h_desc);
+  long *ho = reinterpret_cast<long *>(hd + R);
   for (int r = 0; r < R; r++) {
+    hd[r] = ds[r];
     ho[r] = ds[r].p_off, ho[R + r] = ds[r].b_off, ho[2 * R + r] = ds[r].c_off;
     ho[3 * R + r] = ds[r].s_off, ho[4 * R + r] = ds[r].g_off;
   }
-  SCK(cudaMemcpyAsync(dd, ds.data(), sizeof(SysDesc) * R, cudaMemcpyHostToDevice, s));
-  SCK(cudaMemcpyAsync(offs, ho.data(), sizeof(long) * 5 * R, cudaMemcpyHostToDevice, s));
+  SCK(cudaMemcpyAsync(dd, hd, sizeof(SysDesc) * R, cudaMemcpyHostToDevice, s));
+  SCK(cudaMemcpyAsync(offs, ho, sizeof(long) * 5 * R, cudaMemcpyHostToDevice, s));
   const long *poff = offs, *boff = offs + R, *coff = offs + 2 * R, *goffs = offs + 4 * R;
 
   BrickPoint<T> *pts;
@@ -953,12 +960,7 @@ int geometry_batch(npme_handle **hs, int R, cudaStream_t s) {
   // the counts, for the host to read when the set-up has completed
   SetupCounts *dc;
   if ((rc = scratch(h, kCountsDev, sizeof(SetupCounts) * R, &dc))) return rc;
-  if (h->counts_cap < R) {
-    if (h->h_counts) cudaFreeHost(h->h_counts);
-    h->h_counts = nullptr, h->counts_cap = 0;
-    SCK(cudaHostAlloc(&h->h_counts, sizeof(SetupCounts) * R, cudaHostAllocDefault));
-    h->counts_cap = R;
-  }
+  if ((rc = pinned_block(h, &h->h_counts, &h->counts_cap, sizeof(SetupCounts) * R))) return rc;
   collect_counts_kernel<<<blocks_for(R, 64), 64, 0, s>>>(dd, R, st, goff, pos, segoff, hsegoff,
                                                          dc);
   SCK(cudaMemcpyAsync(h->h_counts, dc, sizeof(SetupCounts) * R, cudaMemcpyDeviceToHost, s));

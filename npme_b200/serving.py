@@ -107,7 +107,7 @@ class Server:
     collects the results."""
 
     def __init__(self, device=0, precision="fp32", max_batch=64, hbm_budget=48e9,
-                 setup_workers=4, pool_capacity=64, setup_batch=16):
+                 setup_workers=4, pool_capacity=256, setup_batch=4):
         self.device = device
         self.precision = precision
         self.srv = api.NativeServer(device, setup_workers, max_batch, hbm_budget, pool_capacity,
