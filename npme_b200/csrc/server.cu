@@ -8,9 +8,11 @@
 // parameters with npme_gpu_set_params where they differ, else a new one),
 // set them all up in one pass of the set-up kernels and upload their
 // charges; one dispatch thread runs every set-up request it finds as one
-// batched CalcV (npme_gpu_calcv_batch), copies each result into the caller's
-// buffer and completes the tickets.  Set-up of the next requests overlaps the
-// batch on the GPU.  All state is guarded by one mutex; the GPU work itself runs
+// batched CalcV (npme_gpu_calcv_batch) and hands the batch to a completion
+// thread, which copies each result into the caller's buffer, returns the
+// handles to the pool and completes the tickets.  Set-up of the next
+// requests and the copies of the last batch's results overlap the batch on
+// the GPU.  All state is guarded by one mutex; the GPU work itself runs
 // outside it.
 #include <cuda_runtime.h>
 
@@ -90,7 +92,18 @@ struct npme_server {
   size_t idle_bytes = 0;             // device bytes they hold
   npme_server_stats stats;
   std::vector<std::thread> workers;
-  std::thread dispatcher;
+  std::thread dispatcher, copier;
+  // batches run by the dispatch thread whose results the completion thread
+  // copies back
+  struct Finished {
+    std::vector<Request *> rs;
+    int rc = NPME_OK;
+    std::string msg;
+  };
+  std::deque<Finished> finished;
+  std::condition_variable cv_copy;
+  bool dispatch_done = false;
+  cudaStream_t copy_stream = nullptr;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
@@ -173,10 +186,12 @@ struct npme_server {
     else stats.failed++;
     admit();
     cv_done.notify_all();
+    if (stopping) cv_ready.notify_all();  // the dispatch thread may be done
   }
 
   void setup_loop();
   void dispatch_loop();
+  void copy_loop();
 };
 
 void npme_server::setup_loop() {
@@ -292,7 +307,11 @@ void npme_server::dispatch_loop() {
         return !ready.empty() ||
                (stopping && waiting.empty() && admitted.empty() && in_flight == 0);
       });
-      if (ready.empty()) return;
+      if (ready.empty()) {
+        dispatch_done = true;
+        cv_copy.notify_all();
+        return;
+      }
       rs.clear();
       while (!ready.empty() && (int)rs.size() < cfg.max_batch) {
         rs.push_back(ready.front());
@@ -315,16 +334,41 @@ void npme_server::dispatch_loop() {
       npme_gpu_batch_last_error(batch, buf, sizeof buf);
       msg = buf;
     }
-    std::vector<int> rcs(rs.size(), rc);
-    if (!rc) {
-      for (size_t i = 0; i < rs.size(); i++) {
-        Request *r = rs[i];
+    // results go back on the completion thread, so their copies overlap
+    // the next batch
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stats.batches++;
+      stats.batched_requests += rs.size();
+      for (Request *r : rs) r->batch_size = (int)rs.size();
+      finished.push_back(Finished{rs, rc, msg});
+    }
+    cv_copy.notify_one();
+  }
+}
+
+void npme_server::copy_loop() {
+  cudaSetDevice(cfg.device);
+  for (;;) {
+    Finished f;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv_copy.wait(lk, [&] { return !finished.empty() || dispatch_done; });
+      if (finished.empty()) return;
+      f = std::move(finished.front());
+      finished.pop_front();
+    }
+    std::vector<int> rcs(f.rs.size(), f.rc);
+    std::string msg = f.msg;
+    if (!f.rc) {
+      for (size_t i = 0; i < f.rs.size(); i++) {
+        Request *r = f.rs[i];
         const size_t words = (complex_kernel(r->p) ? 8 : 4) * r->n;
         cudaError_t e = cudaMemcpyAsync(r->V, r->h->d_V, sizeof(double) * words,
-                                        cudaMemcpyDeviceToHost, stream);
+                                        cudaMemcpyDeviceToHost, copy_stream);
         if (e != cudaSuccess) rcs[i] = NPME_ECUDA;
       }
-      cudaError_t e = cudaStreamSynchronize(stream);
+      cudaError_t e = cudaStreamSynchronize(copy_stream);
       if (e != cudaSuccess) {
         std::fill(rcs.begin(), rcs.end(), (int)NPME_ECUDA);
         msg = std::string("result copy: ") + cudaGetErrorString(e);
@@ -333,11 +377,8 @@ void npme_server::dispatch_loop() {
     std::vector<npme_handle *> drop;
     {
       std::lock_guard<std::mutex> lk(mu);
-      stats.batches++;
-      stats.batched_requests += rs.size();
-      for (size_t i = 0; i < rs.size(); i++) {
-        Request *r = rs[i];
-        r->batch_size = (int)rs.size();
+      for (size_t i = 0; i < f.rs.size(); i++) {
+        Request *r = f.rs[i];
         if (npme_handle *d = give_back(r->h)) drop.push_back(d);
         r->h = nullptr;
         finish(r, rcs[i], rcs[i] ? (msg.empty() ? std::string("result copy failed") : msg) : "");
@@ -378,18 +419,22 @@ int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
     s->cfg.hbm_budget = fr / 2;
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
+    if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return NPME_ECUDA;
   }
   int rc = npme_gpu_batch_create(cfg->device, &s->batch);
   if (rc) {
     cudaStreamDestroy(s->stream);
+    cudaStreamDestroy(s->copy_stream);
     delete s;
     return rc;
   }
   for (int i = 0; i < cfg->setup_threads; i++) s->workers.emplace_back([s] { s->setup_loop(); });
   s->dispatcher = std::thread([s] { s->dispatch_loop(); });
+  s->copier = std::thread([s] { s->copy_loop(); });
   *out = s;
   return NPME_OK;
 }
@@ -502,10 +547,12 @@ int npme_gpu_server_destroy(npme_server *s) {
   s->cv_ready.notify_all();
   for (auto &t : s->workers) t.join();
   s->dispatcher.join();
+  s->copier.join();
   for (npme_handle *h : s->idle) npme_gpu_destroy(h);
   for (auto &kv : s->tickets) delete kv.second;
   npme_gpu_batch_destroy(s->batch);
   cudaStreamDestroy(s->stream);
+  cudaStreamDestroy(s->copy_stream);
   delete s;
   return NPME_OK;
 }
