@@ -321,6 +321,18 @@ int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs);
  * stage alone (the call takes ~1 % longer); 0: off. */
 int npme_gpu_set_timing(npme_handle *h, int enable);
 
+/* CalcV as a CUDA graph (enable = 1, the default): a handle's CalcV launches
+ * depend only on its set-up and on the device buffers of the call, so the
+ * second npme_gpu_calcv_device (or host-buffer CalcV) with the same buffers
+ * after a set-up is captured, and later calls with those buffers launch the
+ * captured graph on the caller's stream: one launch instead of ~20 kernel
+ * launches and cuFFT calls, which is what bounds CalcV of small systems.  A
+ * set-up, npme_gpu_set_params or npme_gpu_set_user_kernel discards the
+ * graph; the timing mode and caller-defined kernels always launch plainly.
+ * enable = 0: every call enqueues its launches.  No counterpart in the
+ * reference (a CPU library). */
+int npme_gpu_set_graph(npme_handle *h, int enable);
+
 int npme_gpu_get_info(const npme_handle *h, npme_info *info);
 
 /* Copies the last error message of h (or of the library when h is NULL). */

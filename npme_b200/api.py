@@ -104,7 +104,7 @@ EXPORTS = (
     "npme_gpu_calcv_exact_real", "npme_gpu_calcv_exact_complex",
     "npme_gpu_batch_create", "npme_gpu_calcv_batch", "npme_gpu_batch_sync",
     "npme_gpu_batch_last_error", "npme_gpu_batch_destroy",
-    "npme_gpu_count_pairs", "npme_gpu_set_timing", "npme_gpu_get_info",
+    "npme_gpu_count_pairs", "npme_gpu_set_timing", "npme_gpu_set_graph", "npme_gpu_get_info",
     "npme_gpu_last_error",
     "npme_gpu_destroy",
     "npme_gpu_server_default_config", "npme_gpu_server_create", "npme_gpu_submit",
@@ -149,6 +149,7 @@ def load_library():
     L.npme_gpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, sz]
     L.npme_gpu_batch_destroy.argtypes = [vp]
     L.npme_gpu_set_timing.argtypes = [vp, ctypes.c_int]
+    L.npme_gpu_set_graph.argtypes = [vp, ctypes.c_int]
     L.npme_gpu_count_pairs.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.npme_gpu_get_info.argtypes = [vp, ctypes.POINTER(Info)]
     L.npme_gpu_last_error.argtypes = [vp, ctypes.c_char_p, sz]
@@ -302,6 +303,12 @@ class Solver:
         """Stage timings for later calls; serial=True runs the direct sum after
         the reciprocal chain so each stage is timed alone."""
         self._check(self.L.npme_gpu_set_timing(self.h, (2 if serial else 1) if on else 0))
+
+    def set_graph(self, on=True):
+        """CalcV replayed as a CUDA graph after the second call with the same
+        buffers (default on); off: every call enqueues its launches."""
+        self._check(self.L.npme_gpu_set_graph(self.h, 1 if on else 0))
+        return self
 
     def info(self):
         i = Info()

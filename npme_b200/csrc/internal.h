@@ -168,6 +168,16 @@ struct npme_handle {
   bool timing_pending = false;
   float stage_ms[8] = {0};
   int launches = 0;
+
+  // CalcV replayed as a CUDA graph: captured at the second call with the
+  // same device buffers after a set-up, launched as one graph from then on.
+  // setup_gen counts set-ups and parameter changes; a graph belongs to one.
+  bool graph_enabled = true;
+  cudaGraphExec_t graph = nullptr;
+  unsigned long long setup_gen = 1, graph_gen = 0, seen_gen = 0, nograph_gen = 0;
+  double *graph_V = nullptr, *seen_V = nullptr;
+  const double *graph_q = nullptr, *seen_q = nullptr;
+  int graph_launches = 0;
 };
 
 namespace npme {

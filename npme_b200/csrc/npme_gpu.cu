@@ -351,6 +351,7 @@ static int setup_prepare(npme_handle *h, size_t n, const double *coord) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->stream2) cudaStreamSynchronize(h->stream2);
   h->ready = false;
+  h->setup_gen++;  // a captured CalcV belongs to the previous geometry
   h->n = n;
   const npme_params &p = h->p;
   // box (src/RecSumSupportFunctions.cpp:182-201, 276-296) from the points'
@@ -523,6 +524,7 @@ int npme_gpu_set_params(npme_handle *h, const npme_params *p) {
     return rc;
   }
   h->ready = false;  // buffers and plans are kept; setup rebuilds the rest
+  h->setup_gen++;
   return NPME_OK;
 }
 
@@ -537,6 +539,7 @@ int npme_gpu_set_user_kernel(npme_handle *h, const npme_user_ops *ops) {
   h->fself_r = ops->fself, h->fself_i = ops->fself_i;
   h->complex_kernel = ops->complex_kernel != 0;
   h->ready = false;  // the kernel transform depends on f_LR: set up again
+  h->setup_gen++;
   return NPME_OK;
 }
 
@@ -550,12 +553,8 @@ static void tmark(npme_handle *h, int i, cudaStream_t s) {
   if (h->timing.enabled) cudaEventRecord(h->timing.ev[i], s);
 }
 
-int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, void *stream) {
-  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
-  if (!h->ready) return fail(h, NPME_ESTATE, "calcv before setup");
-  if (!d_V || !d_charge) return fail(h, NPME_EINVAL, "null buffer");
-  CK(cudaSetDevice(h->device));
-  cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
+// Enqueues one CalcV on stream s (the launches; no checks).
+static int enqueue_calcv(npme_handle *h, double *d_V, const double *d_charge, cudaStream_t s) {
   h->launches = 0;
   tmark(h, 0, s);
   npme::launch_gather_charges(h, d_charge, s);
@@ -598,6 +597,75 @@ int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, v
   h->timing_pending = h->timing.enabled;
   CK(cudaGetLastError());
   return NPME_OK;
+}
+
+namespace {
+
+void drop_graph(npme_handle *h) {
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_V = nullptr, h->graph_q = nullptr;
+}
+
+// Captures one CalcV on the handle's stream (thread-local capture mode, so
+// other threads of the process stay free to allocate) and instantiates it.
+// On any failure the capture is ended and discarded and the call is enqueued
+// as plain launches instead; the failure is not an error of the call.
+bool capture_calcv(npme_handle *h, double *d_V, const double *d_charge) {
+  cudaStream_t cs = h->stream;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const int rc = enqueue_calcv(h, d_V, d_charge, cs);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(cs, &g);
+  cudaGraphExec_t x = nullptr;
+  if (!rc && e == cudaSuccess && g) e = cudaGraphInstantiate(&x, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (rc || e != cudaSuccess || !x) {
+    if (x) cudaGraphExecDestroy(x);
+    cudaGetLastError();
+    return false;
+  }
+  drop_graph(h);
+  h->graph = x;
+  h->graph_gen = h->setup_gen;
+  h->graph_V = d_V, h->graph_q = d_charge;
+  h->graph_launches = h->launches;
+  return true;
+}
+
+}  // namespace
+
+int npme_gpu_calcv_device(npme_handle *h, double *d_V, const double *d_charge, void *stream) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (!h->ready) return fail(h, NPME_ESTATE, "calcv before setup");
+  if (!d_V || !d_charge) return fail(h, NPME_EINVAL, "null buffer");
+  CK(cudaSetDevice(h->device));
+  cudaStream_t s = (cudaStream_t)stream;  // NULL: the default stream
+  // Graph replay: the launches of a CalcV depend only on the set-up and the
+  // two buffers, so the second call with the same buffers after a set-up is
+  // captured and later ones launch the graph (caller-defined kernels and the
+  // timing mode always run as plain launches).
+  if (h->graph_enabled && !h->timing.enabled && !h->user_kernel) {
+    if (h->graph && h->graph_gen == h->setup_gen && h->graph_V == d_V && h->graph_q == d_charge) {
+      CK(cudaGraphLaunch(h->graph, s));
+      h->launches = h->graph_launches;
+      return NPME_OK;
+    }
+    if (h->seen_gen == h->setup_gen && h->seen_V == d_V && h->seen_q == d_charge &&
+        h->nograph_gen != h->setup_gen) {
+      if (capture_calcv(h, d_V, d_charge)) {
+        CK(cudaGraphLaunch(h->graph, s));
+        h->launches = h->graph_launches;
+        return NPME_OK;
+      }
+      h->nograph_gen = h->setup_gen;  // not capturable: plain launches until the next set-up
+    }
+    h->seen_gen = h->setup_gen, h->seen_V = d_V, h->seen_q = d_charge;
+  }
+  return enqueue_calcv(h, d_V, d_charge, s);
 }
 
 // Reads the stage events of the last timed calcv (waits for its last event).
@@ -744,6 +812,13 @@ int npme_gpu_count_pairs(npme_handle *h, unsigned long long *unordered_pairs) {
   return NPME_OK;
 }
 
+int npme_gpu_set_graph(npme_handle *h, int enable) {
+  if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
+  if (enable < 0 || enable > 1) return fail(h, NPME_EINVAL, "graph mode must be 0 or 1");
+  h->graph_enabled = enable != 0;
+  return NPME_OK;
+}
+
 int npme_gpu_set_timing(npme_handle *h, int enable) {
   if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
   if (enable < 0 || enable > 2) return fail(h, NPME_EINVAL, "timing mode must be 0, 1 or 2");
@@ -795,6 +870,7 @@ int npme_gpu_destroy(npme_handle *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->stream2) cudaStreamSynchronize(h->stream2);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
   release(h);
   pool_release(h);
   npme::pinned_return((void **)&h->h_fstage, &h->fstage_cap);
