@@ -474,7 +474,8 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   switch (nd) {                             \
     case 3: NPME_BSYM(KD, FN, 3); break;    \
     case 6: NPME_BSYM(KD, FN, 6); break;    \
-    default: NPME_BSYM(KD, FN, 8); break;   \
+    case 8: NPME_BSYM(KD, FN, 8); break;    \
+    default: NPME_BSYM(KD, FN, 0); break;   \
   }
       if (f == NPME_FUNC_HELMHOLTZ) { NPME_BSYM_ND(1, 2); }
       else if (sp == NPME_SPLIT_LAPLACE_ORIG) { NPME_BSYM(2, 0, 0); }

@@ -431,15 +431,29 @@ constexpr int kPackedBlock = NPME_PACKED_BLOCK;
 // r^alpha: f0 = s^(alpha/2) - P(s), t = -alpha s^(alpha/2) / s + D(s), with
 // P, D the DM polynomials (src/KernelFunctionLaplace.cpp:394-436,
 // src/KernelFunctionRalpha.cpp:342-384).
+// ND > 0: the derivative-match order as a compile-time constant (the
+// polynomials fully unrolled); ND = 0: any order up to kMaxDeriv, evaluated
+// as the polynomials of degree kMaxDeriv whose coefficients above the order
+// are zero (make_pair_coef), so Horner's leading steps give exactly 0 and
+// the result is bit for bit that of the exact degree, at the cost of the
+// extra steps but with every coefficient at a fixed offset of the parameter
+// bank (a loop over a run-time degree indexes it dynamically and is ~2x
+// slower still).
+template <int ND>
+constexpr int dm_degree() {
+  return ND > 0 ? ND : kMaxDeriv;
+}
+
 template <int FUNC, int ND>
 __device__ __forceinline__ void dm_eval2(const PairCoef<float> &k, float2 sv, float2 &f0,
                                          float2 &t) {
-  float2 np = k.nar2[ND];  // -Rdir^(-alpha) f_LR polynomial
+  constexpr int nd = dm_degree<ND>();
+  float2 np = k.nar2[nd];  // -Rdir^(-alpha) f_LR polynomial
 #pragma unroll
-  for (int n = ND - 1; n >= 0; n--) np = __ffma2_rn(np, sv, k.nar2[n]);
-  float2 d = k.br2[ND - 1];  // Rdir^(2-alpha) (1/r) d f_LR / dr polynomial
+  for (int n = nd - 1; n >= 0; n--) np = __ffma2_rn(np, sv, k.nar2[n]);
+  float2 d = k.br2[nd - 1];  // Rdir^(2-alpha) (1/r) d f_LR / dr polynomial
 #pragma unroll
-  for (int n = ND - 2; n >= 0; n--) d = __ffma2_rn(d, sv, k.br2[n]);
+  for (int n = nd - 2; n >= 0; n--) d = __ffma2_rn(d, sv, k.br2[n]);
   if (FUNC == 0) {
     const float2 ri = make_float2(rsqrtf(sv.x), rsqrtf(sv.y));
     f0 = __fadd2_rn(ri, np);                    // Rdir (1/r - f_LR)
@@ -459,12 +473,13 @@ __device__ __forceinline__ void dm_eval2(const PairCoef<float> &k, float2 sv, fl
 template <int FUNC, int ND>
 __device__ __forceinline__ void dm_eval1(const PairCoef<float> &k, float sv, float &f0,
                                          float &t) {
-  float np = k.nar2[ND].x;
+  constexpr int nd = dm_degree<ND>();
+  float np = k.nar2[nd].x;
 #pragma unroll
-  for (int n = ND - 1; n >= 0; n--) np = fmaf(np, sv, k.nar2[n].x);
-  float d = k.br2[ND - 1].x;
+  for (int n = nd - 1; n >= 0; n--) np = fmaf(np, sv, k.nar2[n].x);
+  float d = k.br2[nd - 1].x;
 #pragma unroll
-  for (int n = ND - 2; n >= 0; n--) d = fmaf(d, sv, k.br2[n].x);
+  for (int n = nd - 2; n >= 0; n--) d = fmaf(d, sv, k.br2[n].x);
   const float ri = rsqrtf(sv);
   if (FUNC == 0) {
     f0 = ri + np;
@@ -919,12 +934,13 @@ __device__ __forceinline__ void helm_eval(const PairCoef<float> &k, float rr, fl
   const float2 E1 = __ffma2_rn(E, make_float2(-ri2, -ri2), __fmul2_rn(IK, make_float2(ri, ri)));
   const float sv = rr * k.invR2;
   const float2 s2 = make_float2(sv, sv);
-  float2 P = k.nac2[ND];
+  constexpr int nd = dm_degree<ND>();  // ND = 0: zero-padded to kMaxDeriv
+  float2 P = k.nac2[nd];
 #pragma unroll
-  for (int n = ND - 1; n >= 0; n--) P = __ffma2_rn(P, s2, k.nac2[n]);
-  float2 D = k.nbc2[ND - 1];
+  for (int n = nd - 1; n >= 0; n--) P = __ffma2_rn(P, s2, k.nac2[n]);
+  float2 D = k.nbc2[nd - 1];
 #pragma unroll
-  for (int n = ND - 2; n >= 0; n--) D = __ffma2_rn(D, s2, k.nbc2[n]);
+  for (int n = nd - 2; n >= 0; n--) D = __ffma2_rn(D, s2, k.nbc2[n]);
   F0 = __fadd2_rn(E, P);
   F1 = __fadd2_rn(E1, D);
 }
@@ -1163,7 +1179,7 @@ __device__ __forceinline__ void direct_group_body(
     float refine2, double fself_r, double fself_i, double *__restrict__ V, float4 *sp,
     float4 *slo, int lane) {
 #if !defined(NPME_SCALAR_DIRECT)
-  if constexpr (!CPLX && SPLIT == 0 && ND > 0 && std::is_same<PK, BuiltinPair>::value) {
+  if constexpr (!CPLX && SPLIT == 0 && std::is_same<PK, BuiltinPair>::value) {
     direct_group_packed<FUNC, ND>(k, gpos, spos, qs, qcaller, G, c, segs, perm, refine2, fself_r,
                                   V, sp, slo, lane);
     return;
@@ -1218,7 +1234,7 @@ __device__ __forceinline__ void direct_group_body(
     NPME_PREFETCH
     float p0 = 0, p1 = 0, p2 = 0, p3 = 0, p0i = 0, p1i = 0, p2i = 0, p3i = 0;
 #if !defined(NPME_SCALAR_DIRECT)
-    if constexpr (CPLX && SPLIT == 0 && ND > 0 && std::is_same<PK, BuiltinPair>::value) {
+    if constexpr (CPLX && SPLIT == 0 && std::is_same<PK, BuiltinPair>::value) {
       float2 Pv = make_float2(0.f, 0.f), Gx = Pv, Gy = Pv, Gz = Pv;
       helmholtz_steps<ND>(k, sp, slo, cnt, tx, ty, tz, tlx, tly, tlz, refine2, Pv, Gx, Gy, Gz);
       p0 = Pv.x, p0i = Pv.y, p1 = Gx.x, p1i = Gx.y, p2 = Gy.x, p2i = Gy.y, p3 = Gz.x, p3i = Gz.y;

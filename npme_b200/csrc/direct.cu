@@ -51,6 +51,14 @@ PairCoef<T> make_pair_coef(const npme_handle *h) {
     k.br2[i].x = k.br2[i].y = (T)(h->b_r[i] * s * std::pow(R, 2.0 - al));
     s *= R2;
   }
+  // the radial-derivative polynomials have degree nder - 1: their entry nder
+  // is zero, as are all entries above nder (the zero-padded evaluation of
+  // the packed bodies relies on it)
+  if (k.nder >= 0 && k.nder <= kMaxDeriv) {
+    k.br[k.nder] = k.bi[k.nder] = (T)0;
+    k.br2[k.nder].x = k.br2[k.nder].y = (T)0;
+    k.nbc2[k.nder].x = k.nbc2[k.nder].y = (T)0;
+  }
   {
     const double al = h->p.funcType == NPME_FUNC_RALPHA ? h->p.alpha : -1.0;
     k.invR = 1.0 / R;
@@ -294,18 +302,17 @@ void launch_merge_source(npme_handle *h, double *V, cudaStream_t s, double vs, d
 }
 
 // The pair-once form applies to the built-in kernels: in FP32 the DM kernels
-// (1/r, r^alpha, Helmholtz) with a tabulated derivative order and the
-// original Ewald split, in FP64 the real kernels (any order, original Ewald
-// included); FP64 Helmholtz and caller-defined kernels walk the full segments.
+// (1/r, r^alpha, Helmholtz; derivative orders 3, 6 and 8 compiled with the
+// order fixed, the others with the order read at run time) and the original
+// Ewald split, in FP64 the real kernels (any order, original Ewald
+// included); FP64 Helmholtz and caller-defined complex kernels walk the full
+// segments.
 bool pairs_once(const npme_handle *h) {
   if (!h->use_sym || h->n_hgroups == 0) return false;
   if (h->user_kernel) return !h->complex_kernel;  // the functor's scalar pair kernel
-  const int f = h->p.funcType, nd = h->p.nDeriv;
-  const bool tabulated = nd == 3 || nd == 6 || nd == 8;
-  if (f == NPME_FUNC_HELMHOLTZ) return h->fp32 && tabulated;
-  if (f != NPME_FUNC_LAPLACE && f != NPME_FUNC_RALPHA) return false;
-  if (!h->fp32 || h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) return true;
-  return tabulated;
+  const int f = h->p.funcType;
+  if (f == NPME_FUNC_HELMHOLTZ) return h->fp32;
+  return f == NPME_FUNC_LAPLACE || f == NPME_FUNC_RALPHA;
 }
 
 static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
@@ -314,7 +321,8 @@ static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   if (f == NPME_FUNC_HELMHOLTZ) {
     if (nd == 3) sym_helm_launch_nd<3>(h, a, s);
     else if (nd == 6) sym_helm_launch_nd<6>(h, a, s);
-    else sym_helm_launch_nd<8>(h, a, s);
+    else if (nd == 8) sym_helm_launch_nd<8>(h, a, s);
+    else sym_helm_launch_nd<0>(h, a, s);
     return true;
   }
   if (h->fp32 && h->p.EwaldSplit == NPME_SPLIT_LAPLACE_ORIG) {
@@ -337,11 +345,13 @@ static bool sym_launch(npme_handle *h, const DirectArgs &a, cudaStream_t s) {
   if (f == NPME_FUNC_LAPLACE) {
     if (nd == 3) sym_launch_nd<0, 3>(h, a, s);
     else if (nd == 6) sym_launch_nd<0, 6>(h, a, s);
-    else sym_launch_nd<0, 8>(h, a, s);
+    else if (nd == 8) sym_launch_nd<0, 8>(h, a, s);
+    else sym_launch_nd<0, 0>(h, a, s);
   } else {
     if (nd == 3) sym_launch_nd<1, 3>(h, a, s);
     else if (nd == 6) sym_launch_nd<1, 6>(h, a, s);
-    else sym_launch_nd<1, 8>(h, a, s);
+    else if (nd == 8) sym_launch_nd<1, 8>(h, a, s);
+    else sym_launch_nd<1, 0>(h, a, s);
   }
   return true;
 }

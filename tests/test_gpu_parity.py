@@ -294,6 +294,27 @@ def test_pairs_once_matches_both_sides(name, prec, monkeypatch):
         assert rel(V[:, 1:], Vo[:, 1:]) < tol[1]
 
 
+@pytest.mark.parametrize("nd", [4, 5, 7, 10])
+@pytest.mark.parametrize("name", ["laplace_dm_4k", "ralpha_dm_small", "helmholtz_dm_small"])
+def test_pairs_once_runtime_derivative_orders(name, nd, monkeypatch):
+    # derivative-match orders outside the compiled set (3, 6, 8) take the FP32
+    # pair-once walk with the order read at run time; it agrees with the
+    # one-sided walk and with the oracle
+    torch = pytest.importorskip("torch")
+    w = dataclasses.replace(SMALL[name], nDeriv=nd)
+    c, q = w.generate()
+    Vo = ob.direct(ob.params_from_workload(w), c, q)
+    got = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("NPME_PAIRS_ONCE", mode)
+        got[mode] = _direct(w, c, q, torch)
+        assert _direct.pairs_once == (mode == "1")
+    assert rel(got["1"], got["0"]) < 1e-6
+    for V in got.values():
+        assert rel(V[:, 0], Vo[:, 0]) < FP32_V_TOL
+        assert rel(V[:, 1:], Vo[:, 1:]) < FP32_G_TOL
+
+
 def test_pairs_once_on_a_lattice():
     # a cubic lattice: many points share z (ties in the column order that
     # splits the half shell) and sit on column boundaries
