@@ -303,7 +303,8 @@ void launch_merge_source(npme_handle *h, double *V, cudaStream_t s, double vs, d
 
 // The pair-once form applies to the built-in kernels: in FP32 the DM kernels
 // (1/r, r^alpha, Helmholtz; derivative orders 3, 6 and 8 compiled with the
-// order fixed, the others with the order read at run time) and the original
+// order fixed, the others by one instance at degree kMaxDeriv with
+// zero-padded coefficients) and the original
 // Ewald split, in FP64 the real kernels (any order, original Ewald
 // included); FP64 Helmholtz and caller-defined complex kernels walk the full
 // segments.
