@@ -328,7 +328,13 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     }
   }
   const int m = (int)f32.size();
-  if (m == 0) return NPME_OK;
+  if (m == 0) {
+    // the members' own CalcVs are on `stream`: npme_gpu_batch_sync waits for them
+    if (cudaEventRecord(b->ev_done, s) != cudaSuccess)
+      return bfail(b, NPME_ECUDA, "batch: event record failed");
+    b->pending = true;
+    return NPME_OK;
+  }
 
   // descriptors
   std::vector<BatchSys> desc(m);

@@ -271,3 +271,39 @@ def test_batched_setup_of_mixed_requests_equals_alone():
     st = srv.stats()
     assert st["completed"] == len(reqs) and st["failed"] == 1
     srv.close()
+
+
+@pytest.mark.gpu
+def test_batch_sync_covers_plain_members():
+    """npme_gpu_batch_sync waits for every member of the batch, also when all
+    members are FP64 (plain) handles, which run their own CalcV on the batch's
+    stream: a copy on an unrelated stream right after the sync sees the
+    results."""
+    torch = pytest.importorskip("torch")
+    reqs = _mixed_systems()[:4]
+    solvers, dq, dV, alone = [], [], [], []
+    for r in reqs:
+        s = npme_b200.Solver(serving.params_for(r, precision="fp64")).setup(r.coord)
+        solvers.append(s)
+        alone.append(s.calcv(r.q))
+        qv = np.ascontiguousarray(r.q)
+        dq.append(torch.from_numpy(qv.view(np.float64) if np.iscomplexobj(qv) else qv).cuda())
+        dV.append(torch.zeros((r.n, 8 if np.iscomplexobj(qv) else 4), dtype=torch.float64,
+                              device="cuda"))
+    b = api.Batch(0)
+    st, other = torch.cuda.Stream(), torch.cuda.Stream()
+    for _ in range(2):
+        for V in dV:
+            V.zero_()
+        torch.cuda.synchronize()
+        b.calcv(solvers, [x.data_ptr() for x in dV], [x.data_ptr() for x in dq], st.cuda_stream)
+        b.sync()
+        with torch.cuda.stream(other):
+            host = [V.to("cpu") for V in dV]
+        for r, V, ref in zip(reqs, host, alone):
+            got = V.numpy()
+            got = got.view(np.complex128) if np.iscomplexobj(r.q) else got
+            assert rel(got, ref) < 1e-12, r.rid
+    b.close()
+    for s in solvers:
+        s.close()
