@@ -125,8 +125,6 @@ struct npme_handle {
   void *h_counts = nullptr;    // set-up counts of the batches this handle owned
   void *h_desc = nullptr;      // set-up descriptors of those batches
   size_t fstage_cap = 0, counts_cap = 0, desc_cap = 0;
-  double *d_fdct[3] = {nullptr, nullptr, nullptr};  // DCT-I matrices per axis
-  long fdct_N[3] = {0, 0, 0};                        // the FFT lengths they were built for
   // device set-up scratch (sort keys, counts, group records), kept to reuse
   void *d_su[npme::kSetupScratch] = {};
 

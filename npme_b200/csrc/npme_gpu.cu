@@ -163,7 +163,6 @@ void release(npme_handle *h) {
   h->caps.clear();
   h->n_groups = h->n_segs = 0;
   h->n_hgroups = h->n_hsegs = 0;
-  h->fdct_N[0] = h->fdct_N[1] = h->fdct_N[2] = 0;  // the DCT matrices went with the buffers
   h->dev_bytes = 0;
   h->ready = false;
 }

@@ -15,6 +15,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "bodies.cuh"
@@ -69,15 +70,21 @@ struct BuiltinLR {
   __device__ double2 operator()(double r2) const { return lr_eval(k, r2); }
 };
 
+// CPLX: complex samples (double2); else the real part only (double), for
+// the real kernels, whose transform then runs in real arithmetic.
+template <bool CPLX>
 __global__ void sample_fhat_kernel(LRKernel k, int M1, int M2, int M3,
                                    const double *__restrict__ ax,  // 4*M per axis: x1,x2,T1,T2
                                    const double *__restrict__ ay,
-                                   const double *__restrict__ az, double2 *out) {
+                                   const double *__restrict__ az, void *out) {
   const long total = (long)M1 * M2 * M3;
   const BuiltinLR lr{k};
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x)
-    out[idx] = fhat_sample_body(lr, idx, M1, M2, M3, ax, ay, az);
+       idx += (long)gridDim.x * blockDim.x) {
+    const double2 f = fhat_sample_body(lr, idx, M1, M2, M3, ax, ay, az);
+    if (CPLX) static_cast<double2 *>(out)[idx] = f;
+    else static_cast<double *>(out)[idx] = f.x;
+  }
 }
 
 // The DCT-I along one axis of the M1 x M2 x M3 compact octant,
@@ -104,14 +111,19 @@ __device__ __forceinline__ long dct_addr(int ax, long line, int j, int M2, int M
 }
 
 // Tiled FP64 GEMM: a CTA computes 64 outputs k for 32 lines; tiles of C
-// (64 x 16) and of the complex input (16 x 32) pass through shared memory.
+// (64 x 16) and of the input (16 x 32) pass through shared memory.  CPLX:
+// complex lines (double2); else real lines (double), half the work.
 constexpr int kDctK = 64, kDctL = 32, kDctJ = 16;
-__global__ void __launch_bounds__(256) dct1_gemm_kernel(const double2 *__restrict__ in,
-                                                        double2 *__restrict__ out,
+template <bool CPLX>
+__global__ void __launch_bounds__(256) dct1_gemm_kernel(const void *__restrict__ in_,
+                                                        void *__restrict__ out_,
                                                         const double *__restrict__ C, int ax,
                                                         int M, long nlines, int M2, int M3) {
+  using V = typename std::conditional<CPLX, double2, double>::type;
+  const V *__restrict__ in = static_cast<const V *>(in_);
+  V *__restrict__ out = static_cast<V *>(out_);
   __shared__ double Cs[kDctK][kDctJ + 1];
-  __shared__ double2 Fs[kDctJ][kDctL];
+  __shared__ V Fs[kDctJ][kDctL];
   const int tl = threadIdx.x & 31, tk = threadIdx.x >> 5;  // line in tile, k group
   const long l0 = (long)blockIdx.x * kDctL;
   const int k0 = blockIdx.y * kDctK;
@@ -126,18 +138,21 @@ __global__ void __launch_bounds__(256) dct1_gemm_kernel(const double2 *__restric
     for (int t = threadIdx.x; t < kDctJ * kDctL; t += 256) {
       const int jj = t / kDctL, ll = t % kDctL;
       const long line = l0 + ll;
-      Fs[jj][ll] = (line < nlines && j0 + jj < M) ? in[dct_addr(ax, line, j0 + jj, M2, M3)]
-                                                  : make_double2(0.0, 0.0);
+      Fs[jj][ll] = (line < nlines && j0 + jj < M) ? in[dct_addr(ax, line, j0 + jj, M2, M3)] : V{};
     }
     __syncthreads();
 #pragma unroll
     for (int jj = 0; jj < kDctJ; jj++) {
-      const double2 f = Fs[jj][tl];
+      const V f = Fs[jj][tl];
 #pragma unroll
       for (int r = 0; r < 8; r++) {
         const double c = Cs[tk + 8 * r][jj];
-        ar[r] = fma(c, f.x, ar[r]);
-        ai[r] = fma(c, f.y, ai[r]);
+        if constexpr (CPLX) {
+          ar[r] = fma(c, f.x, ar[r]);
+          ai[r] = fma(c, f.y, ai[r]);
+        } else {
+          ar[r] = fma(c, f, ar[r]);
+        }
       }
     }
     __syncthreads();
@@ -147,12 +162,17 @@ __global__ void __launch_bounds__(256) dct1_gemm_kernel(const double2 *__restric
 #pragma unroll
   for (int r = 0; r < 8; r++) {
     const int k = k0 + tk + 8 * r;
-    if (k < M) out[dct_addr(ax, line, k, M2, M3)] = make_double2(ar[r], ai[r]);
+    if (k >= M) continue;
+    if constexpr (CPLX) out[dct_addr(ax, line, k, M2, M3)] = make_double2(ar[r], ai[r]);
+    else out[dct_addr(ax, line, k, M2, M3)] = ar[r];
   }
 }
 
-template <typename T, bool CPLX>
-__global__ void scale_fhat_kernel(const double2 *__restrict__ F, int M1, int M2, int M3,
+// G = F * lambda^2 products / volume.  CPLX_IN: F complex (double2), else
+// real (double); CPLX: the complex kernel's (re, im) output, else the real
+// part only.
+template <typename T, bool CPLX, bool CPLX_IN>
+__global__ void scale_fhat_kernel(const void *__restrict__ F_, int M1, int M2, int M3,
                                   const double *__restrict__ l1, const double *__restrict__ l2,
                                   const double *__restrict__ l3, double inv_vol, T *G) {
   const long total = (long)M1 * M2 * M3;
@@ -160,11 +180,13 @@ __global__ void scale_fhat_kernel(const double2 *__restrict__ F, int M1, int M2,
        idx += (long)gridDim.x * blockDim.x) {
     const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
     const double s = l1[i1] * l2[i2] * l3[i3] * inv_vol;
+    const double2 F = CPLX_IN ? static_cast<const double2 *>(F_)[idx]
+                              : make_double2(static_cast<const double *>(F_)[idx], 0.0);
     if (CPLX) {
-      G[2 * idx] = (T)(F[idx].x * s);
-      G[2 * idx + 1] = (T)(F[idx].y * s);
+      G[2 * idx] = (T)(F.x * s);
+      G[2 * idx + 1] = (T)(F.y * s);
     } else {
-      G[idx] = (T)(F[idx].x * s);
+      G[idx] = (T)(F.x * s);
     }
   }
 }
@@ -274,6 +296,49 @@ static void window_axis(long N, double X, double del, double a, std::vector<doub
     }                                                          \
   } while (0)
 
+// DCT-I matrices, one per (device, FFT length) for the whole process, like
+// the FFT plans: a serving process meets the same few lengths again and
+// again, while its handles move between lengths.  Built on the stream of the
+// first handle that needs one; later users wait for that construction's
+// event (complete long before, as a rule) and share the matrix read-only.
+// Never freed: M x M doubles per length seen (133 KB at N = 256).
+namespace {
+struct DctMatrix {
+  double *d = nullptr;
+  cudaEvent_t built = nullptr;
+};
+std::mutex g_dct_mu;
+std::map<std::pair<int, long>, DctMatrix> g_dct;
+}  // namespace
+
+static int dct_matrix(npme_handle *h, long N, const double *d_cos, double **out) {
+  std::lock_guard<std::mutex> lk(g_dct_mu);
+  DctMatrix &m = g_dct[std::make_pair(h->device, N)];
+  if (!m.d) {
+    const long M = N / 2 + 1;
+    cudaError_t e = cudaMalloc(&m.d, sizeof(double) * M * M);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m.built, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+      dct1_matrix_kernel<<<(unsigned)((M * M + 255) / 256), 256, 0, h->stream>>>(d_cos, (int)M,
+                                                                              (int)N, m.d);
+      e = cudaEventRecord(m.built, h->stream);
+    }
+    if (e != cudaSuccess) {
+      if (m.d) cudaFree(m.d);
+      if (m.built) cudaEventDestroy(m.built);
+      m = DctMatrix{};
+      cudaGetLastError();
+      h->err = std::string("DCT matrix: ") + cudaGetErrorString(e);
+      return NPME_ECUDA;
+    }
+  } else if (cudaStreamWaitEvent(h->stream, m.built, 0) != cudaSuccess) {
+    h->err = "DCT matrix: stream wait failed";
+    return NPME_ECUDA;
+  }
+  *out = m.d;
+  return NPME_OK;
+}
+
 int build_kernel_transform(npme_handle *h) {
   const long *N = h->grid.N;
   const int M1 = N[0] / 2 + 1, M2 = N[1] / 2 + 1, M3 = N[2] / 2 + 1;
@@ -328,47 +393,50 @@ int build_kernel_transform(npme_handle *h) {
     h->d_fcos[d] = h->d_ftab + off[d][2];
   }
   const int threads = 256, blocks = 148 * 8;
+  // the built-in real kernels sample and transform real values; complex
+  // kernels and caller-defined ones (whose sampler writes complex values)
+  // run the complex transform
+  const bool cplx_ft = h->complex_kernel || h->user_kernel;
   if (h->user_kernel) {
     if ((rc = h->uops.sample_lr(h, M1, M2, M3, h->d_fax[0], h->d_fax[1], h->d_fax[2], h->d_ft0,
                                 h->stream)))
       return rc;
+  } else if (cplx_ft) {
+    sample_fhat_kernel<true><<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, h->d_fax[0],
+                                                                h->d_fax[1], h->d_fax[2], h->d_ft0);
   } else {
-    sample_fhat_kernel<<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, h->d_fax[0],
-                                                          h->d_fax[1], h->d_fax[2], h->d_ft0);
+    sample_fhat_kernel<false><<<blocks, threads, 0, h->stream>>>(
+        k, M1, M2, M3, h->d_fax[0], h->d_fax[1], h->d_fax[2], h->d_ft0);
   }
-  double2 *src = h->d_ft0, *dst = h->d_ft1;
+  void *src = h->d_ft0, *dst = h->d_ft1;
   const int Ms[3] = {M1, M2, M3};
   for (int d = 0; d < 3; d++) {
-    // the DCT matrix of this axis, rebuilt only when the axis length changed
     const int M = Ms[d];
-    if ((rc = handle_buffer(h, (void **)&h->d_fdct[d], sizeof(double) * M * M))) return rc;
-    if (h->fdct_N[d] != N[d]) {
-      dct1_matrix_kernel<<<(unsigned)(((long)M * M + 255) / 256), 256, 0, h->stream>>>(
-          h->d_fcos[d], M, (int)N[d], h->d_fdct[d]);
-      h->fdct_N[d] = N[d];
-    }
+    double *C = nullptr;
+    if ((rc = dct_matrix(h, N[d], h->d_fcos[d], &C))) return rc;
     const long nlines = MT / M;
     const dim3 grid((unsigned)((nlines + kDctL - 1) / kDctL), (unsigned)((M + kDctK - 1) / kDctK));
-    dct1_gemm_kernel<<<grid, 256, 0, h->stream>>>(src, dst, h->d_fdct[d], d, M, nlines, M2, M3);
+    if (cplx_ft)
+      dct1_gemm_kernel<true><<<grid, 256, 0, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+    else
+      dct1_gemm_kernel<false><<<grid, 256, 0, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
     std::swap(src, dst);
   }
   const double inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);
   double *const *l = h->d_flam;
+#define NPME_SCALE(T, CX, CI)                                                                \
+  scale_fhat_kernel<T, CX, CI><<<blocks, threads, 0, h->stream>>>(src, M1, M2, M3, l[0], l[1], \
+                                                                  l[2], inv_vol, (T *)h->d_G)
   if (h->fp32) {
-    if (h->complex_kernel)
-      scale_fhat_kernel<float, true><<<blocks, threads, 0, h->stream>>>(
-          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (float *)h->d_G);
-    else
-      scale_fhat_kernel<float, false><<<blocks, threads, 0, h->stream>>>(
-          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (float *)h->d_G);
+    if (h->complex_kernel) NPME_SCALE(float, true, true);
+    else if (cplx_ft) NPME_SCALE(float, false, true);
+    else NPME_SCALE(float, false, false);
   } else {
-    if (h->complex_kernel)
-      scale_fhat_kernel<double, true><<<blocks, threads, 0, h->stream>>>(
-          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (double *)h->d_G);
-    else
-      scale_fhat_kernel<double, false><<<blocks, threads, 0, h->stream>>>(
-          src, M1, M2, M3, l[0], l[1], l[2], inv_vol, (double *)h->d_G);
+    if (h->complex_kernel) NPME_SCALE(double, true, true);
+    else if (cplx_ft) NPME_SCALE(double, false, true);
+    else NPME_SCALE(double, false, false);
   }
+#undef NPME_SCALE
   // launch errors now; npme_gpu_setup waits for the stream before it returns
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
