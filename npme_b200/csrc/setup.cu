@@ -245,7 +245,9 @@ __global__ void bin_kernel(const SysDesc *__restrict__ d, const long *__restrict
   bp.orig = (uint32_t)i;
   pts[p] = bp;
   bkey[p] = ((unsigned long long)r << (bbits + 5)) | ((unsigned long long)bid << 5) | key;
-  if (!out) atomicAdd(&bcount[D.b_off + bid], 1);
+  // every point is counted in the brick its key names (a point outside the
+  // octant in brick 0), so that the brick starts index the sorted keys
+  atomicAdd(&bcount[D.b_off + bid], 1);
   int cs[2], ss[2];
 #pragma unroll
   for (int a = 0; a < 2; a++) {
@@ -264,22 +266,44 @@ __global__ void bin_kernel(const SysDesc *__restrict__ d, const long *__restrict
   iota[p] = (unsigned)p;
 }
 
-// Round-robin key (system and brick, rank inside its bank, bank): sorting by
-// it puts the r-th point of every bank of a brick into round r.  The rank is
-// the distance to the first equal key of the sorted (system, brick, bank)
-// keys, found by binary search.
-__global__ void round_key_kernel(const unsigned long long *__restrict__ key, long P, int rankbits,
-                                 unsigned long long *__restrict__ rkey) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= P) return;
-  const unsigned long long kk = key[k];
-  long lo = 0, hi = k;  // first position with key == kk in [0, k]
-  while (lo < hi) {
-    const long m = (lo + hi) >> 1;
-    if (key[m] < kk) lo = m + 1;
-    else hi = m;
+// Brick order inside each brick in rounds over the banks: round r holds the
+// r-th point (in index order) of every bank with more than r points, banks
+// ascending, i.e. the order of a stable sort by (system, brick, rank inside
+// the bank, bank).  Input: the point indices sorted by (system, brick, bank)
+// and those keys; one warp per brick slot, lane b owns bank b (keys carry the
+// bank in their low 5 bits).
+__global__ void round_place_kernel(const unsigned long long *__restrict__ key,
+                                   const unsigned *__restrict__ in, const int *__restrict__ bstart,
+                                   const int *__restrict__ bcount, long B,
+                                   unsigned *__restrict__ out) {
+  const long b = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (b >= B) return;  // warp-uniform
+  const int c = bcount[b];
+  if (c == 0) return;
+  const long s = bstart[b], e = s + c;
+  // first position in [s, e) whose bank is >= v (banks ascend in the brick)
+  auto first = [&](unsigned v) {
+    long lo = s, hi = e;
+    while (lo < hi) {
+      const long m = (lo + hi) >> 1;
+      if ((unsigned)(key[m] & 31ull) < v) lo = m + 1;
+      else hi = m;
+    }
+    return lo;
+  };
+  const long lo = first((unsigned)lane), hi = first((unsigned)lane + 1u);
+  const int cnt = (int)(hi - lo);
+  int rounds = cnt;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) rounds = max(rounds, __shfl_xor_sync(0xffffffffu, rounds, o));
+  const unsigned below = (1u << lane) - 1u;
+  long base = s;
+  for (int r = 0; r < rounds; r++) {
+    const unsigned m = __ballot_sync(0xffffffffu, cnt > r);
+    if (cnt > r) out[base + __popc(m & below)] = in[lo + r];
+    base += __popc(m);
   }
-  rkey[k] = ((kk >> 5) << (rankbits + 5)) | ((unsigned long long)(k - lo) << 5) | (kk & 31ull);
 }
 
 // Final brick order of every system: its records, the brick-order
@@ -619,7 +643,7 @@ enum Scratch {
   kPts, kBKey, kBKeyOut, kIota, kBPerm, kCKey, kSKey, kKeyOut, kCOrder, kSOrder, kBOrder,
   kCounts3, kBStart, kFlag, kPos, kCStart, kSStart, kZs, kCPos, kFCPos, kGCount, kGOff,
   kGRec, kBLo, kBHi, kCen, kGroupCounters, kSegOff, kHSegOff, kUGroups, kUHGroups,
-  kWKey, kWKeyOut, kOrd, kGIota, kStats, kSysStats, kDesc, kOffs, kCub, kRKey, kBPos, kCountsDev,
+  kWKey, kWKeyOut, kOrd, kGIota, kStats, kSysStats, kDesc, kOffs, kCub, kBPos, kCountsDev,
   kScratchCount
 };
 static_assert(kScratchCount <= kSetupScratch, "raise kSetupScratch");
@@ -817,9 +841,8 @@ int geometry_batch(npme_handle **hs, int R, cudaStream_t s) {
     return record_error(h, NPME_EINVAL, "set-up batch too large for 32-bit indices");
   const int rbits = bits_for((unsigned long long)R);
   const int bbits = bits_for(nbtmax), cbits = bits_for(ncolmax), sbits = bits_for(nscolmax);
-  const int rankbits = bits_for((unsigned long long)nmax);
   const int wbits = bits_for((unsigned long long)nmax + 1) + 1;
-  if (rbits + bbits + rankbits + 5 > 64 || rbits + sbits + kZField > 64)
+  if (rbits + bbits + 5 > 64 || rbits + sbits + kZField > 64)
     return record_error(h, NPME_EINVAL, "set-up batch keys exceed 64 bits");
 
   // descriptors and the index-space starts (points, bricks, columns, fine
@@ -846,7 +869,7 @@ int geometry_batch(npme_handle **hs, int R, cudaStream_t s) {
   const long *poff = offs, *boff = offs + R, *coff = offs + 2 * R, *goffs = offs + 4 * R;
 
   BrickPoint<T> *pts;
-  unsigned long long *bkey, *bkey_out, *ckey, *skey, *key_out, *rkey;
+  unsigned long long *bkey, *bkey_out, *ckey, *skey, *key_out;
   unsigned *iota, *border, *corder, *sorder, *border2, *bpos, *zs, *cpos, *fcpos;
   int *counts, *bstart, *flag, *pos, *cstart, *sstart, *gcount, *goff;
   SysStats *st;
@@ -856,7 +879,6 @@ int geometry_batch(npme_handle **hs, int R, cudaStream_t s) {
       (rc = scratch(h, kCKey, sizeof(unsigned long long) * P, &ckey)) ||
       (rc = scratch(h, kSKey, sizeof(unsigned long long) * P, &skey)) ||
       (rc = scratch(h, kKeyOut, sizeof(unsigned long long) * P, &key_out)) ||
-      (rc = scratch(h, kRKey, sizeof(unsigned long long) * P, &rkey)) ||
       (rc = scratch(h, kIota, sizeof(unsigned) * P, &iota)) ||
       (rc = scratch(h, kBPerm, sizeof(unsigned) * P, &border)) ||
       (rc = scratch(h, kBOrder, sizeof(unsigned) * P, &border2)) ||
@@ -886,14 +908,13 @@ int geometry_batch(npme_handle **hs, int R, cudaStream_t s) {
   SCK(cudaGetLastError());
 
   // --- brick order: by (system, brick), inside a brick in rounds over the
-  // banks: (system, brick, bank, index) first, then (system, brick, rank
-  // inside the bank, bank) ---
+  // banks: a sort by (system, brick, bank, index), then each brick's banks
+  // interleaved in rounds ---
   if ((rc = sort_pairs(h, bkey, bkey_out, iota, border, P, rbits + bbits + 5, s))) return rc;
-  round_key_kernel<<<blocks_for(P), 256, 0, s>>>(bkey_out, P, rankbits, rkey);
-  if ((rc = sort_pairs(h, rkey, key_out, border, border2, P, rbits + bbits + rankbits + 5, s)))
-    return rc;
-  place_bricks_kernel<T><<<blocks_for(P), 256, 0, s>>>(dd, poff, R, P, border2, pts, bpos);
   if ((rc = exclusive_sum(h, bcount, bstart, B, s))) return rc;
+  round_place_kernel<<<blocks_for(32 * B), 256, 0, s>>>(bkey_out, border, bstart, bcount, B,
+                                                       border2);
+  place_bricks_kernel<T><<<blocks_for(P), 256, 0, s>>>(dd, poff, R, P, border2, pts, bpos);
   nonempty_flags_kernel<<<blocks_for(B), 256, 0, s>>>(bcount, B, flag);
   if ((rc = exclusive_sum(h, flag, pos, B, s))) return rc;
   bricks_kernel<<<blocks_for(B), 256, 0, s>>>(dd, boff, R, B, bcount, bstart, pos);
