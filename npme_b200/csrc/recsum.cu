@@ -168,6 +168,108 @@ __global__ void __launch_bounds__(256) dct1_gemm_kernel(const void *__restrict__
   }
 }
 
+// The same transform with the CTA's whole panel staged at once: the 64 rows
+// k0.. of C (all M columns) and its 32 lines (all M elements) go to shared
+// memory in one load phase, then every thread runs its 8 outputs over all j.
+// The per-output sums run over j in the same order as the tiled kernel (whose
+// padding adds exact zeros), so both give the same values; this one pays the
+// load latency once instead of once per 16 columns, which is what bounds the
+// transform at the small FFT boxes of a serving stream.  Used while the panel
+// fits the shared memory of a CTA (on B200: M <= 299 real, 223 complex).
+template <bool CPLX>
+__global__ void __launch_bounds__(256) dct1_panel_kernel(const void *__restrict__ in_,
+                                                         void *__restrict__ out_,
+                                                         const double *__restrict__ C, int ax,
+                                                         int M, long nlines, int M2, int M3) {
+  using V = typename std::conditional<CPLX, double2, double>::type;
+  const V *__restrict__ in = static_cast<const V *>(in_);
+  V *__restrict__ out = static_cast<V *>(out_);
+  extern __shared__ double2 dct_panel[];
+  // Fs rows padded by one element: the loads along j (lines of the last
+  // axis) then store to different banks
+  constexpr int FL = kDctL + 1;
+  double *Cs = reinterpret_cast<double *>(dct_panel);        // [kDctK][M]
+  V *Fs = reinterpret_cast<V *>(Cs + (long)kDctK * M);       // [M][FL]
+  const int tl = threadIdx.x & 31, tk = threadIdx.x >> 5;
+  const long l0 = (long)blockIdx.x * kDctL;
+  const int k0 = blockIdx.y * kDctK;
+  const int krows = min(kDctK, M - k0);
+  for (int t = threadIdx.x; t < kDctK * M; t += 256)
+    Cs[t] = t < krows * M ? C[(long)k0 * M + t] : 0.0;  // rows k0.. are contiguous
+  for (int t = threadIdx.x; t < M * kDctL; t += 256) {
+    // consecutive threads on consecutive addresses: along j for lines of the
+    // last axis (contiguous), along the lines otherwise
+    int jj, ll;
+    if (ax == 2) ll = t / M, jj = t - ll * M;
+    else jj = t / kDctL, ll = t - jj * kDctL;
+    const long line = l0 + ll;
+    Fs[jj * FL + ll] = line < nlines ? in[dct_addr(ax, line, jj, M2, M3)] : V{};
+  }
+  __syncthreads();
+  double ar[8], ai[8];
+#pragma unroll
+  for (int r = 0; r < 8; r++) ar[r] = ai[r] = 0.0;
+  for (int j = 0; j < M; j++) {
+    const V f = Fs[j * FL + tl];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const double c = Cs[(tk + 8 * r) * M + j];
+      if constexpr (CPLX) {
+        ar[r] = fma(c, f.x, ar[r]);
+        ai[r] = fma(c, f.y, ai[r]);
+      } else {
+        ar[r] = fma(c, f, ar[r]);
+      }
+    }
+  }
+  const long line = l0 + tl;
+  if (line >= nlines) return;
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const int k = k0 + tk + 8 * r;
+    if (k >= M) continue;
+    if constexpr (CPLX) out[dct_addr(ax, line, k, M2, M3)] = make_double2(ar[r], ai[r]);
+    else out[dct_addr(ax, line, k, M2, M3)] = ar[r];
+  }
+}
+
+// Shared memory of a dct1_panel_kernel CTA, or 0 when the panel does not fit
+// the limit.
+static size_t dct_panel_bytes(int M, bool cplx, size_t limit) {
+  const size_t b = sizeof(double) * (size_t)M * (kDctK + (cplx ? 2 : 1) * (kDctL + 1));
+  return b <= limit ? b : 0;
+}
+
+// The panel kernels' dynamic shared-memory limit, raised once per device to
+// the device's opt-in maximum.  The size a launch needs varies with M, and a
+// cudaFuncSetAttribute before each launch would race between host threads
+// that set up handles at the same time (one lowering the limit under
+// another's launch).  The handle's device is current.
+static int dct_panel_limit(npme_handle *h, size_t *limit) {
+  static std::mutex mu;
+  static std::map<int, size_t> done;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find(h->device);
+  if (it == done.end()) {
+    int optin = 0;
+    cudaError_t e =
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(dct1_panel_kernel<true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(dct1_panel_kernel<false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) {
+      h->err = std::string("DCT panel limit: ") + cudaGetErrorString(e);
+      return NPME_ECUDA;
+    }
+    it = done.emplace(h->device, (size_t)optin).first;
+  }
+  *limit = it->second;
+  return NPME_OK;
+}
+
 // G = F * lambda^2 products / volume.  CPLX_IN: F complex (double2), else
 // real (double); CPLX: the complex kernel's (re, im) output, else the real
 // part only.
@@ -416,10 +518,18 @@ int build_kernel_transform(npme_handle *h) {
     if ((rc = dct_matrix(h, N[d], h->d_fcos[d], &C))) return rc;
     const long nlines = MT / M;
     const dim3 grid((unsigned)((nlines + kDctL - 1) / kDctL), (unsigned)((M + kDctK - 1) / kDctK));
-    if (cplx_ft)
+    size_t limit = 0;
+    if ((rc = dct_panel_limit(h, &limit))) return rc;
+    const size_t pb = dct_panel_bytes(M, cplx_ft, limit);
+    if (pb && cplx_ft) {
+      dct1_panel_kernel<true><<<grid, 256, pb, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+    } else if (pb) {
+      dct1_panel_kernel<false><<<grid, 256, pb, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+    } else if (cplx_ft) {
       dct1_gemm_kernel<true><<<grid, 256, 0, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
-    else
+    } else {
       dct1_gemm_kernel<false><<<grid, 256, 0, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+    }
     std::swap(src, dst);
   }
   const double inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);
