@@ -79,13 +79,14 @@ def serving_stream(count=2048, rate=200.0, n_min=1000, n_max=200_000, seed=1005,
     return out
 
 
-def warm_stream(count=128):
+def warm_stream(count=256):
     """Start-up traffic for a server: requests drawn from the serving
     distribution with another seed (not the requests it will serve), all
     available at once.  Serving them once grows the handle pool, the device
-    memory pool and the pinned staging blocks to the sizes the stream needs,
-    and loads the kernels of every (kernel, order) the autotuner picks, so
-    that the first live requests do not pay for it."""
+    memory pool and the pinned staging blocks to what a full pass of that
+    many requests in flight needs, and loads the kernels of every (kernel,
+    order) the autotuner picks, so that the first live requests do not pay
+    for it."""
     return serving_stream(count=count, seed=99)
 
 
