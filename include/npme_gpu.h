@@ -236,9 +236,15 @@ typedef struct {
   int max_batch;       /* systems per batched CalcV (default 64) */
   size_t hbm_budget;   /* device bytes in flight; 0: half the free memory */
   int pool_capacity;   /* idle handles kept for reuse (default 256; their
-                          device bytes also stay under hbm_budget) */
+                          device bytes stay under pool_bytes) */
   int setup_batch;     /* admitted requests one set-up thread prepares in one
                           pass of the set-up kernels (default 4) */
+  size_t pool_bytes;   /* device bytes the idle handles may hold; 0: half the
+                          free memory at creation.  A handle keeps the largest
+                          buffers it has needed, so a pool that serves a
+                          stream of mixed sizes holds more than the requests
+                          in flight; one kept below that evicts handles that
+                          the next requests then create again */
 } npme_server_config;
 enum {
   NPME_TICKET_QUEUED = 0,  /* waiting for admission */
@@ -263,6 +269,8 @@ typedef struct {
   int idle_handles;
   size_t in_flight_bytes, hbm_budget;
   double clock_s;       /* seconds since server creation */
+  unsigned long long handles_dropped;  /* let go because the pool was full */
+  size_t idle_bytes, pool_bytes;       /* device bytes of the idle handles, limit */
 } npme_server_stats;
 void npme_gpu_server_default_config(npme_server_config *c);
 int npme_gpu_server_create(const npme_server_config *c, npme_server **out);

@@ -71,7 +71,8 @@ class UserOps(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("setup_threads", ctypes.c_int),
                 ("max_batch", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
-                ("pool_capacity", ctypes.c_int), ("setup_batch", ctypes.c_int)]
+                ("pool_capacity", ctypes.c_int), ("setup_batch", ctypes.c_int),
+                ("pool_bytes", ctypes.c_size_t)]
 
 
 class TicketInfo(ctypes.Structure):
@@ -89,7 +90,8 @@ class ServerStats(ctypes.Structure):
                 ("handles_created", ctypes.c_ulonglong),
                 ("handles_retuned", ctypes.c_ulonglong), ("idle_handles", ctypes.c_int),
                 ("in_flight_bytes", ctypes.c_size_t), ("hbm_budget", ctypes.c_size_t),
-                ("clock_s", ctypes.c_double)]
+                ("clock_s", ctypes.c_double), ("handles_dropped", ctypes.c_ulonglong),
+                ("idle_bytes", ctypes.c_size_t), ("pool_bytes", ctypes.c_size_t)]
 
 
 TICKET_QUEUED, TICKET_SETUP, TICKET_READY, TICKET_RUNNING, TICKET_DONE, TICKET_FAILED = range(6)
@@ -413,13 +415,13 @@ class NativeServer:
     releases the ticket, so the buffers outlive the work."""
 
     def __init__(self, device=0, setup_threads=8, max_batch=64, hbm_budget=0,
-                 pool_capacity=256, setup_batch=4):
+                 pool_capacity=256, setup_batch=4, pool_bytes=0):
         self.L = load_library()
         c = ServerConfig()
         self.L.npme_gpu_server_default_config(ctypes.byref(c))
         c.device, c.setup_threads, c.max_batch = device, setup_threads, max_batch
         c.hbm_budget, c.pool_capacity = int(hbm_budget), pool_capacity
-        c.setup_batch = setup_batch
+        c.setup_batch, c.pool_bytes = setup_batch, int(pool_bytes)
         s = ctypes.c_void_p()
         rc = self.L.npme_gpu_server_create(ctypes.byref(c), ctypes.byref(s))
         if rc:

@@ -429,17 +429,22 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     if (b->h_pinned) cudaFreeHost(b->h_pinned);
     b->h_pinned = nullptr;
     b->h_cap = 0;
-    if (cudaMallocHost((void **)&b->h_pinned, bytes * 2) != cudaSuccess)
+    // at least 1 MiB: a serving loop then never grows it (cudaMallocHost /
+    // cudaFreeHost are slow and take driver locks other threads wait for)
+    const size_t cap = std::max<size_t>(bytes * 2, size_t(1) << 20);
+    if (cudaMallocHost((void **)&b->h_pinned, cap) != cudaSuccess)
       return bfail(b, NPME_ENOMEM, "pinned descriptor buffer");
-    b->h_cap = bytes * 2;
+    b->h_cap = cap;
   }
   if (bytes > b->d_cap) {
     if (b->d_block) cudaFree(b->d_block);
     b->d_block = nullptr;
     b->d_cap = 0;
-    if (cudaMalloc((void **)&b->d_block, bytes * 2) != cudaSuccess)
+    // the same floor: cudaFree waits for the whole device
+    const size_t cap = std::max<size_t>(bytes * 2, size_t(1) << 20);
+    if (cudaMalloc((void **)&b->d_block, cap) != cudaSuccess)
       return bfail(b, NPME_ENOMEM, "device descriptor buffer");
-    b->d_cap = bytes * 2;
+    b->d_cap = cap;
   }
   for (Class *c : all) {
     BatchSys *dd = (BatchSys *)(b->h_pinned + c->desc_at);

@@ -170,13 +170,17 @@ void release(npme_handle *h) {
 // Device buffer of at least `bytes`: reused when the handle already holds a
 // large enough one (set-up of a new geometry on the same handle allocates
 // only what grew), otherwise freed and allocated again from the pool, in
-// the order of the handle's stream.
+// the order of the handle's stream.  A buffer that grows takes half again
+// its old capacity at least, so a handle serving systems of varying sizes
+// settles after a few growths instead of reallocating (and the pool
+// reserving more memory) on every larger system.
 template <typename P>
 int dalloc(npme_handle *h, P **ptr, size_t bytes) {
   if (bytes == 0) bytes = 16;
   size_t &cap = h->caps[(void *)ptr];
   if (*ptr && cap >= bytes) return NPME_OK;
   if (*ptr) {
+    bytes = std::max(bytes, cap + cap / 2);
     cudaFreeAsync(*ptr, h->stream);
     h->dev_bytes -= cap;
     *ptr = nullptr;

@@ -155,21 +155,23 @@ struct npme_server {
   }
 
   // Keeps h for reuse; with the pool full (pool_capacity handles, or idle
-  // device bytes up to the budget), the smallest of the pool and h is let go.  Caller holds mu; returns the handle to destroy outside the lock,
+  // device bytes up to pool_bytes), the smallest of the pool and h is let
+  // go.  Caller holds mu; returns the handle to destroy outside the lock,
   // if any.
   npme_handle *give_back(npme_handle *h) {
     if (!h) return nullptr;
-    if ((int)idle.size() < cfg.pool_capacity && idle_bytes + h->dev_bytes <= cfg.hbm_budget) {
+    if ((int)idle.size() < cfg.pool_capacity && idle_bytes + h->dev_bytes <= cfg.pool_bytes) {
       idle.push_back(h);
       idle_bytes += h->dev_bytes;
       return nullptr;
     }
+    stats.handles_dropped++;
     if (idle.empty()) return h;
     size_t small = 0;
     for (size_t i = 1; i < idle.size(); i++)
       if (idle[i]->dev_bytes < idle[small]->dev_bytes) small = i;
     const size_t swapped = idle_bytes - idle[small]->dev_bytes + h->dev_bytes;
-    if (idle[small]->dev_bytes >= h->dev_bytes || swapped > cfg.hbm_budget) return h;
+    if (idle[small]->dev_bytes >= h->dev_bytes || swapped > cfg.pool_bytes) return h;
     idle_bytes = swapped;
     std::swap(idle[small], h);
     return h;
@@ -399,6 +401,7 @@ void npme_gpu_server_default_config(npme_server_config *c) {
   c->hbm_budget = 0;
   c->pool_capacity = 256;
   c->setup_batch = 4;
+  c->pool_bytes = 0;
 }
 
 int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
@@ -413,10 +416,11 @@ int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
   s->t0 = Clock::now();
   memset(&s->stats, 0, sizeof(s->stats));
   cudaError_t e = cudaSetDevice(cfg->device);
-  if (e == cudaSuccess && s->cfg.hbm_budget == 0) {
+  if (e == cudaSuccess && (s->cfg.hbm_budget == 0 || s->cfg.pool_bytes == 0)) {
     size_t fr = 0, tot = 0;
     e = cudaMemGetInfo(&fr, &tot);
-    s->cfg.hbm_budget = fr / 2;
+    if (s->cfg.hbm_budget == 0) s->cfg.hbm_budget = fr / 2;
+    if (s->cfg.pool_bytes == 0) s->cfg.pool_bytes = fr / 2;
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
@@ -525,6 +529,8 @@ int npme_gpu_server_stats(npme_server *s, npme_server_stats *st) {
   st->in_flight_bytes = s->in_flight;
   st->hbm_budget = s->cfg.hbm_budget;
   st->clock_s = s->now();
+  st->idle_bytes = s->idle_bytes;
+  st->pool_bytes = s->cfg.pool_bytes;
   return NPME_OK;
 }
 

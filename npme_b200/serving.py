@@ -118,11 +118,11 @@ class Server:
     collects the results."""
 
     def __init__(self, device=0, precision="fp32", max_batch=64, hbm_budget=48e9,
-                 setup_workers=4, pool_capacity=256, setup_batch=4):
+                 setup_workers=4, pool_capacity=256, setup_batch=4, pool_bytes=0):
         self.device = device
         self.precision = precision
         self.srv = api.NativeServer(device, setup_workers, max_batch, hbm_budget, pool_capacity,
-                                    setup_batch)
+                                    setup_batch, pool_bytes=pool_bytes)
         # host clock of the server's clock zero
         self.offset = time.perf_counter() - self.srv.stats()["clock_s"]
 
@@ -191,4 +191,5 @@ class Server:
                 "setup_ms_p90": 1e3 * float(np.percentile([r.setup_s for r in reqs], 90)),
                 "gpu_wait_ms_median": float(np.median(run_ms)),
                 "handles_created": st["handles_created"] - base["handles_created"],
-                "handles_retuned": st["handles_retuned"] - base["handles_retuned"]}
+                "handles_retuned": st["handles_retuned"] - base["handles_retuned"],
+                "handles_dropped": st["handles_dropped"] - base["handles_dropped"]}

@@ -307,3 +307,27 @@ def test_batch_sync_covers_plain_members():
     b.close()
     for s in solvers:
         s.close()
+
+
+@pytest.mark.gpu
+def test_pool_keeps_handles_under_its_own_byte_budget():
+    """Idle handles are kept under their own byte budget (pool_bytes), apart
+    from the admission budget: with the default, two passes of the same
+    requests let no handle go, and every handle ever created is idle in the
+    pool afterwards (a pass may still create one when more of its requests
+    are in flight at once than in the pass before); with a one-byte pool
+    every handle is let go when it comes back."""
+    reqs = serving.serving_stream(count=24, n_min=1000, n_max=20000, seed=21, rate=1e4)
+    srv = serving.Server(max_batch=8, hbm_budget=1 << 40)  # all admitted at once
+    for _ in range(2):
+        st = srv.run(reqs, realtime=False)
+        assert st["handles_dropped"] == 0
+    s = srv.srv.stats()
+    assert s["handles_dropped"] == 0 and s["idle_handles"] == s["handles_created"]
+    assert 0 < s["idle_bytes"] <= s["pool_bytes"]
+    srv.close()
+    tiny = serving.Server(max_batch=8, pool_bytes=1)
+    st = tiny.run(reqs[:6], realtime=False)
+    s = tiny.srv.stats()
+    assert s["idle_handles"] == 0 and st["handles_dropped"] >= 1
+    tiny.close()
