@@ -5,6 +5,7 @@
 #include <cufft.h>
 #include <stdint.h>
 
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <string>
@@ -267,5 +268,30 @@ int launch_exact(npme_handle *h, const double *d_q, double *d_V, cudaStream_t s,
 void launch_count_pairs(npme_handle *h, unsigned long long *d_count, cudaStream_t s);
 template <typename T>
 PairCoef<T> make_pair_coef(const npme_handle *h);
+
+// Device memory reservation for a server: the device's stream-ordered pool
+// (which every handle allocates from) is grown to hold at least `bytes`, and
+// the reservation counts as one live user of the pool, so the pool keeps the
+// memory until pool_unreserve.  Growing the pool while kernels run stalls the
+// driver for every host thread (tenths of a second at a time under a serving
+// load), so a server grows it once, at creation.  Best effort: without the
+// memory the pool grows on demand.
+int pool_reserve(int device, size_t bytes);
+void pool_unreserve(int device);
+
+// Slow-step log of the serving queue and of set-up: with NPME_SERVER_TRACE
+// set in the environment, a step that takes longer than 5 ms is reported on
+// stderr with its name and how many requests or systems it served.  Off by
+// default (one check of a cached flag per step).
+bool step_trace_on();
+struct StepTimer {
+  const char *name;
+  size_t count;
+  std::chrono::steady_clock::time_point t0;
+  bool on;
+  StepTimer(const char *step, size_t n)
+      : name(step), count(n), t0(std::chrono::steady_clock::now()), on(step_trace_on()) {}
+  ~StepTimer();
+};
 
 }  // namespace npme

@@ -117,33 +117,48 @@ double min_x_compact(double X0, double del, long order, long N) {
 std::mutex g_pool_mu;
 std::map<int, std::pair<cudaMemPool_t, int>> g_pools;  // device -> (pool, live handles)
 
-int pool_acquire(npme_handle *h) {
-  std::lock_guard<std::mutex> lk(g_pool_mu);
-  auto it = g_pools.find(h->device);
+// The device's pool, created on first use; *count gets its live users.
+// Caller holds g_pool_mu.
+static int pool_get(int device, cudaMemPool_t *out, std::string &err) {
+  auto it = g_pools.find(device);
   if (it == g_pools.end()) {
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.handleTypes = cudaMemHandleTypeNone;
     props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = h->device;
+    props.location.id = device;
     cudaMemPool_t pool;
     cudaError_t e = cudaMemPoolCreate(&pool, &props);
-    if (e != cudaSuccess)
-      return fail(h, NPME_ECUDA, std::string("cudaMemPoolCreate: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+      err = std::string("cudaMemPoolCreate: ") + cudaGetErrorString(e);
+      return NPME_ECUDA;
+    }
     unsigned long long keep = ~0ull;  // keep freed blocks for reuse
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    it = g_pools.emplace(h->device, std::make_pair(pool, 0)).first;
+    it = g_pools.emplace(device, std::make_pair(pool, 0)).first;
   }
   it->second.second++;
-  h->pool = it->second.first;
+  *out = it->second.first;
   return NPME_OK;
+}
+
+int pool_acquire(npme_handle *h) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  std::string err;
+  const int rc = pool_get(h->device, &h->pool, err);
+  return rc ? fail(h, rc, err) : NPME_OK;
+}
+
+// One live user less; the last one returns the pool's memory to the device.
+static void pool_put(int device) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(device);
+  if (it != g_pools.end() && --it->second.second == 0) cudaMemPoolTrimTo(it->second.first, 0);
 }
 
 void pool_release(npme_handle *h) {
   if (!h->pool) return;
-  std::lock_guard<std::mutex> lk(g_pool_mu);
-  auto it = g_pools.find(h->device);
-  if (it != g_pools.end() && --it->second.second == 0) cudaMemPoolTrimTo(it->second.first, 0);
+  pool_put(h->device);
   h->pool = nullptr;
 }
 
@@ -244,6 +259,32 @@ void npme::pinned_return(void **block, size_t *cap) {
   if (!keep) cudaFreeHost(*block);
   *block = nullptr, *cap = 0;
 }
+
+int npme::pool_reserve(int device, size_t bytes) {
+  cudaMemPool_t pool;
+  std::string err;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (pool_get(device, &pool, err)) return NPME_ECUDA;
+  }
+  size_t cur = 0;
+  cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &cur);
+  if (cur < bytes) {
+    // one allocation of the difference, freed at once: the pool keeps the
+    // memory (its release threshold is unlimited) and hands it out later
+    cudaStream_t st = nullptr;
+    void *q = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+      if (cudaMallocFromPoolAsync(&q, bytes - cur, pool, st) == cudaSuccess) cudaFreeAsync(q, st);
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+    cudaGetLastError();  // not enough memory: the pool grows on demand instead
+  }
+  return NPME_OK;
+}
+
+void npme::pool_unreserve(int device) { pool_put(device); }
 
 double npme::compact_extent(double X0, double del, long order, long N) {
   return min_x_compact(X0, del, order, N);
@@ -406,7 +447,10 @@ int npme::setup_many(npme_handle **hs, int R, const size_t *n, const double *con
                      int *status) {
   std::vector<int> st(R, NPME_OK);
   // per handle: checks, coordinates, box
-  for (int r = 0; r < R; r++) st[r] = setup_prepare(hs[r], n[r], coord[r]);
+  for (int r = 0; r < R; r++) {
+    npme::StepTimer t("set-up: checks, coordinates, box", n[r]);
+    st[r] = setup_prepare(hs[r], n[r], coord[r]);
+  }
   // the geometry of the prepared handles, one pass per precision
   for (int prec = 0; prec < 2; prec++) {
     std::vector<npme_handle *> group;
@@ -415,7 +459,11 @@ int npme::setup_many(npme_handle **hs, int R, const size_t *n, const double *con
       if (!st[r] && hs[r]->fp32 == (prec == 0)) group.push_back(hs[r]), idx.push_back(r);
     if (group.empty()) continue;
     npme_handle *owner = group[0];
-    int rc = npme::setup_geometry(group.data(), (int)group.size(), owner->stream);
+    int rc;
+    {
+      npme::StepTimer t("set-up: geometry enqueue", group.size());
+      rc = npme::setup_geometry(group.data(), (int)group.size(), owner->stream);
+    }
     if (rc) {
       for (size_t k = 0; k < group.size(); k++) {
         if (group[k] != owner) group[k]->err = owner->err;
@@ -423,7 +471,11 @@ int npme::setup_many(npme_handle **hs, int R, const size_t *n, const double *con
       }
       continue;
     }
-    for (size_t k = 0; k < group.size(); k++) st[idx[k]] = setup_transform(group[k]);
+    for (size_t k = 0; k < group.size(); k++) {
+      npme::StepTimer t("set-up: FFT plans and kernel transform enqueue", 1);
+      st[idx[k]] = setup_transform(group[k]);
+    }
+    npme::StepTimer t_wait("set-up: wait for the device and read the counts", group.size());
     // the owner's stream carries the shared passes; every handle's stream
     // its own transform: CalcV may be enqueued on any stream, so the set-up
     // completes here (and the counts arrive)

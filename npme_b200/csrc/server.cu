@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -30,6 +32,18 @@
 #include <vector>
 
 #include "internal.h"
+
+bool npme::step_trace_on() {
+  static const bool on = std::getenv("NPME_SERVER_TRACE") != nullptr;
+  return on;
+}
+
+npme::StepTimer::~StepTimer() {
+  if (!on) return;
+  const double ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (ms > 5.0) std::fprintf(stderr, "npme server: %s took %.1f ms (%zu)\n", name, ms, count);
+}
 
 namespace {
 
@@ -104,6 +118,7 @@ struct npme_server {
   std::condition_variable cv_copy;
   bool dispatch_done = false;
   cudaStream_t copy_stream = nullptr;
+  bool reserved = false;  // holds a reservation of the device pool
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
@@ -235,6 +250,7 @@ void npme_server::setup_loop() {
     rcs.assign(m, NPME_OK);
     msgs.assign(m, std::string());
     for (size_t k = 0; k < m; k++) {
+      npme::StepTimer t("set-up thread: create or retune a handle", 1);
       if (!hs[k]) {
         rcs[k] = npme_gpu_create(&rs[k]->p, &hs[k]);
         if (rcs[k]) {
@@ -253,12 +269,14 @@ void npme_server::setup_loop() {
       if (!rcs[k]) sh.push_back(hs[k]), sn.push_back(rs[k]->n), sc.push_back(rs[k]->coord),
             si.push_back(k);
     if (!sh.empty()) {
+      npme::StepTimer t("set-up thread: setup_many", sh.size());
       st.assign(sh.size(), NPME_OK);
       npme::setup_many(sh.data(), (int)sh.size(), sn.data(), sc.data(), st.data());
       for (size_t j = 0; j < sh.size(); j++)
         if (st[j]) rcs[si[j]] = st[j], msgs[si[j]] = sh[j]->err;
     }
     // charges: every upload enqueued, then one wait per stream
+    npme::StepTimer t_up("set-up thread: charge uploads and waits", m);
     for (size_t k = 0; k < m; k++) {
       if (rcs[k]) continue;
       const size_t words = (complex_kernel(rs[k]->p) ? 2 : 1) * rs[k]->n;
@@ -292,7 +310,10 @@ void npme_server::setup_loop() {
       }
       if (any) cv_ready.notify_one();
     }
-    for (npme_handle *d : drop) npme_gpu_destroy(d);
+    for (npme_handle *d : drop) {
+      npme::StepTimer t("set-up thread: destroy a handle", 1);
+      npme_gpu_destroy(d);
+    }
   }
 }
 
@@ -328,8 +349,15 @@ void npme_server::dispatch_loop() {
       dV.push_back(r->h->d_V);
       dq.push_back(r->h->d_q_in);
     }
-    int rc = npme_gpu_calcv_batch(batch, hs.data(), (int)hs.size(), dV.data(), dq.data(), stream);
-    if (!rc) rc = npme_gpu_batch_sync(batch);
+    int rc;
+    {
+      npme::StepTimer t("dispatch: batched CalcV enqueue", hs.size());
+      rc = npme_gpu_calcv_batch(batch, hs.data(), (int)hs.size(), dV.data(), dq.data(), stream);
+    }
+    if (!rc) {
+      npme::StepTimer t("dispatch: batched CalcV wait", hs.size());
+      rc = npme_gpu_batch_sync(batch);
+    }
     std::string msg;
     if (rc) {
       char buf[512];
@@ -363,6 +391,7 @@ void npme_server::copy_loop() {
     std::vector<int> rcs(f.rs.size(), f.rc);
     std::string msg = f.msg;
     if (!f.rc) {
+      npme::StepTimer t("completion: result copies", f.rs.size());
       for (size_t i = 0; i < f.rs.size(); i++) {
         Request *r = f.rs[i];
         const size_t words = (complex_kernel(r->p) ? 8 : 4) * r->n;
@@ -386,7 +415,10 @@ void npme_server::copy_loop() {
         finish(r, rcs[i], rcs[i] ? (msg.empty() ? std::string("result copy failed") : msg) : "");
       }
     }
-    for (npme_handle *d : drop) npme_gpu_destroy(d);
+    for (npme_handle *d : drop) {
+      npme::StepTimer t("completion: destroy a handle", 1);
+      npme_gpu_destroy(d);
+    }
   }
 }
 
@@ -422,10 +454,15 @@ int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
     if (s->cfg.hbm_budget == 0) s->cfg.hbm_budget = fr / 2;
     if (s->cfg.pool_bytes == 0) s->cfg.pool_bytes = fr / 2;
   }
+  // the idle pool's budget reserved in the device pool now, so that serving
+  // never waits for the pool to grow
+  if (e == cudaSuccess && npme::pool_reserve(cfg->device, s->cfg.pool_bytes) == NPME_OK)
+    s->reserved = true;
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->reserved) npme::pool_unreserve(cfg->device);
     delete s;
     return NPME_ECUDA;
   }
@@ -433,6 +470,7 @@ int npme_gpu_server_create(const npme_server_config *cfg, npme_server **out) {
   if (rc) {
     cudaStreamDestroy(s->stream);
     cudaStreamDestroy(s->copy_stream);
+    if (s->reserved) npme::pool_unreserve(cfg->device);
     delete s;
     return rc;
   }
@@ -559,6 +597,7 @@ int npme_gpu_server_destroy(npme_server *s) {
   npme_gpu_batch_destroy(s->batch);
   cudaStreamDestroy(s->stream);
   cudaStreamDestroy(s->copy_stream);
+  if (s->reserved) npme::pool_unreserve(s->cfg.device);
   delete s;
   return NPME_OK;
 }
