@@ -244,7 +244,12 @@ typedef struct {
                           buffers it has needed, so a pool that serves a
                           stream of mixed sizes holds more than the requests
                           in flight; one kept below that evicts handles that
-                          the next requests then create again */
+                          the next requests then create again.  The server
+                          reserves this much of the library's device memory
+                          pool at creation (best effort) and keeps it until
+                          npme_gpu_server_destroy: growing the pool while
+                          kernels run stalls every host thread of the
+                          process for tenths of a second */
 } npme_server_config;
 enum {
   NPME_TICKET_QUEUED = 0,  /* waiting for admission */

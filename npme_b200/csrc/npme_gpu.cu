@@ -194,14 +194,21 @@ int dalloc(npme_handle *h, P **ptr, size_t bytes) {
   if (bytes == 0) bytes = 16;
   size_t &cap = h->caps[(void *)ptr];
   if (*ptr && cap >= bytes) return NPME_OK;
+  size_t want = bytes;
   if (*ptr) {
-    bytes = std::max(bytes, cap + cap / 2);
+    want = std::max(bytes, cap + cap / 2);
     cudaFreeAsync(*ptr, h->stream);
     h->dev_bytes -= cap;
     *ptr = nullptr;
     cap = 0;
   }
-  cudaError_t e = cudaMallocFromPoolAsync((void **)ptr, bytes, h->pool, h->stream);
+  cudaError_t e = cudaMallocFromPoolAsync((void **)ptr, want, h->pool, h->stream);
+  if (e != cudaSuccess && want > bytes) {  // no room for the headroom: exact size
+    cudaGetLastError();
+    want = bytes;
+    e = cudaMallocFromPoolAsync((void **)ptr, want, h->pool, h->stream);
+  }
+  bytes = want;
   if (e != cudaSuccess) {
     *ptr = nullptr;
     cudaGetLastError();
