@@ -125,7 +125,9 @@ struct npme_handle {
   double *h_fstage = nullptr;  // the kernel transform's per-axis tables
   void *h_counts = nullptr;    // set-up counts of the batches this handle owned
   void *h_desc = nullptr;      // set-up descriptors of those batches
-  size_t fstage_cap = 0, counts_cap = 0, desc_cap = 0;
+  void *h_ktdesc = nullptr;    // kernel-transform descriptors of those batches
+  size_t fstage_cap = 0, counts_cap = 0, desc_cap = 0, ktdesc_cap = 0;
+  void *d_ktdesc = nullptr;    // the same on the device
   // device set-up scratch (sort keys, counts, group records), kept to reuse
   void *d_su[npme::kSetupScratch] = {};
 
@@ -223,6 +225,11 @@ int fft_inverse(npme_handle *h, cudaStream_t s);
 
 // recsum.cu
 int build_kernel_transform(npme_handle *h);  // F-hat, lambda^2 -> d_G
+// The kernel transforms of several handles (one precision), on the owner's
+// stream: one launch per stage for every class of two or more handles with
+// a built-in kernel (real, complex), the rest one by one on their own
+// streams.  status[k] gets each handle's result.
+void build_kernel_transforms(npme_handle **hs, int R, npme_handle *owner, int *status);
 void launch_gather_charges(npme_handle *h, const double *d_q, cudaStream_t s);
 void launch_spread(npme_handle *h, cudaStream_t s);
 void launch_multiply(npme_handle *h, cudaStream_t s);

@@ -379,8 +379,9 @@ void fill_default_del(npme_params &p) {
 
 // Set-up in three stages: per handle, the checks, coordinates and box
 // (setup_prepare); for all handles at once, the geometry on the device
-// (npme::setup_geometry); per handle, FFT plans and the kernel transform
-// (setup_transform); then one wait and the counts (npme::finish_setup).
+// (npme::setup_geometry), then per handle the FFT plans and for all handles
+// the kernel transforms (npme::build_kernel_transforms); then one wait and
+// the counts (npme::finish_setup).
 static int setup_prepare(npme_handle *h, size_t n, const double *coord) {
   if (!h) return fail(nullptr, NPME_EINVAL, "null handle");
   if (h->user_kernel && !h->uops.direct)
@@ -444,12 +445,6 @@ static int setup_prepare(npme_handle *h, size_t n, const double *coord) {
   return NPME_OK;
 }
 
-static int setup_transform(npme_handle *h) {
-  int rc;
-  if ((rc = npme::prepare_plans(h))) return rc;
-  return npme::build_kernel_transform(h);
-}
-
 int npme::setup_many(npme_handle **hs, int R, const size_t *n, const double *const *coord,
                      int *status) {
   std::vector<int> st(R, NPME_OK);
@@ -478,9 +473,17 @@ int npme::setup_many(npme_handle **hs, int R, const size_t *n, const double *con
       }
       continue;
     }
+    std::vector<npme_handle *> kt;
+    std::vector<int> kidx;
     for (size_t k = 0; k < group.size(); k++) {
-      npme::StepTimer t("set-up: FFT plans and kernel transform enqueue", 1);
-      st[idx[k]] = setup_transform(group[k]);
+      st[idx[k]] = npme::prepare_plans(group[k]);
+      if (!st[idx[k]]) kt.push_back(group[k]), kidx.push_back(idx[k]);
+    }
+    if (!kt.empty()) {
+      npme::StepTimer t("set-up: kernel transforms enqueue", kt.size());
+      std::vector<int> kst(kt.size(), NPME_OK);
+      npme::build_kernel_transforms(kt.data(), (int)kt.size(), owner, kst.data());
+      for (size_t k = 0; k < kt.size(); k++) st[kidx[k]] = kst[k];
     }
     npme::StepTimer t_wait("set-up: wait for the device and read the counts", group.size());
     // the owner's stream carries the shared passes; every handle's stream
@@ -938,6 +941,7 @@ int npme_gpu_destroy(npme_handle *h) {
   npme::pinned_return((void **)&h->h_fstage, &h->fstage_cap);
   npme::pinned_return(&h->h_counts, &h->counts_cap);
   npme::pinned_return(&h->h_desc, &h->desc_cap);
+  npme::pinned_return(&h->h_ktdesc, &h->ktdesc_cap);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);

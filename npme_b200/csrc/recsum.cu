@@ -70,6 +70,13 @@ struct BuiltinLR {
   __device__ double2 operator()(double r2) const { return lr_eval(k, r2); }
 };
 
+// The same, reading the parameters where they lie (a batch's descriptors in
+// global memory) instead of copying them
+struct BuiltinLRRef {
+  const LRKernel *k;
+  __device__ double2 operator()(double r2) const { return lr_eval(*k, r2); }
+};
+
 // CPLX: complex samples (double2); else the real part only (double), for
 // the real kernels, whose transform then runs in real arithmetic.
 template <bool CPLX>
@@ -177,22 +184,22 @@ __global__ void __launch_bounds__(256) dct1_gemm_kernel(const void *__restrict__
 // transform at the small FFT boxes of a serving stream.  Used while the panel
 // fits the shared memory of a CTA (on B200: M <= 299 real, 223 complex).
 template <bool CPLX>
-__global__ void __launch_bounds__(256) dct1_panel_kernel(const void *__restrict__ in_,
-                                                         void *__restrict__ out_,
-                                                         const double *__restrict__ C, int ax,
-                                                         int M, long nlines, int M2, int M3) {
+__device__ __forceinline__ void dct1_panel_body(const void *__restrict__ in_,
+                                                void *__restrict__ out_,
+                                                const double *__restrict__ C, int ax, int M,
+                                                long nlines, int M2, int M3, long bx, int by,
+                                                double2 *dct_panel) {
   using V = typename std::conditional<CPLX, double2, double>::type;
   const V *__restrict__ in = static_cast<const V *>(in_);
   V *__restrict__ out = static_cast<V *>(out_);
-  extern __shared__ double2 dct_panel[];
   // Fs rows padded by one element: the loads along j (lines of the last
   // axis) then store to different banks
   constexpr int FL = kDctL + 1;
   double *Cs = reinterpret_cast<double *>(dct_panel);        // [kDctK][M]
   V *Fs = reinterpret_cast<V *>(Cs + (long)kDctK * M);       // [M][FL]
   const int tl = threadIdx.x & 31, tk = threadIdx.x >> 5;
-  const long l0 = (long)blockIdx.x * kDctL;
-  const int k0 = blockIdx.y * kDctK;
+  const long l0 = bx * kDctL;
+  const int k0 = by * kDctK;
   const int krows = min(kDctK, M - k0);
   for (int t = threadIdx.x; t < kDctK * M; t += 256)
     Cs[t] = t < krows * M ? C[(long)k0 * M + t] : 0.0;  // rows k0.. are contiguous
@@ -233,6 +240,15 @@ __global__ void __launch_bounds__(256) dct1_panel_kernel(const void *__restrict_
   }
 }
 
+template <bool CPLX>
+__global__ void __launch_bounds__(256) dct1_panel_kernel(const void *__restrict__ in,
+                                                         void *__restrict__ out,
+                                                         const double *__restrict__ C, int ax,
+                                                         int M, long nlines, int M2, int M3) {
+  extern __shared__ double2 dct_panel[];
+  dct1_panel_body<CPLX>(in, out, C, ax, M, nlines, M2, M3, blockIdx.x, blockIdx.y, dct_panel);
+}
+
 // Shared memory of a dct1_panel_kernel CTA, or 0 when the panel does not fit
 // the limit.
 static size_t dct_panel_bytes(int M, bool cplx, size_t limit) {
@@ -240,57 +256,35 @@ static size_t dct_panel_bytes(int M, bool cplx, size_t limit) {
   return b <= limit ? b : 0;
 }
 
-// The panel kernels' dynamic shared-memory limit, raised once per device to
-// the device's opt-in maximum.  The size a launch needs varies with M, and a
-// cudaFuncSetAttribute before each launch would race between host threads
-// that set up handles at the same time (one lowering the limit under
-// another's launch).  The handle's device is current.
-static int dct_panel_limit(npme_handle *h, size_t *limit) {
-  static std::mutex mu;
-  static std::map<int, size_t> done;
-  std::lock_guard<std::mutex> lk(mu);
-  auto it = done.find(h->device);
-  if (it == done.end()) {
-    int optin = 0;
-    cudaError_t e =
-        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(dct1_panel_kernel<true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(dct1_panel_kernel<false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    if (e != cudaSuccess) {
-      h->err = std::string("DCT panel limit: ") + cudaGetErrorString(e);
-      return NPME_ECUDA;
-    }
-    it = done.emplace(h->device, (size_t)optin).first;
-  }
-  *limit = it->second;
-  return NPME_OK;
-}
-
 // G = F * lambda^2 products / volume.  CPLX_IN: F complex (double2), else
 // real (double); CPLX: the complex kernel's (re, im) output, else the real
 // part only.
+template <typename T, bool CPLX, bool CPLX_IN>
+__device__ __forceinline__ void scale_fhat_body(const void *__restrict__ F_, long idx, int M2,
+                                                int M3, const double *__restrict__ l1,
+                                                const double *__restrict__ l2,
+                                                const double *__restrict__ l3, double inv_vol,
+                                                T *G) {
+  const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
+  const double s = l1[i1] * l2[i2] * l3[i3] * inv_vol;
+  const double2 F = CPLX_IN ? static_cast<const double2 *>(F_)[idx]
+                            : make_double2(static_cast<const double *>(F_)[idx], 0.0);
+  if (CPLX) {
+    G[2 * idx] = (T)(F.x * s);
+    G[2 * idx + 1] = (T)(F.y * s);
+  } else {
+    G[idx] = (T)(F.x * s);
+  }
+}
+
 template <typename T, bool CPLX, bool CPLX_IN>
 __global__ void scale_fhat_kernel(const void *__restrict__ F_, int M1, int M2, int M3,
                                   const double *__restrict__ l1, const double *__restrict__ l2,
                                   const double *__restrict__ l3, double inv_vol, T *G) {
   const long total = (long)M1 * M2 * M3;
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x) {
-    const int i3 = idx % M3, i2 = (idx / M3) % M2, i1 = idx / ((long)M2 * M3);
-    const double s = l1[i1] * l2[i2] * l3[i3] * inv_vol;
-    const double2 F = CPLX_IN ? static_cast<const double2 *>(F_)[idx]
-                              : make_double2(static_cast<const double *>(F_)[idx], 0.0);
-    if (CPLX) {
-      G[2 * idx] = (T)(F.x * s);
-      G[2 * idx + 1] = (T)(F.y * s);
-    } else {
-      G[idx] = (T)(F.x * s);
-    }
-  }
+       idx += (long)gridDim.x * blockDim.x)
+    scale_fhat_body<T, CPLX, CPLX_IN>(F_, idx, M2, M3, l1, l2, l3, inv_vol, G);
 }
 
 // Host B-spline (same recurrence as the device one) for lambda^2.
@@ -413,7 +407,8 @@ std::mutex g_dct_mu;
 std::map<std::pair<int, long>, DctMatrix> g_dct;
 }  // namespace
 
-static int dct_matrix(npme_handle *h, long N, const double *d_cos, double **out) {
+static int dct_matrix(npme_handle *h, cudaStream_t s, long N, const double *d_cos,
+                      double **out) {
   std::lock_guard<std::mutex> lk(g_dct_mu);
   DctMatrix &m = g_dct[std::make_pair(h->device, N)];
   if (!m.d) {
@@ -421,9 +416,8 @@ static int dct_matrix(npme_handle *h, long N, const double *d_cos, double **out)
     cudaError_t e = cudaMalloc(&m.d, sizeof(double) * M * M);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m.built, cudaEventDisableTiming);
     if (e == cudaSuccess) {
-      dct1_matrix_kernel<<<(unsigned)((M * M + 255) / 256), 256, 0, h->stream>>>(d_cos, (int)M,
-                                                                              (int)N, m.d);
-      e = cudaEventRecord(m.built, h->stream);
+      dct1_matrix_kernel<<<(unsigned)((M * M + 255) / 256), 256, 0, s>>>(d_cos, (int)M, (int)N, m.d);
+      e = cudaEventRecord(m.built, s);
     }
     if (e != cudaSuccess) {
       if (m.d) cudaFree(m.d);
@@ -433,7 +427,7 @@ static int dct_matrix(npme_handle *h, long N, const double *d_cos, double **out)
       h->err = std::string("DCT matrix: ") + cudaGetErrorString(e);
       return NPME_ECUDA;
     }
-  } else if (cudaStreamWaitEvent(h->stream, m.built, 0) != cudaSuccess) {
+  } else if (cudaStreamWaitEvent(s, m.built, 0) != cudaSuccess) {
     h->err = "DCT matrix: stream wait failed";
     return NPME_ECUDA;
   }
@@ -441,7 +435,25 @@ static int dct_matrix(npme_handle *h, long N, const double *d_cos, double **out)
   return NPME_OK;
 }
 
-int build_kernel_transform(npme_handle *h) {
+// One handle's kernel transform as its launches see it.
+struct KtSys {
+  LRKernel k;
+  const double *ax[3];   // window tables x1, x2, T1, T2 per axis
+  const double *lam[3];  // lambda^2 per axis
+  const double *C[3];    // DCT-I matrix per axis
+  void *ft0, *ft1;       // scratch octants
+  void *G;               // output: the handle's d_G
+  double inv_vol;
+  int M[3];
+  long start;            // first element in a batch's concatenated octants
+  long tile0[3];         // first DCT tile in the batch, per axis
+};
+
+// Host side of a handle's kernel transform: scratch, per-axis tables copied
+// to the device on stream s, the DCT-I matrices, and the descriptor of its
+// launches.  Buffers come from the handle's stream; when s is another
+// stream, s waits for them.
+static int kt_prepare(npme_handle *h, cudaStream_t s, KtSys *d) {
   const long *N = h->grid.N;
   const int M1 = N[0] / 2 + 1, M2 = N[1] / 2 + 1, M3 = N[2] / 2 + 1;
   const long MT = (long)M1 * M2 * M3;
@@ -449,11 +461,12 @@ int build_kernel_transform(npme_handle *h) {
   const double as[3] = {h->p.a1, h->p.a2, h->p.a3};
   std::vector<double> ax[3];
   std::shared_ptr<const AxisTables> tab[3];
-  for (int d = 0; d < 3; d++) {
-    window_axis(N[d], h->box[d], dels[d], as[d], ax[d]);
-    tab[d] = axis_tables(N[d], h->grid.order);
+  for (int a = 0; a < 3; a++) {
+    window_axis(N[a], h->box[a], dels[a], as[a], ax[a]);
+    tab[a] = axis_tables(N[a], h->grid.order);
   }
-  LRKernel k{};
+  LRKernel &k = d->k;
+  k = LRKernel{};
   k.func = h->p.funcType;
   k.split = h->p.EwaldSplit;
   k.nder = h->p.nDeriv;
@@ -463,7 +476,6 @@ int build_kernel_transform(npme_handle *h) {
   k.k0r = h->p.k0_r;
   k.k0i = h->p.k0_i;
   for (int i = 0; i <= k.nder && i < 32; i++) k.ar[i] = h->a_r[i], k.ai[i] = h->a_i[i];
-
   // scratch kept by the handle, so a new geometry on the same handle reuses it
   int rc = NPME_OK;
   if ((rc = handle_buffer(h, (void **)&h->d_ft0, sizeof(double2) * MT)) ||
@@ -471,72 +483,194 @@ int build_kernel_transform(npme_handle *h) {
     return rc;
   // the per-axis tables (window x1, x2, T1, T2; lambda^2; cosines of the
   // DCT) go through one pinned staging block kept by the handle, in one
-  // asynchronous copy; the next set-up on the handle waits for the handle's
-  // stream before it refills the block
+  // asynchronous copy; the next set-up on the handle waits for the copy
+  // before it refills the block
   size_t off[3][3], total = 0;
-  for (int d = 0; d < 3; d++) {
-    off[d][0] = total, total += ax[d].size();
-    off[d][1] = total, total += tab[d]->lam.size();
-    off[d][2] = total, total += (size_t)N[d];
+  for (int a = 0; a < 3; a++) {
+    off[a][0] = total, total += ax[a].size();
+    off[a][1] = total, total += tab[a]->lam.size();
+    off[a][2] = total, total += (size_t)N[a];
   }
   if ((rc = pinned_block(h, (void **)&h->h_fstage, &h->fstage_cap, sizeof(double) * total)))
     return rc;
-  for (int d = 0; d < 3; d++) {
-    std::copy(ax[d].begin(), ax[d].end(), h->h_fstage + off[d][0]);
-    std::copy(tab[d]->lam.begin(), tab[d]->lam.end(), h->h_fstage + off[d][1]);
-    std::copy(tab[d]->cosines.begin(), tab[d]->cosines.end(), h->h_fstage + off[d][2]);
+  for (int a = 0; a < 3; a++) {
+    std::copy(ax[a].begin(), ax[a].end(), h->h_fstage + off[a][0]);
+    std::copy(tab[a]->lam.begin(), tab[a]->lam.end(), h->h_fstage + off[a][1]);
+    std::copy(tab[a]->cosines.begin(), tab[a]->cosines.end(), h->h_fstage + off[a][2]);
   }
   if ((rc = handle_buffer(h, (void **)&h->d_ftab, sizeof(double) * total))) return rc;
-  NPME_CK(cudaMemcpyAsync(h->d_ftab, h->h_fstage, sizeof(double) * total, cudaMemcpyHostToDevice,
-                          h->stream));
-  for (int d = 0; d < 3; d++) {
-    h->d_fax[d] = h->d_ftab + off[d][0];
-    h->d_flam[d] = h->d_ftab + off[d][1];
-    h->d_fcos[d] = h->d_ftab + off[d][2];
+  if (s != h->stream) {
+    NPME_CK(cudaEventRecord(h->ev_fork, h->stream));
+    NPME_CK(cudaStreamWaitEvent(s, h->ev_fork, 0));
   }
+  NPME_CK(cudaMemcpyAsync(h->d_ftab, h->h_fstage, sizeof(double) * total, cudaMemcpyHostToDevice,
+                          s));
+  for (int a = 0; a < 3; a++) {
+    h->d_fax[a] = h->d_ftab + off[a][0];
+    h->d_flam[a] = h->d_ftab + off[a][1];
+    h->d_fcos[a] = h->d_ftab + off[a][2];
+    d->ax[a] = h->d_fax[a];
+    d->lam[a] = h->d_flam[a];
+    double *C = nullptr;
+    if ((rc = dct_matrix(h, s, N[a], h->d_fcos[a], &C))) return rc;
+    d->C[a] = C;
+  }
+  d->ft0 = h->d_ft0, d->ft1 = h->d_ft1, d->G = h->d_G;
+  d->inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);
+  d->M[0] = M1, d->M[1] = M2, d->M[2] = M3;
+  d->start = 0;
+  d->tile0[0] = d->tile0[1] = d->tile0[2] = 0;
+  return NPME_OK;
+}
+
+// DCT tiles of one axis: (lines / 32) x (outputs / 64)
+static long kt_tiles(const KtSys &d, int a, long *nx) {
+  const int M = d.M[a];
+  const long nlines = (long)d.M[0] * d.M[1] * d.M[2] / M;
+  *nx = (nlines + kDctL - 1) / kDctL;
+  return *nx * ((M + kDctK - 1) / kDctK);
+}
+
+// Batched stages: every handle of a set-up pass is a system with its own
+// octant; element and tile indices run over the concatenation of the
+// systems' octants and tiles, mapped back by binary search over their starts.
+__device__ __forceinline__ int kt_owner_elem(const KtSys *__restrict__ d, int R, long idx) {
+  int lo = 0, hi = R - 1;
+  while (lo < hi) {
+    const int m = (lo + hi + 1) >> 1;
+    if (d[m].start <= idx) lo = m;
+    else hi = m - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int kt_owner_tile(const KtSys *__restrict__ d, int R, int a, long t) {
+  int lo = 0, hi = R - 1;
+  while (lo < hi) {
+    const int m = (lo + hi + 1) >> 1;
+    if (d[m].tile0[a] <= t) lo = m;
+    else hi = m - 1;
+  }
+  return lo;
+}
+
+template <bool CPLX>
+__global__ void batch_sample_fhat_kernel(const KtSys *__restrict__ d, int R, long total) {
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const KtSys &D = d[kt_owner_elem(d, R, idx)];
+    const long i = idx - D.start;
+    const BuiltinLRRef lr{&D.k};
+    const double2 f = fhat_sample_body(lr, i, D.M[0], D.M[1], D.M[2], D.ax[0], D.ax[1], D.ax[2]);
+    if (CPLX) static_cast<double2 *>(D.ft0)[i] = f;
+    else static_cast<double *>(D.ft0)[i] = f.x;
+  }
+}
+
+// Axis a of every system: pass 0 reads ft0 and writes ft1, pass 1 back,
+// pass 2 ft0 -> ft1 again (the single-system order).
+template <bool CPLX>
+__global__ void __launch_bounds__(256) batch_dct1_panel_kernel(const KtSys *__restrict__ d, int R,
+                                                               int a) {
+  extern __shared__ double2 dct_panel[];
+  const KtSys &D = d[kt_owner_tile(d, R, a, blockIdx.x)];
+  const long t = blockIdx.x - D.tile0[a];
+  const int M = D.M[a];
+  const long nlines = (long)D.M[0] * D.M[1] * D.M[2] / M;
+  const long nx = (nlines + kDctL - 1) / kDctL;
+  const void *src = (a == 1) ? D.ft1 : D.ft0;
+  void *dst = (a == 1) ? D.ft0 : D.ft1;
+  dct1_panel_body<CPLX>(src, dst, D.C[a], a, M, nlines, D.M[1], D.M[2], t % nx, (int)(t / nx),
+                        dct_panel);
+}
+
+template <typename T, bool CPLX, bool CPLX_IN>
+__global__ void batch_scale_fhat_kernel(const KtSys *__restrict__ d, int R, long total) {
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const KtSys &D = d[kt_owner_elem(d, R, idx)];
+    // after three passes the transform is in ft1
+    scale_fhat_body<T, CPLX, CPLX_IN>(D.ft1, idx - D.start, D.M[1], D.M[2], D.lam[0], D.lam[1],
+                                      D.lam[2], D.inv_vol, (T *)D.G);
+  }
+}
+
+// The panel kernels' dynamic shared-memory limit, raised once per device to
+// the device's opt-in maximum.  The size a launch needs varies with M, and a
+// cudaFuncSetAttribute before each launch would race between host threads
+// that set up handles at the same time (one lowering the limit under
+// another's launch).  The handle's device is current.
+static int dct_panel_limit(npme_handle *h, size_t *limit) {
+  static std::mutex mu;
+  static std::map<int, size_t> done;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find(h->device);
+  if (it == done.end()) {
+    int optin = 0;
+    cudaError_t e =
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    const void *kernels[4] = {(const void *)dct1_panel_kernel<true>,
+                              (const void *)dct1_panel_kernel<false>,
+                              (const void *)batch_dct1_panel_kernel<true>,
+                              (const void *)batch_dct1_panel_kernel<false>};
+    for (int i = 0; i < 4 && e == cudaSuccess; i++)
+      e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) {
+      h->err = std::string("DCT panel limit: ") + cudaGetErrorString(e);
+      return NPME_ECUDA;
+    }
+    it = done.emplace(h->device, (size_t)optin).first;
+  }
+  *limit = it->second;
+  return NPME_OK;
+}
+
+// The launches of one handle's transform on stream s.
+static int kt_launch_one(npme_handle *h, const KtSys &d, cudaStream_t s) {
+  const int M1 = d.M[0], M2 = d.M[1], M3 = d.M[2];
+  const long MT = (long)M1 * M2 * M3;
   const int threads = 256, blocks = 148 * 8;
   // the built-in real kernels sample and transform real values; complex
   // kernels and caller-defined ones (whose sampler writes complex values)
   // run the complex transform
   const bool cplx_ft = h->complex_kernel || h->user_kernel;
+  int rc = NPME_OK;
   if (h->user_kernel) {
-    if ((rc = h->uops.sample_lr(h, M1, M2, M3, h->d_fax[0], h->d_fax[1], h->d_fax[2], h->d_ft0,
-                                h->stream)))
+    if ((rc = h->uops.sample_lr(h, M1, M2, M3, d.ax[0], d.ax[1], d.ax[2], (double2 *)d.ft0, s)))
       return rc;
   } else if (cplx_ft) {
-    sample_fhat_kernel<true><<<blocks, threads, 0, h->stream>>>(k, M1, M2, M3, h->d_fax[0],
-                                                                h->d_fax[1], h->d_fax[2], h->d_ft0);
+    sample_fhat_kernel<true><<<blocks, threads, 0, s>>>(d.k, M1, M2, M3, d.ax[0], d.ax[1],
+                                                        d.ax[2], d.ft0);
   } else {
-    sample_fhat_kernel<false><<<blocks, threads, 0, h->stream>>>(
-        k, M1, M2, M3, h->d_fax[0], h->d_fax[1], h->d_fax[2], h->d_ft0);
+    sample_fhat_kernel<false><<<blocks, threads, 0, s>>>(d.k, M1, M2, M3, d.ax[0], d.ax[1],
+                                                         d.ax[2], d.ft0);
   }
-  void *src = h->d_ft0, *dst = h->d_ft1;
-  const int Ms[3] = {M1, M2, M3};
-  for (int d = 0; d < 3; d++) {
-    const int M = Ms[d];
-    double *C = nullptr;
-    if ((rc = dct_matrix(h, N[d], h->d_fcos[d], &C))) return rc;
+  void *src = d.ft0, *dst = d.ft1;
+  size_t limit = 0;
+  if ((rc = dct_panel_limit(h, &limit))) return rc;
+  for (int a = 0; a < 3; a++) {
+    const int M = d.M[a];
+    const double *C = d.C[a];
+    long nx;
+    kt_tiles(d, a, &nx);
     const long nlines = MT / M;
-    const dim3 grid((unsigned)((nlines + kDctL - 1) / kDctL), (unsigned)((M + kDctK - 1) / kDctK));
-    size_t limit = 0;
-    if ((rc = dct_panel_limit(h, &limit))) return rc;
+    const dim3 grid((unsigned)nx, (unsigned)((M + kDctK - 1) / kDctK));
     const size_t pb = dct_panel_bytes(M, cplx_ft, limit);
     if (pb && cplx_ft) {
-      dct1_panel_kernel<true><<<grid, 256, pb, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+      dct1_panel_kernel<true><<<grid, 256, pb, s>>>(src, dst, C, a, M, nlines, M2, M3);
     } else if (pb) {
-      dct1_panel_kernel<false><<<grid, 256, pb, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+      dct1_panel_kernel<false><<<grid, 256, pb, s>>>(src, dst, C, a, M, nlines, M2, M3);
     } else if (cplx_ft) {
-      dct1_gemm_kernel<true><<<grid, 256, 0, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+      dct1_gemm_kernel<true><<<grid, 256, 0, s>>>(src, dst, C, a, M, nlines, M2, M3);
     } else {
-      dct1_gemm_kernel<false><<<grid, 256, 0, h->stream>>>(src, dst, C, d, M, nlines, M2, M3);
+      dct1_gemm_kernel<false><<<grid, 256, 0, s>>>(src, dst, C, a, M, nlines, M2, M3);
     }
     std::swap(src, dst);
   }
-  const double inv_vol = 1.0 / ((double)N[0] * N[1] * N[2]);
-  double *const *l = h->d_flam;
-#define NPME_SCALE(T, CX, CI)                                                                \
-  scale_fhat_kernel<T, CX, CI><<<blocks, threads, 0, h->stream>>>(src, M1, M2, M3, l[0], l[1], \
-                                                                  l[2], inv_vol, (T *)h->d_G)
+  const double *const *l = d.lam;
+#define NPME_SCALE(T, CX, CI)                                                               \
+  scale_fhat_kernel<T, CX, CI><<<blocks, threads, 0, s>>>(src, M1, M2, M3, l[0], l[1], l[2], \
+                                                          d.inv_vol, (T *)d.G)
   if (h->fp32) {
     if (h->complex_kernel) NPME_SCALE(float, true, true);
     else if (cplx_ft) NPME_SCALE(float, false, true);
@@ -547,13 +681,139 @@ int build_kernel_transform(npme_handle *h) {
     else NPME_SCALE(double, false, false);
   }
 #undef NPME_SCALE
-  // launch errors now; npme_gpu_setup waits for the stream before it returns
+  // launch errors now; set-up waits for the stream before it returns
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     h->err = std::string("kernel transform: ") + cudaGetErrorString(e);
     rc = NPME_ECUDA;
   }
   return rc;
+}
+
+int build_kernel_transform(npme_handle *h) {
+  KtSys d;
+  const int rc = kt_prepare(h, h->stream, &d);
+  return rc ? rc : kt_launch_one(h, d, h->stream);
+}
+
+// Layout of one class of handles (the same precision and kernel type,
+// built-in kernels) in a batch: element and tile starts, the largest panel.
+// False when a panel does not fit a CTA or a launch would need 2^31 blocks
+// or more: then the class goes handle by handle (tiled transform).
+static bool kt_layout(std::vector<KtSys> &ds, bool cplx, size_t limit, long *total,
+                      long tiles[3], size_t *pb) {
+  *total = 0, tiles[0] = tiles[1] = tiles[2] = 0, *pb = 0;
+  for (KtSys &d : ds) {
+    d.start = *total;
+    *total += (long)d.M[0] * d.M[1] * d.M[2];
+    for (int a = 0; a < 3; a++) {
+      long nx;
+      d.tile0[a] = tiles[a];
+      tiles[a] += kt_tiles(d, a, &nx);
+      const size_t b = dct_panel_bytes(d.M[a], cplx, limit);
+      if (!b) return false;
+      *pb = std::max(*pb, b);
+    }
+  }
+  return tiles[0] < (1L << 31) && tiles[1] < (1L << 31) && tiles[2] < (1L << 31);
+}
+
+// One launch per stage for a class whose descriptors are at dd on the
+// device.
+static void kt_launch_class(const KtSys *dd, int R, bool cplx, bool fp32, long total,
+                            const long tiles[3], size_t pb, cudaStream_t s) {
+  const unsigned eb = (unsigned)std::min<long>((total + 255) / 256, 148 * 8);
+  if (cplx) batch_sample_fhat_kernel<true><<<eb, 256, 0, s>>>(dd, R, total);
+  else batch_sample_fhat_kernel<false><<<eb, 256, 0, s>>>(dd, R, total);
+  for (int a = 0; a < 3; a++) {
+    if (cplx) batch_dct1_panel_kernel<true><<<(unsigned)tiles[a], 256, pb, s>>>(dd, R, a);
+    else batch_dct1_panel_kernel<false><<<(unsigned)tiles[a], 256, pb, s>>>(dd, R, a);
+  }
+  if (fp32) {
+    if (cplx) batch_scale_fhat_kernel<float, true, true><<<eb, 256, 0, s>>>(dd, R, total);
+    else batch_scale_fhat_kernel<float, false, false><<<eb, 256, 0, s>>>(dd, R, total);
+  } else {
+    if (cplx) batch_scale_fhat_kernel<double, true, true><<<eb, 256, 0, s>>>(dd, R, total);
+    else batch_scale_fhat_kernel<double, false, false><<<eb, 256, 0, s>>>(dd, R, total);
+  }
+}
+
+// The kernel transforms of a set-up pass (one precision), on the owner's
+// stream: a class of two or more handles (built-in real kernels, built-in
+// complex kernels) in one launch per stage, caller-defined kernels and
+// classes of one handle by handle on their own streams.  One launch per
+// stage instead of five per handle: about 4 % more served capacity at the
+// best passes of a serving stream.
+void build_kernel_transforms(npme_handle **hs, int R, npme_handle *owner, int *status) {
+  npme_handle *h = owner;  // errors of the shared steps are recorded on the owner
+  const cudaStream_t s = owner->stream;
+  std::vector<int> cls(R, -1);
+  int count[2] = {0, 0};
+  for (int r = 0; r < R; r++)
+    if (!hs[r]->user_kernel) cls[r] = hs[r]->complex_kernel ? 1 : 0, count[cls[r]]++;
+  for (int r = 0; r < R; r++) {
+    if (cls[r] >= 0 && count[cls[r]] >= 2) continue;
+    cls[r] = -1;
+    status[r] = build_kernel_transform(hs[r]);
+  }
+  size_t limit = 0;
+  int rc = NPME_OK;
+  const bool any = std::any_of(cls.begin(), cls.end(), [](int c) { return c >= 0; });
+  if (!any) return;
+  if ((rc = dct_panel_limit(h, &limit))) {
+    for (int r = 0; r < R; r++)
+      if (cls[r] >= 0) status[r] = rc, hs[r]->err = h->err;
+    return;
+  }
+  // every class's descriptors, in one staging block and one copy (two
+  // classes must not share a pinned block that an earlier copy still reads)
+  std::vector<KtSys> ds[2];
+  std::vector<int> at[2];
+  for (int r = 0; r < R; r++) {
+    if (cls[r] < 0) continue;
+    KtSys d;
+    status[r] = kt_prepare(hs[r], s, &d);
+    if (!status[r]) ds[cls[r]].push_back(d), at[cls[r]].push_back(r);
+  }
+  long total[2] = {0, 0}, tiles[2][3];
+  size_t pb[2] = {0, 0};
+  bool batched[2] = {false, false};
+  for (int c = 0; c < 2; c++) {
+    if (ds[c].empty()) continue;
+    batched[c] = kt_layout(ds[c], c == 1, limit, &total[c], tiles[c], &pb[c]);
+    if (!batched[c])
+      for (size_t k = 0; k < ds[c].size(); k++)
+        status[at[c][k]] = kt_launch_one(hs[at[c][k]], ds[c][k], s);
+  }
+  const size_t n0 = batched[0] ? ds[0].size() : 0, n1 = batched[1] ? ds[1].size() : 0;
+  if (n0 + n1 == 0) return;
+  const size_t bytes = sizeof(KtSys) * (n0 + n1);
+  auto fail_all = [&](int code) {
+    for (int c = 0; c < 2; c++)
+      if (batched[c])
+        for (int r : at[c]) {
+          status[r] = code;
+          if (hs[r] != h) hs[r]->err = h->err;
+        }
+  };
+  if ((rc = pinned_block(h, &h->h_ktdesc, &h->ktdesc_cap, bytes)) ||
+      (rc = handle_buffer(h, &h->d_ktdesc, bytes)))
+    return fail_all(rc);
+  KtSys *hd = static_cast<KtSys *>(h->h_ktdesc);
+  if (n0) std::copy(ds[0].begin(), ds[0].end(), hd);
+  if (n1) std::copy(ds[1].begin(), ds[1].end(), hd + n0);
+  cudaError_t e = cudaMemcpyAsync(h->d_ktdesc, hd, bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    const KtSys *dd = static_cast<const KtSys *>(h->d_ktdesc);
+    const bool fp32 = owner->fp32;
+    if (n0) kt_launch_class(dd, (int)n0, false, fp32, total[0], tiles[0], pb[0], s);
+    if (n1) kt_launch_class(dd + n0, (int)n1, true, fp32, total[1], tiles[1], pb[1], s);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    h->err = std::string("kernel transform: ") + cudaGetErrorString(e);
+    return fail_all(NPME_ECUDA);
+  }
 }
 
 // ---------------------------------------------------------------------------
