@@ -56,6 +56,10 @@ struct BatchSys {
   const uint32_t *bperm;   // brick-order position -> caller index
   float refine2;
   double fself_r, fself_i;
+  // pair-once systems: the interpolation adds the source-side sums into V
+  // (potential times vs, gradient times gs) and clears them
+  int fold;
+  double vs, gs;
 };
 
 __device__ __forceinline__ int find_sys(const long long *__restrict__ off, int count,
@@ -125,7 +129,8 @@ __global__ void __launch_bounds__(256) batch_interp_kernel(const BatchSys *__res
   const BatchSys &S = sys[s];
   interp_brick_body<float, P, CPLX>(S.brick_list[u - off[s]], S.brick_start, S.bpts, S.grid, S.V,
                                     S.nb2, S.nb3, S.N1, S.N2, S.N3, S.c1, S.c2, S.c3,
-                                    reinterpret_cast<float *>(smem_raw));
+                                    reinterpret_cast<float *>(smem_raw),
+                                    S.fold ? (void *)S.vsrc : nullptr, S.vs, S.gs);
 }
 
 template <bool CPLX, int FUNC, int SPLIT, int ND>
@@ -172,42 +177,6 @@ __global__ void __launch_bounds__(32 * kGroupWarps) batch_sym_kernel(
     direct_group_sym_scalar<0, 1, 0>(k, S.gpos, S.spos, S.qc, S.q, S.hgroups[g], S.hcen[g],
                                      S.hsegs, S.cperm, S.refine2, S.fself_r, S.V, S.vsrc,
                                      ta[wid], tb[wid], lane);
-}
-
-// V[caller(j)] += the source-side sums of brick-order slot j (scaled by vs
-// for the potential, gs for the gradient; complex: re, im pairs), then zero
-// them.
-template <bool CPLX>
-__global__ void batch_merge_kernel(const BatchSys *__restrict__ sys,
-                                   const long long *__restrict__ off, int count, double vs,
-                                   double gs) {
-  const long long total = off[count];
-  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total;
-       u += (long long)gridDim.x * blockDim.x) {
-    const int s = find_sys(off, count, u);
-    const BatchSys &S = sys[s];
-    const long j = (long)(u - off[s]);
-    double4 *o = reinterpret_cast<double4 *>(S.V);
-    if (CPLX) {
-      o += 2 * (long)S.bperm[j];
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const float4 a = S.vsrc[2 * j + h];
-        S.vsrc[2 * j + h] = make_float4(0.f, 0.f, 0.f, 0.f);
-        double4 v = o[h];
-        v.x += a.x, v.y += a.y, v.z += a.z, v.w += a.w;
-        o[h] = v;
-      }
-    } else {
-      o += S.bperm[j];
-      const float4 a = S.vsrc[j];
-      S.vsrc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-      double4 v = *o;
-      v.x += vs * (double)a.x, v.y += gs * (double)a.y;
-      v.z += gs * (double)a.z, v.w += gs * (double)a.w;
-      *o = v;
-    }
-  }
 }
 
 }  // namespace npme
@@ -373,13 +342,19 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     S.refine2 = (float)h->refine2;
     S.fself_r = h->fself_r;
     S.fself_i = h->fself_i;
+    S.fold = pairs_once(h) ? 1 : 0;
+    const bool scaled =
+        h->p.funcType != NPME_FUNC_HELMHOLTZ && h->p.EwaldSplit != NPME_SPLIT_LAPLACE_ORIG;
+    const PairCoef<float> pc = make_pair_coef<float>(h);
+    S.vs = scaled ? pc.vscale : 1.0;
+    S.gs = scaled ? pc.gscale : 1.0;
   }
 
   // launch classes
   std::map<int, Class> gath, mult;                           // key: complex
   std::map<std::pair<int, int>, Class> spr;                  // (order, complex)
   typedef std::tuple<int, int, int, int, double, double, double, double, double> DKey;
-  std::map<DKey, Class> dir, mrg;  // direct sums; source-side merges of pair-once classes
+  std::map<DKey, Class> dir;  // direct sums
   for (int k = 0; k < m; k++) {
     const npme_handle *h = hs[f32[k]];
     const int cx = h->complex_kernel ? 1 : 0;
@@ -389,7 +364,6 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
     const DKey key(pairs_once(h) ? 1 : 0, h->p.funcType, h->p.EwaldSplit, h->p.nDeriv,
                    h->p.Rdir, h->p.alpha, h->p.k0_r, h->p.k0_i, h->beta);
     dir[key].members.push_back(k);
-    if (std::get<0>(key)) mrg[key].members.push_back(k);
   }
   auto units_gather = [&](int k) { return (long long)hs[f32[k]]->n; };
   auto units_spread = [&](int k) { return (long long)hs[f32[k]]->n_nonempty; };
@@ -418,7 +392,6 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
   for (auto &kv : mult) lay(kv.second, units_mult);
   for (auto &kv : spr) lay(kv.second, units_spread);  // spread and interpolation: bricks
   for (auto &kv : dir) lay(kv.second, units_dir);
-  for (auto &kv : mrg) lay(kv.second, units_gather);  // merges: source points
 
   // the pinned staging buffer is reused: wait for the previous batch's copy
   if (b->pending) {
@@ -494,15 +467,7 @@ int npme_gpu_calcv_batch(npme_batch *b, npme_handle *const *hs, int count,
       else { NPME_BSYM_ND(0, 0); }
 #undef NPME_BSYM_ND
 #undef NPME_BSYM
-      b->launches++;
-      const Class &mc = mrg.at(kv.first);
-      const unsigned gm = grid_of(mc.off.back(), 256, 148 * 16);
-      const bool scaled = f != NPME_FUNC_HELMHOLTZ && sp != NPME_SPLIT_LAPLACE_ORIG;
-      if (f == NPME_FUNC_HELMHOLTZ)
-        batch_merge_kernel<true><<<gm, 256, 0, b->stream2>>>(D(mc), O(mc), cnt, 1.0, 1.0);
-      else
-        batch_merge_kernel<false><<<gm, 256, 0, b->stream2>>>(
-            D(mc), O(mc), cnt, scaled ? k.vscale : 1.0, scaled ? k.gscale : 1.0);
+      // the source-side sums are folded into V by the interpolation below
       b->launches++;
       continue;
     }
