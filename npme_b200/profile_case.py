@@ -12,7 +12,7 @@ per-point work as the full configuration.
 
 serves the first 64 requests of the serving stream through the native queue
 (all available at t = 0, FP32 bulk, batched), after the server's start-up
-(FFT plans, one pass over start-up requests of the same distribution), so
+(FFT plans, two passes over start-up requests of the same distribution), so
 that a launch list shows the set-up and batched-CalcV kernels of a pass.
 """
 import argparse
@@ -63,7 +63,8 @@ def serve(count):
     reqs = serving.serving_stream(count=2048)[:count]
     srv = serving.Server()
     srv.warm_plans(reqs)
-    srv.run(serving.warm_stream(), realtime=False)
+    for _ in range(2):
+        srv.run(serving.warm_stream(), realtime=False)
     import torch
     torch.cuda.synchronize()
     # a profiler started with --profile-from-start off records this pass only
